@@ -1,0 +1,350 @@
+"""Benchmark: projected energy + orbital gradient throughput (grid points per second).
+
+Workload (one step = one full energy + gradient evaluation, as one call of PHF.py's EandG):
+  c2: n = 64 spatial orbitals (M = 128 spin orbitals), N = 32 electrons, L = 400 Cholesky
+      vectors, grid = Lebedev 50 x 16 gamma x 4 C2v operations = 3200 points; seeded
+      synthetic h, B_L and determinant (no molecular input is available offline).
+
+Arms:
+  --impl ours       the GPU path.  `value` is device time of the evaluation with C resident in
+                    HBM (CUDA events on the launching stream, max over ranks); `e2e` is the same
+                    metric through the C ABI with host buffers (phf_buildhsg_chol: host -> device
+                    copies of h, B, Ref, Z and the grid, and the device -> host copy of Hmat,
+                    Smat, Gradmat, Rdmmat inside the timed region).
+  --impl reference  the reference algorithm on the host cores: the C/OpenMP restatement of
+                    PHF_fort/PHFTools.f90 BuildHSG (dense HTwo, MakeGamma) timed on a bounded
+                    sample of grid points (the reference Fortran cannot be compiled here).
+
+Multi-GPU (torchrun, one process per GPU): every rank evaluates its own independent instance
+(weak scaling, no collective on the data path); value = points of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "projected E+grad grid-pts/s, split-prec vs FP64 GPU @|ΔE|≤1e-8 Eh; vs host CPU"
+UNIT = "grid-pts/s"
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def problem_for(name: str, seed: int):
+    from phf_pcc_b200 import synth
+    return synth.config_problem(name, seed=seed)
+
+
+def api_kwargs(p):
+    kw = p.grid_kwargs()
+    return dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+                r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+                roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+
+
+def jk_flops_per_point(p):
+    """Algorithmic real flops of the Cholesky J/K contraction per grid point (executed form):
+    T = V^H X (8 L N^2 M), Q = X T' (8 L N^2 M), GX = sum_L B_L Q_L (8 L n^2 N)."""
+    n, N, M, L = p.n, p.N, p.M, p.L
+    return 8.0 * L * N * N * M * 2 + 8.0 * L * n * n * N
+
+
+def survey_flops_per_point(p):
+    """Per-point work figure of the benchmark description: 32 L n^3 + 8 L n^2 (J/K) plus
+    16 M^2 N + 16 M N^2 + 8 N^3 + 16 M^3 (small algebra)."""
+    n, N, M, L = p.n, p.N, p.M, p.L
+    return 32.0 * L * n ** 3 + 8.0 * L * n ** 2 + 16.0 * M * M * N + 16.0 * M * N * N + 8.0 * N ** 3 + 16.0 * M ** 3
+
+
+def measure_fp64_peak(torch, dev):
+    """cuBLAS DGEMM throughput (TFLOP/s) as the FP64 roofline denominator (best of 5, 8192^3)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_sample(p, seconds_target=20.0, nthreads=0):
+    """Time the C oracle (dense HTwo MakeGamma, the reference's algorithm) on a bounded sample.
+
+    Ref = I and the Thouless form Z = C_vir C_occ^-1 span the same determinant as C, so the
+    per-point cost is that of the reference with this Hamiltonian.  Returns (points/s,
+    threads, description)."""
+    from oracle import phf_oracle as orc
+    from oracle import phf_oracle_c as corc
+
+    M, N = p.M, p.N
+    H2 = orc.dense_htwo_from_chol(p.B).astype(np.complex128)
+    H1 = p.hone_ao()
+    Z = p.C[N:] @ np.linalg.inv(p.C[:N])
+    kw = p.grid_kwargs()
+    nth = nthreads or os.cpu_count() or 1
+    total = p.grid.npoints
+    # calibrate with one point per thread, then size the sample for ~seconds_target
+    npts = min(total, nth)
+    t0 = time.perf_counter()
+    corc.buildhsg(H1, H2, np.eye(M), Z, omega_list=np.arange(npts), nthreads=nth, **kw)
+    t1 = time.perf_counter() - t0
+    per_round = t1
+    rounds = max(1, int(seconds_target / max(per_round, 1e-3)))
+    npts2 = min(total, nth * rounds)
+    t0 = time.perf_counter()
+    corc.buildhsg(H1, H2, np.eye(M), Z, omega_list=np.arange(npts2), nthreads=nth, **kw)
+    t2 = time.perf_counter() - t0
+    del H2
+    return npts2 / t2, nth, f"{npts2} of {total} grid points (dense HTwo, M={M}), {t2:.1f} s"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    p = problem_for(args.config, seed=0)
+    vals = []
+    desc = ""
+    nth = os.cpu_count() or 1
+    for i in range(args.warmup + args.steps):
+        v, nth, desc = cpu_sample(p, seconds_target=args.cpu_seconds, nthreads=nth)
+        if i >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * p.grid.npoints / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": workload_name(p), "points_per_step": p.grid.npoints},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_name(p):
+    g = p.grid
+    return (f"n={p.n} M={p.M} N={p.N} L={p.L}, grid {g.ngrid[0]}x{g.ngrid[1]}x{g.npg} = {g.npoints} points "
+            f"({'C2v' if g.npg == 4 else 'no PG'}), FP64-accurate E+grad")
+
+
+def run_ours(args):
+    import torch
+
+    from phf_pcc_b200 import _lib, api
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    p = problem_for(args.config, seed=1000 + rank)
+    Ref, Z = p.ref_and_z()
+    kw = api_kwargs(p)
+    plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, **kw)
+    C = torch.from_numpy(p.C).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+
+    def step():
+        hs, yg, yr = plan.eval_device(C, stream=stream)
+        S = hs[0, 1]
+        E = hs[0, 0].real / S.real.abs()
+        G = (yg[0] - E * yr[0]) / S
+        return E, G
+
+    for _ in range(args.warmup):
+        E, G = step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = _lib.kernel_launches()
+    _lib.profile_enable(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.zero_()                       # L2 flush between timed steps (not timed)
+            ev[i][0].record(stream)
+            E, G = step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.kernel_launches() - launches0
+    jk_ms, jk_n = _lib.profile_read(_lib.PROF_JK)
+    all_ms = sum(_lib.profile_read(c)[0] for c in range(4))
+    _lib.profile_enable(False)
+    step_ms = sum(s.elapsed_time(e) for s, e in ev) / args.steps
+    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item())
+    value = world * p.grid.npoints / (step_ms * 1e-3)
+
+    # end-to-end through the C ABI with host buffers (one-shot drop-in call per step)
+    e2e_vals = []
+    h2d = d2h = 0
+    if args.e2e_steps > 0:
+        z0 = np.zeros((p.M - p.N, p.N), dtype=np.complex128)
+        for i in range(1 + args.e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = api.buildhsg_chol(p.h, p.B, Ref, z0, check_hermitian=False, **kw)
+            t1 = time.perf_counter()
+            if i > 0:
+                e2e_vals.append(p.grid.npoints / (t1 - t0))
+        h2d = (p.h.nbytes + p.B.nbytes + Ref.nbytes + z0.nbytes + kw["r1"].nbytes + kw["r2"].nbytes +
+               kw["rpg"].nbytes + kw["weightsp"].nbytes + kw["weightpg"].nbytes)
+        d2h = sum(x.nbytes for x in out)
+    e2e_val = statistics.median(e2e_vals) * world if e2e_vals else None
+
+    line = None
+    if rank == 0:
+        peaks = _peaks()
+        fp64_peak = measure_fp64_peak(torch, dev) if args.precision == "fp64" else None
+        flops_pt = jk_flops_per_point(p)
+        # J/K kernels: achieved = algorithmic J/K flops of the timed steps / their summed device time
+        jk_flops_total = flops_pt * p.grid.npoints * args.steps
+        achieved = jk_flops_total / (jk_ms * 1e-3) / 1e12 if jk_ms > 0 else None
+        if args.precision == "fp64":
+            roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": (achieved / fp64_peak) if achieved and fp64_peak else None, "traffic": None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
+                    "kernel": "zgemm_kernel (J/K contraction GEMMs)", "jk_share_of_device_time": jk_ms / all_ms,
+                    "jk_launches": jk_n}
+        else:
+            peak = peaks.get("bf16_tflops")
+            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if achieved and peak else None, "traffic": None,
+                    "kernel": "J/K contraction", "jk_share_of_device_time": jk_ms / all_ms, "jk_launches": jk_n}
+        roof["flops_per_point"] = flops_pt
+        roof["survey_flops_per_point"] = survey_flops_per_point(p)
+        cpu = None
+        if not args.no_cpu:
+            v, nth, desc = cpu_sample(p, seconds_target=args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision,
+                "data": "synthetic (seeded h, B_L, determinant)",
+                "config": {"workload": workload_name(p), "precision": args.precision,
+                           "points_per_step": p.grid.npoints, "chunk": plan.chunk,
+                           "l2": "flushed (256 MB write) between timed steps",
+                           "parallelism": f"{world} independent instances, one per GPU"},
+                "energy": float(E.item()),
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "path": "phf_buildhsg_chol (C ABI, host buffers)"},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki_i8", "bf16x3", "tf32"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

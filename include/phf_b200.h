@@ -1,0 +1,164 @@
+/*
+ * phf_b200 -- C ABI of the B200 projected-HF grid kernel.
+ *
+ * Drop-in for the two routines of the reference's f2py module PHFTools_F (module phftools,
+ * built by PHF_fort/makefile:7) that PHF.py calls for the projected energy and gradient:
+ *
+ *   phftools.buildhsg  -> phf_buildhsg       (PHF_fort/PHFTools.f90:10-201, called at PHF.py:44-45,70-71)
+ *   phftools.localg    -> phf_localg         (PHF_fort/PHFTools.f90:203-247, called at PHF.py:76)
+ *
+ * Arrays use the reference's Fortran dummy-argument layouts (column-major), complex128 as
+ * {re, im} pairs, so a binding passes f2py/numpy Fortran-ordered buffers unchanged:
+ *   HOne(i,j)       = hone[i + M*j]                     M = nso spin orbitals
+ *   HTwo(i,j,k,l)   = htwo[i + M*(j + M*(k + M*l))]     antisymmetrised <ij||kl>
+ *   Ref(i,j)        = ref[i + M*j];   Z(a,i) = z[a + (M-nocc)*i]
+ *   R1(il,i,j)      = r1[il + ngrid[0]*(i + M*j)];   R2(iy,i,j) = r2[iy + ngrid[1]*(i + M*j)]
+ *   Rpg(ig,i,j)     = rpg[ig + npg*(i + M*j)]
+ *   weightsp(il,iy) = weightsp[il + ngrid[0]*iy]
+ *   weightpg(ig,p,q)= weightpg[ig + npg*(p + ncipg*q)]
+ *   roota: ngrid[0] entries; rootb: ngrid[0] entries (ngrid[1] when sp == 2);
+ *   rooty: ngrid[1] entries (ngrid[0] when sp == 2)
+ *   Hmat(m,n)       = hmat[m + nci*n];   Gradmat(m,n,i,j) = gradmat[m + nci*(n + nci*(i + M*j))]
+ *
+ * Every entry point returns a status code instead of the reference's Fortran STOP.  All
+ * computation runs on the current CUDA device; there is no CPU fallback: without a device
+ * the calls return PHF_ERR_NO_DEVICE.
+ */
+#ifndef PHF_B200_H
+#define PHF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    double re, im;
+} phf_complex;
+
+enum phf_status {
+    PHF_OK = 0,
+    PHF_ERR_ARG = 1,            /* inconsistent sizes or arguments */
+    PHF_ERR_SINGULAR = 2,       /* a rotated overlap C^H R C is exactly singular
+                                   (reference: STOP "Error in ZGetRF", Wrappers.f90:311) */
+    PHF_ERR_NOT_HERMITIAN = 3,  /* Hmat/Smat fail the check of PHFTools.f90:195-200
+                                   (reference: STOP "Not Hermitian"); outputs are still written */
+    PHF_ERR_NONFINITE = 4,      /* NaN/Inf in inputs or results */
+    PHF_ERR_CUDA = 5,           /* CUDA runtime error */
+    PHF_ERR_OOM = 6,            /* device allocation failed */
+    PHF_ERR_UNSUPPORTED = 7,    /* size or option outside what this build implements */
+    PHF_ERR_NO_DEVICE = 8       /* no CUDA device */
+};
+
+/* Arithmetic of the J/K contraction (the overlap inverse, determinants, weights and the
+ * compensated grid sums are FP64 in every mode). */
+enum phf_precision {
+    PHF_PREC_FP64 = 0,      /* FP64 CUDA-core GEMMs (the plain FP64 form) */
+    PHF_PREC_OZAKI_I8 = 1,  /* FP64-accurate emulation: int8 slices on tcgen05 tensor cores */
+    PHF_PREC_BF16X3 = 2,    /* split-BF16, 3 products, FP32 accumulation (tcgen05) */
+    PHF_PREC_TF32 = 3       /* TF32, FP32 accumulation (tcgen05) */
+};
+
+/* ---------------------------------------------------------------- drop-in entry points */
+
+/* BuildHSG (PHF_fort/PHFTools.f90:10-48 declaration).  Dense HTwo in the Ref-MO basis, as
+ * PHF.py passes it.  Host buffers in, host buffers out (outputs overwritten).
+ * Returns PHF_ERR_NOT_HERMITIAN (outputs written) where the reference would STOP. */
+int phf_buildhsg(const phf_complex *hone, const phf_complex *htwo, const phf_complex *ref, const phf_complex *z,
+                 const int *ngrid, int npg, int nci, int cmplxconj, int ncisp, int ncipg, int nocc, int nso,
+                 const phf_complex *r1, const phf_complex *r2, const phf_complex *rpg, const double *weightsp,
+                 const double *weightpg, const double *roota, const double *rootb, const double *rooty, int qj,
+                 int sp, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat, phf_complex *rdmmat);
+
+/* BuildHSG with the two-electron integrals given as spatial Cholesky vectors in the
+ * orthonormal AO basis: (pq|rs) = sum_L B_L(p,q) B_L(r,s), B_L(p,q) = bvec[p + n*(q + n*L)],
+ * and the one-electron matrix h(p,q) = h[p + n*q] (n = nso/2).  Equivalent to phf_buildhsg with
+ * HOne = Ref^H blockdiag(h,h) Ref and HTwo = the Ref-MO transform of the antisymmetrised
+ * spin-orbital integrals (Main_PHF.py:22-33), without forming the n^4 tensor.
+ * Requires Ref unitary (the reference's Ref is an orthonormal MO matrix). */
+int phf_buildhsg_chol(const double *h, const double *bvec, int nchol, const phf_complex *ref, const phf_complex *z,
+                      const int *ngrid, int npg, int nci, int cmplxconj, int ncisp, int ncipg, int nocc, int nso,
+                      const phf_complex *r1, const phf_complex *r2, const phf_complex *rpg, const double *weightsp,
+                      const double *weightpg, const double *roota, const double *rootb, const double *rooty, int qj,
+                      int sp, int precision, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
+                      phf_complex *rdmmat);
+
+/* LocalG (PHF_fort/PHFTools.f90:203-247 declaration): G(M,M) = (sum f*f Gradmat - e0 sum f*f
+ * Rdmmat) / sum f*f Smat.  fk has 1 entry (2 when cmplxconj == 2).  Host buffers. */
+int phf_localg(const phf_complex *gradmat, const phf_complex *rdmmat, const phf_complex *smat, phf_complex e0,
+               int nso, const phf_complex *fsp, const phf_complex *fpg, const phf_complex *fk, int nci, int ncisp,
+               int ncipg, int cmplxconj, phf_complex *g);
+
+/* ---------------------------------------------------------------- plan API
+ * A plan holds the Hamiltonian, the grid and the device workspace, so that repeated
+ * energy/gradient evaluations (one per optimiser step, PHF.py:55-91) upload only Z or C. */
+typedef struct phf_plan phf_plan;
+
+typedef struct {
+    int nso, nocc;
+    int nchol;                                /* > 0: Cholesky form (h, bvec); 0: dense (hone, htwo) */
+    const double *h, *bvec;                   /* Cholesky form, layouts as phf_buildhsg_chol */
+    const phf_complex *hone, *htwo;           /* dense form, layouts as phf_buildhsg */
+    const phf_complex *ref;                   /* Ref(M,M) */
+    const int *ngrid;
+    int npg, nci, ncisp, ncipg, cmplxconj, qj, sp;
+    const phf_complex *r1, *r2, *rpg;
+    const double *weightsp, *weightpg, *roota, *rootb, *rooty;
+    int precision;                            /* enum phf_precision */
+    int slices;                               /* int8 slices per operand for PHF_PREC_OZAKI_I8 (0 = default) */
+    size_t workspace_bytes;                   /* per-chunk workspace budget (0 = default 6 GiB) */
+    int jk_form;                              /* Cholesky form only: 0 = automatic, 1 = exchange through the
+                                                 spatial ERI matrix (n^2 x n^2, built once per plan),
+                                                 2 = factorized (no n^4 tensor); automatic picks 1 for n <= 128 */
+} phf_plan_desc;
+
+int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);
+int phf_plan_destroy(phf_plan *plan);
+
+/* buildhsg semantics for a new Z with the plan's Hamiltonian, grid and Ref (host buffers). */
+int phf_plan_buildhsg(phf_plan *plan, const phf_complex *z, phf_complex *hmat, phf_complex *smat,
+                      phf_complex *gradmat, phf_complex *rdmmat);
+
+/* Device-resident evaluation for a determinant C (device, M x N row-major, [alpha; beta]
+ * spin-orbital order, in the basis of the plan's Hamiltonian: AO for the Cholesky form).
+ * Writes, in device memory on `stream` (a cudaStream_t, 0 = legacy default stream):
+ *   d_hs[2*a], d_hs[2*a+1]   -- sum_w W_a(w) N_w h_w and sum_w W_a(w) N_w for slot a = m + nci*n
+ *   d_yg[a*M*N + r*N + j]    -- sum_w W_a(w) N_w [(1 - rho_w) F_w X_w + h_w X_w]
+ *   d_yr[a*M*N + r*N + j]    -- sum_w W_a(w) N_w X_w,   X_w = R_w C (C^H R_w C)^-1
+ * so that Gradmat_a = Yg_a C^H, Rdmmat_a = Yr_a C^H, and for nci == 1 the energy is
+ * E = Re H / |Re S| and dE/dC* = (Yg - E Yr) / S.  cmplxconj must be 0 or 1. */
+int phf_plan_eval_device(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
+                         phf_complex *d_yr, void *stream);
+
+/* Grid points per pipeline chunk chosen by the plan, and its device workspace in bytes. */
+int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes);
+
+/* FP64-accurate real GEMM on the int8 tensor cores (the arithmetic of PHF_PREC_OZAKI_I8):
+ * D (m x n, row-major, ldd) = A (m x k, row-major, lda) * B, with B given transposed as
+ * Bt (n x k, row-major, ldb).  `slices` int8 slices per operand (1..7; 6 gives about
+ * 2^-49 k max|A_i.| max|B_.j| per entry).  Device pointers; synchronous on `stream`.
+ * No counterpart in the reference (its J/K is a dense FP64 loop, PHFTools.f90:310-337). */
+int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
+                    long long ldb, double *dD, long long ldd, void *stream);
+
+/* ---------------------------------------------------------------- diagnostics */
+const char *phf_status_string(int status);
+/* Message of the last failing call on this thread ("" when none). */
+const char *phf_last_error(void);
+/* Number of kernels this library has launched in this process. */
+unsigned long long phf_kernel_launches(void);
+/* Per-kernel-class timing with CUDA events on the launching stream, for roofline reports:
+ * class 0 = J/K contraction GEMMs, 1 = other GEMMs, 2 = overlap inverse, 3 = memory-bound
+ * kernels.  Enabling clears earlier records; read returns the summed device time of the
+ * launches recorded since (it waits for their end events). */
+int phf_profile_enable(int on);
+int phf_profile_read(int kernel_class, double *total_ms, unsigned long long *launches);
+/* Library version string. */
+const char *phf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHF_B200_H */

@@ -1,0 +1,269 @@
+"""Host-side API over the C ABI: one-shot calls and reusable plans.
+
+All arrays follow the reference's conventions (complex128 spin-orbital matrices in
+[alpha; beta] order, Fortran shapes of PHF_fort/PHFTools.f90:15-26).  The compute runs in
+libphf_b200.so on the GPU; this module only converts and checks arguments.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import PREC, PHFError, check, phf_complex, phf_plan_desc
+
+__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "PHFError"]
+
+
+def _fz(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.complex128))
+
+
+def _fd(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+class _Grid:
+    """Grid arguments of buildhsg converted to the C ABI layouts (kept alive by the instance)."""
+
+    def __init__(self, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty,
+                 qj, sp, npg=None, ncipg=None, nso=None):
+        self.r1, self.r2, self.rpg = _fz(r1), _fz(r2), _fz(rpg)
+        if self.r1.ndim != 3 or self.r2.ndim != 3 or self.rpg.ndim != 3:
+            raise ValueError("r1, r2, rpg must be (count, nso, nso) arrays")
+        self.nso = int(nso) if nso is not None else int(self.rpg.shape[1])
+        self.npg = int(npg) if npg is not None else int(self.rpg.shape[0])
+        self.weightpg = _fd(weightpg)
+        self.ncipg = int(ncipg) if ncipg is not None else int(self.weightpg.shape[1])
+        self.ngrid = np.ascontiguousarray(np.asarray(ngrid, dtype=np.int32).reshape(2))
+        self.weightsp = _fd(weightsp)
+        self.roota = np.ascontiguousarray(np.atleast_1d(np.asarray(roota, dtype=np.float64)))
+        self.rootb = np.ascontiguousarray(np.atleast_1d(np.asarray(rootb, dtype=np.float64)))
+        self.rooty = np.ascontiguousarray(np.atleast_1d(np.asarray(rooty, dtype=np.float64)))
+        self.nci, self.cmplxconj, self.ncisp, self.nocc = int(nci), int(cmplxconj), int(ncisp), int(nocc)
+        self.qj, self.sp = int(qj), int(sp)
+        nl, ny = int(self.ngrid[0]), int(self.ngrid[1])
+        M = self.nso
+        if self.r1.shape != (nl, M, M) or self.r2.shape != (ny, M, M) or self.rpg.shape != (self.npg, M, M):
+            raise ValueError(f"rotation shapes {self.r1.shape}, {self.r2.shape}, {self.rpg.shape} do not match "
+                             f"ngrid={list(self.ngrid)}, npg={self.npg}, nso={M}")
+        if self.weightsp.shape != (nl, ny):
+            raise ValueError(f"weightsp shape {self.weightsp.shape} != {(nl, ny)}")
+        if self.weightpg.shape != (self.npg, self.ncipg, self.ncipg):
+            raise ValueError(f"weightpg shape {self.weightpg.shape} != {(self.npg, self.ncipg, self.ncipg)}")
+        need_b = ny if self.sp == 2 else nl
+        need_y = nl if self.sp == 2 else ny
+        if self.roota.size < nl or self.rootb.size < need_b or self.rooty.size < need_y:
+            raise ValueError("roota/rootb/rooty are shorter than the grid")
+
+    def fill(self, d: phf_plan_desc):
+        d.nso, d.nocc = self.nso, self.nocc
+        d.ngrid = _ptr(self.ngrid)
+        d.npg, d.nci, d.ncisp, d.ncipg = self.npg, self.nci, self.ncisp, self.ncipg
+        d.cmplxconj, d.qj, d.sp = self.cmplxconj, self.qj, self.sp
+        d.r1, d.r2, d.rpg = _ptr(self.r1), _ptr(self.r2), _ptr(self.rpg)
+        d.weightsp, d.weightpg = _ptr(self.weightsp), _ptr(self.weightpg)
+        d.roota, d.rootb, d.rooty = _ptr(self.roota), _ptr(self.rootb), _ptr(self.rooty)
+
+    def outputs(self):
+        nci, M = self.nci, self.nso
+        return (np.zeros((nci, nci), dtype=np.complex128, order="F"),
+                np.zeros((nci, nci), dtype=np.complex128, order="F"),
+                np.zeros((nci, nci, M, M), dtype=np.complex128, order="F"),
+                np.zeros((nci, nci, M, M), dtype=np.complex128, order="F"))
+
+
+def _z_array(z, nso, nocc):
+    z = _fz(z)
+    if z.shape != (nso - nocc, nocc):
+        raise ValueError(f"z shape {z.shape} != {(nso - nocc, nocc)}")
+    return z
+
+
+def _bvec_fortran(B, n):
+    """Cholesky vectors B[L, p, q] (shape (L, n, n)) as the (n, n, L) Fortran array of the C ABI."""
+    B = np.asarray(B, dtype=np.float64)
+    if B.ndim != 3 or B.shape[1:] != (n, n):
+        raise ValueError(f"Cholesky vectors must have shape (L, {n}, {n}), got {B.shape}")
+    return np.asfortranarray(np.transpose(B, (1, 2, 0)))
+
+
+def buildhsg(hone, htwo, ref, z, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota,
+             rootb, rooty, qj, sp, npg=None, ncipg=None, nso=None, check_hermitian=True):
+    """BuildHSG with a dense HTwo (PHF_fort/PHFTools.f90:10-201) on the GPU.
+
+    Returns (Hmat, Smat, Gradmat, Rdmmat).  Raises PHFError where the reference STOPs; with
+    ``check_hermitian=False`` a non-Hermitian result is returned instead."""
+    g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj, sp,
+              npg, ncipg, nso)
+    M = g.nso
+    hone, htwo, ref = _fz(hone), _fz(htwo), _fz(ref)
+    if hone.shape != (M, M) or htwo.shape != (M, M, M, M) or ref.shape != (M, M):
+        raise ValueError("hone/htwo/ref shapes do not match nso")
+    z = _z_array(z, M, g.nocc)
+    H, S, G, R = g.outputs()
+    lib = _lib.load()
+    st = lib.phf_buildhsg(_ptr(hone), _ptr(htwo), _ptr(ref), _ptr(z), _ptr(g.ngrid), g.npg, g.nci, g.cmplxconj,
+                          g.ncisp, g.ncipg, g.nocc, M, _ptr(g.r1), _ptr(g.r2), _ptr(g.rpg), _ptr(g.weightsp),
+                          _ptr(g.weightpg), _ptr(g.roota), _ptr(g.rootb), _ptr(g.rooty), g.qj, g.sp, _ptr(H),
+                          _ptr(S), _ptr(G), _ptr(R))
+    if st == _lib.PHF_ERR_NOT_HERMITIAN and not check_hermitian:
+        return H, S, G, R
+    check(st, "phf_buildhsg")
+    return H, S, G, R
+
+
+def buildhsg_chol(h, B, ref, z, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
+                  rooty, qj, sp, npg=None, ncipg=None, nso=None, precision="fp64", check_hermitian=True):
+    """BuildHSG with Cholesky two-electron integrals (see phf_buildhsg_chol in include/phf_b200.h)."""
+    g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj, sp,
+              npg, ncipg, nso)
+    M = g.nso
+    n = M // 2
+    h = _fd(h)
+    bvec = _bvec_fortran(B, n)
+    ref = _fz(ref)
+    z = _z_array(z, M, g.nocc)
+    H, S, G, R = g.outputs()
+    lib = _lib.load()
+    st = lib.phf_buildhsg_chol(_ptr(h), _ptr(bvec), bvec.shape[2], _ptr(ref), _ptr(z), _ptr(g.ngrid), g.npg, g.nci,
+                               g.cmplxconj, g.ncisp, g.ncipg, g.nocc, M, _ptr(g.r1), _ptr(g.r2), _ptr(g.rpg),
+                               _ptr(g.weightsp), _ptr(g.weightpg), _ptr(g.roota), _ptr(g.rootb), _ptr(g.rooty), g.qj,
+                               g.sp, PREC[precision], _ptr(H), _ptr(S), _ptr(G), _ptr(R))
+    if st == _lib.PHF_ERR_NOT_HERMITIAN and not check_hermitian:
+        return H, S, G, R
+    check(st, "phf_buildhsg_chol")
+    return H, S, G, R
+
+
+def localg(gradmat, rdmmat, smat, e0, fsp, fpg, fk, cmplxconj, nso=None, nci=None, ncisp=None, ncipg=None):
+    """LocalG (PHF_fort/PHFTools.f90:203-247) on the GPU; returns the full (nso, nso) G."""
+    gradmat, rdmmat, smat = _fz(gradmat), _fz(rdmmat), _fz(smat)
+    fsp = np.ascontiguousarray(np.atleast_1d(np.asarray(fsp, dtype=np.complex128)))
+    fpg = np.ascontiguousarray(np.atleast_1d(np.asarray(fpg, dtype=np.complex128)))
+    fk = np.ascontiguousarray(np.atleast_1d(np.asarray(fk, dtype=np.complex128)))
+    nci = int(nci) if nci is not None else gradmat.shape[0]
+    nso = int(nso) if nso is not None else gradmat.shape[2]
+    ncisp = int(ncisp) if ncisp is not None else fsp.size
+    ncipg = int(ncipg) if ncipg is not None else fpg.size
+    if int(cmplxconj) == 2 and fk.size < 2:
+        raise ValueError("fk needs 2 entries when cmplxconj == 2")
+    G = np.zeros((nso, nso), dtype=np.complex128, order="F")
+    e = complex(np.asarray(e0).item())
+    lib = _lib.load()
+    st = lib.phf_localg(_ptr(gradmat), _ptr(rdmmat), _ptr(smat), phf_complex(e.real, e.imag), nso, _ptr(fsp),
+                        _ptr(fpg), _ptr(fk), nci, ncisp, ncipg, int(cmplxconj), _ptr(G))
+    check(st, "phf_localg")
+    return G
+
+
+class Plan:
+    """A reusable evaluation plan (Hamiltonian, grid and workspace resident on the GPU).
+
+    Cholesky form: pass ``h`` (n, n) and ``B`` (L, n, n); dense form: ``hone`` and
+    ``htwo``.  Grid arguments as buildhsg.  ``precision``: "fp64" or "ozaki_i8" (FP64-accurate
+    int8 tensor-core slices, ``slices`` per operand, default 6); ``jk_form``: "auto", "eri"
+    (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"."""
+
+    def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
+                 rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
+                 workspace_bytes=0, jk_form="auto", npg=None, ncipg=None, nso=None):
+        self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
+                        sp, npg, ncipg, nso)
+        g = self._g
+        M = g.nso
+        d = phf_plan_desc()
+        g.fill(d)
+        self._keep = []
+        self.ref = _fz(ref)
+        d.ref = _ptr(self.ref)
+        if B is not None:
+            self._h = _fd(h)
+            self._b = _bvec_fortran(B, M // 2)
+            d.nchol = self._b.shape[2]
+            d.h, d.bvec = _ptr(self._h), _ptr(self._b)
+        else:
+            self._hone, self._htwo = _fz(hone), _fz(htwo)
+            d.nchol = 0
+            d.hone, d.htwo = _ptr(self._hone), _ptr(self._htwo)
+        d.precision = PREC[precision]
+        d.slices = int(slices)
+        d.workspace_bytes = int(workspace_bytes)
+        d.jk_form = {"auto": 0, "eri": 1, "factorized": 2}[jk_form]
+        self.precision = precision
+        handle = ctypes.c_void_p()
+        lib = _lib.load()
+        check(lib.phf_plan_create(ctypes.byref(d), ctypes.byref(handle)), "phf_plan_create")
+        self._handle = handle
+        # the Hamiltonian now lives on the device; drop the host copies
+        self._h = self._b = self._hone = self._htwo = None
+        self.nso, self.nocc, self.nci = M, g.nocc, g.nci
+
+    @property
+    def chunk(self) -> int:
+        c = ctypes.c_int()
+        s = ctypes.c_size_t()
+        _lib.load().phf_plan_info(self._handle, ctypes.byref(c), ctypes.byref(s))
+        return int(c.value)
+
+    @property
+    def workspace_bytes(self) -> int:
+        c = ctypes.c_int()
+        s = ctypes.c_size_t()
+        _lib.load().phf_plan_info(self._handle, ctypes.byref(c), ctypes.byref(s))
+        return int(s.value)
+
+    def buildhsg(self, z, check_hermitian=True):
+        z = _z_array(z, self.nso, self.nocc)
+        H, S, G, R = self._g.outputs()
+        st = _lib.load().phf_plan_buildhsg(self._handle, _ptr(z), _ptr(H), _ptr(S), _ptr(G), _ptr(R))
+        if st == _lib.PHF_ERR_NOT_HERMITIAN and not check_hermitian:
+            return H, S, G, R
+        check(st, "phf_plan_buildhsg")
+        return H, S, G, R
+
+    def eval_device(self, C, out=None, stream=None):
+        """Accumulators for a device-resident C (torch complex128 (M, N) CUDA tensor).
+
+        Returns (hs (nci*nci, 2), yg (nci*nci, M, N), yr (nci*nci, M, N)) as torch tensors."""
+        import torch
+
+        if C.dtype != torch.complex128 or not C.is_cuda or tuple(C.shape) != (self.nso, self.nocc):
+            raise ValueError(f"C must be a complex128 CUDA tensor of shape {(self.nso, self.nocc)}")
+        C = C.contiguous()
+        ns = self.nci * self.nci
+        if out is None:
+            hs = torch.empty((ns, 2), dtype=torch.complex128, device=C.device)
+            yg = torch.empty((ns, self.nso, self.nocc), dtype=torch.complex128, device=C.device)
+            yr = torch.empty_like(yg)
+        else:
+            hs, yg, yr = out
+        if stream is None:
+            stream = torch.cuda.current_stream(C.device)
+        st = _lib.load().phf_plan_eval_device(self._handle, ctypes.c_void_p(C.data_ptr()),
+                                              ctypes.c_void_p(hs.data_ptr()), ctypes.c_void_p(yg.data_ptr()),
+                                              ctypes.c_void_p(yr.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+        check(st, "phf_plan_eval_device")
+        return hs, yg, yr
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            _lib.load().phf_plan_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

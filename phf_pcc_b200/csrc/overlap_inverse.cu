@@ -1,0 +1,166 @@
+// Batched FP64 complex inverse, determinant and log-determinant of the rotated overlaps
+// S_w = bra^H R_w ket (N x N), one CTA per grid point, the matrix resident in shared memory.
+//
+// Replaces InvertC (ZGETRF + ZGETRI) and determinantC (ZGETRF) of PHF_fort/Wrappers.f90:195-336
+// as called from RDM (PHF_fort/PHFTools.f90:259-260).  Algorithm: in-place Gauss-Jordan
+// elimination with partial (row) pivoting -- the pivot is the first row of maximal |re| + |im|
+// in the column, the choice LAPACK's izamax makes -- followed by the column interchanges
+// in reverse order.  The pivots are those of LU with partial pivoting, so
+//   det S = (-1)^{#interchanges} * prod(pivots),
+//   log det S = sum log|pivot| + i (sum arg(pivot) + pi #interchanges).
+// A zero pivot is reported as status 1 (the reference STOPs "Error in ZGetRF"); a
+// non-finite entry as status 2.  Both are OR-ed into *flag and the outputs of that grid
+// point are zeroed.
+#include "phf_common.cuh"
+
+namespace phf {
+
+namespace {
+
+constexpr int NT = 256;
+
+__global__ void __launch_bounds__(NT) gj_inverse_kernel(int N, const zc *__restrict__ S, long long s_rs,
+                                                        long long s_bs, zc *__restrict__ Sinv, long long i_rs,
+                                                        long long i_bs, zc *__restrict__ det, zc *__restrict__ logdet,
+                                                        int *__restrict__ flag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    zc *A = reinterpret_cast<zc *>(smem_raw);                 // N*N, row-major
+    zc *rowk = A + (size_t)N * N;                             // N
+    zc *colk = rowk + N;                                      // N
+    int *perm = reinterpret_cast<int *>(colk + N);            // N
+    __shared__ double red_v[NT];
+    __shared__ int red_i[NT];
+    __shared__ int s_bad;
+
+    const int tid = threadIdx.x;
+    const long long b = blockIdx.x;
+    const zc *Sb = S + b * s_bs;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    for (int e = tid; e < N * N; e += NT) {
+        int i = e / N, j = e - i * N;
+        zc v = Sb[(long long)i * s_rs + j];
+        if (!isfinite(v.x) || !isfinite(v.y)) s_bad = 2;
+        A[e] = v;
+    }
+    __syncthreads();
+
+    double logabs = 0.0, phase = 0.0;
+    zc d = mkz(1.0, 0.0);
+    int nswap = 0;
+    for (int k = 0; k < N && s_bad == 0; ++k) {
+        // pivot search: first index of the maximal |re| + |im| in rows k..N-1 of column k
+        double best = -1.0;
+        int bi = N;
+        for (int i = k + tid; i < N; i += NT) {
+            double a = abs1(A[i * N + k]);
+            if (a > best) { best = a; bi = i; }
+        }
+        red_v[tid] = best;
+        red_i[tid] = bi;
+        __syncthreads();
+        for (int s = NT / 2; s > 0; s >>= 1) {
+            if (tid < s) {
+                double ov = red_v[tid + s];
+                int oi = red_i[tid + s];
+                if (ov > red_v[tid] || (ov == red_v[tid] && oi < red_i[tid])) {
+                    red_v[tid] = ov;
+                    red_i[tid] = oi;
+                }
+            }
+            __syncthreads();
+        }
+        const int p = red_i[0];
+        const double pv = red_v[0];
+        __syncthreads();
+        if (!(pv > 0.0)) {  // exactly singular (or NaN pivot)
+            if (tid == 0) s_bad = (pv == 0.0) ? 1 : 2;
+            __syncthreads();
+            break;
+        }
+        if (p != k) {
+            for (int j = tid; j < N; j += NT) {
+                zc t = A[k * N + j];
+                A[k * N + j] = A[p * N + j];
+                A[p * N + j] = t;
+            }
+        }
+        if (tid == 0) perm[k] = p;
+        __syncthreads();
+        const zc piv = A[k * N + k];
+        // running determinant and log-determinant (every thread keeps the same copy)
+        d = d * piv;
+        logabs += log(hypot(piv.x, piv.y));
+        phase += atan2(piv.y, piv.x);
+        if (p != k) {
+            d = mkz(-d.x, -d.y);
+            ++nswap;
+        }
+        const zc inv = divz(mkz(1.0, 0.0), piv);
+        // scaled pivot row (with 1/piv in column k) and the saved column k
+        for (int j = tid; j < N; j += NT) rowk[j] = (j == k) ? inv : A[k * N + j] * inv;
+        for (int i = tid; i < N; i += NT) colk[i] = A[i * N + k];
+        __syncthreads();
+        for (int e = tid; e < N * N; e += NT) {
+            int i = e / N, j = e - i * N;
+            if (i == k) {
+                A[e] = rowk[j];
+            } else {
+                zc a = (j == k) ? mkz(0.0, 0.0) : A[e];
+                A[e] = a - colk[i] * rowk[j];
+            }
+        }
+        __syncthreads();
+    }
+    const int bad = s_bad;
+    if (bad == 0) {
+        // undo the row interchanges as column interchanges, in reverse order
+        for (int k = N - 1; k >= 0; --k) {
+            const int p = perm[k];
+            if (p != k) {
+                for (int i = tid; i < N; i += NT) {
+                    zc t = A[i * N + k];
+                    A[i * N + k] = A[i * N + p];
+                    A[i * N + p] = t;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    zc *Ib = Sinv + b * i_bs;
+    for (int e = tid; e < N * N; e += NT) {
+        int i = e / N, j = e - i * N;
+        Ib[(long long)i * i_rs + j] = bad ? mkz(0.0, 0.0) : A[e];
+    }
+    if (tid == 0) {
+        if (bad) {
+            det[b] = mkz(0.0, 0.0);
+            logdet[b] = mkz(-INFINITY, 0.0);
+            atomicOr(flag, bad);
+        } else {
+            det[b] = d;
+            const double pi = 3.14159265358979323846;
+            double ph = fmod(phase + pi * (nswap & 1), 2.0 * pi);
+            if (ph > pi) ph -= 2.0 * pi;
+            if (ph <= -pi) ph += 2.0 * pi;
+            logdet[b] = mkz(logabs, ph);
+        }
+    }
+}
+
+}  // namespace
+
+size_t overlap_inverse_smem(int N) { return (size_t)N * N * sizeof(zc) + 2 * (size_t)N * sizeof(zc) + N * sizeof(int); }
+
+int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_bs, zc *Sinv, long long i_rs,
+                    long long i_bs, zc *det, zc *logdet, int *flag, cudaStream_t st) {
+    size_t smem = overlap_inverse_smem(N);
+    PHF_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ProfScope prof(st, PROF_INVERSE);
+    gj_inverse_kernel<<<batch, NT, smem, st>>>(N, S, s_rs, s_bs, Sinv, i_rs, i_bs, det, logdet, flag);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+}  // namespace phf

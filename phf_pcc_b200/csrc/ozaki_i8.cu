@@ -1,0 +1,522 @@
+// FP64-accurate GEMM on the tcgen05 int8 tensor cores (Ozaki-style error-free slicing).
+//
+// D = A B with A (m x k) and B (k x n) given as FP64.  Each row of A is scaled by a power of
+// two 2^ea so that |a| < 1 and cut into S signed 7-bit slices, a = sum_t a_t 2^{-7t}
+// (a_t in [-127, 127], truncation, the last slice rounded); each column of B likewise with
+// 2^eb.  Then
+//     D_ij = 2^{ea_i + eb_j} sum_{g=2}^{S+1} 2^{-7g} sum_{t+u=g} (A_t B_u)_ij
+// where every A_t B_u is an exact int8 x int8 -> int32 product on the tensor cores, the
+// products of one group g share one int32 accumulator (exact while (g-1) k 127^2 < 2^31),
+// and the S group sums are combined in FP64 in the epilogue.  Terms with t + u > S + 1 are
+// dropped; the error of an entry is below about (S+1) k 2^{-7(S+1)} max|A_i.| max|B_.j|.
+// (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
+// fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
+//
+// Kernel shape (one CTA per 128 x 64 output tile, 6 warps):
+//   warp 0      TMA producer: per 64-byte k-block one box of all S slices of the A tile
+//               (S x 128 x 64 B) and of the B tile (S x 64 x 64 B), SWIZZLE_64B, into a
+//               ring of stages guarded by full/empty mbarriers
+//   warp 1      TMEM allocation (512 columns) and the single-thread tcgen05.mma issuer:
+//               S(S+1)/2 slice pairs x 2 k-steps of 32 per stage, group g accumulating in
+//               TMEM columns [64 (g-2), 64 (g-1)); tcgen05.commit frees each stage
+//   warps 2-5   epilogue: tcgen05.ld 32x32b.x32 of each group, int32 -> FP64, 2^{-7g} scaling,
+//               2^{ea+eb} scaling, store (or add) into D
+// Every mbarrier wait gives up after ~2^31 clock cycles, sets *err and lets the CTA finish.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "phf_internal.h"
+
+namespace phf {
+
+namespace {
+
+constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 64;  // tile rows, tile columns, k-block bytes
+constexpr int OZ_THREADS = 192;
+constexpr int OZ_MAX_S = 7;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on an mbarrier phase.  Returns false (and sets *err) after ~2^31 cycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+    const uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1LL << 31)) {
+            atomicOr(err, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_64B (8 rows x 64 B atoms, SBO = 512 B).
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;                           // layout: SWIZZLE_64B
+    return d;
+}
+
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 64.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
+                              ((uint32_t)(OZ_BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct OzArgs {
+    int m, n, kb0, kblocks, S, stages;
+    const int *ea, *eb;  // row / column exponents
+    double *D;
+    long long ldd;
+    int accumulate;      // D += result instead of D = result
+    int *err;
+};
+
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
+    extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
+    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
+    const int S = args.S, STAGES = args.stages;
+    const uint32_t a_bytes = (uint32_t)S * OZ_BM * OZ_BK, b_bytes = (uint32_t)S * OZ_BN * OZ_BK;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)STAGES * stage_bytes);
+    uint64_t *empty_bar = full_bar + STAGES;
+    uint64_t *done_bar = empty_bar + STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done_bar + 1);
+    __shared__ int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * OZ_BM, n0 = blockIdx.x * OZ_BN;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_base = *tmem_slot;
+    const int KB = args.kblocks;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            for (int kb = 0; kb < KB; ++kb) {
+                const int s = kb % STAGES, use = kb / STAGES;
+                if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
+                    abort_flag = 1;
+                    break;
+                }
+                if (abort_flag) break;
+                unsigned char *sa = smem + (size_t)s * stage_bytes;
+                mbar_arrive_expect_tx(&full_bar[s], stage_bytes);
+                tma_load_3d(&tmA, &full_bar[s], sa, (args.kb0 + kb) * OZ_BK, m0, 0);
+                tma_load_3d(&tmB, &full_bar[s], sa + a_bytes, (args.kb0 + kb) * OZ_BK, n0, 0);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            bool ok = true;
+            for (int kb = 0; kb < KB && ok; ++kb) {
+                const int s = kb % STAGES, use = kb / STAGES;
+                if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
+                    ok = false;
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sa = smem_u32(smem + (size_t)s * stage_bytes);
+                const uint32_t sb = sa + a_bytes;
+                for (int g = 2; g <= S + 1; ++g) {
+                    const uint32_t dcol = tmem_base + (uint32_t)(g - 2) * OZ_BN;
+                    for (int t = 1; t < g; ++t) {
+                        const int u = g - t;
+#pragma unroll
+                        for (int kk = 0; kk < OZ_BK / 32; ++kk) {
+                            const uint64_t da = sdesc_sw64(sa + (uint32_t)(t - 1) * OZ_BM * OZ_BK + kk * 32);
+                            const uint64_t db = sdesc_sw64(sb + (uint32_t)(u - 1) * OZ_BN * OZ_BK + kk * 32);
+                            const uint32_t acc = (kb > 0 || t > 1 || kk > 0) ? 1u : 0u;
+                            mma_i8(dcol, da, db, acc);
+                        }
+                    }
+                }
+                mma_commit(&empty_bar[s]);  // stage s reusable once these MMAs have read it
+            }
+            mma_commit(done_bar);  // accumulators final once every issued MMA completes
+        }
+    } else {
+        // epilogue warps 2..5 cover TMEM lane quarters (warp % 4)
+        const int quarter = warp & 3;
+        const bool ok = mbar_wait(done_bar, 0, args.err, 4);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int row = m0 + quarter * 32 + lane;
+        const bool row_ok = row < args.m;
+        const int ea = row_ok ? args.ea[row] : 0;
+        if (ok && !abort_flag) {
+#pragma unroll 1
+            for (int c = 0; c < OZ_BN / 32; ++c) {
+                double acc[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+#pragma unroll 1
+                for (int g = S + 1; g >= 2; --g) {
+                    uint32_t v[32];
+                    const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(g - 2) * OZ_BN + c * 32;
+                    tmem_ld32(taddr, v);
+                    const double sc = ldexp(1.0, -7 * g);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                }
+                if (row_ok) {
+                    double *drow = args.D + (long long)row * args.ldd;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = n0 + c * 32 + j;
+                        if (col < args.n) {
+                            const double val = ldexp(acc[j], ea + args.eb[col]);
+                            drow[col] = args.accumulate ? drow[col] + val : val;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
+    }
+}
+
+// ------------------------------------------------------------------ slicing kernels
+__device__ __forceinline__ int exp_of_max(double mx) {
+    if (!(mx > 0.0) || !isfinite(mx)) return 0;
+    int e;
+    frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1): |x| 2^-e < 1
+    return e;
+}
+
+__device__ __forceinline__ void slice_value(double x, int e, int S, signed char *out, long long stride) {
+    double r = ldexp(x, -e);
+    for (int t = 0; t < S; ++t) {
+        r *= 128.0;
+        double a = (t + 1 < S) ? trunc(r) : rint(r);
+        a = fmin(127.0, fmax(-127.0, a));
+        r -= a;
+        out[(long long)t * stride] = (signed char)(int)a;
+    }
+}
+
+constexpr int SL_NT = 256;
+
+__device__ double block_max(double v, double *sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Rows of a real row-major matrix A (m x k, lda) -> slices [S][mpad][kpad] and ea[m].
+__global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const double *A, long long lda, int S,
+                                                           long long mpad, long long kpad, signed char *out, int *ea) {
+    __shared__ double sh[SL_NT];
+    const long long row = blockIdx.x;
+    const double *a = A + row * lda;
+    double mx = 0.0;
+    for (int j = threadIdx.x; j < k; j += SL_NT) mx = fmax(mx, fabs(a[j]));
+    mx = block_max(mx, sh);
+    const int e = exp_of_max(mx);
+    if (threadIdx.x == 0) ea[row] = e;
+    const long long stride = mpad * kpad;
+    for (long long j = threadIdx.x; j < kpad; j += SL_NT) {
+        double x = (j < k) ? a[j] : 0.0;
+        slice_value(x, e, S, out + row * kpad + j, stride);
+    }
+}
+
+// Columns of the exchange operand: for grid point w and spin block (sigma, tau) of rho_w
+// (M x M complex, interleaved spin order, row-major, rows at rho + w * M * M), column
+// c = (w * 4 + sigma * 2 + tau) * 2 + part holds part(rho_w[2l + sigma][2j + tau]) at k = l n + j.
+__global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *rho, int S, long long npad,
+                                                               long long kpad, signed char *out, int *eb) {
+    __shared__ double sh[SL_NT];
+    const long long c = blockIdx.x;
+    const int part = (int)(c & 1), st = (int)((c >> 1) & 3);
+    const long long w = c >> 3;
+    const int sg = st >> 1, tu = st & 1;
+    const int M = 2 * n;
+    const zc *R = rho + w * (long long)M * M;
+    const int k = n * n;
+    double mx = 0.0;
+    for (int e = threadIdx.x; e < k; e += SL_NT) {
+        int l = e / n, j = e - l * n;
+        zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
+        mx = fmax(mx, fabs(part ? v.y : v.x));
+    }
+    mx = block_max(mx, sh);
+    const int ex = exp_of_max(mx);
+    if (threadIdx.x == 0) eb[c] = ex;
+    const long long stride = npad * kpad;
+    for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
+        double x = 0.0;
+        if (e < k) {
+            int l = (int)(e / n), j = (int)(e - (long long)l * n);
+            zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
+            x = part ? v.y : v.x;
+        }
+        slice_value(x, ex, S, out + c * kpad + e, stride);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_slice_map(CUtensorMap *map, const signed char *base, long long kpad, long long rows_pad, int S, int box_rows) {
+    auto enc = get_encode();
+    if (!enc) {
+        set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+        return PHF_ERR_CUDA;
+    }
+    cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows_pad, (cuuint64_t)S};
+    cuuint64_t strides[2] = {(cuuint64_t)kpad, (cuuint64_t)(kpad * rows_pad)};
+    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, (cuuint32_t)S};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+        return PHF_ERR_CUDA;
+    }
+    return PHF_OK;
+}
+
+}  // namespace
+
+long long oz_pad_rows(long long m) { return (m + OZ_BM - 1) / OZ_BM * OZ_BM; }
+long long oz_pad_cols(long long n) { return (n + OZ_BN - 1) / OZ_BN * OZ_BN; }
+long long oz_pad_k(long long k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
+
+int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long rows_pad, signed char *out, int *ea,
+                  cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    slice_rows_kernel<<<m, SL_NT, 0, st>>>(m, k, A, lda, S, rows_pad, oz_pad_k(k), out, ea);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st) {
+    const long long ncols = 8LL * b;
+    ProfScope prof(st, PROF_MEMORY);
+    slice_rho_cols_kernel<<<(unsigned)ncols, SL_NT, 0, st>>>(n, rho, S, oz_pad_cols(ncols), oz_pad_k((long long)n * n),
+                                                             out, eb);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int oz_stages(int S) {
+    const size_t stage = (size_t)S * (OZ_BM + OZ_BN) * OZ_BK;
+    const size_t budget = 227 * 1024 - 1024 - 256;
+    int st = (int)(budget / stage);
+    return st > 4 ? 4 : st;
+}
+
+size_t oz_smem_bytes(int S) {
+    const int STAGES = oz_stages(S);
+    return 1024 + (size_t)STAGES * S * (OZ_BM + OZ_BN) * OZ_BK + (2 * STAGES + 1) * 8 + 16;
+}
+
+// D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
+// k is split into passes short enough for exact int32 group sums; later passes add into D.
+int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
+            double *D, long long ldd, int accumulate, int *err, cudaStream_t st) {
+    if (S < 1 || S > OZ_MAX_S) {
+        set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
+        return PHF_ERR_ARG;
+    }
+    const int stages = oz_stages(S);
+    if (stages < 2) {
+        set_error(PHF_ERR_UNSUPPORTED, "oz_gemm: too many slices for two pipeline stages");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    CUtensorMap ta, tb;
+    const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
+    PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
+    PHF_TRY(make_slice_map(&tb, Bsl, kpad, npad, S, OZ_BN));
+    // k-blocks per pass: S * kpass * 127^2 < 2^31
+    long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
+    if (kb_pass < 1) kb_pass = 1;
+    const long long kb_total = kpad / OZ_BK;
+    const size_t smem = oz_smem_bytes(S);
+    PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)(npad / OZ_BN), (unsigned)(mpad / OZ_BM), 1);
+    for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
+        OzArgs a;
+        a.m = m;
+        a.n = n;
+        a.kb0 = (int)kb0;
+        a.kblocks = (int)std::min(kb_pass, kb_total - kb0);
+        a.S = S;
+        a.stages = stages;
+        a.ea = ea;
+        a.eb = eb;
+        a.D = D;
+        a.ldd = ldd;
+        a.accumulate = (kb0 > 0) ? 1 : accumulate;
+        a.err = err;
+        {
+            ProfScope prof(st, PROF_JK);
+            ozaki_i8_gemm_kernel<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+        }
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+    }
+    return PHF_OK;
+}
+
+}  // namespace phf
+
+extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
+                               long long ldb, double *dD, long long ldd, void *stream) {
+    using namespace phf;
+    set_error(PHF_OK, "");
+    if (m <= 0 || n <= 0 || k <= 0 || !dA || !dBt || !dD || lda < k || ldb < k || ldd < n) {
+        set_error(PHF_ERR_ARG, "phf_ozaki_dgemm: bad sizes or null pointer");
+        return PHF_ERR_ARG;
+    }
+    if (slices < 1 || slices > OZ_MAX_S) {
+        set_error(PHF_ERR_ARG, "phf_ozaki_dgemm: slices must be 1..7");
+        return PHF_ERR_ARG;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n), kp = oz_pad_k(k);
+    signed char *As = nullptr, *Bs = nullptr;
+    int *ea = nullptr, *eb = nullptr, *err = nullptr;
+    int status = PHF_OK;
+    auto al = [&](void **p, size_t bytes) {
+        if (status != PHF_OK) return;
+        if (cudaMalloc(p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error(PHF_ERR_OOM, "phf_ozaki_dgemm: cudaMalloc failed");
+            status = PHF_ERR_OOM;
+        }
+    };
+    al((void **)&As, (size_t)slices * mp * kp);
+    al((void **)&Bs, (size_t)slices * np * kp);
+    al((void **)&ea, mp * sizeof(int));
+    al((void **)&eb, np * sizeof(int));
+    al((void **)&err, sizeof(int));
+    if (status == PHF_OK) {
+        cudaMemsetAsync(As, 0, (size_t)slices * mp * kp, st);
+        cudaMemsetAsync(Bs, 0, (size_t)slices * np * kp, st);
+        cudaMemsetAsync(err, 0, sizeof(int), st);
+        status = oz_slice_rows(m, k, dA, lda, slices, mp, As, ea, st);
+        if (status == PHF_OK) status = oz_slice_rows(n, k, dBt, ldb, slices, np, Bs, eb, st);
+        if (status == PHF_OK) status = oz_gemm(m, n, k, slices, As, ea, Bs, eb, dD, ldd, 0, err, st);
+        int herr = 0;
+        if (status == PHF_OK) {
+            cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm: stream synchronize failed");
+                status = PHF_ERR_CUDA;
+            } else if (herr) {
+                set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm: pipeline wait timed out");
+                status = PHF_ERR_CUDA;
+            }
+        }
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(As);
+    cudaFree(Bs);
+    cudaFree(ea);
+    cudaFree(eb);
+    cudaFree(err);
+    return status;
+}

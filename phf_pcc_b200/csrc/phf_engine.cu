@@ -1,0 +1,858 @@
+// Plan, grid-point pipeline and C ABI of the projected-HF grid kernel.
+//
+// The reference (PHF_fort/PHFTools.f90:84-170) loops over grid points w = (il, iy, ipg) and,
+// per point, forms R = Ref^H R1 R2 Rpg Ref (five M^3 products), the M x M transition density
+// rho_w, the dense O(M^4) MakeGamma, and M^3 gradient products.  This engine instead runs
+// chunks of b grid points through a fixed sequence of batched kernels, keeping every
+// per-point quantity in the rank-N form (M x N, never M x M except where the dense
+// two-electron operator needs vec(rho)):
+//
+//   Y_w  = R_w ket                          R applied to the N occupied columns only
+//   S_w  = bra^H Y_w ; S_w^-1, det, logdet  FP64 Gauss-Jordan, one CTA per point
+//   X_w  = Y_w S_w^-1                       rho_w = X_w bra^H
+//   HX_w = H1 X_w ; e1_w = tr(bra^H HX_w)   one-electron energy tr(H1 rho)
+//   GX_w = Gamma(rho_w) X_w                 dense: Gamma = H2r vec(rho); Cholesky: T = V^H X,
+//                                           T' = tr(T) 1 - T, Q = X T', GX = sum_L B_L Q_L
+//   e2_w = 1/2 tr(Gamma rho)                dense: tr(bra^H GX)/2; Cholesky: sum_L (d^2 - tr T^2)/2
+//   W_w  = bra^H (HX_w + GX_w)
+//   Yg_w = N_w [(HX + GX - X W) + h_w X],   Yr_w = N_w X_w,   h_w = e1 + e2   (Gradient :291-308)
+//   acc_a += sum_w Wt[a, w] (N h, N, Yg, Yr)   Wigner x character x spin weights (:120-166)
+//
+// and at the end Gradmat_a = Yg_a bra^H, Rdmmat_a = Yr_a bra^H (Ref-MO basis).
+// In the Cholesky form the spin-orbital index runs in the interleaved order r' = 2p + sigma
+// so that B_L (x) I_2 acts on plain row-major blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "phf_common.cuh"
+#include "phf_internal.h"
+
+namespace phf {
+
+unsigned long long g_launches = 0;
+
+// ---------------------------------------------------------------- per-class event timing
+namespace {
+struct ProfState {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;       // pairs (start, end)
+    std::vector<int> cls;              // class of each recorded pair
+    size_t used = 0;
+};
+ProfState g_prof;
+thread_local int t_prof_class = PROF_GEMM;
+}  // namespace
+
+void prof_set_class(int c) { t_prof_class = c; }
+int prof_class() { return t_prof_class; }
+
+ProfScope::ProfScope(cudaStream_t s, int c) : st(s), slot(-1) {
+    if (!g_prof.on) return;
+    if (g_prof.used * 2 + 2 > g_prof.ev.size()) {
+        for (int i = 0; i < 512; ++i) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            g_prof.ev.push_back(e);
+        }
+    }
+    slot = (int)g_prof.used++;
+    if ((int)g_prof.cls.size() <= slot) g_prof.cls.resize(slot + 1);
+    g_prof.cls[slot] = (c < 0) ? t_prof_class : c;
+    cudaEventRecord(g_prof.ev[2 * slot], st);
+}
+
+ProfScope::~ProfScope() {
+    if (slot >= 0) cudaEventRecord(g_prof.ev[2 * slot + 1], st);
+}
+
+int profile_enable(int on) {
+    g_prof.on = on != 0;
+    g_prof.used = 0;
+    return PHF_OK;
+}
+
+int profile_read(int c, double *ms, unsigned long long *count) {
+    double tot = 0.0;
+    unsigned long long n = 0;
+    for (size_t i = 0; i < g_prof.used; ++i) {
+        if (g_prof.cls[i] != c) continue;
+        float t = 0.f;
+        cudaEventSynchronize(g_prof.ev[2 * i + 1]);
+        if (cudaEventElapsedTime(&t, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]) == cudaSuccess) tot += t;
+        ++n;
+    }
+    if (ms) *ms = tot;
+    if (count) *count = n;
+    return PHF_OK;
+}
+
+static thread_local std::string t_last_error;
+static thread_local int t_last_status = PHF_OK;
+
+void set_error(int status, const std::string &msg) {
+    t_last_status = status;
+    t_last_error = msg;
+}
+int last_status() { return t_last_status; }
+std::string &last_error_string() { return t_last_error; }
+
+namespace {
+
+
+
+inline View vz(const void *p, long long rs, long long cs, long long bs0 = 0, long long bs1 = 0, int conj = 0) {
+    View v;
+    v.p = p;
+    v.rs = rs;
+    v.cs = cs;
+    v.bs0 = bs0;
+    v.bs1 = bs1;
+    v.conj = conj;
+    v.real = 0;
+    return v;
+}
+inline View vd(const void *p, long long rs, long long cs, long long bs0 = 0, long long bs1 = 0) {
+    View v = vz(p, rs, cs, bs0, bs1, 0);
+    v.real = 1;
+    return v;
+}
+inline OutView vo(zc *p, long long rs, long long cs, long long bs0 = 0, long long bs1 = 0) {
+    OutView o;
+    o.p = p;
+    o.rs = rs;
+    o.cs = cs;
+    o.bs0 = bs0;
+    o.bs1 = bs1;
+    return o;
+}
+
+const zc Z1{1.0, 0.0}, Z0{0.0, 0.0}, ZM1{-1.0, 0.0};
+
+double wigner_small_d(int j, int n, int m, double beta) {
+    auto fact = [](int k) {
+        double r = 1.0;
+        for (int i = 2; i <= k; ++i) r *= i;
+        return r;
+    };
+    double pre = std::sqrt(fact(j + n) * fact(j - n) * fact(j + m) * fact(j - m));
+    int smax = std::min(j + m, j - n), smin = std::max(0, m - n);
+    double acc = 0.0;
+    for (int s = smin; s <= smax; ++s) {
+        int p1 = n - m + s, p2 = 2 * j + m - n - 2 * s, p3 = n - m + 2 * s;
+        double num = ((p1 & 1) ? -1.0 : 1.0) * std::pow(std::cos(beta / 2), p2) * std::pow(std::sin(beta / 2), p3);
+        acc += num / (fact(j + m - s) * fact(s) * fact(n - m + s) * fact(j - n - s));
+    }
+    return pre * acc;
+}
+
+// Wignerfac (PHF_fort/PHFTools.f90:350-376)
+cd wignerfac(int j, int n, int m, double a, double b, double g) {
+    return std::exp(cd(0.0, -n * a)) * wigner_small_d(j, n, m, b) * std::exp(cd(0.0, -m * g));
+}
+
+}  // namespace
+
+namespace {
+
+int check_device(int *dev) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        set_error(PHF_ERR_NO_DEVICE, "no CUDA device available");
+        return PHF_ERR_NO_DEVICE;
+    }
+    PHF_CUDA(cudaGetDevice(dev));
+    return PHF_OK;
+}
+
+// complex128 Fortran array element
+inline cd fz(const phf_complex *a, size_t idx) { return cd(a[idx].re, a[idx].im); }
+
+int upload(zc *dst, const std::vector<cd> &src) {
+    PHF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(zc), cudaMemcpyHostToDevice));
+    return PHF_OK;
+}
+
+int validate(const phf_plan_desc *d) {
+    if (!d || d->nso <= 0 || d->nocc <= 0 || d->nocc > d->nso || !d->ngrid || d->ngrid[0] <= 0 || d->ngrid[1] <= 0 ||
+        d->npg <= 0 || d->ncisp <= 0 || d->ncipg <= 0 || d->qj < 0 || !d->ref || !d->r1 || !d->r2 || !d->rpg ||
+        !d->weightsp || !d->weightpg || !d->roota || !d->rootb || !d->rooty) {
+        set_error(PHF_ERR_ARG, "missing or non-positive plan argument");
+        return PHF_ERR_ARG;
+    }
+    const int ncik = d->cmplxconj == 2 ? 2 : 1;
+    if (d->cmplxconj < 0 || d->cmplxconj > 2) {
+        set_error(PHF_ERR_ARG, "cmplxconj must be 0, 1 or 2");
+        return PHF_ERR_ARG;
+    }
+    if (d->nci != d->ncisp * d->ncipg * ncik) {
+        set_error(PHF_ERR_ARG, "nci != ncisp * ncipg * ncik");
+        return PHF_ERR_ARG;
+    }
+    if (d->ncisp != 2 * d->qj + 1) {
+        set_error(PHF_ERR_ARG, "ncisp must equal 2*qj + 1 (Wigner slots ni, nj = -qj..qj)");
+        return PHF_ERR_ARG;
+    }
+    if (d->nchol > 0) {
+        if (!d->h || !d->bvec || (d->nso & 1)) {
+            set_error(PHF_ERR_ARG, "Cholesky form needs h, bvec and an even nso");
+            return PHF_ERR_ARG;
+        }
+    } else if (!d->hone || !d->htwo) {
+        set_error(PHF_ERR_ARG, "dense form needs hone and htwo");
+        return PHF_ERR_ARG;
+    }
+    if (d->nocc > kMaxOverlapN) {
+        set_error(PHF_ERR_UNSUPPORTED, "nocc > " + std::to_string(kMaxOverlapN) +
+                                           " (the overlap inverse keeps the N x N matrix in shared memory)");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    if (d->precision < PHF_PREC_FP64 || d->precision > PHF_PREC_TF32) {
+        set_error(PHF_ERR_ARG, "unknown precision");
+        return PHF_ERR_ARG;
+    }
+    if (d->precision != PHF_PREC_FP64 && d->nchol <= 0) {
+        set_error(PHF_ERR_UNSUPPORTED, "tensor-core precisions are implemented for the Cholesky form");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    if (d->jk_form < 0 || d->jk_form > 2) {
+        set_error(PHF_ERR_ARG, "jk_form must be 0, 1 or 2");
+        return PHF_ERR_ARG;
+    }
+    return PHF_OK;
+}
+
+}  // namespace
+
+namespace {
+int build_exchange_matrix(PlanImpl &p);
+}  // namespace
+
+int plan_create(const phf_plan_desc *d, phf_plan **out) {
+    *out = nullptr;
+    PHF_TRY(validate(d));
+    auto P = std::make_unique<phf_plan>();
+    PlanImpl &p = P->impl;
+    PHF_TRY(check_device(&p.device));
+    p.chol = d->nchol > 0;
+    p.M = d->nso;
+    p.n = d->nso / 2;
+    p.N = d->nocc;
+    p.L = d->nchol;
+    p.prec = d->precision;
+    p.slices = d->slices > 0 ? d->slices : 6;
+    if (p.chol) p.eri = (d->jk_form == 1) || (d->jk_form == 0 && d->nso / 2 <= 128);
+    if (p.prec == PHF_PREC_OZAKI_I8 && !p.eri) {
+        set_error(PHF_ERR_UNSUPPORTED, "the int8 tensor-core path needs the spatial-ERI exchange form (jk_form 0/1)");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    if (p.prec == PHF_PREC_BF16X3 || p.prec == PHF_PREC_TF32) {
+        set_error(PHF_ERR_UNSUPPORTED, "BF16x3 and TF32 contractions are not built into this library version");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    p.nl = d->ngrid[0];
+    p.ny = d->ngrid[1];
+    p.npg = d->npg;
+    p.nomega = p.nl * p.ny * p.npg;
+    p.nci = d->nci;
+    p.ncisp = d->ncisp;
+    p.ncipg = d->ncipg;
+    p.cmplxconj = d->cmplxconj;
+    p.qj = d->qj;
+    p.sp = d->sp;
+    p.nb = p.ncisp * p.ncipg;
+    const int M = p.M, N = p.N, n = p.n;
+    const size_t MM = (size_t)M * M;
+
+    // working order
+    p.perm.resize(M);
+    for (int r = 0; r < M; ++r) p.perm[r] = p.chol ? ((r & 1) * n + (r >> 1)) : r;
+    std::vector<int> inv(M);
+    for (int r = 0; r < M; ++r) inv[p.perm[r]] = r;
+
+    // rotation matrices in working order, row-major
+    auto rot = [&](const phf_complex *src, int cnt, zc **dst) -> int {
+        PHF_TRY(p.arena.alloc(dst, (size_t)cnt * MM));
+        std::vector<cd> h((size_t)cnt * MM);
+        for (int g = 0; g < cnt; ++g)
+            for (int i = 0; i < M; ++i)
+                for (int j = 0; j < M; ++j)
+                    h[(size_t)g * MM + (size_t)i * M + j] =
+                        fz(src, (size_t)g + (size_t)cnt * ((size_t)p.perm[i] + (size_t)M * p.perm[j]));
+        return upload(*dst, h);
+    };
+    // dense form: R acts in the reference AO order (Y is mapped to MO afterwards with Ref^H)
+    PHF_TRY(rot(d->r1, p.nl, &p.R1));
+    PHF_TRY(rot(d->r2, p.ny, &p.R2));
+    PHF_TRY(rot(d->rpg, p.npg, &p.Rpg));
+
+    // Ref (row-major, reference order kept on the host; rows in working order on the device)
+    p.ref_host.resize(MM);
+    for (int i = 0; i < M; ++i)
+        for (int j = 0; j < M; ++j) p.ref_host[(size_t)i * M + j] = fz(d->ref, (size_t)i + (size_t)M * j);
+    {
+        std::vector<cd> rw(MM);
+        for (int r = 0; r < M; ++r)
+            for (int j = 0; j < M; ++j) rw[(size_t)r * M + j] = p.ref_host[(size_t)p.perm[r] * M + j];
+        PHF_TRY(p.arena.alloc(&p.Refw, MM));
+        PHF_TRY(upload(p.Refw, rw));
+        if (p.chol) {  // Ref must be unitary for the AO-basis formulation
+            double dev = 0.0;
+            for (int i = 0; i < M; ++i)
+                for (int j = 0; j < M; ++j) {
+                    cd s = 0;
+                    for (int k = 0; k < M; ++k) s += std::conj(p.ref_host[(size_t)k * M + i]) * p.ref_host[(size_t)k * M + j];
+                    dev = std::max(dev, std::abs(s - cd(i == j ? 1.0 : 0.0)));
+                }
+            if (dev > 1e-8) {
+                set_error(PHF_ERR_ARG, "Cholesky form needs a unitary Ref (max |Ref^H Ref - I| = " + std::to_string(dev) + ")");
+                return PHF_ERR_ARG;
+            }
+        }
+    }
+    {  // [0, M): working -> reference index; [M, 2M): reference -> working index
+        std::vector<int> both(2 * (size_t)M);
+        for (int r = 0; r < M; ++r) {
+            both[r] = p.perm[r];
+            both[M + r] = inv[r];
+        }
+        PHF_TRY(p.arena.alloc(&p.permdev, 2 * (size_t)M));
+        PHF_CUDA(cudaMemcpy(p.permdev, both.data(), 2 * (size_t)M * sizeof(int), cudaMemcpyHostToDevice));
+    }
+
+    // weight table Wt[s, w], s = m + nb n over the base block, w = (il ny + iy) npg + ipg
+    {
+        const int nb = p.nb, nw = p.nomega;
+        std::vector<cd> Wt((size_t)nb * nb * nw, cd(0, 0));
+        const int qj = p.qj;
+        for (int il = 0; il < p.nl; ++il)
+            for (int iy = 0; iy < p.ny; ++iy)
+                for (int ig = 0; ig < p.npg; ++ig) {
+                    const int w = (il * p.ny + iy) * p.npg + ig;
+                    const double wsp = d->weightsp[(size_t)il + (size_t)p.nl * iy];
+                    for (int ni = -qj; ni <= qj; ++ni)
+                        for (int nj = -qj; nj <= qj; ++nj) {
+                            cd wig = (p.sp == 2) ? wignerfac(qj, ni, nj, d->roota[il], d->rootb[iy], d->rooty[il])
+                                                 : wignerfac(qj, ni, nj, d->roota[il], d->rootb[il], d->rooty[iy]);
+                            for (int pp = 0; pp < p.ncipg; ++pp)
+                                for (int q = 0; q < p.ncipg; ++q) {
+                                    double wpg = d->weightpg[(size_t)ig + (size_t)p.npg * ((size_t)pp + (size_t)p.ncipg * q)];
+                                    int m = ni + qj + pp * p.ncisp, nn = nj + qj + q * p.ncisp;
+                                    Wt[(size_t)(m + nb * nn) * nw + w] += wsp * wpg * wig;
+                                }
+                        }
+                }
+        PHF_TRY(p.arena.alloc(&p.Wt, Wt.size()));
+        PHF_TRY(upload(p.Wt, Wt));
+        // slot maps of the four (bra, ket) variants (PHFTools.f90:149-162)
+        std::vector<int> sm(4 * (size_t)nb * nb);
+        const int dm[4] = {0, 0, 1, 1}, dn[4] = {0, 1, 1, 0};
+        for (int v = 0; v < 4; ++v)
+            for (int m = 0; m < nb; ++m)
+                for (int nn = 0; nn < nb; ++nn)
+                    sm[(size_t)v * nb * nb + m + nb * nn] = (m + dm[v] * nb) + p.nci * (nn + dn[v] * nb);
+        PHF_TRY(p.arena.alloc(&p.slotmap, sm.size()));
+        PHF_CUDA(cudaMemcpy(p.slotmap, sm.data(), sm.size() * sizeof(int), cudaMemcpyHostToDevice));
+        // GEMM offsets of Y_w = R1[il] T2[iy, ig]
+        std::vector<long long> offs(3 * (size_t)nw);
+        for (int w = 0; w < nw; ++w) {
+            int il = w / (p.ny * p.npg), rem = w % (p.ny * p.npg);
+            offs[3 * w] = (long long)il * MM;
+            offs[3 * w + 1] = (long long)rem * M * N;
+            offs[3 * w + 2] = 0;
+        }
+        PHF_TRY(p.arena.alloc(&p.offs, offs.size()));
+        PHF_CUDA(cudaMemcpy(p.offs, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    }
+
+    // Hamiltonian
+    if (p.chol) {
+        const int L = p.L;
+        std::vector<double> hh((size_t)n * n), Bst((size_t)L * n * n);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) hh[(size_t)i * n + j] = d->h[(size_t)i + (size_t)n * j];
+        for (int l = 0; l < L; ++l)
+            for (int pp = 0; pp < n; ++pp)
+                for (int q = 0; q < n; ++q)
+                    Bst[((size_t)l * n + pp) * n + q] = d->bvec[(size_t)pp + (size_t)n * ((size_t)q + (size_t)n * l)];
+        PHF_TRY(p.arena.alloc(&p.h, hh.size()));
+        PHF_TRY(p.arena.alloc(&p.Bst, Bst.size()));
+        PHF_CUDA(cudaMemcpy(p.h, hh.data(), hh.size() * sizeof(double), cudaMemcpyHostToDevice));
+        PHF_CUDA(cudaMemcpy(p.Bst, Bst.data(), Bst.size() * sizeof(double), cudaMemcpyHostToDevice));
+        if (p.eri) PHF_TRY(build_exchange_matrix(p));
+    } else {
+        std::vector<cd> h1(MM);
+        for (int i = 0; i < M; ++i)
+            for (int j = 0; j < M; ++j) h1[(size_t)i * M + j] = fz(d->hone, (size_t)i + (size_t)M * j);
+        PHF_TRY(p.arena.alloc(&p.H1, MM));
+        PHF_TRY(upload(p.H1, h1));
+        zc *h2 = nullptr;
+        PHF_TRY(p.arena.alloc(&p.H2r, MM * MM));
+        PHF_CUDA(cudaMalloc(&h2, MM * MM * sizeof(zc)));
+        cudaError_t e = cudaMemcpy(h2, d->htwo, MM * MM * sizeof(zc), cudaMemcpyHostToDevice);
+        int st = (e == cudaSuccess) ? launch_permute_h2(M, h2, p.H2r, 0) : PHF_ERR_CUDA;
+        if (e == cudaSuccess && st == PHF_OK) e = cudaDeviceSynchronize();
+        cudaFree(h2);
+        if (e != cudaSuccess) {
+            set_error(PHF_ERR_CUDA, std::string("uploading HTwo: ") + cudaGetErrorString(e));
+            return PHF_ERR_CUDA;
+        }
+        PHF_TRY(st);
+    }
+
+    // per-evaluation buffers
+    const size_t MN = (size_t)M * N;
+    PHF_TRY(p.arena.alloc(&p.bra, MN));
+    PHF_TRY(p.arena.alloc(&p.ket, MN));
+    PHF_TRY(p.arena.alloc(&p.kety, MN));
+    PHF_TRY(p.arena.alloc(&p.newmo, MN));
+    PHF_TRY(p.arena.alloc(&p.T1, (size_t)p.npg * MN));
+    PHF_TRY(p.arena.alloc(&p.T2, (size_t)p.ny * p.npg * MN));
+    if (p.chol) PHF_TRY(p.arena.alloc(&p.V, (size_t)p.L * MN));
+    const size_t nslot = (size_t)p.nci * p.nci;
+    PHF_TRY(p.arena.alloc(&p.accG, nslot * MN));
+    PHF_TRY(p.arena.alloc(&p.compG, nslot * MN));
+    PHF_TRY(p.arena.alloc(&p.accR, nslot * MN));
+    PHF_TRY(p.arena.alloc(&p.compR, nslot * MN));
+    PHF_TRY(p.arena.alloc(&p.accHS, 2 * nslot));
+    PHF_TRY(p.arena.alloc(&p.compHS, 2 * nslot));
+    PHF_TRY(p.arena.alloc(&p.tmpG, MN));
+    PHF_TRY(p.arena.alloc(&p.outMM, MM));
+    PHF_TRY(p.arena.alloc(&p.flag, 1));
+
+    // chunk size from the workspace budget
+    {
+        const size_t budget = d->workspace_bytes ? d->workspace_bytes : ((size_t)6 << 30);
+        size_t per = 5 * MN + 3 * (size_t)N * N + 8;
+        const size_t n2 = (size_t)n * n;
+        if (p.chol && p.eri) {
+            per += 2 * MM + 2 * n2 + p.L;                       // Rho, Gam, Pvec, Jvec, dvec
+            if (p.prec == PHF_PREC_FP64) per += 8 * n2;         // Kin, Kvec
+            else per += 4 * n2 + (8 * n2 * p.slices) / sizeof(zc) + 1;  // Dk, int8 slices
+        } else if (p.chol) {
+            per += (size_t)p.L * N * N + (size_t)p.L * MN + p.L;
+        } else {
+            per += 2 * MM;
+        }
+        per *= sizeof(zc);
+        per += split_bytes_per_point(p);
+        long long bmax = (long long)(budget / std::max<size_t>(per, 1));
+        bmax = std::max<long long>(1, std::min<long long>(bmax, 1024));
+        p.b = (int)std::min<long long>(bmax, p.nomega);
+    }
+    const size_t bMN = (size_t)p.b * MN, bNN = (size_t)p.b * N * N;
+    PHF_TRY(p.arena.alloc(&p.Ys, bMN));
+    if (!p.chol) PHF_TRY(p.arena.alloc(&p.Ys2, bMN));
+    PHF_TRY(p.arena.alloc(&p.S, bNN));
+    PHF_TRY(p.arena.alloc(&p.Sinv, bNN));
+    PHF_TRY(p.arena.alloc(&p.W, bNN));
+    PHF_TRY(p.arena.alloc(&p.Xs, bMN));
+    PHF_TRY(p.arena.alloc(&p.HX, bMN));
+    PHF_TRY(p.arena.alloc(&p.GX, bMN));
+    PHF_TRY(p.arena.alloc(&p.det, p.b));
+    PHF_TRY(p.arena.alloc(&p.logdet, p.b));
+    PHF_TRY(p.arena.alloc(&p.e1, p.b));
+    PHF_TRY(p.arena.alloc(&p.e2, p.b));
+    PHF_TRY(p.arena.alloc(&p.scal, 2 * (size_t)p.b));
+    if (p.chol && p.eri) {
+        const size_t n2 = (size_t)n * n, b = (size_t)p.b;
+        PHF_TRY(p.arena.alloc(&p.Rho, b * MM));
+        PHF_TRY(p.arena.alloc(&p.Gam, b * MM));
+        PHF_TRY(p.arena.alloc(&p.Pvec, b * n2));
+        PHF_TRY(p.arena.alloc(&p.Jvec, b * n2));
+        PHF_TRY(p.arena.alloc(&p.dvec, b * p.L));
+        if (p.prec == PHF_PREC_FP64) {
+            PHF_TRY(p.arena.alloc(&p.Kin, 4 * b * n2));
+            PHF_TRY(p.arena.alloc(&p.Kvec, 4 * b * n2));
+        } else {
+            PHF_TRY(p.arena.alloc(&p.Dk, 8 * b * n2));
+            const size_t bsl = (size_t)p.slices * oz_pad_cols(8 * (long long)b) * oz_pad_k((long long)n2);
+            PHF_TRY(p.arena.alloc(&p.Bsl, bsl));
+            PHF_CUDA(cudaMemset(p.Bsl, 0, bsl));
+            PHF_TRY(p.arena.alloc(&p.eb, (size_t)oz_pad_cols(8 * (long long)b)));
+        }
+    } else if (p.chol) {
+        PHF_TRY(p.arena.alloc(&p.T, (size_t)p.L * bNN));
+        PHF_TRY(p.arena.alloc(&p.Q, (size_t)p.L * bMN));
+        PHF_TRY(p.arena.alloc(&p.e2part, (size_t)p.L * p.b));
+    } else {
+        PHF_TRY(p.arena.alloc(&p.Pv, (size_t)p.b * MM));
+        PHF_TRY(p.arena.alloc(&p.Gv, (size_t)p.b * MM));
+    }
+    PHF_TRY(split_setup(p));
+    *out = P.release();
+    return PHF_OK;
+}
+
+namespace {
+
+// EK[(i n + k) n^2 + (l n + j)] = sum_L B_L[i][l] B_L[k][j] = (il|kj): the exchange operator
+// K(rho)_ik = sum_{lj} (il|jk) rho_lj as an n^2 x n^2 matrix acting on vec(rho) (built as n^2
+// batched n x n x L products); sliced to int8 for the tensor-core back-end.
+int build_exchange_matrix(PlanImpl &p) {
+    const int n = p.n, L = p.L;
+    const long long n2 = (long long)n * n;
+    double *EK = nullptr;
+    PHF_TRY(p.arena.alloc(&EK, (size_t)(n2 * n2)));
+    OutView o = vo(reinterpret_cast<zc *>(EK), n, 1, n2, n2 * n);
+    o.real = 1;
+    View Bv = vd(p.Bst, n2, 1, n, 0);
+    PHF_TRY(zgemm_strided(n, n, L, n, n, Z1, vd(p.Bst, 1, n2, 0, n), Bv, Z0, o, nullptr, 0));
+    if (p.prec == PHF_PREC_OZAKI_I8) {
+        const size_t bytes = (size_t)p.slices * oz_pad_rows(n2) * oz_pad_k(n2);
+        PHF_TRY(p.arena.alloc(&p.EKsl, bytes));
+        PHF_CUDA(cudaMemset(p.EKsl, 0, bytes));
+        PHF_TRY(p.arena.alloc(&p.ea, (size_t)oz_pad_rows(n2)));
+        PHF_TRY(p.arena.alloc(&p.ozerr, 1));
+        PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
+        PHF_TRY(oz_slice_rows((int)n2, (int)n2, EK, n2, p.slices, oz_pad_rows(n2), p.EKsl, p.ea, 0));
+    }
+    PHF_CUDA(cudaDeviceSynchronize());
+    p.EK = EK;  // kept for the FP64 back-end
+    return PHF_OK;
+}
+
+// Gamma(rho_w) X_w through the spatial ERI matrix:
+//   rho_w = X_w bra^H;  J = B^T (B vec P), P = rho_aa + rho_bb;  K_st = EK vec(rho_st);
+//   Gamma_w = I (x) J - K;  GX_w = Gamma_w X_w;  e2_w = tr(bra^H GX_w) / 2
+int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
+    const int M = p.M, N = p.N, n = p.n, L = p.L, b = p.b;
+    const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
+    PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0, vo(p.Rho, M, 1, MM),
+                          nullptr, st));
+    PHF_TRY(launch_gather_p(n, bc, p.Rho, p.Pvec, b, st));
+    PHF_TRY(zgemm_strided(L, bc, (int)n2, 1, 1, Z1, vd(p.Bst, n2, 1), vz(p.Pvec, b, 1), Z0, vo(p.dvec, b, 1), nullptr,
+                          st));
+    PHF_TRY(zgemm_strided((int)n2, bc, L, 1, 1, Z1, vd(p.Bst, 1, n2), vz(p.dvec, b, 1), Z0, vo(p.Jvec, b, 1), nullptr,
+                          st));
+    prof_set_class(PROF_JK);
+    if (p.prec == PHF_PREC_FP64) {
+        PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
+        PHF_TRY(zgemm_strided((int)n2, 4 * bc, (int)n2, 1, 1, Z1, vd(p.EK, n2, 1), vz(p.Kin, 4LL * b, 1), Z0,
+                              vo(p.Kvec, 4LL * b, 1), nullptr, st));
+        prof_set_class(PROF_GEMM);
+        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, p.Kvec, nullptr, 4LL * b, p.Gam, st));
+    } else {
+        PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
+        PHF_TRY(oz_gemm((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, 8LL * b, 0, p.ozerr, st));
+        prof_set_class(PROF_GEMM);
+        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, p.Dk, 8LL * b, p.Gam, st));
+    }
+    PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
+                          st));
+    PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st));
+    return PHF_OK;
+}
+
+// One (bra, ket) variant over all grid points, accumulated into slot map `v`.
+// bra, ket: M x N row-major in the working basis; kety: the vector R_w multiplies
+// (dense form: Ref ket in AO order; Cholesky form: ket itself).
+int run_variant(PlanImpl &p, int v, cudaStream_t st) {
+    const int M = p.M, N = p.N, n = p.n, L = p.L, b = p.b;
+    const long long MN = (long long)M * N, ld = (long long)b * N, MM = (long long)M * M;
+    // T1[g] = Rpg[g] kety ; T2[y, g] = R2[y] T1[g]
+    PHF_TRY(zgemm_strided(M, N, M, p.npg, 1, Z1, vz(p.Rpg, M, 1, MM), vz(p.kety, N, 1, 0), Z0, vo(p.T1, N, 1, MN),
+                          nullptr, st));
+    PHF_TRY(zgemm_strided(M, N, M, p.npg, p.ny, Z1, vz(p.R2, M, 1, 0, MM), vz(p.T1, N, 1, MN, 0), Z0,
+                          vo(p.T2, N, 1, MN, (long long)p.npg * MN), nullptr, st));
+    if (p.chol) {
+        // V_L = (B_L (x) I_2) bra: (L n x n) x (n x 2N), rows (L, p), columns (sigma, j)
+        PHF_TRY(zgemm_strided(L * n, 2 * N, n, 1, 1, Z1, vd(p.Bst, n, 1), vz(p.bra, 2 * N, 1), Z0, vo(p.V, 2 * N, 1),
+                              nullptr, st));
+    }
+    for (int w0 = 0; w0 < p.nomega; w0 += b) {
+        const int bc = std::min(b, p.nomega - w0);
+        // Y_w = R1[il] T2[iy, ig]
+        PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.R1, M, 1), vz(p.T2, N, 1), Z0, vo(p.Ys, ld, 1, N), p.offs + 3LL * w0,
+                              st));
+        zc *Y = p.Ys;
+        if (!p.chol) {  // Ref-MO basis: Y <- Ref^H Y
+            PHF_TRY(zgemm_strided(M, bc * N, M, 1, 1, Z1, vz(p.Refw, 1, M, 0, 0, 1), vz(p.Ys, ld, 1), Z0, vo(p.Ys2, ld, 1),
+                                  nullptr, st));
+            Y = p.Ys2;
+        }
+        // S_w = bra^H Y_w
+        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(Y, ld, 1), Z0, vo(p.S, ld, 1), nullptr,
+                              st));
+        PHF_TRY(overlap_inverse(N, bc, p.S, ld, N, p.Sinv, ld, N, p.det, p.logdet, p.flag, st));
+        // X_w = Y_w S_w^-1
+        PHF_TRY(zgemm_strided(M, N, N, bc, 1, Z1, vz(Y, ld, 1, N), vz(p.Sinv, ld, 1, N), Z0, vo(p.Xs, ld, 1, N), nullptr,
+                              st));
+        // HX and e1 = tr(bra^H H1 X)
+        // (Cholesky form: X viewed as n x (2 ld) with spin sigma at column offset sigma*ld, batched over sigma)
+        if (p.chol)
+            PHF_TRY(zgemm_strided(n, bc * N, n, 2, 1, Z1, vd(p.h, n, 1), vz(p.Xs, 2 * ld, 1, ld), Z0,
+                                  vo(p.HX, 2 * ld, 1, ld), nullptr, st));
+        else
+            PHF_TRY(zgemm_strided(M, bc * N, M, 1, 1, Z1, vz(p.H1, M, 1), vz(p.Xs, ld, 1), Z0, vo(p.HX, ld, 1), nullptr, st));
+        PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.HX, ld, p.e1, 1.0, st));
+        // Gamma(rho_w) X_w and e2
+        if (p.chol && p.eri) {
+            PHF_TRY(gamma_x_eri(p, bc, st));
+        } else if (p.chol) {
+            if (p.prec == PHF_PREC_FP64) {
+                prof_set_class(PROF_JK);
+                // T_Lw = V_L^H X_w : batched over L, (N x M) x (M x bN)
+                PHF_TRY(zgemm_strided(N, bc * N, M, L, 1, Z1, vz(p.V, 1, N, MN, 0, 1), vz(p.Xs, ld, 1), Z0,
+                                      vo(p.T, ld, 1, (long long)N * ld), nullptr, st));
+                PHF_TRY(launch_tprime(L, N, bc, p.T, ld, p.e2part, st));
+                // Q_Lw = X_w T'_Lw : batched over (w, L)
+                PHF_TRY(zgemm_strided(M, N, N, bc, L, Z1, vz(p.Xs, ld, 1, N, 0), vz(p.T, ld, 1, N, (long long)N * ld), Z0,
+                                      vo(p.Q, ld, 1, N, (long long)M * ld), nullptr, st));
+                // GX = [B_1 .. B_L] Q : (n x L n) x (L n x b N) for each spin sigma (column offset sigma*ld)
+                PHF_TRY(zgemm_strided(n, bc * N, L * n, 2, 1, Z1, vd(p.Bst, 1, n), vz(p.Q, 2 * ld, 1, ld), Z0,
+                                      vo(p.GX, 2 * ld, 1, ld), nullptr, st));
+                prof_set_class(PROF_GEMM);
+            } else {
+                PHF_TRY(split_gamma_x(p, bc, st));
+            }
+            PHF_TRY(launch_rowsum(bc, L, p.e2part, p.e2, 0.5, st));
+        } else {
+            prof_set_class(PROF_JK);
+            // rho_w = X_w bra^H stored as vec: Pv[(l M + j) b + w]
+            PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0,
+                                  vo(p.Pv, (long long)M * bc, bc, 1), nullptr, st));
+            PHF_TRY(zgemm_strided((int)MM, bc, (int)MM, 1, 1, Z1, vz(p.H2r, MM, 1), vz(p.Pv, bc, 1), Z0, vo(p.Gv, bc, 1),
+                                  nullptr, st));
+            PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gv, (long long)M * bc, bc, 1), vz(p.Xs, ld, 1, N), Z0,
+                                  vo(p.GX, ld, 1, N), nullptr, st));
+            prof_set_class(PROF_GEMM);
+            PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st));
+        }
+        // W = bra^H (HX + GX);  GX <- GX - X W
+        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.HX, ld, 1), Z0, vo(p.W, ld, 1),
+                              nullptr, st));
+        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.GX, ld, 1), Z1, vo(p.W, ld, 1),
+                              nullptr, st));
+        PHF_TRY(zgemm_strided(M, N, N, bc, 1, ZM1, vz(p.Xs, ld, 1, N), vz(p.W, ld, 1, N), Z1, vo(p.GX, ld, 1, N), nullptr,
+                              st));
+        PHF_TRY(launch_epilogue(M, N, bc, p.HX, p.GX, p.Xs, ld, p.det, p.e1, p.e2, p.scal, st));
+        const int nb2 = p.nb * p.nb;
+        PHF_TRY(launch_accumulate(nb2, M, N, bc, p.Wt, p.nomega, w0, p.slotmap + (size_t)v * nb2, p.GX, p.Xs, ld, p.scal,
+                                  p.accG, p.compG, p.accR, p.compR, p.accHS, p.compHS, st));
+    }
+    return PHF_OK;
+}
+
+int zero_acc(PlanImpl &p, cudaStream_t st) {
+    const size_t nslot = (size_t)p.nci * p.nci, MN = (size_t)p.M * p.N;
+    PHF_CUDA(cudaMemsetAsync(p.accG, 0, nslot * MN * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.compG, 0, nslot * MN * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.accR, 0, nslot * MN * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.compR, 0, nslot * MN * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.accHS, 0, 2 * nslot * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.compHS, 0, 2 * nslot * sizeof(zc), st));
+    PHF_CUDA(cudaMemsetAsync(p.flag, 0, sizeof(int), st));
+    return PHF_OK;
+}
+
+int fold_acc(PlanImpl &p, cudaStream_t st) {
+    const long long nslot = (long long)p.nci * p.nci, MN = (long long)p.M * p.N;
+    PHF_TRY(launch_fold_comp(nslot * MN, p.accG, p.compG, st));
+    PHF_TRY(launch_fold_comp(nslot * MN, p.accR, p.compR, st));
+    PHF_TRY(launch_fold_comp(2 * nslot, p.accHS, p.compHS, st));
+    return PHF_OK;
+}
+
+int read_flag(PlanImpl &p, cudaStream_t st) {
+    int flag = 0, oz = 0;
+    PHF_CUDA(cudaMemcpyAsync(&flag, p.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (p.ozerr) PHF_CUDA(cudaMemcpyAsync(&oz, p.ozerr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PHF_CUDA(cudaStreamSynchronize(st));
+    if (oz) {
+        set_error(PHF_ERR_CUDA, "tensor-core GEMM pipeline wait timed out (code " + std::to_string(oz) + ")");
+        return PHF_ERR_CUDA;
+    }
+    if (flag & 1) {
+        set_error(PHF_ERR_SINGULAR, "a rotated overlap bra^H R ket is exactly singular");
+        return PHF_ERR_SINGULAR;
+    }
+    if (flag & 2) {
+        set_error(PHF_ERR_NONFINITE, "non-finite rotated overlap");
+        return PHF_ERR_NONFINITE;
+    }
+    return PHF_OK;
+}
+
+// Hermiticity check of PHFTools.f90:195-200 on host copies
+bool hermitian_ok(const std::vector<cd> &H, const std::vector<cd> &S, int nci) {
+    double w1 = 0, w2 = 0, mh = 0, ms = 0;
+    for (int i = 0; i < nci; ++i)
+        for (int j = 0; j < nci; ++j) {
+            cd a = H[i + (size_t)nci * j], at = H[j + (size_t)nci * i];
+            cd s = S[i + (size_t)nci * j], stt = S[j + (size_t)nci * i];
+            w1 = std::max(w1, std::abs((std::conj(at) - a).imag()));
+            w2 = std::max(w2, std::abs((std::conj(stt) - s).imag()));
+            mh = std::max(mh, std::abs(a));
+            ms = std::max(ms, std::abs(s));
+        }
+    return !(w1 > mh * 1e-5 || w2 > ms * 1e-5);
+}
+
+}  // namespace
+
+// buildhsg semantics: newMO = [I; Z] (MO basis), outputs in Fortran layout on the host.
+int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
+                  phf_complex *rdmmat) {
+    const int M = p.M, N = p.N;
+    const size_t MN = (size_t)M * N;
+    cudaStream_t st = 0;
+    PHF_CUDA(cudaSetDevice(p.device));
+    // newMO and its conjugate in the MO basis
+    std::vector<cd> mo(MN, cd(0, 0));
+    for (int i = 0; i < N; ++i) mo[(size_t)i * N + i] = 1.0;
+    for (int a = 0; a < M - N; ++a)
+        for (int i = 0; i < N; ++i) {
+            cd v = fz(z, (size_t)a + (size_t)(M - N) * i);
+            if (p.cmplxconj == 0) v = cd(v.real(), 0.0);
+            mo[(size_t)(N + a) * N + i] = v;
+        }
+    auto to_work = [&](const std::vector<cd> &m_mo, std::vector<cd> &bra_w, std::vector<cd> &kety) {
+        // AO vector Ref m (reference order) and its working-order copy
+        std::vector<cd> ao(MN, cd(0, 0));
+        for (int r = 0; r < M; ++r)
+            for (int k = 0; k < M; ++k) {
+                cd rv = p.ref_host[(size_t)r * M + k];
+                if (rv == cd(0, 0)) continue;
+                for (int j = 0; j < N; ++j) ao[(size_t)r * N + j] += rv * m_mo[(size_t)k * N + j];
+            }
+        bra_w.assign(MN, cd(0, 0));
+        if (p.chol) {
+            for (int r = 0; r < M; ++r)
+                for (int j = 0; j < N; ++j) bra_w[(size_t)r * N + j] = ao[(size_t)p.perm[r] * N + j];
+            kety = bra_w;
+        } else {
+            bra_w = m_mo;
+            kety = ao;
+        }
+    };
+    std::vector<cd> moc(MN);
+    for (size_t i = 0; i < MN; ++i) moc[i] = std::conj(mo[i]);
+    std::vector<cd> bw0, ky0, bw1, ky1;
+    to_work(mo, bw0, ky0);
+    to_work(moc, bw1, ky1);
+
+    PHF_TRY(zero_acc(p, st));
+    const int nvar = p.cmplxconj == 2 ? 4 : 1;
+    // variants (bra, ket): 0 (C, C), 1 (C, C*), 2 (C*, C*), 3 (C*, C)   -- RDM / RDMConj calls of :91-107
+    for (int v = 0; v < nvar; ++v) {
+        const bool cb = (v >= 2), ck = (v == 1 || v == 2);
+        PHF_TRY(upload(p.bra, cb ? bw1 : bw0));
+        PHF_TRY(upload(p.kety, ck ? ky1 : ky0));
+        PHF_TRY(run_variant(p, v, st));
+    }
+    PHF_TRY(fold_acc(p, st));
+    PHF_TRY(read_flag(p, st));
+
+    // Gradmat_a = T Yg_a bra_a^H, Rdmmat likewise (T = Ref^H in the Cholesky form)
+    const int nci = p.nci, nb = p.nb;
+    const long long ns = (long long)nci * nci;
+    for (int a = 0; a < nci * nci; ++a) {
+        const int m = a % nci;
+        const bool conj_bra = (p.cmplxconj == 2) && (m >= nb);
+        PHF_TRY(upload(p.newmo, conj_bra ? moc : mo));
+        for (int which = 0; which < 2; ++which) {
+            zc *acc = (which == 0 ? p.accG : p.accR) + (size_t)a * MN;
+            const zc *src = acc;
+            if (p.chol) {
+                PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, 1, M, 0, 0, 1), vz(acc, N, 1), Z0, vo(p.tmpG, N, 1),
+                                      nullptr, st));
+                src = p.tmpG;
+            }
+            zc *outp = p.outMM;
+            PHF_TRY(zgemm_strided(M, M, N, 1, 1, Z1, vz(src, N, 1), vz(p.newmo, 1, N, 0, 0, 1), Z0, vo(outp, 1, M),
+                                  nullptr, st));
+            // outp holds the M x M block in column-major order; scatter into the (nci, nci, M, M) array on the host
+            std::vector<cd> blk((size_t)M * M);
+            PHF_CUDA(cudaMemcpyAsync(blk.data(), outp, blk.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
+            PHF_CUDA(cudaStreamSynchronize(st));
+            phf_complex *dst = which == 0 ? gradmat : rdmmat;
+            for (size_t ij = 0; ij < (size_t)M * M; ++ij) {
+                dst[(size_t)a + (size_t)ns * ij].re = blk[ij].real();
+                dst[(size_t)a + (size_t)ns * ij].im = blk[ij].imag();
+            }
+        }
+    }
+    std::vector<cd> hs(2 * (size_t)ns);
+    PHF_CUDA(cudaMemcpyAsync(hs.data(), p.accHS, hs.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
+    PHF_CUDA(cudaStreamSynchronize(st));
+    std::vector<cd> H(ns), S(ns);
+    for (int a = 0; a < ns; ++a) {
+        H[a] = hs[2 * a];
+        S[a] = hs[2 * a + 1];
+    }
+    if (p.cmplxconj == 2) {  // PHFTools.f90:174-179
+        const int d = nb;
+        for (int i = 0; i < d; ++i)
+            for (int j = 0; j < d; ++j) {
+                H[(d + i) + (size_t)nci * j] = std::conj(H[j + (size_t)nci * (d + i)]);
+                S[(d + i) + (size_t)nci * j] = std::conj(S[j + (size_t)nci * (d + i)]);
+                H[(d + i) + (size_t)nci * (d + j)] = H[i + (size_t)nci * j];
+                S[(d + i) + (size_t)nci * (d + j)] = S[i + (size_t)nci * j];
+            }
+    }
+    bool finite = true;
+    for (int a = 0; a < ns; ++a) {
+        hmat[a].re = H[a].real();
+        hmat[a].im = H[a].imag();
+        smat[a].re = S[a].real();
+        smat[a].im = S[a].imag();
+        finite = finite && std::isfinite(H[a].real()) && std::isfinite(H[a].imag()) && std::isfinite(S[a].real()) &&
+                 std::isfinite(S[a].imag());
+    }
+    if (!finite) {
+        set_error(PHF_ERR_NONFINITE, "non-finite Hmat/Smat");
+        return PHF_ERR_NONFINITE;
+    }
+    if (!hermitian_ok(H, S, nci)) {
+        set_error(PHF_ERR_NOT_HERMITIAN, "Hmat/Smat are not Hermitian to 1e-5 (reference: STOP \"Not Hermitian\")");
+        return PHF_ERR_NOT_HERMITIAN;
+    }
+    return PHF_OK;
+}
+
+int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st) {
+    if (p.cmplxconj == 2) {
+        set_error(PHF_ERR_UNSUPPORTED, "phf_plan_eval_device: cmplxconj == 2 needs phf_plan_buildhsg");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    const int M = p.M, N = p.N;
+    const long long MN = (long long)M * N;
+    PHF_CUDA(cudaSetDevice(p.device));
+    if (p.chol) {
+        // rows of C from [alpha; beta] order to the working order: bra[r'] = C[perm[r']]
+        PHF_TRY(launch_permute_rows(M, N, 1, p.permdev, d_c, N, 0, p.bra, 0, st));
+    } else {
+        PHF_CUDA(cudaMemcpyAsync(p.bra, d_c, MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    }
+    if (p.chol) {
+        PHF_CUDA(cudaMemcpyAsync(p.kety, p.bra, MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    } else {
+        // kety = Ref C (reference AO order)
+        PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(p.bra, N, 1), Z0, vo(p.kety, N, 1), nullptr, st));
+    }
+    PHF_TRY(zero_acc(p, st));
+    PHF_TRY(run_variant(p, 0, st));
+    PHF_TRY(fold_acc(p, st));
+    const long long ns = (long long)p.nci * p.nci;
+    PHF_CUDA(cudaMemcpyAsync(d_hs, p.accHS, 2 * ns * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    if (p.chol) {
+        // back to [alpha; beta] order: out[r] = acc[inv[r]]
+        PHF_TRY(launch_permute_rows(M, N, (int)ns, p.permdev + M, p.accG, N, MN, d_yg, MN, st));
+        PHF_TRY(launch_permute_rows(M, N, (int)ns, p.permdev + M, p.accR, N, MN, d_yr, MN, st));
+    } else {
+        PHF_CUDA(cudaMemcpyAsync(d_yg, p.accG, ns * MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+        PHF_CUDA(cudaMemcpyAsync(d_yr, p.accR, ns * MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    }
+    return read_flag(p, st);
+}
+
+}  // namespace phf

@@ -1,0 +1,156 @@
+// Internal interfaces between the translation units of the library.
+#pragma once
+#include <algorithm>
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "phf_common.cuh"
+
+namespace phf {
+
+using cd = std::complex<double>;
+
+// Device allocations owned by a plan, freed together.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Arena {
+    std::vector<DevBuf> bufs;
+    size_t total = 0;
+    ~Arena() { release(); }
+    void release() {
+        for (auto &b : bufs)
+            if (b.p) cudaFree(b.p);
+        bufs.clear();
+        total = 0;
+    }
+    template <typename T>
+    int alloc(T **out, size_t count) {
+        size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error(PHF_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+            return PHF_ERR_OOM;
+        }
+        bufs.push_back({p, bytes});
+        total += bytes;
+        *out = reinterpret_cast<T *>(p);
+        return PHF_OK;
+    }
+};
+
+
+// Largest N (occupied orbitals) whose N x N overlap fits the shared-memory inverse.
+constexpr int kMaxOverlapN = 112;
+
+
+// overlap_inverse.cu
+size_t overlap_inverse_smem(int N);
+int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_bs, zc *Sinv, long long i_rs,
+                    long long i_bs, zc *det, zc *logdet, int *flag, cudaStream_t st);
+
+// phf_kernels.cu
+int launch_tprime(int Ltot, int N, int b, zc *T, long long ldT, zc *e2part, cudaStream_t st);
+int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cudaStream_t st);
+int launch_trace_conj(int M, int N, int b, const zc *C, const zc *X, long long ldX, zc *out, double scale,
+                      cudaStream_t st);
+int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
+                    const zc *e2, zc *scal, cudaStream_t st);
+int launch_accumulate(int nslot, int M, int N, int b, const zc *Wt, long long nomega, long long w0, const int *slotmap,
+                      const zc *G, const zc *R, long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
+                      zc *compR, zc *accHS, zc *compHS, cudaStream_t st);
+int launch_fold_comp(long long n, zc *a, const zc *c, cudaStream_t st);
+int launch_permute_h2(int M, const zc *H2, zc *H2r, cudaStream_t st);
+int launch_permute_rows(int M, int N, int nbatch, const int *rowmap, const zc *in, long long ldin, long long bs_in,
+                        zc *out, long long bs_out, cudaStream_t st);
+int launch_localg(int MM, int nterm, const zc *coef_g, const zc *coef_r, const long long *slot_of_term,
+                  const int *conj_of_term, const zc *gradmat, const zc *rdmmat, long long nslot, zc e0, zc ovlp, zc *G,
+                  cudaStream_t st);
+
+int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStream_t st);
+int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st);
+int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const zc *Kc, const double *Kr, long long ldk,
+                          zc *Gam, cudaStream_t st);
+
+// ozaki_i8.cu: FP64-accurate GEMM from int8 slices on tcgen05
+long long oz_pad_rows(long long m);
+long long oz_pad_cols(long long n);
+long long oz_pad_k(long long k);
+int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long rows_pad, signed char *out, int *ea,
+                  cudaStream_t st);
+int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
+int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
+            double *D, long long ldd, int accumulate, int *err, cudaStream_t st);
+
+// phf_split.cu: tensor-core (tcgen05) J/K contraction workspace
+struct SplitWork {
+    void *ws = nullptr;
+    size_t bytes = 0;
+};
+
+// Everything a plan owns: sizes, grid tables, Hamiltonian and the chunk workspace.
+struct PlanImpl {
+    int device = 0;
+    bool chol = false;
+    int n = 0, M = 0, N = 0, L = 0;
+    int prec = PHF_PREC_FP64, slices = 0;
+    int eri = 0;                     // exchange via the spatial ERI matrix (1) or factorized Cholesky (0)
+    int nl = 0, ny = 0, npg = 0, nomega = 0;
+    int nci = 0, ncisp = 0, ncipg = 0, cmplxconj = 1, qj = 0, sp = 1, nb = 0;
+    std::vector<int> perm;           // working index -> reference index
+    std::vector<cd> ref_host;        // Ref row-major (reference order)
+
+    Arena arena;
+    // persistent device data
+    zc *R1 = nullptr, *R2 = nullptr, *Rpg = nullptr;  // working order, row-major
+    zc *Refw = nullptr;                                // Ref with rows in working order, row-major
+    zc *Wt = nullptr;                                  // nb^2 x nomega
+    long long *offs = nullptr;                         // 3 * nomega
+    int *slotmap = nullptr;                            // 4 x nb^2
+    int *permdev = nullptr;                            // 2M: [0,M) working->reference, [M,2M) reference->working
+    double *h = nullptr, *Bst = nullptr;               // Cholesky form
+    zc *H1 = nullptr, *H2r = nullptr;                  // dense form
+    // per evaluation
+    zc *bra = nullptr, *ket = nullptr, *kety = nullptr, *newmo = nullptr;
+    zc *T1 = nullptr, *T2 = nullptr, *V = nullptr;
+    // chunk workspace
+    int b = 0;
+    zc *Ys = nullptr, *Ys2 = nullptr, *S = nullptr, *Sinv = nullptr, *Xs = nullptr, *HX = nullptr, *GX = nullptr,
+       *W = nullptr, *T = nullptr, *Q = nullptr, *Pv = nullptr, *Gv = nullptr, *det = nullptr, *logdet = nullptr,
+       *e1 = nullptr, *e2 = nullptr, *e2part = nullptr, *scal = nullptr;
+    int *flag = nullptr;
+    // accumulators
+    zc *accG = nullptr, *compG = nullptr, *accR = nullptr, *compR = nullptr, *accHS = nullptr, *compHS = nullptr;
+    zc *tmpG = nullptr, *outMM = nullptr;
+    // spatial-ERI exchange form
+    double *EK = nullptr;              // EK[(i n + k) n^2 + l n + j] = (il|kj), FP64 back-end
+    signed char *EKsl = nullptr;       // its int8 slices, Ozaki back-end
+    int *ea = nullptr, *eb = nullptr, *ozerr = nullptr;
+    zc *Rho = nullptr, *Pvec = nullptr, *dvec = nullptr, *Jvec = nullptr, *Kin = nullptr, *Kvec = nullptr, *Gam = nullptr;
+    double *Dk = nullptr;
+    signed char *Bsl = nullptr;
+    SplitWork split;  // tensor-core path workspace (phf_split.cu)
+};
+
+size_t split_bytes_per_point(const PlanImpl &p);
+int split_setup(PlanImpl &p);
+int split_gamma_x(PlanImpl &p, int bc, cudaStream_t st);
+
+// phf_engine.cu
+int profile_enable(int on);
+int profile_read(int cls, double *ms, unsigned long long *count);
+int plan_create(const phf_plan_desc *d, phf_plan **out);
+int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
+                  phf_complex *rdmmat);
+int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st);
+
+}  // namespace phf
+
+struct phf_plan {
+    phf::PlanImpl impl;
+};

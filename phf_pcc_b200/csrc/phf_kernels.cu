@@ -1,0 +1,345 @@
+// Memory-bound kernels of the projected-HF pipeline: traces of the Cholesky-projected
+// overlaps, the energy/gradient epilogue, the weighted (Wigner x point-group) accumulation
+// over grid points, and layout transforms.  All reductions run in a fixed order, so two
+// runs give bit-identical results.
+#include "phf_common.cuh"
+
+namespace phf {
+
+namespace {
+
+constexpr int NT = 256;
+
+// block-wide complex sum with a fixed tree (deterministic for a fixed block size)
+__device__ zc block_sum(zc v, zc *sh) {
+    const int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (tid < s) sh[tid] = sh[tid] + sh[tid + s];
+        __syncthreads();
+    }
+    zc r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// For each Cholesky vector L and grid point w, with T_Lw = bra^H B_L X_w (N x N):
+//   d = tr T, e2part[w*L_tot + L] = d^2 - tr(T T), and T <- d I - T  (in place).
+// T_Lw is the block at rows L*N, columns w*N of a (L_tot*N) x ldT matrix.
+__global__ void __launch_bounds__(NT) tprime_kernel(int Ltot, int N, zc *T, long long ldT, zc *e2part) {
+    __shared__ zc sh[NT];
+    const long long L = blockIdx.x, w = blockIdx.y;
+    zc *base = T + L * N * ldT + w * N;
+    zc dd = mkz(0, 0), t2 = mkz(0, 0);
+    for (int j = threadIdx.x; j < N; j += NT) dd = dd + base[(long long)j * ldT + j];
+    for (int e = threadIdx.x; e < N * N; e += NT) {
+        int j = e / N, jp = e - j * N;
+        t2 = t2 + base[(long long)j * ldT + jp] * base[(long long)jp * ldT + j];
+    }
+    dd = block_sum(dd, sh);
+    t2 = block_sum(t2, sh);
+    if (threadIdx.x == 0) e2part[w * Ltot + L] = dd * dd - t2;
+    for (int e = threadIdx.x; e < N * N; e += NT) {
+        int j = e / N, jp = e - j * N;
+        long long o = (long long)j * ldT + jp;
+        zc t = base[o];
+        base[o] = (j == jp) ? (dd - t) : mkz(-t.x, -t.y);
+    }
+}
+
+// out[r] = scale * sum_c in[r * ncols + c]
+__global__ void __launch_bounds__(NT) rowsum_kernel(int ncols, const zc *in, zc *out, double scale) {
+    __shared__ zc sh[NT];
+    const long long r = blockIdx.x;
+    zc s = mkz(0, 0);
+    for (int c = threadIdx.x; c < ncols; c += NT) s = s + in[r * ncols + c];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[r] = scale * s;
+}
+
+// out[w] = scale * sum_{r,j} conj(C[r*N + j]) * X[r*ldX + w*N + j]   (tr(C^H X_w))
+__global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *C, const zc *X, long long ldX, zc *out,
+                                                        double scale) {
+    __shared__ zc sh[NT];
+    const long long w = blockIdx.x;
+    zc s = mkz(0, 0);
+    for (int e = threadIdx.x; e < M * N; e += NT) {
+        int r = e / N, j = e - r * N;
+        s = s + conjz(C[e]) * X[(long long)r * ldX + w * N + j];
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[w] = scale * s;
+}
+
+// Energy/gradient epilogue over a chunk of b grid points (Gradient, PHFTools.f90:291-308, in
+// the rank-N form): with h_w = e1_w + e2_w and N_w = det S_w,
+//   G <- N_w (HX + G + h_w X)    where G already holds GammaX - X W_w
+//   X <- N_w X
+//   scal[2w] = N_w h_w, scal[2w+1] = N_w
+__global__ void __launch_bounds__(NT) epilogue_kernel(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX,
+                                                      const zc *det, const zc *e1, const zc *e2, zc *scal) {
+    const long long total = (long long)M * b * N;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        long long r = e / ((long long)b * N);
+        long long c = e - r * ((long long)b * N);
+        int w = (int)(c / N);
+        long long o = r * ldX + c;
+        zc h = e1[w] + e2[w];
+        zc nd = det[w];
+        zc x = X[o];
+        G[o] = nd * (HX[o] + G[o] + h * x);
+        X[o] = nd * x;
+    }
+    if (blockIdx.x == 0) {
+        for (int w = threadIdx.x; w < b; w += NT) {
+            zc h = e1[w] + e2[w];
+            scal[2 * w] = det[w] * h;
+            scal[2 * w + 1] = det[w];
+        }
+    }
+}
+
+// Neumaier compensated add of a complex term into (s, c)
+__device__ __forceinline__ void neumaier(double &s, double &c, double x) {
+    double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+// Weighted accumulation over a chunk of grid points (PHFTools.f90:137-166):
+//   accG[a] += sum_w Wt[s, w0 + w] * G_w,  accR[a] += sum_w Wt[s, w0 + w] * R_w,
+//   accHS[a] += sum_w Wt[s, w0 + w] * (N h, N)_w      with a = slotmap[s],
+// summed over w in order with Neumaier compensation (comp arrays carried across chunks).
+__global__ void __launch_bounds__(NT) accumulate_kernel(int nslot, int M, int N, int b, const zc *Wt, long long nomega,
+                                                        long long w0, const int *slotmap, const zc *G, const zc *R,
+                                                        long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
+                                                        zc *compR, zc *accHS, zc *compHS) {
+    const long long MN = (long long)M * N;
+    const long long total = (long long)nslot * MN;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        int s = (int)(e / MN);
+        long long rj = e - (long long)s * MN;
+        long long r = rj / N, j = rj - r * N;
+        long long a = (long long)slotmap[s] * MN + rj;
+        double gs_r = accG[a].x, gs_i = accG[a].y, gc_r = compG[a].x, gc_i = compG[a].y;
+        double rs_r = accR[a].x, rs_i = accR[a].y, rc_r = compR[a].x, rc_i = compR[a].y;
+        const zc *wrow = Wt + (long long)s * nomega + w0;
+        for (int w = 0; w < b; ++w) {
+            zc wt = wrow[w];
+            long long o = r * ldX + (long long)w * N + j;
+            zc tg = wt * G[o], tr = wt * R[o];
+            neumaier(gs_r, gc_r, tg.x);
+            neumaier(gs_i, gc_i, tg.y);
+            neumaier(rs_r, rc_r, tr.x);
+            neumaier(rs_i, rc_i, tr.y);
+        }
+        accG[a] = mkz(gs_r, gs_i);
+        compG[a] = mkz(gc_r, gc_i);
+        accR[a] = mkz(rs_r, rs_i);
+        compR[a] = mkz(rc_r, rc_i);
+        if (rj == 0) {
+            long long ah = 2LL * slotmap[s];
+            double hs_r = accHS[ah].x, hs_i = accHS[ah].y, hc_r = compHS[ah].x, hc_i = compHS[ah].y;
+            double ss_r = accHS[ah + 1].x, ss_i = accHS[ah + 1].y, sc_r = compHS[ah + 1].x, sc_i = compHS[ah + 1].y;
+            for (int w = 0; w < b; ++w) {
+                zc wt = wrow[w];
+                zc th = wt * scal[2 * w], ts = wt * scal[2 * w + 1];
+                neumaier(hs_r, hc_r, th.x);
+                neumaier(hs_i, hc_i, th.y);
+                neumaier(ss_r, sc_r, ts.x);
+                neumaier(ss_i, sc_i, ts.y);
+            }
+            accHS[ah] = mkz(hs_r, hs_i);
+            compHS[ah] = mkz(hc_r, hc_i);
+            accHS[ah + 1] = mkz(ss_r, ss_i);
+            compHS[ah + 1] = mkz(sc_r, sc_i);
+        }
+    }
+}
+
+// a[i] += c[i]  (fold the compensation terms into the sums)
+__global__ void fold_comp_kernel(long long n, zc *a, const zc *c) {
+    for (long long i = blockIdx.x * (long long)NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT)
+        a[i] = a[i] + c[i];
+}
+
+// H2r[(i M + k) M^2 + (l M + j)] = H2(i, j, k, l) with H2 in Fortran order (MakeGamma operand
+// reshaped to an M^2 x M^2 matrix acting on vec(rho) with rho(l, j) at l M + j)
+__global__ void permute_h2_kernel(int M, const zc *H2, zc *H2r) {
+    const long long M2 = (long long)M * M, tot = M2 * M2;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        long long row = e / M2, col = e - row * M2;
+        long long i = row / M, k = row - i * M, l = col / M, j = col - l * M;
+        H2r[e] = H2[i + M * (j + M * (k + M * l))];
+    }
+}
+
+// out[r*N + j] = in[rowmap[r]*ldin + j]  (row permutation of an M x N matrix, batched by blockIdx.y)
+__global__ void permute_rows_kernel(int M, int N, const int *rowmap, const zc *in, long long ldin, long long bs_in,
+                                    zc *out, long long bs_out) {
+    const long long tot = (long long)M * N;
+    const zc *src = in + blockIdx.y * bs_in;
+    zc *dst = out + blockIdx.y * bs_out;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        long long r = e / N, j = e - r * N;
+        dst[e] = src[(long long)rowmap[r] * ldin + j];
+    }
+}
+
+// P[(p n + q) ldp + w] = rho_w[2p][2q] + rho_w[2p+1][2q+1]  (spin-summed density for J)
+__global__ void gather_p_kernel(int n, int b, const zc *rho, zc *P, long long ldp) {
+    const int M = 2 * n;
+    const long long tot = (long long)n * n * b;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        long long pq = e / b, w = e - pq * b;
+        int p = (int)(pq / n), q = (int)(pq - (long long)p * n);
+        const zc *R = rho + w * (long long)M * M;
+        P[pq * ldp + w] = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
+    }
+}
+
+// Kin[(l n + j) ldk + 4 w + 2 sigma + tau] = rho_w[2l + sigma][2j + tau]  (exchange operand)
+__global__ void gather_kin_kernel(int n, int b, const zc *rho, zc *Kin, long long ldk) {
+    const int M = 2 * n;
+    const long long tot = (long long)n * n * b * 4;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        long long lj = e / (4LL * b), c = e - lj * 4LL * b;
+        long long w = c >> 2;
+        int sg = (int)((c >> 1) & 1), tu = (int)(c & 1);
+        int l = (int)(lj / n), j = (int)(lj - (long long)l * n);
+        Kin[lj * ldk + c] = rho[w * (long long)M * M + (long long)(2 * l + sg) * M + 2 * j + tu];
+    }
+}
+
+// Gamma_w[2i + sigma][2k + tau] = delta_{sigma tau} J[(i n + k) ldj + w] - K_{sigma tau}[(i, k), w]
+// K from a complex array Kc[(i n + k) ldk + 4 w + st] or from real/imaginary pairs
+// Kr[(i n + k) ldk + 2 (4 w + st) + part].
+__global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, const zc *Kc, const double *Kr,
+                                      long long ldk, zc *Gam) {
+    const int M = 2 * n;
+    const long long tot = (long long)M * M * b;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        long long w = e / ((long long)M * M), rc = e - w * (long long)M * M;
+        int r = (int)(rc / M), c = (int)(rc - (long long)r * M);
+        int i = r >> 1, sg = r & 1, k = c >> 1, tu = c & 1;
+        long long ik = (long long)i * n + k;
+        int st = sg * 2 + tu;
+        zc kv;
+        if (Kc) kv = Kc[ik * ldk + 4 * w + st];
+        else kv = mkz(Kr[ik * ldk + 2 * (4 * w + st)], Kr[ik * ldk + 2 * (4 * w + st) + 1]);
+        zc g = mkz(-kv.x, -kv.y);
+        if (sg == tu) g = g + J[ik * ldj + w];
+        Gam[e] = g;
+    }
+}
+
+inline int grid_for(long long n) {
+    long long g = (n + NT - 1) / NT;
+    if (g > 148LL * 16) g = 148LL * 16;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+int launch_tprime(int Ltot, int N, int b, zc *T, long long ldT, zc *e2part, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    tprime_kernel<<<dim3(Ltot, b), NT, 0, st>>>(Ltot, N, T, ldT, e2part);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    rowsum_kernel<<<nrows, NT, 0, st>>>(ncols, in, out, scale);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_trace_conj(int M, int N, int b, const zc *C, const zc *X, long long ldX, zc *out, double scale,
+                      cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    trace_conj_kernel<<<b, NT, 0, st>>>(M, N, C, X, ldX, out, scale);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
+                    const zc *e2, zc *scal, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    epilogue_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, N, b, HX, G, X, ldX, det, e1, e2, scal);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_accumulate(int nslot, int M, int N, int b, const zc *Wt, long long nomega, long long w0, const int *slotmap,
+                      const zc *G, const zc *R, long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
+                      zc *compR, zc *accHS, zc *compHS, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    accumulate_kernel<<<grid_for((long long)nslot * M * N), NT, 0, st>>>(nslot, M, N, b, Wt, nomega, w0, slotmap, G, R,
+                                                                         ldX, scal, accG, compG, accR, compR, accHS,
+                                                                         compHS);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_fold_comp(long long n, zc *a, const zc *c, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    fold_comp_kernel<<<grid_for(n), NT, 0, st>>>(n, a, c);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_permute_h2(int M, const zc *H2, zc *H2r, cudaStream_t st) {
+    long long tot = (long long)M * M * M * M;
+    ProfScope prof(st, PROF_MEMORY);
+    permute_h2_kernel<<<grid_for(tot), NT, 0, st>>>(M, H2, H2r);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_permute_rows(int M, int N, int nbatch, const int *rowmap, const zc *in, long long ldin, long long bs_in,
+                        zc *out, long long bs_out, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    permute_rows_kernel<<<dim3(grid_for((long long)M * N), nbatch), NT, 0, st>>>(M, N, rowmap, in, ldin, bs_in, out,
+                                                                                 bs_out);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    gather_p_kernel<<<grid_for((long long)n * n * b), NT, 0, st>>>(n, b, rho, P, ldp);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    gather_kin_kernel<<<grid_for((long long)n * n * b * 4), NT, 0, st>>>(n, b, rho, Kin, ldk);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const zc *Kc, const double *Kr, long long ldk,
+                          zc *Gam, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, ldj, Kc, Kr, ldk, Gam);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+}  // namespace phf

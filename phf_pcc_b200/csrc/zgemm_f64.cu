@@ -1,0 +1,186 @@
+// FP64 strided batched complex GEMM: the building block of the plain FP64 form.
+//
+// C[b] = alpha * A[b] * B[b] + beta * C[b] with every operand given as a strided view
+// (row stride, column stride, two batch strides, optional per-batch offsets), so that
+// transposes, conjugate transposes and the column-blocked layouts of the grid-point
+// batches need no copies.  A may be real (real x complex products: Cholesky vectors and
+// the one-electron matrix applied to complex orbitals).
+//
+// Tiling: 64 x 64 output tile per 256-thread CTA, k-step 16, each thread owns a 4 x 4
+// block of complex accumulators (rows ty + 16 i, columns tx + 16 j); the next k-tile is
+// prefetched into registers while the current one is consumed from shared memory.
+#include <type_traits>
+
+#include "phf_common.cuh"
+
+namespace phf {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+template <bool AREAL>
+struct ATile {
+    using T = typename std::conditional<AREAL, double, zc>::type;
+};
+
+__device__ __forceinline__ zc load_z(const View &v, long long off) {
+    if (v.real) return zc{reinterpret_cast<const double *>(v.p)[off], 0.0};
+    zc z = reinterpret_cast<const zc *>(v.p)[off];
+    if (v.conj) z.y = -z.y;
+    return z;
+}
+
+__device__ __forceinline__ double load_d(const View &v, long long off) {
+    return reinterpret_cast<const double *>(v.p)[off];
+}
+
+template <bool AREAL>
+__global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
+                                                   zc beta, OutView C, const long long *__restrict__ offs) {
+    using TA = typename ATile<AREAL>::T;
+    __shared__ TA As[BK][BM + 1];
+    __shared__ zc Bs[BK][BN + 1];
+
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const long long bz = blockIdx.x / ntn;
+    const int tn = blockIdx.x - bz * ntn;
+    const int row0 = blockIdx.y * BM, col0 = tn * BN;
+    const long long b0 = bz % nb0, b1 = bz / nb0;
+    long long oa = b0 * A.bs0 + b1 * A.bs1, ob = b0 * B.bs0 + b1 * B.bs1, oc = b0 * C.bs0 + b1 * C.bs1;
+    if (offs) {
+        oa += offs[3 * bz];
+        ob += offs[3 * bz + 1];
+        oc += offs[3 * bz + 2];
+    }
+    const bool a_mfast = (A.rs == 1);  // element order of the A tile loads
+    const bool b_nfast = (B.cs == 1);
+
+    TA ra[4];
+    zc rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int e = tid + NT * r;
+            int i, kk;
+            if (a_mfast) { i = e & (BM - 1); kk = e >> 6; }
+            else { kk = e & (BK - 1); i = e >> 4; }
+            int gi = row0 + i, gk = k0 + kk;
+            if (gi < m && gk < k) {
+                long long off = oa + (long long)gi * A.rs + (long long)gk * A.cs;
+                if constexpr (AREAL) ra[r] = load_d(A, off);
+                else ra[r] = load_z(A, off);
+            } else {
+                if constexpr (AREAL) ra[r] = 0.0;
+                else ra[r] = zc{0.0, 0.0};
+            }
+            int j;
+            if (b_nfast) { j = e & (BN - 1); kk = e >> 6; }
+            else { kk = e & (BK - 1); j = e >> 4; }
+            int gj = col0 + j;
+            gk = k0 + kk;
+            rb[r] = (gj < n && gk < k) ? load_z(B, ob + (long long)gk * B.rs + (long long)gj * B.cs) : zc{0.0, 0.0};
+        }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int e = tid + NT * r;
+            int i, kk;
+            if (a_mfast) { i = e & (BM - 1); kk = e >> 6; }
+            else { kk = e & (BK - 1); i = e >> 4; }
+            As[kk][i] = ra[r];
+            int j;
+            if (b_nfast) { j = e & (BN - 1); kk = e >> 6; }
+            else { kk = e & (BK - 1); j = e >> 4; }
+            Bs[kk][j] = rb[r];
+        }
+    };
+
+    double accr[4][4], acci[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) accr[i][j] = acci[i][j] = 0.0;
+
+    fetch(0);
+    for (int k0 = 0; k0 < k; k0 += BK) {
+        __syncthreads();
+        stash();
+        __syncthreads();
+        if (k0 + BK < k) fetch(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            TA a[4];
+            zc b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if constexpr (AREAL) {
+                        accr[i][j] = fma(a[i], b[j].x, accr[i][j]);
+                        acci[i][j] = fma(a[i], b[j].y, acci[i][j]);
+                    } else {
+                        accr[i][j] = fma(a[i].x, b[j].x, accr[i][j]);
+                        accr[i][j] = fma(-a[i].y, b[j].y, accr[i][j]);
+                        acci[i][j] = fma(a[i].x, b[j].y, acci[i][j]);
+                        acci[i][j] = fma(a[i].y, b[j].x, acci[i][j]);
+                    }
+                }
+        }
+    }
+    const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        int gi = row0 + ty + 16 * i;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int gj = col0 + tx + 16 * j;
+            if (gj >= n) continue;
+            long long off = oc + (long long)gi * C.rs + (long long)gj * C.cs;
+            zc v = alpha * zc{accr[i][j], acci[i][j]};
+            if (C.real) {
+                double *cp = reinterpret_cast<double *>(C.p);
+                cp[off] = use_beta ? v.x + beta.x * cp[off] : v.x;
+            } else {
+                if (use_beta) v = v + beta * C.p[off];
+                C.p[off] = v;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
+                  const OutView &C, const long long *offs, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || nb0 <= 0 || nb1 <= 0) return PHF_OK;
+    if (k <= 0) {
+        set_error(PHF_ERR_ARG, "zgemm_strided: k <= 0");
+        return PHF_ERR_ARG;
+    }
+    const int ntn = (n + BN - 1) / BN, ntm = (m + BM - 1) / BM;
+    const long long nbatch = (long long)nb0 * nb1;
+    const long long gx = nbatch * ntn;
+    if (gx > 2147483647LL || ntm > 65535) {
+        set_error(PHF_ERR_ARG, "zgemm_strided: grid too large");
+        return PHF_ERR_ARG;
+    }
+    dim3 grid((unsigned)gx, (unsigned)ntm, 1);
+    ProfScope prof(st, -1);
+    if (A.real)
+        zgemm_kernel<true><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+    else
+        zgemm_kernel<false><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+}  // namespace phf

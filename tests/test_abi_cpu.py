@@ -1,0 +1,62 @@
+"""The C ABI library without a GPU: it loads, exports every declared symbol, and fails loudly."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from phf_pcc_b200 import _lib, api
+from phf_pcc_b200.PHFTools_F import phftools
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"\b(phf_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert "phf_buildhsg" in names and "phf_localg" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    # the ctypes signature table covers every declared entry point
+    assert set(names) <= set(_lib.SIGNATURES)
+
+
+def test_version_and_status_strings():
+    lib = _lib.load()
+    assert lib.phf_version().startswith(b"phf_b200")
+    assert lib.phf_status_string(_lib.PHF_ERR_SINGULAR) == b"singular rotated overlap"
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device error path")
+def test_no_device_raises_instead_of_cpu_fallback():
+    with pytest.raises(_lib.PHFError) as ei:
+        api.localg(np.zeros((1, 1, 4, 4)), np.zeros((1, 1, 4, 4)), np.ones((1, 1)), 1.0, [1.0], [1.0], [1.0], 1)
+    assert ei.value.status == _lib.PHF_ERR_NO_DEVICE
+
+
+def test_shim_checks_shapes_before_calling_the_library():
+    M, N = 6, 2
+    eye = np.eye(M, dtype=complex)[None]
+    with pytest.raises(ValueError):
+        phftools.buildhsg(np.eye(M), np.zeros((M, M, M, M)), np.eye(M), np.zeros((M - N, N)), [1, 1], 1, 1, 1, N,
+                          eye, eye, eye, np.ones((1, 2)), np.ones((1, 1, 1)), [0.0], [0.0], [0.0], 0, 1, 0)
+    with pytest.raises(ValueError):  # wrong z shape
+        phftools.buildhsg(np.eye(M), np.zeros((M, M, M, M)), np.eye(M), np.zeros((M, N)), [1, 1], 1, 1, 1, N,
+                          eye, eye, eye, np.ones((1, 1)), np.ones((1, 1, 1)), [0.0], [0.0], [0.0], 0, 1, 0)

@@ -1,0 +1,79 @@
+"""The int8-sliced tensor-core GEMM (phf_ozaki_dgemm) against FP64 products, and the
+energy/gradient pipeline in that precision against the golden vectors.
+
+Tolerances: with S slices an entry's error is below about (S+1) k 2^{-7(S+1)} max|A_i.| max|B_.j|;
+the test bound is 2^{-7(S+1)} k (S+1) * 4 in those units.  Pipeline: |dE| <= 1e-9 Eh relative
+to FP64, gradient elements <= 1e-8 (the benchmark target is 1e-8 Eh and 1e-7).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from phf_pcc_b200 import _lib, api
+from tests._golden import CASES, grid_kwargs, load
+
+pytestmark = pytest.mark.gpu
+
+
+def _dgemm(A, Bt, S):
+    import torch
+
+    dA = torch.from_numpy(np.ascontiguousarray(A)).cuda()
+    dB = torch.from_numpy(np.ascontiguousarray(Bt)).cuda()
+    m, k = A.shape
+    n = Bt.shape[0]
+    dD = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+    st = _lib.load().phf_ozaki_dgemm(m, n, k, S, ctypes.c_void_p(dA.data_ptr()), k, ctypes.c_void_p(dB.data_ptr()),
+                                     k, ctypes.c_void_p(dD.data_ptr()), n, ctypes.c_void_p(0))
+    _lib.check(st, "phf_ozaki_dgemm")
+    return dD.cpu().numpy()
+
+
+def _bound_units(A, Bt):
+    return np.abs(A).max(axis=1)[:, None] * np.abs(Bt).max(axis=1)[None, :]
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 64, 64), (200, 150, 333), (256, 192, 1000), (64, 40, 17)])
+@pytest.mark.parametrize("S", [6, 3])
+def test_ozaki_dgemm_matches_fp64(m, n, k, S):
+    rng = np.random.default_rng(m * 7 + n * 3 + k + S)
+    A = rng.normal(size=(m, k)) * 10.0 ** rng.uniform(-3, 3, size=(m, 1))
+    Bt = rng.normal(size=(n, k)) * 10.0 ** rng.uniform(-3, 3, size=(n, 1))
+    D = _dgemm(A, Bt, S)
+    ref = A @ Bt.T
+    err = np.abs(D - ref) / _bound_units(A, Bt)
+    assert err.max() <= 4.0 * (S + 1) * k * 2.0 ** (-7 * (S + 1)), err.max()
+    if S == 3:  # the truncation is really there: 3 slices are far from FP64
+        assert err.max() > 1e-12
+
+
+def test_ozaki_dgemm_long_k_splits_into_exact_passes():
+    rng = np.random.default_rng(5)
+    A = rng.normal(size=(128, 30000))
+    Bt = rng.normal(size=(64, 30000))
+    D = _dgemm(A, Bt, 6)
+    err = np.abs(D - A @ Bt.T) / _bound_units(A, Bt)
+    assert err.max() <= 4.0 * 7 * 30000 * 2.0 ** -49
+
+
+def _api_kwargs(c):
+    k = grid_kwargs(c)
+    return dict(ngrid=k["ngrid"], nci=k["nci"], cmplxconj=k["CmplxConj"], ncisp=k["ncisp"], nocc=k["NOcc"],
+                r1=k["R1"], r2=k["R2"], rpg=k["Rpg"], weightsp=k["weightsp"], weightpg=k["weightpg"],
+                roota=k["roota"], rootb=k["rootb"], rooty=k["rooty"], qj=k["QJ"], sp=k["SP"])
+
+
+def _close(a, b, rel):
+    return float(np.abs(a - b).max()) <= rel * max(1.0, float(np.abs(b).max()))
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("form,precision", [("factorized", "fp64"), ("eri", "fp64"), ("eri", "ozaki_i8")])
+def test_forms_and_precisions_match_golden(name, form, precision):
+    c = load(name)
+    rel = 1e-10 if precision == "fp64" else 1e-9
+    with api.Plan(ref=c["Ref"], h=c["h"], B=c["B"], jk_form=form, precision=precision, **_api_kwargs(c)) as plan:
+        out = plan.buildhsg(c["Z"], check_hermitian=False)
+    for x, key in zip(out, ("Hmat", "Smat", "Gradmat", "Rdmmat")):
+        assert _close(x, c[key], rel), (key, float(np.abs(x - c[key]).max()))

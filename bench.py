@@ -114,11 +114,25 @@ def api_kwargs(p):
                 roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
 
 
-def jk_flops_per_point(p):
-    """Algorithmic real flops of the Cholesky J/K contraction per grid point (executed form):
-    T = V^H X (8 L N^2 M), Q = X T' (8 L N^2 M), GX = sum_L B_L Q_L (8 L n^2 N)."""
+def jk_form_of(p):
+    return "eri" if p.n <= 128 else "factorized"
+
+
+def jk_flops_per_point(p, form):
+    """Algorithmic real flops of the exchange/Coulomb contraction kernels per grid point.
+
+    eri form:        K = EK (n^2 x n^2, real) times 4 complex density columns: 16 n^4
+    factorized form: T = V^H X (8 L N^2 M), Q = X T' (8 L N^2 M), GX = sum_L B_L Q_L (8 L n^2 N)"""
     n, N, M, L = p.n, p.N, p.M, p.L
+    if form == "eri":
+        return 16.0 * n ** 4
     return 8.0 * L * N * N * M * 2 + 8.0 * L * n * n * N
+
+
+def int8_ops_per_point(p, slices):
+    """Executed int8 tensor-core operations per grid point in the eri form: S(S+1)/2 slice
+    products of the (n^2 x n^2) x (n^2 x 8) real GEMM, 2 ops per multiply-add."""
+    return slices * (slices + 1) / 2 * 2.0 * p.n ** 4 * 8
 
 
 def survey_flops_per_point(p):
@@ -126,6 +140,26 @@ def survey_flops_per_point(p):
     16 M^2 N + 16 M N^2 + 8 N^3 + 16 M^3 (small algebra)."""
     n, N, M, L = p.n, p.N, p.M, p.L
     return 32.0 * L * n ** 3 + 8.0 * L * n ** 2 + 16.0 * M * M * N + 16.0 * M * N * N + 8.0 * N ** 3 + 16.0 * M ** 3
+
+
+def measure_int8_peak(torch, dev):
+    """cuBLASLt int8 GEMM throughput (TOP/s, 8192^3, best of 5), or None if unavailable."""
+    try:
+        a = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=dev).t()
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            e.synchronize()
+            best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+        return best
+    except Exception:
+        return None
 
 
 def measure_fp64_peak(torch, dev):
@@ -207,6 +241,36 @@ def workload_name(p):
             f"({'C2v' if g.npg == 4 else 'no PG'}), FP64-accurate E+grad")
 
 
+def time_plan(torch, plan, C, stream, steps, warmup, flush, lib, sampler=None):
+    """Device time (ms) per energy+gradient step, with the per-class event profile."""
+    from phf_pcc_b200.autograd import energy_and_gradient
+
+    for _ in range(warmup):
+        E, G = energy_and_gradient(C, plan)
+    torch.cuda.synchronize()
+    launches0 = lib.kernel_launches()
+    lib.profile_enable(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if sampler:
+        sampler.__enter__()
+    try:
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.zero_()                        # L2 flush between timed steps (not timed)
+            ev[i][0].record(stream)
+            E, G = energy_and_gradient(C, plan)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    finally:
+        if sampler:
+            sampler.__exit__(None, None, None)
+    launches = lib.kernel_launches() - launches0
+    prof = {c: lib.profile_read(c) for c in range(4)}
+    lib.profile_enable(False)
+    step_ms = sum(s.elapsed_time(e) for s, e in ev) / steps
+    return step_ms, E, G, launches, prof
+
+
 def run_ours(args):
     import torch
 
@@ -227,44 +291,34 @@ def run_ours(args):
     p = problem_for(args.config, seed=1000 + rank)
     Ref, Z = p.ref_and_z()
     kw = api_kwargs(p)
-    plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, **kw)
+    form = jk_form_of(p)
     C = torch.from_numpy(p.C).to(dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
 
-    def step():
-        hs, yg, yr = plan.eval_device(C, stream=stream)
-        S = hs[0, 1]
-        E = hs[0, 0].real / S.real.abs()
-        G = (yg[0] - E * yr[0]) / S
-        return E, G
-
-    for _ in range(args.warmup):
-        E, G = step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    launches0 = _lib.kernel_launches()
-    _lib.profile_enable(True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        for i in range(args.steps):
-            flush.zero_()                       # L2 flush between timed steps (not timed)
-            ev[i][0].record(stream)
-            E, G = step()
-            ev[i][1].record(stream)
-        torch.cuda.synchronize()
-    launches = _lib.kernel_launches() - launches0
-    jk_ms, jk_n = _lib.profile_read(_lib.PROF_JK)
-    all_ms = sum(_lib.profile_read(c)[0] for c in range(4))
-    _lib.profile_enable(False)
-    step_ms = sum(s.elapsed_time(e) for s, e in ev) / args.steps
+    plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, **kw)
+    clk = ClockSampler(local)
+    step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
+    slices = args.slices or 6
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     step_ms = float(t.item())
     value = world * p.grid.npoints / (step_ms * 1e-3)
+    chunk = plan.chunk
+    plan.close()
+
+    # the plain FP64 form on the same problem (comparison and error reference)
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64:
+        plan64 = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="fp64", **kw)
+        ms64, E64, G64, _, prof64 = time_plan(torch, plan64, C, stream, max(1, min(args.steps, 3)), 1, flush, _lib)
+        plan64.close()
+        dE = abs(E.item() - E64.item())
+        dG = float((G - G64).abs().max().item())
+        fp64 = {"value": p.grid.npoints / (ms64 * 1e-3), "ms_per_step": ms64, "energy": E64.item(),
+                "abs_dE_vs_fp64": dE, "max_abs_dgrad_vs_fp64": dG, "speedup": ms64 / step_ms,
+                "meets_1e-8_Eh": dE <= 1e-8}
 
     # end-to-end through the C ABI with host buffers (one-shot drop-in call per step)
     e2e_vals = []
@@ -274,7 +328,7 @@ def run_ours(args):
         for i in range(1 + args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            out = api.buildhsg_chol(p.h, p.B, Ref, z0, check_hermitian=False, **kw)
+            out = api.buildhsg_chol(p.h, p.B, Ref, z0, precision=args.precision, check_hermitian=False, **kw)
             t1 = time.perf_counter()
             if i > 0:
                 e2e_vals.append(p.grid.npoints / (t1 - t0))
@@ -283,46 +337,55 @@ def run_ours(args):
         d2h = sum(x.nbytes for x in out)
     e2e_val = statistics.median(e2e_vals) * world if e2e_vals else None
 
-    line = None
     if rank == 0:
         peaks = _peaks()
-        fp64_peak = measure_fp64_peak(torch, dev) if args.precision == "fp64" else None
-        flops_pt = jk_flops_per_point(p)
-        # J/K kernels: achieved = algorithmic J/K flops of the timed steps / their summed device time
-        jk_flops_total = flops_pt * p.grid.npoints * args.steps
-        achieved = jk_flops_total / (jk_ms * 1e-3) / 1e12 if jk_ms > 0 else None
+        jk_ms, jk_n = prof[0]
+        all_ms = sum(v[0] for v in prof.values())
+        pts = p.grid.npoints * args.steps
+        alg = jk_flops_per_point(p, form)
+        fp64_peak = measure_fp64_peak(torch, dev)
         if args.precision == "fp64":
+            achieved = alg * pts / (jk_ms * 1e-3) / 1e12
             roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                    "frac": (achieved / fp64_peak) if achieved and fp64_peak else None, "traffic": None,
-                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
-                    "kernel": "zgemm_kernel (J/K contraction GEMMs)", "jk_share_of_device_time": jk_ms / all_ms,
-                    "jk_launches": jk_n}
+                    "frac": achieved / fp64_peak, "traffic": None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                    "kernel": "zgemm_kernel<true> (exchange GEMM)"}
         else:
-            peak = peaks.get("bf16_tflops")
-            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": (achieved / peak) if achieved and peak else None, "traffic": None,
-                    "kernel": "J/K contraction", "jk_share_of_device_time": jk_ms / all_ms, "jk_launches": jk_n}
-        roof["flops_per_point"] = flops_pt
-        roof["survey_flops_per_point"] = survey_flops_per_point(p)
+            i8 = measure_int8_peak(torch, dev)
+            bf16 = peaks.get("bf16_tflops")
+            peak = i8 if i8 else 2.0 * bf16
+            achieved = int8_ops_per_point(p, slices) * pts / (jk_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": ("cuBLASLt int8 GEMM 8192^3 measured in this run" if i8 else
+                                    "2 x measured bf16 burst (MEASURED_PEAKS.json)"),
+                    "bf16_tflops_measured": bf16,
+                    "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::i8, exchange GEMM)",
+                    "fp64_equivalent_tflops": alg * pts / (jk_ms * 1e-3) / 1e12,
+                    "fp64_dgemm_peak_tflops": fp64_peak}
+        roof.update({"jk_form": form, "jk_launches": jk_n, "jk_ms_per_step": jk_ms / args.steps,
+                     "jk_share_of_device_time": jk_ms / all_ms if all_ms else None,
+                     "device_ms_by_class": {k: v[0] / args.steps for k, v in
+                                            zip(("jk", "other_gemm", "overlap_inverse", "memory"), prof.values())},
+                     "alg_flops_per_point": alg, "survey_flops_per_point": survey_flops_per_point(p)})
         cpu = None
         if not args.no_cpu:
             v, nth, desc = cpu_sample(p, seconds_target=args.cpu_seconds)
             cpu = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc}
+        dtype = "f64" if args.precision == "fp64" else f"int8 x{slices} slices (FP64-accurate emulation) + f64"
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision,
-                "data": "synthetic (seeded h, B_L, determinant)",
-                "config": {"workload": workload_name(p), "precision": args.precision,
-                           "points_per_step": p.grid.npoints, "chunk": plan.chunk,
+                "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded h, B_L, determinant)",
+                "config": {"workload": workload_name(p), "precision": args.precision, "jk_form": form,
+                           "points_per_step": p.grid.npoints, "chunk": chunk,
                            "l2": "flushed (256 MB write) between timed steps",
-                           "parallelism": f"{world} independent instances, one per GPU"},
-                "energy": float(E.item()),
+                           "parallelism": f"{world} independent instance(s), one per GPU"},
+                "energy": float(E.item()), "fp64_gpu": fp64,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "path": "phf_buildhsg_chol (C ABI, host buffers)"},
                 "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    plan.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -336,7 +399,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki_i8", "bf16x3", "tf32"])
+    ap.add_argument("--precision", default="ozaki_i8", choices=["fp64", "ozaki_i8"])
+    ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")

@@ -8,7 +8,9 @@
 // where every A_t B_u is an exact int8 x int8 -> int32 product on the tensor cores, the
 // products of one group g share one int32 accumulator (exact while (g-1) k 127^2 < 2^31),
 // and the S group sums are combined in FP64 in the epilogue.  Terms with t + u > S + 1 are
-// dropped; the error of an entry is below about (S+1) k 2^{-7(S+1)} max|A_i.| max|B_.j|.
+// dropped; since a slice is an integer up to 127 ~ 2^7 (times 2^{-7t}), the dropped terms and
+// the slicing remainder are of order 2^{-7S}: an entry's error is below about
+// (S+1) k 2^{-7S} max|A_i.| max|B_.j| (random-sign errors grow like sqrt(k) in practice).
 // (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
 // fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
 //

@@ -1,0 +1,85 @@
+"""The differentiable projected energy: values against the golden vectors, gradient against
+central finite differences (h = 1e-5) and against the reference's own gradient (LocalG)."""
+import numpy as np
+import pytest
+
+from phf_pcc_b200 import api, synth
+from phf_pcc_b200.autograd import energy_and_gradient, projected_energy
+from tests._golden import grid_kwargs, load
+
+pytestmark = pytest.mark.gpu
+
+
+def _plan_kwargs_from_grid(kw, nocc):
+    return dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=nocc,
+                r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+                roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "ozaki_i8"])
+def test_energy_and_gradient_match_reference_golden(precision):
+    import torch
+
+    c = load("c1")
+    M, N = int(c["M"]), int(c["N"])
+    C = c["Ref"] @ np.vstack([np.eye(N), c["Z"]])
+    with api.Plan(ref=np.eye(M), h=c["h"], B=c["B"], precision=precision,
+                  **_plan_kwargs_from_grid(grid_kwargs(c), N)) as plan:
+        Ct = torch.from_numpy(C).cuda().requires_grad_(True)
+        E = projected_energy(Ct, plan)
+        E.backward()
+        g = Ct.grad.cpu().numpy() / 2.0          # dE/dC*
+    assert abs(E.item() - c["E0"]) <= 1e-9
+    Gz = (c["Ref"].conj().T @ g)[N:, :]           # dE/dZ* in the Ref-MO basis
+    assert np.abs(Gz - c["G"]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "ozaki_i8"])
+def test_gradient_matches_central_finite_differences(precision):
+    import torch
+
+    p = synth.make_problem(16, 8, 40, ngrid=(14, 8), seed=21, pg="C2v")
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=precision,
+                  **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
+        C = torch.from_numpy(p.C).cuda()
+        E0, G = energy_and_gradient(C, plan)
+        grad = 2.0 * G
+        rng = np.random.default_rng(3)
+        for _ in range(3):
+            d = rng.normal(size=C.shape) + 1j * rng.normal(size=C.shape)
+            d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
+            h = 1e-5
+            ep, _ = energy_and_gradient(C + h * d, plan)
+            em, _ = energy_and_gradient(C - h * d, plan)
+            fd = (ep - em).item() / (2 * h)
+            an = torch.real(torch.sum(torch.conj(grad) * d)).item()
+            assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
+
+
+def test_recompute_mode_equals_fused_mode():
+    import torch
+
+    p = synth.make_problem(12, 6, 30, ngrid=(14, 4), seed=4)
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
+        grads = []
+        for mode in ("fused", "recompute"):
+            C = torch.from_numpy(p.C).cuda().requires_grad_(True)
+            projected_energy(C, plan, mode).backward()
+            grads.append(C.grad.clone())
+    assert torch.equal(grads[0], grads[1])
+
+
+def test_energy_invariant_under_occupied_rotation_at_config2_size():
+    """Size-independent property at the benchmark size: E(C U) = E(C) for unitary U (N x N)."""
+    import torch
+
+    p = synth.config_problem("c2", seed=7)
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="ozaki_i8",
+                  **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
+        C = torch.from_numpy(p.C).cuda()
+        U = torch.from_numpy(synth.random_unitary(p.N, np.random.default_rng(1))).cuda()
+        E1, G1 = energy_and_gradient(C, plan)
+        E2, G2 = energy_and_gradient(C @ U, plan)
+    assert abs(E1.item() - E2.item()) <= 1e-9 * abs(E1.item())
+    # the gradient transforms covariantly: G(C U) = G(C) U
+    assert torch.allclose(G2, G1 @ U, rtol=0, atol=1e-9 * float(G1.abs().max()))

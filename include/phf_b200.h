@@ -142,6 +142,23 @@ int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes);
 int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
                     long long ldb, double *dD, long long ldd, void *stream);
 
+/* The same product as phf_ozaki_dgemm for callers that cannot allocate device memory at the
+ * point of the call: code that runs while another component is capturing a CUDA graph,
+ * programs whose device memory is owned by another allocator (a framework's caching pool, a
+ * fixed arena reserved at start-up), and loops that must never enter the driver's allocator.
+ * No counterpart in the reference.  Scratch (int8 slices, exponents, error flag) lives in one
+ * static device array of 32 MiB that every GPU loading this library holds until exit; sizes
+ * needing more (see phf_ozaki_dgemm_noalloc_scratch_bytes) return PHF_ERR_UNSUPPORTED.  No
+ * cudaMalloc/cudaFree or allocating library call is made.  All calls share the array and it
+ * keeps the last call's contents (the parts that must start at zero are cleared on each call):
+ * calls that overlap on the GPU race.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current); make that first call before any
+ * stream capture.  Synchronous on `stream`. */
+int phf_ozaki_dgemm_noalloc(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
+                            long long ldb, double *dD, long long ldd, void *stream);
+/* Scratch bytes phf_ozaki_dgemm_noalloc needs for these sizes. */
+size_t phf_ozaki_dgemm_noalloc_scratch_bytes(int m, int n, int k, int slices);
+
 /* ---------------------------------------------------------------- diagnostics */
 const char *phf_status_string(int status);
 /* Message of the last failing call on this thread ("" when none). */

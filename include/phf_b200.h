@@ -111,6 +111,13 @@ typedef struct {
     int jk_form;                              /* Cholesky form only: 0 = automatic, 1 = exchange through the
                                                  spatial ERI matrix (n^2 x n^2, built once per plan),
                                                  2 = factorized (no n^4 tensor); automatic picks 1 for n <= 128 */
+    int gradient_mode;                        /* phf_plan_eval_device only: 0 = the reference's gradient
+                                                 (bra-side derivative, Gradient/LocalG of PHFTools.f90);
+                                                 1 = exact dE/dC* of E = Re H/|Re S|, adding the ket-side
+                                                 term (spatial-ERI form, nci == 1) */
+    int fp64_library_gemm;                    /* PHF_PREC_FP64, spatial-ERI form: 1 = run the exchange GEMM
+                                                 with cuBLAS DGEMM instead of this library's FP64 kernel
+                                                 (a library-tuned FP64 comparison form) */
 } phf_plan_desc;
 
 int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);
@@ -127,7 +134,11 @@ int phf_plan_buildhsg(phf_plan *plan, const phf_complex *z, phf_complex *hmat, p
  *   d_yg[a*M*N + r*N + j]    -- sum_w W_a(w) N_w [(1 - rho_w) F_w X_w + h_w X_w]
  *   d_yr[a*M*N + r*N + j]    -- sum_w W_a(w) N_w X_w,   X_w = R_w C (C^H R_w C)^-1
  * so that Gradmat_a = Yg_a C^H, Rdmmat_a = Yr_a C^H, and for nci == 1 the energy is
- * E = Re H / |Re S| and dE/dC* = (Yg - E Yr) / S.  cmplxconj must be 0 or 1. */
+ * E = Re H / |Re S| and the reference's gradient is (Yg - E Yr) / S.  With gradient_mode 1 the
+ * outputs are the symmetrised sums Yg = (Yg_bra + Yg_ket)/2, Yr = (Yr_bra + Yr_ket)/2, where
+ * Yg_ket = sum_w conj(W_a(w) N_w) R_w^H [(H1 + Gamma_w^H) C - C W_w^H + conj(h_w) C] S_w^-H and
+ * Yr_ket = sum_w conj(W_a(w) N_w) R_w^H C S_w^-H, and dE/dC* = (Yg - E sgn(Re S) Yr) / |Re S|
+ * exactly.  cmplxconj must be 0 or 1. */
 int phf_plan_eval_device(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
                          phf_complex *d_yr, void *stream);
 

@@ -42,6 +42,8 @@ class phf_plan_desc(ctypes.Structure):
         ("precision", ctypes.c_int), ("slices", ctypes.c_int),
         ("workspace_bytes", ctypes.c_size_t),
         ("jk_form", ctypes.c_int),
+        ("gradient_mode", ctypes.c_int),
+        ("fp64_library_gemm", ctypes.c_int),
     ]
 
 

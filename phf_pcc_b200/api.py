@@ -168,11 +168,14 @@ class Plan:
     Cholesky form: pass ``h`` (n, n) and ``B`` (L, n, n); dense form: ``hone`` and
     ``htwo``.  Grid arguments as buildhsg.  ``precision``: "fp64" or "ozaki_i8" (FP64-accurate
     int8 tensor-core slices, ``slices`` per operand, default 6); ``jk_form``: "auto", "eri"
-    (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"."""
+    (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"; ``gradient``: "reference"
+    (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the ket-side term;
+    used by autograd)."""
 
     def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
                  rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
-                 workspace_bytes=0, jk_form="auto", npg=None, ncipg=None, nso=None):
+                 workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False, npg=None,
+                 ncipg=None, nso=None):
         self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
                         sp, npg, ncipg, nso)
         g = self._g
@@ -195,6 +198,9 @@ class Plan:
         d.slices = int(slices)
         d.workspace_bytes = int(workspace_bytes)
         d.jk_form = {"auto": 0, "eri": 1, "factorized": 2}[jk_form]
+        d.gradient_mode = {"reference": 0, "exact": 1}[gradient]
+        d.fp64_library_gemm = 1 if fp64_library_gemm else 0
+        self.gradient = gradient
         self.precision = precision
         handle = ctypes.c_void_p()
         lib = _lib.load()

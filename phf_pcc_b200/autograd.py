@@ -13,6 +13,11 @@ Fock matrix).  Nothing per grid point is stored between forward and backward: th
 state is two M x N matrices.  ``mode="recompute"`` keeps only C from the forward and
 re-runs the pass in backward (for callers that evaluate many energies and few gradients).
 
+The reference's gradient is the derivative through C^H (the bra) only; it equals dE/dC*
+when the grid sum is exactly Hermitian.  A plan created with gradient="exact" also accumulates
+the derivative through R C (the ket) and returns the exact dE/dC* for any grid; that is the
+gradient finite differences see.
+
 PyTorch's gradient of a real function of complex C is 2 dE/dC* (conjugate Wirtinger
 convention), which is what ``backward`` returns.
 """
@@ -26,12 +31,19 @@ from .api import Plan
 __all__ = ["ProjectedEnergy", "projected_energy", "energy_and_gradient"]
 
 
-def _combine(hs, yg, yr, nci, ncisp, ncipg, tol=1e-6):
-    """Energy and dE/dC* from the slot accumulators (EigenSolver + VecDecomp + LocalG)."""
+def _combine(hs, yg, yr, nci, ncisp, ncipg, tol=1e-6, exact=False):
+    """Energy and dE/dC* from the slot accumulators (EigenSolver + VecDecomp + LocalG).
+
+    With ``exact`` the accumulators are the symmetrised bra+ket sums of a plan created with
+    gradient="exact" and the result is the exact derivative of E = Re H / |Re S|."""
     if nci == 1:
         H, S = hs[0, 0], hs[0, 1]
-        E = H.real / S.real.abs()
-        G = (yg[0] - E * yr[0]) / S
+        s = S.real.abs()
+        E = H.real / s
+        if exact:
+            G = (yg[0] - E * torch.sign(S.real) * yr[0]) / s
+        else:
+            G = (yg[0] - E * yr[0]) / S
         return E, G
     # several channels: the small generalized eigenproblem on the host (nci x nci)
     Hm = hs[:, 0].reshape(nci, nci).T.cpu().numpy()   # slot a = m + nci n
@@ -62,7 +74,7 @@ class ProjectedEnergy(torch.autograd.Function):
     @staticmethod
     def forward(ctx, C, plan, mode="fused"):
         hs, yg, yr = plan.eval_device(C.detach())
-        E, G = _combine(hs, yg, yr, plan.nci, plan._g.ncisp, plan._g.ncipg)
+        E, G = _combine(hs, yg, yr, plan.nci, plan._g.ncisp, plan._g.ncipg, exact=plan.gradient == "exact")
         ctx.plan = plan
         ctx.mode = mode
         if mode == "fused":
@@ -78,7 +90,8 @@ class ProjectedEnergy(torch.autograd.Function):
             G = saved
         else:
             hs, yg, yr = ctx.plan.eval_device(saved)
-            _, G = _combine(hs, yg, yr, ctx.plan.nci, ctx.plan._g.ncisp, ctx.plan._g.ncipg)
+            _, G = _combine(hs, yg, yr, ctx.plan.nci, ctx.plan._g.ncisp, ctx.plan._g.ncipg,
+                            exact=ctx.plan.gradient == "exact")
         return 2.0 * gE * G, None, None
 
 
@@ -90,4 +103,4 @@ def projected_energy(C: torch.Tensor, plan: Plan, mode: str = "fused") -> torch.
 def energy_and_gradient(C: torch.Tensor, plan: Plan):
     """(E, dE/dC*) for a device-resident C, one pass of the pipeline."""
     hs, yg, yr = plan.eval_device(C)
-    return _combine(hs, yg, yr, plan.nci, plan._g.ncisp, plan._g.ncipg)
+    return _combine(hs, yg, yr, plan.nci, plan._g.ncisp, plan._g.ncipg, exact=plan.gradient == "exact")

@@ -32,7 +32,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB] + sources()
+    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB] + sources() + ["-lcublas"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -110,7 +110,7 @@ int phf_buildhsg(const phf_complex *hone, const phf_complex *htwo, const phf_com
     int st = phf::plan_create(&d, &plan);
     if (st != PHF_OK) return st;
     st = phf::plan_buildhsg(plan->impl, z, hmat, smat, gradmat, rdmmat);
-    delete plan;
+    phf_plan_destroy(plan);
     return st;
 }
 
@@ -136,7 +136,7 @@ int phf_buildhsg_chol(const double *h, const double *bvec, int nchol, const phf_
     int st = phf::plan_create(&d, &plan);
     if (st != PHF_OK) return st;
     st = phf::plan_buildhsg(plan->impl, z, hmat, smat, gradmat, rdmmat);
-    delete plan;
+    phf_plan_destroy(plan);
     return st;
 }
 
@@ -243,7 +243,7 @@ int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan) {
 }
 
 int phf_plan_destroy(phf_plan *plan) {
-    delete plan;
+    delete plan;  // ~PlanImpl releases the device memory and library handles
     return PHF_OK;
 }
 

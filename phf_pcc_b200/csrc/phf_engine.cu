@@ -31,6 +31,8 @@
 #include <string>
 #include <vector>
 
+#include <cublas_v2.h>
+
 #include "phf_common.cuh"
 #include "phf_internal.h"
 
@@ -223,6 +225,14 @@ int validate(const phf_plan_desc *d) {
         set_error(PHF_ERR_UNSUPPORTED, "tensor-core precisions are implemented for the Cholesky form");
         return PHF_ERR_UNSUPPORTED;
     }
+    if (d->gradient_mode < 0 || d->gradient_mode > 1) {
+        set_error(PHF_ERR_ARG, "gradient_mode must be 0 or 1");
+        return PHF_ERR_ARG;
+    }
+    if (d->gradient_mode == 1 && (d->nchol <= 0 || d->jk_form == 2 || d->nci != 1 || d->cmplxconj == 2)) {
+        set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs the spatial-ERI form, nci == 1 and cmplxconj 0/1");
+        return PHF_ERR_UNSUPPORTED;
+    }
     if (d->jk_form < 0 || d->jk_form > 2) {
         set_error(PHF_ERR_ARG, "jk_form must be 0, 1 or 2");
         return PHF_ERR_ARG;
@@ -250,6 +260,20 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.prec = d->precision;
     p.slices = d->slices > 0 ? d->slices : 6;
     if (p.chol) p.eri = (d->jk_form == 1) || (d->jk_form == 0 && d->nso / 2 <= 128);
+    p.exact = d->gradient_mode == 1;
+    p.library_gemm = (d->fp64_library_gemm != 0) && p.eri && p.prec == PHF_PREC_FP64;
+    if (p.library_gemm) {
+        cublasHandle_t h = nullptr;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) {
+            set_error(PHF_ERR_CUDA, "cublasCreate failed");
+            return PHF_ERR_CUDA;
+        }
+        p.cublas = h;
+    }
+    if (p.exact && !p.eri) {
+        set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs the spatial-ERI exchange form (n <= 128 or jk_form 1)");
+        return PHF_ERR_UNSUPPORTED;
+    }
     if (p.prec == PHF_PREC_OZAKI_I8 && !p.eri) {
         set_error(PHF_ERR_UNSUPPORTED, "the int8 tensor-core path needs the spatial-ERI exchange form (jk_form 0/1)");
         return PHF_ERR_UNSUPPORTED;
@@ -366,11 +390,22 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         for (int w = 0; w < nw; ++w) {
             int il = w / (p.ny * p.npg), rem = w % (p.ny * p.npg);
             offs[3 * w] = (long long)il * MM;
-            offs[3 * w + 1] = (long long)rem * M * N;
+            offs[3 * w + 1] = (long long)rem * N;  // column block of T2 (M x ny npg N)
             offs[3 * w + 2] = 0;
         }
         PHF_TRY(p.arena.alloc(&p.offs, offs.size()));
         PHF_CUDA(cudaMemcpy(p.offs, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        if (d->gradient_mode == 1) {  // R1[il]^H, R2[iy]^H, Rpg[ig]^H per point
+            std::vector<long long> ok(9 * (size_t)nw, 0);
+            for (int w = 0; w < nw; ++w) {
+                const int il = w / (p.ny * p.npg), iy = (w / p.npg) % p.ny, ig = w % p.npg;
+                ok[3 * ((size_t)0 * nw + w)] = (long long)il * MM;
+                ok[3 * ((size_t)1 * nw + w)] = (long long)iy * MM;
+                ok[3 * ((size_t)2 * nw + w)] = (long long)ig * MM;
+            }
+            PHF_TRY(p.arena.alloc(&p.offs_k, ok.size()));
+            PHF_CUDA(cudaMemcpy(p.offs_k, ok.data(), ok.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        }
     }
 
     // Hamiltonian
@@ -426,6 +461,13 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(p.arena.alloc(&p.compHS, 2 * nslot));
     PHF_TRY(p.arena.alloc(&p.tmpG, MN));
     PHF_TRY(p.arena.alloc(&p.outMM, MM));
+    if (p.exact) {
+        PHF_TRY(p.arena.alloc(&p.Hb, MN));
+        PHF_TRY(p.arena.alloc(&p.accKG, nslot * MN));
+        PHF_TRY(p.arena.alloc(&p.compKG, nslot * MN));
+        PHF_TRY(p.arena.alloc(&p.accKR, nslot * MN));
+        PHF_TRY(p.arena.alloc(&p.compKR, nslot * MN));
+    }
     PHF_TRY(p.arena.alloc(&p.flag, 1));
 
     // chunk size from the workspace budget
@@ -442,11 +484,15 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         } else {
             per += 2 * MM;
         }
+        if (p.exact) per += 5 * MN;
         per *= sizeof(zc);
         per += split_bytes_per_point(p);
         long long bmax = (long long)(budget / std::max<size_t>(per, 1));
         bmax = std::max<long long>(1, std::min<long long>(bmax, 1024));
         p.b = (int)std::min<long long>(bmax, p.nomega);
+        // whole Lebedev-point blocks (ny npg points sharing R1[il]) per chunk when they fit
+        const int blk = p.ny * p.npg;
+        if (p.b >= blk) p.b = (p.b / blk) * blk;
     }
     const size_t bMN = (size_t)p.b * MN, bNN = (size_t)p.b * N * N;
     PHF_TRY(p.arena.alloc(&p.Ys, bMN));
@@ -455,8 +501,20 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(p.arena.alloc(&p.Sinv, bNN));
     PHF_TRY(p.arena.alloc(&p.W, bNN));
     PHF_TRY(p.arena.alloc(&p.Xs, bMN));
+    if (p.exact) {
+        PHF_TRY(p.arena.alloc(&p.Vk, bMN));
+        PHF_TRY(p.arena.alloc(&p.Pk, bMN));
+        PHF_TRY(p.arena.alloc(&p.Pk2, bMN));
+        PHF_TRY(p.arena.alloc(&p.Prk, bMN));
+        PHF_TRY(p.arena.alloc(&p.Prk2, bMN));
+    }
     PHF_TRY(p.arena.alloc(&p.HX, bMN));
     PHF_TRY(p.arena.alloc(&p.GX, bMN));
+    {
+        unsigned char *sc = nullptr;
+        PHF_TRY(p.arena.alloc(&sc, accumulate_scratch_bytes(p.nb * p.nb, M, N, p.b)));
+        p.acc_scratch = sc;
+    }
     PHF_TRY(p.arena.alloc(&p.det, p.b));
     PHF_TRY(p.arena.alloc(&p.logdet, p.b));
     PHF_TRY(p.arena.alloc(&p.e1, p.b));
@@ -536,8 +594,23 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
         PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
-        PHF_TRY(zgemm_strided((int)n2, 4 * bc, (int)n2, 1, 1, Z1, vd(p.EK, n2, 1), vz(p.Kin, 4LL * b, 1), Z0,
-                              vo(p.Kvec, 4LL * b, 1), nullptr, st));
+        if (p.library_gemm) {
+            // row-major Kvec (n^2 x 8bc reals) = EK (n^2 x n^2) Kin (n^2 x 8bc reals), i.e. column-major
+            // Kvec^T = Kin^T EK^T
+            cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
+            const double one = 1.0, zero = 0.0;
+            ProfScope prof(st, PROF_JK);
+            if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS ||
+                cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, 8 * bc, (int)n2, (int)n2, &one,
+                            reinterpret_cast<const double *>(p.Kin), 8 * b, p.EK, (int)n2, &zero,
+                            reinterpret_cast<double *>(p.Kvec), 8 * b) != CUBLAS_STATUS_SUCCESS) {
+                set_error(PHF_ERR_CUDA, "cublasDgemm failed");
+                return PHF_ERR_CUDA;
+            }
+        } else {
+            PHF_TRY(zgemm_strided((int)n2, 4 * bc, (int)n2, 1, 1, Z1, vd(p.EK, n2, 1), vz(p.Kin, 4LL * b, 1), Z0,
+                                  vo(p.Kvec, 4LL * b, 1), nullptr, st));
+        }
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, p.Kvec, nullptr, 4LL * b, p.Gam, st));
     } else {
@@ -552,6 +625,40 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     return PHF_OK;
 }
 
+// Ket-side gradient of the chunk (exact mode): with V_w = (H1 + Gamma_w^H) C - C W_w^H + conj(h_w) C,
+//   accKG += sum_w conj(Wt N_w) R_w^H V_w S_w^-H,   accKR += sum_w conj(Wt N_w) R_w^H C S_w^-H
+// where R_w^H = Rpg[ig]^H R2[iy]^H R1[il]^H is applied factor by factor.
+int ket_side(PlanImpl &p, int v, int bc, int w0, cudaStream_t st) {
+    const int M = p.M, N = p.N, b = p.b;
+    const long long ld = (long long)b * N, MM = (long long)M * M;
+    PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, 1, M, MM, 0, 1), vz(p.bra, N, 1), Z0, vo(p.Vk, ld, 1, N),
+                          nullptr, st));
+    PHF_TRY(zgemm_strided(M, N, N, bc, 1, ZM1, vz(p.bra, N, 1), vz(p.W, 1, ld, N, 0, 1), Z1, vo(p.Vk, ld, 1, N),
+                          nullptr, st));
+    PHF_TRY(launch_ket_prep(M, N, bc, p.Hb, p.bra, p.e1, p.e2, p.Vk, ld, st));
+    PHF_TRY(zgemm_strided(M, N, N, bc, 1, Z1, vz(p.Vk, ld, 1, N), vz(p.Sinv, 1, ld, N, 0, 1), Z0, vo(p.Pk, ld, 1, N),
+                          nullptr, st));
+    PHF_TRY(zgemm_strided(M, N, N, bc, 1, Z1, vz(p.bra, N, 1), vz(p.Sinv, 1, ld, N, 0, 1), Z0, vo(p.Prk, ld, 1, N),
+                          nullptr, st));
+    const zc *Rs[3] = {p.R1, p.R2, p.Rpg};
+    zc *src = p.Pk, *dst = p.Pk2, *srcr = p.Prk, *dstr = p.Prk2;
+    for (int f = 0; f < 3; ++f) {
+        const long long *offs = p.offs_k + 3LL * ((long long)f * p.nomega + w0);
+        PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(Rs[f], 1, M, 0, 0, 1), vz(src, ld, 1, N), Z0, vo(dst, ld, 1, N),
+                              offs, st));
+        PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(Rs[f], 1, M, 0, 0, 1), vz(srcr, ld, 1, N), Z0, vo(dstr, ld, 1, N),
+                              offs, st));
+        std::swap(src, dst);
+        std::swap(srcr, dstr);
+    }
+    PHF_TRY(launch_scale_conj_det(M, N, bc, p.det, src, ld, st));
+    PHF_TRY(launch_scale_conj_det(M, N, bc, p.det, srcr, ld, st));
+    const int nb2 = p.nb * p.nb;
+    PHF_TRY(launch_accumulate(nb2, M, N, bc, p.Wt, p.nomega, w0, p.slotmap + (size_t)v * nb2, src, srcr, ld, nullptr,
+                              p.accKG, p.compKG, p.accKR, p.compKR, nullptr, nullptr, p.acc_scratch, st, 1));
+    return PHF_OK;
+}
+
 // One (bra, ket) variant over all grid points, accumulated into slot map `v`.
 // bra, ket: M x N row-major in the working basis; kety: the vector R_w multiplies
 // (dense form: Ref ket in AO order; Cholesky form: ket itself).
@@ -561,18 +668,28 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
     // T1[g] = Rpg[g] kety ; T2[y, g] = R2[y] T1[g]
     PHF_TRY(zgemm_strided(M, N, M, p.npg, 1, Z1, vz(p.Rpg, M, 1, MM), vz(p.kety, N, 1, 0), Z0, vo(p.T1, N, 1, MN),
                           nullptr, st));
+    const long long ld2 = (long long)p.ny * p.npg * N;  // T2 column-blocked: T2[r][(iy npg + ig) N + j]
     PHF_TRY(zgemm_strided(M, N, M, p.npg, p.ny, Z1, vz(p.R2, M, 1, 0, MM), vz(p.T1, N, 1, MN, 0), Z0,
-                          vo(p.T2, N, 1, MN, (long long)p.npg * MN), nullptr, st));
-    if (p.chol) {
+                          vo(p.T2, ld2, 1, N, (long long)p.npg * N), nullptr, st));
+    if (p.exact)  // H1 bra (Cholesky forms: h applied to both spin rows of the interleaved order)
+        PHF_TRY(zgemm_strided(n, 2 * N, n, 1, 1, Z1, vd(p.h, n, 1), vz(p.bra, 2 * N, 1), Z0, vo(p.Hb, 2 * N, 1), nullptr,
+                              st));
+    if (p.chol && !p.eri) {
         // V_L = (B_L (x) I_2) bra: (L n x n) x (n x 2N), rows (L, p), columns (sigma, j)
         PHF_TRY(zgemm_strided(L * n, 2 * N, n, 1, 1, Z1, vd(p.Bst, n, 1), vz(p.bra, 2 * N, 1), Z0, vo(p.V, 2 * N, 1),
                               nullptr, st));
     }
     for (int w0 = 0; w0 < p.nomega; w0 += b) {
         const int bc = std::min(b, p.nomega - w0);
-        // Y_w = R1[il] T2[iy, ig]
-        PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.R1, M, 1), vz(p.T2, N, 1), Z0, vo(p.Ys, ld, 1, N), p.offs + 3LL * w0,
-                              st));
+        // Y_w = R1[il] T2[iy, ig]: one (M x M) x (M x ny npg N) product per Lebedev point when the
+        // chunk holds whole blocks of ny npg points, else per point
+        const int blk = p.ny * p.npg;
+        if (w0 % blk == 0 && bc % blk == 0)
+            PHF_TRY(zgemm_strided(M, (int)ld2, M, bc / blk, 1, Z1, vz(p.R1 + (size_t)(w0 / blk) * MM, M, 1, MM),
+                                  vz(p.T2, ld2, 1), Z0, vo(p.Ys, ld, 1, ld2), nullptr, st));
+        else
+            PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.R1, M, 1), vz(p.T2, ld2, 1), Z0, vo(p.Ys, ld, 1, N),
+                                  p.offs + 3LL * w0, st));
         zc *Y = p.Ys;
         if (!p.chol) {  // Ref-MO basis: Y <- Ref^H Y
             PHF_TRY(zgemm_strided(M, bc * N, M, 1, 1, Z1, vz(p.Refw, 1, M, 0, 0, 1), vz(p.Ys, ld, 1), Z0, vo(p.Ys2, ld, 1),
@@ -637,7 +754,8 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
         PHF_TRY(launch_epilogue(M, N, bc, p.HX, p.GX, p.Xs, ld, p.det, p.e1, p.e2, p.scal, st));
         const int nb2 = p.nb * p.nb;
         PHF_TRY(launch_accumulate(nb2, M, N, bc, p.Wt, p.nomega, w0, p.slotmap + (size_t)v * nb2, p.GX, p.Xs, ld, p.scal,
-                                  p.accG, p.compG, p.accR, p.compR, p.accHS, p.compHS, st));
+                                  p.accG, p.compG, p.accR, p.compR, p.accHS, p.compHS, p.acc_scratch, st));
+        if (p.exact) PHF_TRY(ket_side(p, v, bc, w0, st));
     }
     return PHF_OK;
 }
@@ -651,6 +769,12 @@ int zero_acc(PlanImpl &p, cudaStream_t st) {
     PHF_CUDA(cudaMemsetAsync(p.accHS, 0, 2 * nslot * sizeof(zc), st));
     PHF_CUDA(cudaMemsetAsync(p.compHS, 0, 2 * nslot * sizeof(zc), st));
     PHF_CUDA(cudaMemsetAsync(p.flag, 0, sizeof(int), st));
+    if (p.exact) {
+        PHF_CUDA(cudaMemsetAsync(p.accKG, 0, nslot * MN * sizeof(zc), st));
+        PHF_CUDA(cudaMemsetAsync(p.compKG, 0, nslot * MN * sizeof(zc), st));
+        PHF_CUDA(cudaMemsetAsync(p.accKR, 0, nslot * MN * sizeof(zc), st));
+        PHF_CUDA(cudaMemsetAsync(p.compKR, 0, nslot * MN * sizeof(zc), st));
+    }
     return PHF_OK;
 }
 
@@ -659,6 +783,10 @@ int fold_acc(PlanImpl &p, cudaStream_t st) {
     PHF_TRY(launch_fold_comp(nslot * MN, p.accG, p.compG, st));
     PHF_TRY(launch_fold_comp(nslot * MN, p.accR, p.compR, st));
     PHF_TRY(launch_fold_comp(2 * nslot, p.accHS, p.compHS, st));
+    if (p.exact) {
+        PHF_TRY(launch_fold_comp(nslot * MN, p.accKG, p.compKG, st));
+        PHF_TRY(launch_fold_comp(nslot * MN, p.accKR, p.compKR, st));
+    }
     return PHF_OK;
 }
 
@@ -819,6 +947,15 @@ int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_comp
     return PHF_OK;
 }
 
+void plan_release(PlanImpl &p) {
+    if (p.cublas) {
+        cublasDestroy(reinterpret_cast<cublasHandle_t>(p.cublas));
+        p.cublas = nullptr;
+    }
+}
+
+PlanImpl::~PlanImpl() { plan_release(*this); }
+
 int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st) {
     if (p.cmplxconj == 2) {
         set_error(PHF_ERR_UNSUPPORTED, "phf_plan_eval_device: cmplxconj == 2 needs phf_plan_buildhsg");
@@ -843,6 +980,10 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
     PHF_TRY(run_variant(p, 0, st));
     PHF_TRY(fold_acc(p, st));
     const long long ns = (long long)p.nci * p.nci;
+    if (p.exact) {  // symmetrised bra + ket derivative
+        PHF_TRY(launch_average(ns * MN, p.accG, p.accKG, p.accG, st));
+        PHF_TRY(launch_average(ns * MN, p.accR, p.accKR, p.accR, st));
+    }
     PHF_CUDA(cudaMemcpyAsync(d_hs, p.accHS, 2 * ns * sizeof(zc), cudaMemcpyDeviceToDevice, st));
     if (p.chol) {
         // back to [alpha; beta] order: out[r] = acc[inv[r]]

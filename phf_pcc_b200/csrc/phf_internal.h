@@ -61,10 +61,15 @@ int launch_trace_conj(int M, int N, int b, const zc *C, const zc *X, long long l
                       cudaStream_t st);
 int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
                     const zc *e2, zc *scal, cudaStream_t st);
+size_t accumulate_scratch_bytes(int nslot, int M, int N, int b);
 int launch_accumulate(int nslot, int M, int N, int b, const zc *Wt, long long nomega, long long w0, const int *slotmap,
                       const zc *G, const zc *R, long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
-                      zc *compR, zc *accHS, zc *compHS, cudaStream_t st);
+                      zc *compR, zc *accHS, zc *compHS, void *scratch, cudaStream_t st, int conj_weights = 0);
 int launch_fold_comp(long long n, zc *a, const zc *c, cudaStream_t st);
+int launch_ket_prep(int M, int N, int b, const zc *Hb, const zc *bra, const zc *e1, const zc *e2, zc *V, long long ld,
+                    cudaStream_t st);
+int launch_scale_conj_det(int M, int N, int b, const zc *det, zc *P, long long ld, cudaStream_t st);
+int launch_average(long long n, const zc *a, const zc *b, zc *out, cudaStream_t st);
 int launch_permute_h2(int M, const zc *H2, zc *H2r, cudaStream_t st);
 int launch_permute_rows(int M, int N, int nbatch, const int *rowmap, const zc *in, long long ldin, long long bs_in,
                         zc *out, long long bs_out, cudaStream_t st);
@@ -100,6 +105,9 @@ struct PlanImpl {
     int n = 0, M = 0, N = 0, L = 0;
     int prec = PHF_PREC_FP64, slices = 0;
     int eri = 0;                     // exchange via the spatial ERI matrix (1) or factorized Cholesky (0)
+    int exact = 0;                   // also accumulate the ket-side gradient (gradient_mode 1)
+    int library_gemm = 0;            // FP64 exchange GEMM through cuBLAS (comparison form)
+    void *cublas = nullptr;          // cublasHandle_t when library_gemm
     int nl = 0, ny = 0, npg = 0, nomega = 0;
     int nci = 0, ncisp = 0, ncipg = 0, cmplxconj = 1, qj = 0, sp = 1, nb = 0;
     std::vector<int> perm;           // working index -> reference index
@@ -127,6 +135,11 @@ struct PlanImpl {
     // accumulators
     zc *accG = nullptr, *compG = nullptr, *accR = nullptr, *compR = nullptr, *accHS = nullptr, *compHS = nullptr;
     zc *tmpG = nullptr, *outMM = nullptr;
+    void *acc_scratch = nullptr;       // partial sums of the two-stage accumulation
+    // ket-side gradient (exact mode)
+    zc *Hb = nullptr, *Vk = nullptr, *Pk = nullptr, *Pk2 = nullptr, *Prk = nullptr, *Prk2 = nullptr;
+    zc *accKG = nullptr, *compKG = nullptr, *accKR = nullptr, *compKR = nullptr, *dummyHS = nullptr;
+    long long *offs_k = nullptr;       // 3 x 3 x nomega: GEMM offsets of R1^H, R2^H, Rpg^H per point
     // spatial-ERI exchange form
     double *EK = nullptr;              // EK[(i n + k) n^2 + l n + j] = (il|kj), FP64 back-end
     signed char *EKsl = nullptr;       // its int8 slices, Ozaki back-end
@@ -135,6 +148,7 @@ struct PlanImpl {
     double *Dk = nullptr;
     signed char *Bsl = nullptr;
     SplitWork split;  // tensor-core path workspace (phf_split.cu)
+    ~PlanImpl();
 };
 
 size_t split_bytes_per_point(const PlanImpl &p);
@@ -145,6 +159,7 @@ int split_gamma_x(PlanImpl &p, int bc, cudaStream_t st);
 int profile_enable(int on);
 int profile_read(int cls, double *ms, unsigned long long *count);
 int plan_create(const phf_plan_desc *d, phf_plan **out);
+void plan_release(PlanImpl &p);
 int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
                   phf_complex *rdmmat);
 int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st);

@@ -110,46 +110,97 @@ __device__ __forceinline__ void neumaier(double &s, double &c, double x) {
 
 // Weighted accumulation over a chunk of grid points (PHFTools.f90:137-166):
 //   accG[a] += sum_w Wt[s, w0 + w] * G_w,  accR[a] += sum_w Wt[s, w0 + w] * R_w,
-//   accHS[a] += sum_w Wt[s, w0 + w] * (N h, N)_w      with a = slotmap[s],
-// summed over w in order with Neumaier compensation (comp arrays carried across chunks).
-__global__ void __launch_bounds__(NT) accumulate_kernel(int nslot, int M, int N, int b, const zc *Wt, long long nomega,
-                                                        long long w0, const int *slotmap, const zc *G, const zc *R,
-                                                        long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
-                                                        zc *compR, zc *accHS, zc *compHS) {
+//   accHS[a] += sum_w Wt[s, w0 + w] * (N h, N)_w      with a = slotmap[s].
+// Two stages with a fixed partition, so the result does not depend on scheduling:
+//   stage 1: thread (element, group q) sums the points [q*ACC_GROUP, (q+1)*ACC_GROUP) in order
+//            with Neumaier compensation into part[q] (sum, compensation);
+//   stage 2: thread (element) adds part[0..ngroups) in order into the running (acc, comp).
+constexpr int ACC_GROUP = 32;
+
+struct AccPart {
+    double gs_r, gs_i, gc_r, gc_i, rs_r, rs_i, rc_r, rc_i;
+};
+
+__global__ void __launch_bounds__(NT) accumulate_partial_kernel(int nslot, int M, int N, int b, const zc *Wt,
+                                                                long long nomega, long long w0, const zc *G,
+                                                                const zc *R, long long ldX, const zc *scal,
+                                                                int ngroups, AccPart *part, AccPart *part_hs,
+                                                                int conj_w) {
     const long long MN = (long long)M * N;
-    const long long total = (long long)nslot * MN;
-    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
-        int s = (int)(e / MN);
-        long long rj = e - (long long)s * MN;
-        long long r = rj / N, j = rj - r * N;
-        long long a = (long long)slotmap[s] * MN + rj;
+    const long long nel = (long long)nslot * MN;
+    const long long total = nel * ngroups;
+    for (long long t = blockIdx.x * (long long)NT + threadIdx.x; t < total; t += (long long)gridDim.x * NT) {
+        const int q = (int)(t / nel);
+        const long long e = t - (long long)q * nel;
+        const int s = (int)(e / MN);
+        const long long rj = e - (long long)s * MN;
+        const long long r = rj / N, j = rj - r * N;
+        const int wa = q * ACC_GROUP, wb = min(b, wa + ACC_GROUP);
+        const zc *wrow = Wt + (long long)s * nomega + w0;
+        AccPart P = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int w = wa; w < wb; ++w) {
+            const zc wt = conj_w ? conjz(wrow[w]) : wrow[w];
+            const long long o = r * ldX + (long long)w * N + j;
+            const zc tg = wt * G[o], tr = wt * R[o];
+            neumaier(P.gs_r, P.gc_r, tg.x);
+            neumaier(P.gs_i, P.gc_i, tg.y);
+            neumaier(P.rs_r, P.rc_r, tr.x);
+            neumaier(P.rs_i, P.rc_i, tr.y);
+        }
+        part[t] = P;
+        if (rj == 0 && scal) {  // the two scalars of the slot ride on the element (s, 0, 0)
+            AccPart Q = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int w = wa; w < wb; ++w) {
+                const zc wt = conj_w ? conjz(wrow[w]) : wrow[w];
+                const zc th = wt * scal[2 * w], ts = wt * scal[2 * w + 1];
+                neumaier(Q.gs_r, Q.gc_r, th.x);
+                neumaier(Q.gs_i, Q.gc_i, th.y);
+                neumaier(Q.rs_r, Q.rc_r, ts.x);
+                neumaier(Q.rs_i, Q.rc_i, ts.y);
+            }
+            part_hs[(long long)q * nslot + s] = Q;
+        }
+    }
+}
+
+__device__ __forceinline__ void add_part(double &s, double &c, double ps, double pc) {
+    neumaier(s, c, ps);
+    c += pc;
+}
+
+__global__ void __launch_bounds__(NT) accumulate_final_kernel(int nslot, int M, int N, const int *slotmap,
+                                                              int ngroups, const AccPart *part,
+                                                              const AccPart *part_hs, zc *accG, zc *compG, zc *accR,
+                                                              zc *compR, zc *accHS, zc *compHS) {
+    const long long MN = (long long)M * N;
+    const long long nel = (long long)nslot * MN;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < nel; e += (long long)gridDim.x * NT) {
+        const int s = (int)(e / MN);
+        const long long rj = e - (long long)s * MN;
+        const long long a = (long long)slotmap[s] * MN + rj;
         double gs_r = accG[a].x, gs_i = accG[a].y, gc_r = compG[a].x, gc_i = compG[a].y;
         double rs_r = accR[a].x, rs_i = accR[a].y, rc_r = compR[a].x, rc_i = compR[a].y;
-        const zc *wrow = Wt + (long long)s * nomega + w0;
-        for (int w = 0; w < b; ++w) {
-            zc wt = wrow[w];
-            long long o = r * ldX + (long long)w * N + j;
-            zc tg = wt * G[o], tr = wt * R[o];
-            neumaier(gs_r, gc_r, tg.x);
-            neumaier(gs_i, gc_i, tg.y);
-            neumaier(rs_r, rc_r, tr.x);
-            neumaier(rs_i, rc_i, tr.y);
+        for (int q = 0; q < ngroups; ++q) {
+            const AccPart P = part[(long long)q * nel + e];
+            add_part(gs_r, gc_r, P.gs_r, P.gc_r);
+            add_part(gs_i, gc_i, P.gs_i, P.gc_i);
+            add_part(rs_r, rc_r, P.rs_r, P.rc_r);
+            add_part(rs_i, rc_i, P.rs_i, P.rc_i);
         }
         accG[a] = mkz(gs_r, gs_i);
         compG[a] = mkz(gc_r, gc_i);
         accR[a] = mkz(rs_r, rs_i);
         compR[a] = mkz(rc_r, rc_i);
-        if (rj == 0) {
-            long long ah = 2LL * slotmap[s];
+        if (rj == 0 && accHS) {
+            const long long ah = 2LL * slotmap[s];
             double hs_r = accHS[ah].x, hs_i = accHS[ah].y, hc_r = compHS[ah].x, hc_i = compHS[ah].y;
             double ss_r = accHS[ah + 1].x, ss_i = accHS[ah + 1].y, sc_r = compHS[ah + 1].x, sc_i = compHS[ah + 1].y;
-            for (int w = 0; w < b; ++w) {
-                zc wt = wrow[w];
-                zc th = wt * scal[2 * w], ts = wt * scal[2 * w + 1];
-                neumaier(hs_r, hc_r, th.x);
-                neumaier(hs_i, hc_i, th.y);
-                neumaier(ss_r, sc_r, ts.x);
-                neumaier(ss_i, sc_i, ts.y);
+            for (int q = 0; q < ngroups; ++q) {
+                const AccPart Q = part_hs[(long long)q * nslot + s];
+                add_part(hs_r, hc_r, Q.gs_r, Q.gc_r);
+                add_part(hs_i, hc_i, Q.gs_i, Q.gc_i);
+                add_part(ss_r, sc_r, Q.rs_r, Q.rc_r);
+                add_part(ss_i, sc_i, Q.rs_i, Q.rc_i);
             }
             accHS[ah] = mkz(hs_r, hs_i);
             compHS[ah] = mkz(hc_r, hc_i);
@@ -235,6 +286,34 @@ __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, 
     }
 }
 
+// ket-side gradient: V_w += H1 C + conj(h_w) C   (V already holds Gamma_w^H C - C W_w^H)
+__global__ void ket_prep_kernel(int M, int N, int b, const zc *Hb, const zc *bra, const zc *e1, const zc *e2, zc *V,
+                                long long ld) {
+    const long long total = (long long)M * b * N;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        long long r = e / ((long long)b * N), c = e - r * ((long long)b * N);
+        int w = (int)(c / N), j = (int)(c - (long long)w * N);
+        zc h = conjz(e1[w] + e2[w]);
+        V[r * ld + c] = V[r * ld + c] + Hb[r * N + j] + h * bra[r * N + j];
+    }
+}
+
+// P_w <- conj(det_w) P_w
+__global__ void scale_conj_det_kernel(int M, int N, int b, const zc *det, zc *P, long long ld) {
+    const long long total = (long long)M * b * N;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        long long r = e / ((long long)b * N), c = e - r * ((long long)b * N);
+        int w = (int)(c / N);
+        P[r * ld + c] = conjz(det[w]) * P[r * ld + c];
+    }
+}
+
+// out = (a + b) / 2
+__global__ void average_kernel(long long n, const zc *a, const zc *b, zc *out) {
+    for (long long i = blockIdx.x * (long long)NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT)
+        out[i] = 0.5 * (a[i] + b[i]);
+}
+
 inline int grid_for(long long n) {
     long long g = (n + NT - 1) / NT;
     if (g > 148LL * 16) g = 148LL * 16;
@@ -278,13 +357,54 @@ int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long l
     return PHF_OK;
 }
 
+size_t accumulate_scratch_bytes(int nslot, int M, int N, int b) {
+    const long long ngroups = (b + ACC_GROUP - 1) / ACC_GROUP;
+    return (size_t)ngroups * ((size_t)nslot * M * N + nslot) * sizeof(AccPart);
+}
+
 int launch_accumulate(int nslot, int M, int N, int b, const zc *Wt, long long nomega, long long w0, const int *slotmap,
                       const zc *G, const zc *R, long long ldX, const zc *scal, zc *accG, zc *compG, zc *accR,
-                      zc *compR, zc *accHS, zc *compHS, cudaStream_t st) {
+                      zc *compR, zc *accHS, zc *compHS, void *scratch, cudaStream_t st, int conj_weights) {
+    const int ngroups = (b + ACC_GROUP - 1) / ACC_GROUP;
+    AccPart *part = reinterpret_cast<AccPart *>(scratch);
+    AccPart *part_hs = part + (size_t)ngroups * nslot * M * N;
+    {
+        ProfScope prof(st, PROF_MEMORY);
+        accumulate_partial_kernel<<<grid_for((long long)ngroups * nslot * M * N), NT, 0, st>>>(
+            nslot, M, N, b, Wt, nomega, w0, G, R, ldX, scal, ngroups, part, part_hs, conj_weights);
+    }
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    {
+        ProfScope prof(st, PROF_MEMORY);
+        accumulate_final_kernel<<<grid_for((long long)nslot * M * N), NT, 0, st>>>(
+            nslot, M, N, slotmap, ngroups, part, part_hs, accG, compG, accR, compR, accHS, compHS);
+    }
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_ket_prep(int M, int N, int b, const zc *Hb, const zc *bra, const zc *e1, const zc *e2, zc *V, long long ld,
+                    cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    accumulate_kernel<<<grid_for((long long)nslot * M * N), NT, 0, st>>>(nslot, M, N, b, Wt, nomega, w0, slotmap, G, R,
-                                                                         ldX, scal, accG, compG, accR, compR, accHS,
-                                                                         compHS);
+    ket_prep_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, N, b, Hb, bra, e1, e2, V, ld);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_scale_conj_det(int M, int N, int b, const zc *det, zc *P, long long ld, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    scale_conj_det_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, N, b, det, P, ld);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_average(long long n, const zc *a, const zc *b, zc *out, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    average_kernel<<<grid_for(n), NT, 0, st>>>(n, a, b, out);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -17,7 +17,7 @@ namespace phf {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+constexpr int BK = 16, NT = 256;
 
 template <bool AREAL>
 struct ATile {
@@ -35,15 +35,21 @@ __device__ __forceinline__ double load_d(const View &v, long long off) {
     return reinterpret_cast<const double *>(v.p)[off];
 }
 
-template <bool AREAL>
+// BM x BN output tile, 256 threads in a (BM/4) x (BN/4) grid, 4 x 4 complex accumulators each:
+// thread (ty, tx) owns rows ty + (BM/4) i and columns tx + (BN/4) j.  64 x 64 serves general
+// shapes; 128 x 32 serves the narrow per-point products (N <= 32 columns).
+template <bool AREAL, int BM, int BN>
 __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
                                                    zc beta, OutView C, const long long *__restrict__ offs) {
     using TA = typename ATile<AREAL>::T;
+    constexpr int TX = BN / 4, TY = BM / 4;
+    static_assert(TX * TY == NT, "tile/thread mismatch");
+    constexpr int LA = (BM * BK) / NT, LB = (BN * BK) / NT;  // elements loaded per thread
     __shared__ TA As[BK][BM + 1];
     __shared__ zc Bs[BK][BN + 1];
 
     const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
+    const int tx = tid % TX, ty = tid / TX;
     const long long bz = blockIdx.x / ntn;
     const int tn = blockIdx.x - bz * ntn;
     const int row0 = blockIdx.y * BM, col0 = tn * BN;
@@ -57,15 +63,15 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
     const bool a_mfast = (A.rs == 1);  // element order of the A tile loads
     const bool b_nfast = (B.cs == 1);
 
-    TA ra[4];
-    zc rb[4];
+    TA ra[LA];
+    zc rb[LB];
     auto fetch = [&](int k0) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LA; ++r) {
             int e = tid + NT * r;
             int i, kk;
-            if (a_mfast) { i = e & (BM - 1); kk = e >> 6; }
-            else { kk = e & (BK - 1); i = e >> 4; }
+            if (a_mfast) { i = e % BM; kk = e / BM; }
+            else { kk = e % BK; i = e / BK; }
             int gi = row0 + i, gk = k0 + kk;
             if (gi < m && gk < k) {
                 long long off = oa + (long long)gi * A.rs + (long long)gk * A.cs;
@@ -75,25 +81,32 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
                 if constexpr (AREAL) ra[r] = 0.0;
                 else ra[r] = zc{0.0, 0.0};
             }
-            int j;
-            if (b_nfast) { j = e & (BN - 1); kk = e >> 6; }
-            else { kk = e & (BK - 1); j = e >> 4; }
-            int gj = col0 + j;
-            gk = k0 + kk;
+        }
+#pragma unroll
+        for (int r = 0; r < LB; ++r) {
+            int e = tid + NT * r;
+            int j, kk;
+            if (b_nfast) { j = e % BN; kk = e / BN; }
+            else { kk = e % BK; j = e / BK; }
+            int gj = col0 + j, gk = k0 + kk;
             rb[r] = (gj < n && gk < k) ? load_z(B, ob + (long long)gk * B.rs + (long long)gj * B.cs) : zc{0.0, 0.0};
         }
     };
     auto stash = [&]() {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LA; ++r) {
             int e = tid + NT * r;
             int i, kk;
-            if (a_mfast) { i = e & (BM - 1); kk = e >> 6; }
-            else { kk = e & (BK - 1); i = e >> 4; }
+            if (a_mfast) { i = e % BM; kk = e / BM; }
+            else { kk = e % BK; i = e / BK; }
             As[kk][i] = ra[r];
-            int j;
-            if (b_nfast) { j = e & (BN - 1); kk = e >> 6; }
-            else { kk = e & (BK - 1); j = e >> 4; }
+        }
+#pragma unroll
+        for (int r = 0; r < LB; ++r) {
+            int e = tid + NT * r;
+            int j, kk;
+            if (b_nfast) { j = e % BN; kk = e / BN; }
+            else { kk = e % BK; j = e / BK; }
             Bs[kk][j] = rb[r];
         }
     };
@@ -115,9 +128,9 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
             TA a[4];
             zc b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + TY * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + TX * j];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -137,11 +150,11 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
     const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        int gi = row0 + ty + 16 * i;
+        int gi = row0 + ty + TY * i;
         if (gi >= m) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            int gj = col0 + tx + 16 * j;
+            int gj = col0 + tx + TX * j;
             if (gj >= n) continue;
             long long off = oc + (long long)gi * C.rs + (long long)gj * C.cs;
             zc v = alpha * zc{accr[i][j], acci[i][j]};
@@ -156,15 +169,9 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
     }
 }
 
-}  // namespace
-
-int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
-                  const OutView &C, const long long *offs, cudaStream_t st) {
-    if (m <= 0 || n <= 0 || nb0 <= 0 || nb1 <= 0) return PHF_OK;
-    if (k <= 0) {
-        set_error(PHF_ERR_ARG, "zgemm_strided: k <= 0");
-        return PHF_ERR_ARG;
-    }
+template <int BM, int BN>
+int launch_tile(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
+                const OutView &C, const long long *offs, cudaStream_t st) {
     const int ntn = (n + BN - 1) / BN, ntm = (m + BM - 1) / BM;
     const long long nbatch = (long long)nb0 * nb1;
     const long long gx = nbatch * ntn;
@@ -175,12 +182,25 @@ int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A
     dim3 grid((unsigned)gx, (unsigned)ntm, 1);
     ProfScope prof(st, -1);
     if (A.real)
-        zgemm_kernel<true><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+        zgemm_kernel<true, BM, BN><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
     else
-        zgemm_kernel<false><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+        zgemm_kernel<false, BM, BN><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
+}
+
+}  // namespace
+
+int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
+                  const OutView &C, const long long *offs, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || nb0 <= 0 || nb1 <= 0) return PHF_OK;
+    if (k <= 0) {
+        set_error(PHF_ERR_ARG, "zgemm_strided: k <= 0");
+        return PHF_ERR_ARG;
+    }
+    if (n <= 32 && m >= 96) return launch_tile<128, 32>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    return launch_tile<64, 64>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
 }
 
 }  // namespace phf

@@ -36,10 +36,12 @@ def test_energy_and_gradient_match_reference_golden(precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "ozaki_i8"])
 def test_gradient_matches_central_finite_differences(precision):
+    """Exact-gradient plans against central differences on a coarse grid (14 x 8 x C2v) where the
+    reference's bra-side gradient differs from dE/dC* at the 1e-3 level."""
     import torch
 
     p = synth.make_problem(16, 8, 40, ngrid=(14, 8), seed=21, pg="C2v")
-    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=precision,
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=precision, gradient="exact",
                   **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
         C = torch.from_numpy(p.C).cuda()
         E0, G = energy_and_gradient(C, plan)
@@ -54,6 +56,51 @@ def test_gradient_matches_central_finite_differences(precision):
             fd = (ep - em).item() / (2 * h)
             an = torch.real(torch.sum(torch.conj(grad) * d)).item()
             assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
+
+
+def test_exact_and_reference_gradients_agree_on_fine_symmetric_grid():
+    """On the golden config-1 problem (grid 14 x 8, H/S real to 1e-16) both gradients coincide
+    with the reference's LocalG."""
+    import torch
+
+    c = load("c1")
+    M, N = int(c["M"]), int(c["N"])
+    C = torch.from_numpy(c["Ref"] @ np.vstack([np.eye(N), c["Z"]])).cuda()
+    out = {}
+    for mode in ("reference", "exact"):
+        with api.Plan(ref=np.eye(M), h=c["h"], B=c["B"], gradient=mode,
+                      **_plan_kwargs_from_grid(grid_kwargs(c), N)) as plan:
+            out[mode] = energy_and_gradient(C, plan)
+    assert abs(out["exact"][0].item() - out["reference"][0].item()) < 1e-12
+    diff = (out["exact"][1] - out["reference"][1]).abs().max().item()
+    assert diff <= 1e-6 * out["reference"][1].abs().max().item(), diff
+
+
+def test_gradient_fd_at_config2_orbital_rotation_steps():
+    """Configuration 2 adjoint check: seeded orbital-rotation steps C <- exp(kappa) C, forward +
+    autograd backward, directional derivative against central differences (h = 1e-5)."""
+    import torch
+
+    p = synth.config_problem("c2", seed=2)
+    rng = np.random.default_rng(11)
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="ozaki_i8", gradient="exact",
+                  **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
+        C0 = p.C
+        for step in range(3):
+            C0 = synth.orbital_rotation(C0, 1e-2, rng)
+            C = torch.from_numpy(C0).cuda().requires_grad_(True)
+            E = projected_energy(C, plan)
+            E.backward()
+            g = C.grad
+            d = rng.normal(size=C0.shape) + 1j * rng.normal(size=C0.shape)
+            d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
+            h = 1e-5
+            with torch.no_grad():
+                ep = projected_energy(C.detach() + h * d, plan)
+                em = projected_energy(C.detach() - h * d, plan)
+            fd = (ep - em).item() / (2 * h)
+            an = torch.real(torch.sum(torch.conj(g) * d)).item()
+            assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (step, fd, an)
 
 
 def test_recompute_mode_equals_fused_mode():

@@ -70,11 +70,14 @@ def _close(a, b, rel):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("form,precision", [("factorized", "fp64"), ("eri", "fp64"), ("eri", "ozaki_i8")])
+@pytest.mark.parametrize("form,precision", [("factorized", "fp64"), ("eri", "fp64"), ("eri", "fp64-cublas"),
+                                            ("eri", "ozaki_i8")])
 def test_forms_and_precisions_match_golden(name, form, precision):
     c = load(name)
-    rel = 1e-10 if precision == "fp64" else 1e-9
-    with api.Plan(ref=c["Ref"], h=c["h"], B=c["B"], jk_form=form, precision=precision, **_api_kwargs(c)) as plan:
+    rel = 1e-10 if precision.startswith("fp64") else 1e-9
+    lib_gemm = precision == "fp64-cublas"
+    with api.Plan(ref=c["Ref"], h=c["h"], B=c["B"], jk_form=form, precision=precision.split("-")[0],
+                  fp64_library_gemm=lib_gemm, **_api_kwargs(c)) as plan:
         out = plan.buildhsg(c["Z"], check_hermitian=False)
     for x, key in zip(out, ("Hmat", "Smat", "Gradmat", "Rdmmat")):
         assert _close(x, c[key], rel), (key, float(np.abs(x - c[key]).max()))

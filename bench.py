@@ -121,18 +121,20 @@ def jk_form_of(p):
 def jk_flops_per_point(p, form):
     """Algorithmic real flops of the exchange/Coulomb contraction kernels per grid point.
 
-    eri form:        K = EK (n^2 x n^2, real) times 4 complex density columns: 16 n^4
+    eri form:        K = EK (n^2 x n^2, real) times 4 complex density columns: 16 n^4, and the
+                     Coulomb term d = B vec P, J = B^T d: 8 L n^2
     factorized form: T = V^H X (8 L N^2 M), Q = X T' (8 L N^2 M), GX = sum_L B_L Q_L (8 L n^2 N)"""
     n, N, M, L = p.n, p.N, p.M, p.L
     if form == "eri":
-        return 16.0 * n ** 4
+        return 16.0 * n ** 4 + 8.0 * L * n * n
     return 8.0 * L * N * N * M * 2 + 8.0 * L * n * n * N
 
 
 def int8_ops_per_point(p, slices):
     """Executed int8 tensor-core operations per grid point in the eri form: S(S+1)/2 slice
-    products of the (n^2 x n^2) x (n^2 x 8) real GEMM, 2 ops per multiply-add."""
-    return slices * (slices + 1) / 2 * 2.0 * p.n ** 4 * 8
+    products of the exchange GEMM (n^2 x n^2) x (n^2 x 8) and of the two Coulomb GEMMs
+    (L x n^2) x (n^2 x 2) and (n^2 x L) x (L x 2), 2 ops per multiply-add."""
+    return slices * (slices + 1) / 2 * (16.0 * p.n ** 4 + 8.0 * p.L * p.n ** 2)
 
 
 def survey_flops_per_point(p):
@@ -365,7 +367,7 @@ def run_ours(args):
                     "peak_source": ("cuBLASLt int8 GEMM 8192^3 measured in this run" if i8 else
                                     "2 x measured bf16 burst (MEASURED_PEAKS.json)"),
                     "bf16_tflops_measured": bf16,
-                    "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::i8, exchange GEMM)",
+                    "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::i8, exchange and Coulomb GEMMs)",
                     "fp64_equivalent_tflops": alg * pts / (jk_ms * 1e-3) / 1e12,
                     "fp64_dgemm_peak_tflops": fp64_peak}
         roof.update({"jk_form": form, "jk_launches": jk_n, "jk_ms_per_step": jk_ms / args.steps,

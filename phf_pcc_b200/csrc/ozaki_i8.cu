@@ -14,15 +14,19 @@
 // (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
 // fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
 //
-// Kernel shape (one CTA per 128 x 64 output tile, 6 warps):
-//   warp 0      TMA producer: per 64-byte k-block one box of all S slices of the A tile
-//               (S x 128 x 64 B) and of the B tile (S x 64 x 64 B), SWIZZLE_64B, into a
-//               ring of stages guarded by full/empty mbarriers
-//   warp 1      TMEM allocation (512 columns) and the single-thread tcgen05.mma issuer:
-//               S(S+1)/2 slice pairs x 2 k-steps of 32 per stage, group g accumulating in
-//               TMEM columns [64 (g-2), 64 (g-1)); tcgen05.commit frees each stage
-//   warps 2-5   epilogue: tcgen05.ld 32x32b.x32 of each group, int32 -> FP64, 2^{-7g} scaling,
-//               2^{ea+eb} scaling, store (or add) into D
+// Kernel shape (one CTA per 128 x 256 output tile, 6 warps), with row tiles fastest in the grid so
+// that the CTAs in flight share B column tiles through L2:
+//   warp 0      TMA producer: per 32-byte k-block, boxes of two slices of the A tile (2 x 128 x 32 B)
+//               and of the B tile (2 x 256 x 32 B), SWIZZLE_32B, into a ring of stages guarded by
+//               full/empty mbarriers
+//   warp 1      TMEM allocation (512 columns = two 128 x 256 int32 accumulators) and the
+//               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of two
+//               groups over the whole k range (pass p needs slices 1..2p+2 only); within a stage
+//               every slice pair of the pass's groups is one 128 x 256 x 32 MMA
+//   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of both groups, int32 -> FP64,
+//               2^{-7g} and 2^{ea+eb} scaling, store (first pass) or add into D; then release TMEM
+// With N = 256 an MMA reads 4 KB of A and 8 KB of B from shared memory per 1M MACs, within the
+// shared-memory bandwidth at the full int8 rate (a 64-wide tile needs 1.5x more than available).
 // Every mbarrier wait gives up after ~2^31 clock cycles, sets *err and lets the CTA finish.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -37,7 +41,7 @@ namespace phf {
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 64;  // tile rows, tile columns, k-block bytes
+constexpr int OZ_BM = 128, OZ_BN = 256, OZ_BK = 32;  // tile rows, tile columns, k-block bytes
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_MAX_S = 7;
 
@@ -52,6 +56,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Bounded wait on an mbarrier phase.  Returns false (and sets *err) after ~2^31 cycles.
@@ -83,18 +91,18 @@ __device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, SWIZZLE_64B (8 rows x 64 B atoms, SBO = 512 B).
-__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+// Shared-memory matrix descriptor: K-major, SWIZZLE_32B (8 rows x 32 B atoms, SBO = 256 B).
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
     d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)(256 >> 4) << 32;                  // stride byte offset: 8 rows x 32 B
     d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                           // layout: SWIZZLE_64B
+    d |= (uint64_t)6 << 61;                           // layout: SWIZZLE_32B
     return d;
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 64.
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 256.
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
@@ -129,24 +137,31 @@ struct OzArgs {
     double *D;
     long long ldd;
     int accumulate;      // D += result instead of D = result
+    int trans;           // write D^T: element (i, j) at D[j * ldd + i]
     int *err;
 };
+
+// slices held per stage (an even count: slices are loaded in pairs)
+__host__ __device__ __forceinline__ int oz_spad(int S) { return (S + 1) & ~1; }
 
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = args.S, STAGES = args.stages;
-    const uint32_t a_bytes = (uint32_t)S * OZ_BM * OZ_BK, b_bytes = (uint32_t)S * OZ_BN * OZ_BK;
-    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const int S = args.S, STAGES = args.stages, SP = oz_spad(S);
+    const uint32_t a_slice = OZ_BM * OZ_BK, b_slice = OZ_BN * OZ_BK;  // 4 KB, 8 KB
+    const uint32_t a_bytes = (uint32_t)SP * a_slice;
+    const uint32_t stage_bytes = (uint32_t)SP * (a_slice + b_slice);
+    const int npass = (S + 1) / 2;
     uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)STAGES * stage_bytes);
     uint64_t *empty_bar = full_bar + STAGES;
-    uint64_t *done_bar = empty_bar + STAGES;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done_bar + 1);
+    uint64_t *pass_bar = empty_bar + STAGES;  // MMAs of a pass complete
+    uint64_t *free_bar = pass_bar + 1;        // epilogue has read the pass's accumulators
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(free_bar + 1);
     __shared__ int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * OZ_BM, n0 = blockIdx.x * OZ_BN;
+    const int m0 = blockIdx.x * OZ_BM, n0 = blockIdx.y * OZ_BN;
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -154,7 +169,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        mbar_init(done_bar, 1);
+        mbar_init(pass_bar, 1);
+        mbar_init(free_bar, 128);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
@@ -171,84 +187,110 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
-            for (int kb = 0; kb < KB; ++kb) {
-                const int s = kb % STAGES, use = kb / STAGES;
-                if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
-                    abort_flag = 1;
-                    break;
+            int it = 0;
+            for (int p = 0; p < npass && !abort_flag; ++p) {
+                const int npairs = p + 1;  // slice pairs needed by groups 2p+2, 2p+3
+                const uint32_t bytes = (uint32_t)npairs * 2 * (a_slice + b_slice);
+                for (int kb = 0; kb < KB; ++kb, ++it) {
+                    const int s = it % STAGES, use = it / STAGES;
+                    if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    if (abort_flag) break;
+                    unsigned char *sa = smem + (size_t)s * stage_bytes;
+                    mbar_arrive_expect_tx(&full_bar[s], bytes);
+                    const int kc = (args.kb0 + kb) * OZ_BK;
+                    for (int q = 0; q < npairs; ++q) {
+                        tma_load_3d(&tmA, &full_bar[s], sa + (size_t)(2 * q) * a_slice, kc, m0, 2 * q);
+                        tma_load_3d(&tmB, &full_bar[s], sa + a_bytes + (size_t)(2 * q) * b_slice, kc, n0, 2 * q);
+                    }
                 }
-                if (abort_flag) break;
-                unsigned char *sa = smem + (size_t)s * stage_bytes;
-                mbar_arrive_expect_tx(&full_bar[s], stage_bytes);
-                tma_load_3d(&tmA, &full_bar[s], sa, (args.kb0 + kb) * OZ_BK, m0, 0);
-                tma_load_3d(&tmB, &full_bar[s], sa + a_bytes, (args.kb0 + kb) * OZ_BK, n0, 0);
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
+            int it = 0;
             bool ok = true;
-            for (int kb = 0; kb < KB && ok; ++kb) {
-                const int s = kb % STAGES, use = kb / STAGES;
-                if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
-                    ok = false;
-                    abort_flag = 1;
-                    break;
+            for (int p = 0; p < npass && ok; ++p) {
+                if (p > 0) {  // accumulators drained by the epilogue
+                    if (!mbar_wait(free_bar, (p - 1) & 1, args.err, 8)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t sa = smem_u32(smem + (size_t)s * stage_bytes);
-                const uint32_t sb = sa + a_bytes;
-                for (int g = 2; g <= S + 1; ++g) {
-                    const uint32_t dcol = tmem_base + (uint32_t)(g - 2) * OZ_BN;
-                    for (int t = 1; t < g; ++t) {
-                        const int u = g - t;
-#pragma unroll
-                        for (int kk = 0; kk < OZ_BK / 32; ++kk) {
-                            const uint64_t da = sdesc_sw64(sa + (uint32_t)(t - 1) * OZ_BM * OZ_BK + kk * 32);
-                            const uint64_t db = sdesc_sw64(sb + (uint32_t)(u - 1) * OZ_BN * OZ_BK + kk * 32);
-                            const uint32_t acc = (kb > 0 || t > 1 || kk > 0) ? 1u : 0u;
-                            mma_i8(dcol, da, db, acc);
+                const int g0 = 2 + 2 * p, g1 = min(3 + 2 * p, S + 1);
+                for (int kb = 0; kb < KB; ++kb, ++it) {
+                    const int s = it % STAGES, use = it / STAGES;
+                    if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
+                        ok = false;
+                        abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(smem + (size_t)s * stage_bytes);
+                    const uint32_t sb = sa + a_bytes;
+                    for (int g = g0; g <= g1; ++g) {
+                        const uint32_t dcol = tmem_base + (uint32_t)(g - g0) * OZ_BN;
+                        for (int t = 1; t < g; ++t) {
+                            const int u = g - t;
+                            const uint64_t da = sdesc_sw32(sa + (uint32_t)(t - 1) * a_slice);
+                            const uint64_t db = sdesc_sw32(sb + (uint32_t)(u - 1) * b_slice);
+                            mma_i8(dcol, da, db, (kb > 0 || t > 1) ? 1u : 0u);
                         }
                     }
+                    mma_commit(&empty_bar[s]);  // stage reusable once these MMAs have read it
                 }
-                mma_commit(&empty_bar[s]);  // stage s reusable once these MMAs have read it
+                mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
             }
-            mma_commit(done_bar);  // accumulators final once every issued MMA completes
         }
     } else {
         // epilogue warps 2..5 cover TMEM lane quarters (warp % 4)
         const int quarter = warp & 3;
-        const bool ok = mbar_wait(done_bar, 0, args.err, 4);
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
         const int ea = row_ok ? args.ea[row] : 0;
-        if (ok && !abort_flag) {
+        double *drow = args.D + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
+        const long long cstride = args.trans ? args.ldd : 1;
+        for (int p = 0; p < npass; ++p) {
+            const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int g0 = 2 + 2 * p, g1 = min(3 + 2 * p, S + 1);
+            if (ok && !abort_flag) {
 #pragma unroll 1
-            for (int c = 0; c < OZ_BN / 32; ++c) {
-                double acc[32];
+                for (int c = 0; c < OZ_BN / 32; ++c) {
+                    double acc[32];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 #pragma unroll 1
-                for (int g = S + 1; g >= 2; --g) {
-                    uint32_t v[32];
-                    const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(g - 2) * OZ_BN + c * 32;
-                    tmem_ld32(taddr, v);
-                    const double sc = ldexp(1.0, -7 * g);
+                    for (int g = g1; g >= g0; --g) {
+                        uint32_t v[32];
+                        const uint32_t taddr =
+                            tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(g - g0) * OZ_BN + c * 32;
+                        tmem_ld32(taddr, v);
+                        const double sc = ldexp(1.0, -7 * g);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
-                }
-                if (row_ok) {
-                    double *drow = args.D + (long long)row * args.ldd;
+                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                    }
+                    if (row_ok) {
+                        const bool add = (p > 0) || args.accumulate;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = n0 + c * 32 + j;
-                        if (col < args.n) {
-                            const double val = ldexp(acc[j], ea + args.eb[col]);
-                            drow[col] = args.accumulate ? drow[col] + val : val;
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = n0 + c * 32 + j;
+                            if (col < args.n) {
+                                const double val = ldexp(acc[j], ea + args.eb[col]);
+                                double *dp = drow + (long long)col * cstride;
+                                *dp = add ? *dp + val : val;
+                            }
                         }
                     }
                 }
+            } else {
+                break;
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(free_bar);  // this thread's reads of the pass's accumulators are done
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -292,21 +334,54 @@ __device__ double block_max(double v, double *sh) {
     return r;
 }
 
-// Rows of a real row-major matrix A (m x k, lda) -> slices [S][mpad][kpad] and ea[m].
-__global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const double *A, long long lda, int S,
-                                                           long long mpad, long long kpad, signed char *out, int *ea) {
+// Rows of a real matrix A (element (i, j) at A[i lda + j cs]) -> slices [S][mpad][kpad] and ea[m].
+__global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const double *A, long long lda, long long cs,
+                                                           int S, long long mpad, long long kpad, signed char *out,
+                                                           int *ea) {
     __shared__ double sh[SL_NT];
     const long long row = blockIdx.x;
     const double *a = A + row * lda;
     double mx = 0.0;
-    for (int j = threadIdx.x; j < k; j += SL_NT) mx = fmax(mx, fabs(a[j]));
+    for (int j = threadIdx.x; j < k; j += SL_NT) mx = fmax(mx, fabs(a[(long long)j * cs]));
     mx = block_max(mx, sh);
     const int e = exp_of_max(mx);
     if (threadIdx.x == 0) ea[row] = e;
     const long long stride = mpad * kpad;
     for (long long j = threadIdx.x; j < kpad; j += SL_NT) {
-        double x = (j < k) ? a[j] : 0.0;
+        double x = (j < k) ? a[j * cs] : 0.0;
         slice_value(x, e, S, out + row * kpad + j, stride);
+    }
+}
+
+// Columns of the spin-summed density P_w = rho_aa + rho_bb for the Coulomb term: column
+// c = 2 w + part holds part(rho_w[2p][2q] + rho_w[2p+1][2q+1]) at k = p n + q.
+__global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rho, int S, long long npad,
+                                                             long long kpad, signed char *out, int *eb) {
+    __shared__ double sh[SL_NT];
+    const long long c = blockIdx.x;
+    const int part = (int)(c & 1);
+    const long long w = c >> 1;
+    const int M = 2 * n;
+    const zc *R = rho + w * (long long)M * M;
+    const int k = n * n;
+    double mx = 0.0;
+    for (int e = threadIdx.x; e < k; e += SL_NT) {
+        int p = e / n, q = e - p * n;
+        zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
+        mx = fmax(mx, fabs(part ? v.y : v.x));
+    }
+    mx = block_max(mx, sh);
+    const int ex = exp_of_max(mx);
+    if (threadIdx.x == 0) eb[c] = ex;
+    const long long stride = npad * kpad;
+    for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
+        double x = 0.0;
+        if (e < k) {
+            int p = (int)(e / n), q = (int)(e - (long long)p * n);
+            zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
+            x = part ? v.y : v.x;
+        }
+        slice_value(x, ex, S, out + c * kpad + e, stride);
     }
 }
 
@@ -359,6 +434,8 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 int make_slice_map(CUtensorMap *map, const signed char *base, long long kpad, long long rows_pad, int S, int box_rows) {
+    // boxes of two slices; dimension 2 spans the S slices (a box reaching past slice S - 1 is
+    // zero-filled by the TMA unit and lands in the stage's spare slot)
     auto enc = get_encode();
     if (!enc) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
@@ -366,10 +443,10 @@ int make_slice_map(CUtensorMap *map, const signed char *base, long long kpad, lo
     }
     cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows_pad, (cuuint64_t)S};
     cuuint64_t strides[2] = {(cuuint64_t)kpad, (cuuint64_t)(kpad * rows_pad)};
-    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, (cuuint32_t)S};
+    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 2u};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char *>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -386,8 +463,13 @@ long long oz_pad_k(long long k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
 
 int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long rows_pad, signed char *out, int *ea,
                   cudaStream_t st) {
+    return oz_slice_rows_strided(m, k, A, lda, 1, S, rows_pad, out, ea, st);
+}
+
+int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long long cs, int S, long long rows_pad,
+                          signed char *out, int *ea, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    slice_rows_kernel<<<m, SL_NT, 0, st>>>(m, k, A, lda, S, rows_pad, oz_pad_k(k), out, ea);
+    slice_rows_kernel<<<m, SL_NT, 0, st>>>(m, k, A, lda, cs, S, rows_pad, oz_pad_k(k), out, ea);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
@@ -403,22 +485,37 @@ int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int 
     return PHF_OK;
 }
 
+int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st) {
+    const long long ncols = 2LL * b;
+    ProfScope prof(st, PROF_MEMORY);
+    slice_p_cols_kernel<<<(unsigned)ncols, SL_NT, 0, st>>>(n, rho, S, oz_pad_cols(ncols), oz_pad_k((long long)n * n),
+                                                           out, eb);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 int oz_stages(int S) {
-    const size_t stage = (size_t)S * (OZ_BM + OZ_BN) * OZ_BK;
+    const size_t stage = (size_t)oz_spad(S) * (OZ_BM + OZ_BN) * OZ_BK;
     const size_t budget = 227 * 1024 - 1024 - 256;
     int st = (int)(budget / stage);
-    return st > 4 ? 4 : st;
+    return st > 6 ? 6 : st;
 }
 
 size_t oz_smem_bytes(int S) {
     const int STAGES = oz_stages(S);
-    return 1024 + (size_t)STAGES * S * (OZ_BM + OZ_BN) * OZ_BK + (2 * STAGES + 1) * 8 + 16;
+    return 1024 + (size_t)STAGES * oz_spad(S) * (OZ_BM + OZ_BN) * OZ_BK + (2 * STAGES + 2) * 8 + 16;
 }
 
 // D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
 // k is split into passes short enough for exact int32 group sums; later passes add into D.
 int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
             double *D, long long ldd, int accumulate, int *err, cudaStream_t st) {
+    return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, accumulate, 0, err, st);
+}
+
+int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
+              double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st) {
     if (S < 1 || S > OZ_MAX_S) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
@@ -438,7 +535,7 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
     const long long kb_total = kpad / OZ_BK;
     const size_t smem = oz_smem_bytes(S);
     PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)(npad / OZ_BN), (unsigned)(mpad / OZ_BM), 1);
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // row tiles fastest
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;
@@ -452,6 +549,7 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
         a.D = D;
         a.ldd = ldd;
         a.accumulate = (kb0 > 0) ? 1 : accumulate;
+        a.trans = trans;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);

@@ -478,7 +478,9 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         if (p.chol && p.eri) {
             per += 2 * MM + 2 * n2 + p.L;                       // Rho, Gam, Pvec, Jvec, dvec
             if (p.prec == PHF_PREC_FP64) per += 8 * n2;         // Kin, Kvec
-            else per += 4 * n2 + (8 * n2 * p.slices) / sizeof(zc) + 1;  // Dk, int8 slices
+            else per += 4 * n2 + (8 * n2 * p.slices) / sizeof(zc) + 1  // Dk, exchange slices
+                        + (2 * n2 + 2 * (size_t)p.L) * p.slices / sizeof(zc) + 1    // Coulomb slices
+                        + p.L + n2;                                                // d^T, J pairs
         } else if (p.chol) {
             per += (size_t)p.L * N * N + (size_t)p.L * MN + p.L;
         } else {
@@ -536,6 +538,17 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.Bsl, bsl));
             PHF_CUDA(cudaMemset(p.Bsl, 0, bsl));
             PHF_TRY(p.arena.alloc(&p.eb, (size_t)oz_pad_cols(8 * (long long)b)));
+            const long long c2 = oz_pad_cols(2 * (long long)b);
+            const size_t psl = (size_t)p.slices * c2 * oz_pad_k((long long)n2);
+            const size_t dsl = (size_t)p.slices * c2 * oz_pad_k(p.L);
+            PHF_TRY(p.arena.alloc(&p.Psl, psl));
+            PHF_TRY(p.arena.alloc(&p.dsl, dsl));
+            PHF_CUDA(cudaMemset(p.Psl, 0, psl));
+            PHF_CUDA(cudaMemset(p.dsl, 0, dsl));
+            PHF_TRY(p.arena.alloc(&p.ePc, (size_t)c2));
+            PHF_TRY(p.arena.alloc(&p.edc, (size_t)c2));
+            PHF_TRY(p.arena.alloc(&p.dT, 2 * b * (size_t)p.L));
+            PHF_TRY(p.arena.alloc(&p.Jr, 2 * b * n2));
         }
     } else if (p.chol) {
         PHF_TRY(p.arena.alloc(&p.T, (size_t)p.L * bNN));
@@ -572,6 +585,17 @@ int build_exchange_matrix(PlanImpl &p) {
         PHF_TRY(p.arena.alloc(&p.ozerr, 1));
         PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
         PHF_TRY(oz_slice_rows((int)n2, (int)n2, EK, n2, p.slices, oz_pad_rows(n2), p.EKsl, p.ea, 0));
+        // Coulomb operands: B (L x n^2, rows of Bst) and B^T (n^2 x L, strided rows of Bst)
+        const size_t b1 = (size_t)p.slices * oz_pad_rows(L) * oz_pad_k(n2);
+        const size_t b2 = (size_t)p.slices * oz_pad_rows(n2) * oz_pad_k(L);
+        PHF_TRY(p.arena.alloc(&p.B1sl, b1));
+        PHF_TRY(p.arena.alloc(&p.B2sl, b2));
+        PHF_CUDA(cudaMemset(p.B1sl, 0, b1));
+        PHF_CUDA(cudaMemset(p.B2sl, 0, b2));
+        PHF_TRY(p.arena.alloc(&p.eB1, (size_t)oz_pad_rows(L)));
+        PHF_TRY(p.arena.alloc(&p.eB2, (size_t)oz_pad_rows(n2)));
+        PHF_TRY(oz_slice_rows_strided(L, (int)n2, p.Bst, n2, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
+        PHF_TRY(oz_slice_rows_strided((int)n2, L, p.Bst, 1, n2, p.slices, oz_pad_rows(n2), p.B2sl, p.eB2, 0));
     }
     PHF_CUDA(cudaDeviceSynchronize());
     p.EK = EK;  // kept for the FP64 back-end
@@ -586,11 +610,19 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
     PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0, vo(p.Rho, M, 1, MM),
                           nullptr, st));
-    PHF_TRY(launch_gather_p(n, bc, p.Rho, p.Pvec, b, st));
-    PHF_TRY(zgemm_strided(L, bc, (int)n2, 1, 1, Z1, vd(p.Bst, n2, 1), vz(p.Pvec, b, 1), Z0, vo(p.dvec, b, 1), nullptr,
-                          st));
-    PHF_TRY(zgemm_strided((int)n2, bc, L, 1, 1, Z1, vd(p.Bst, 1, n2), vz(p.dvec, b, 1), Z0, vo(p.Jvec, b, 1), nullptr,
-                          st));
+    if (p.prec == PHF_PREC_FP64) {
+        PHF_TRY(launch_gather_p(n, bc, p.Rho, p.Pvec, b, st));
+        PHF_TRY(zgemm_strided(L, bc, (int)n2, 1, 1, Z1, vd(p.Bst, n2, 1), vz(p.Pvec, b, 1), Z0, vo(p.dvec, b, 1),
+                              nullptr, st));
+        PHF_TRY(zgemm_strided((int)n2, bc, L, 1, 1, Z1, vd(p.Bst, 1, n2), vz(p.dvec, b, 1), Z0, vo(p.Jvec, b, 1),
+                              nullptr, st));
+    } else {
+        // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
+        PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
+        PHF_TRY(oz_gemm_t(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 0, 1, p.ozerr, st));
+        PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, st));
+        PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, 2LL * b, 0, 0, p.ozerr, st));
+    }
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
         PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
@@ -612,12 +644,12 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
                                   vo(p.Kvec, 4LL * b, 1), nullptr, st));
         }
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, p.Kvec, nullptr, 4LL * b, p.Gam, st));
+        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, nullptr, b, p.Kvec, nullptr, 4LL * b, p.Gam, st));
     } else {
         PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
         PHF_TRY(oz_gemm((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, 8LL * b, 0, p.ozerr, st));
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, p.Dk, 8LL * b, p.Gam, st));
+        PHF_TRY(launch_assemble_gamma(n, bc, nullptr, p.Jr, 2LL * b, nullptr, p.Dk, 8LL * b, p.Gam, st));
     }
     PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
                           st));

@@ -264,11 +264,12 @@ __global__ void gather_kin_kernel(int n, int b, const zc *rho, zc *Kin, long lon
     }
 }
 
-// Gamma_w[2i + sigma][2k + tau] = delta_{sigma tau} J[(i n + k) ldj + w] - K_{sigma tau}[(i, k), w]
+// Gamma_w[2i + sigma][2k + tau] = delta_{sigma tau} J[(i, k), w] - K_{sigma tau}[(i, k), w]
+// J from a complex array J[(i n + k) ldj + w] or real/imaginary pairs Jr[(i n + k) ldj + 2 w + part];
 // K from a complex array Kc[(i n + k) ldk + 4 w + st] or from real/imaginary pairs
 // Kr[(i n + k) ldk + 2 (4 w + st) + part].
-__global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, const zc *Kc, const double *Kr,
-                                      long long ldk, zc *Gam) {
+__global__ void assemble_gamma_kernel(int n, int b, const zc *J, const double *Jr, long long ldj, const zc *Kc,
+                                      const double *Kr, long long ldk, zc *Gam) {
     const int M = 2 * n;
     const long long tot = (long long)M * M * b;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
@@ -281,7 +282,7 @@ __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, 
         if (Kc) kv = Kc[ik * ldk + 4 * w + st];
         else kv = mkz(Kr[ik * ldk + 2 * (4 * w + st)], Kr[ik * ldk + 2 * (4 * w + st) + 1]);
         zc g = mkz(-kv.x, -kv.y);
-        if (sg == tu) g = g + J[ik * ldj + w];
+        if (sg == tu) g = g + (J ? J[ik * ldj + w] : mkz(Jr[ik * ldj + 2 * w], Jr[ik * ldj + 2 * w + 1]));
         Gam[e] = g;
     }
 }
@@ -453,10 +454,10 @@ int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaS
     return PHF_OK;
 }
 
-int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const zc *Kc, const double *Kr, long long ldk,
-                          zc *Gam, cudaStream_t st) {
+int launch_assemble_gamma(int n, int b, const zc *J, const double *Jr, long long ldj, const zc *Kc, const double *Kr,
+                          long long ldk, zc *Gam, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, ldj, Kc, Kr, ldk, Gam);
+    assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, Jr, ldj, Kc, Kr, ldk, Gam);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -138,6 +138,8 @@ struct OzArgs {
     long long ldd;
     int accumulate;      // D += result instead of D = result
     int trans;           // write D^T: element (i, j) at D[j * ldd + i]
+    long long dz;        // split-k: CTA z covers k-blocks [z kblocks, (z+1) kblocks) and writes D + z dz
+    int kb_total;        // k-blocks of this launch over all splits
     int *err;
 };
 
@@ -162,6 +164,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * OZ_BM, n0 = blockIdx.y * OZ_BN;
+    const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
+    const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
+    double *const Dz = args.D + (long long)blockIdx.z * args.dz;
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -183,7 +188,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
-    const int KB = args.kblocks;
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     if (abort_flag) break;
                     unsigned char *sa = smem + (size_t)s * stage_bytes;
                     mbar_arrive_expect_tx(&full_bar[s], bytes);
-                    const int kc = (args.kb0 + kb) * OZ_BK;
+                    const int kc = (args.kb0 + kz0 + kb) * OZ_BK;
                     for (int q = 0; q < npairs; ++q) {
                         tma_load_3d(&tmA, &full_bar[s], sa + (size_t)(2 * q) * a_slice, kc, m0, 2 * q);
                         tma_load_3d(&tmB, &full_bar[s], sa + a_bytes + (size_t)(2 * q) * b_slice, kc, n0, 2 * q);
@@ -251,7 +255,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
         const int ea = row_ok ? args.ea[row] : 0;
-        double *drow = args.D + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
+        double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
         const long long cstride = args.trans ? args.ldd : 1;
         for (int p = 0; p < npass; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 #pragma unroll 1
-                    for (int g = g1; g >= g0; --g) {
+                    for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
                         uint32_t v[32];
                         const uint32_t taddr =
                             tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(g - g0) * OZ_BN + c * 32;
@@ -514,6 +518,67 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
     return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, accumulate, 0, err, st);
 }
 
+namespace {
+__global__ void sum_splits_kernel(long long count, int nsplit, long long dz, const double *part, double *D) {
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256)
+    {
+        double s = 0.0;
+        for (int z = 0; z < nsplit; ++z) s += part[z * dz + i];
+        D[i] = s;
+    }
+}
+}  // namespace
+
+// Split-k variant for small outputs with long k: nsplit CTAs per output tile write partial
+// results to part (nsplit x (rows of D) x ldd), summed in split order into D.
+int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl,
+                   const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
+                   cudaStream_t st) {
+    const long long kpad = oz_pad_k(k), kb_total = kpad / OZ_BK;
+    const long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
+    if (nsplit <= 1 || kb_total > kb_pass || kb_total < 2 * nsplit)
+        return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, 0, trans, err, st);
+    const int stages = oz_stages(S);
+    CUtensorMap ta, tb;
+    const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
+    PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
+    PHF_TRY(make_slice_map(&tb, Bsl, kpad, npad, S, OZ_BN));
+    const long long rows = trans ? n : m;
+    const long long dz = rows * ldd;
+    OzArgs a;
+    a.m = m;
+    a.n = n;
+    a.kb0 = 0;
+    a.kblocks = (int)((kb_total + nsplit - 1) / nsplit);
+    a.kb_total = (int)kb_total;
+    a.S = S;
+    a.stages = stages;
+    a.ea = ea;
+    a.eb = eb;
+    a.D = part;
+    a.ldd = ldd;
+    a.accumulate = 0;
+    a.trans = trans;
+    a.dz = dz;
+    a.err = err;
+    const size_t smem = oz_smem_bytes(S);
+    PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), (unsigned)nsplit);
+    {
+        ProfScope prof(st, PROF_JK);
+        ozaki_i8_gemm_kernel<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+    }
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    {
+        ProfScope prof(st, PROF_MEMORY);
+        sum_splits_kernel<<<148 * 4, 256, 0, st>>>(dz, nsplit, dz, part, D);
+    }
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st) {
     if (S < 1 || S > OZ_MAX_S) {
@@ -550,6 +615,8 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.ldd = ldd;
         a.accumulate = (kb0 > 0) ? 1 : accumulate;
         a.trans = trans;
+        a.dz = 0;
+        a.kb_total = a.kblocks;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);

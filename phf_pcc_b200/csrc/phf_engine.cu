@@ -244,6 +244,7 @@ int validate(const phf_plan_desc *d) {
 
 namespace {
 int build_exchange_matrix(PlanImpl &p);
+constexpr int kDSplit = 4;  // split-k of the Coulomb GEMM d = B vec P (small output, k = n^2)
 }  // namespace
 
 int plan_create(const phf_plan_desc *d, phf_plan **out) {
@@ -548,6 +549,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.ePc, (size_t)c2));
             PHF_TRY(p.arena.alloc(&p.edc, (size_t)c2));
             PHF_TRY(p.arena.alloc(&p.dT, 2 * b * (size_t)p.L));
+            PHF_TRY(p.arena.alloc(&p.dpart, (size_t)kDSplit * 2 * b * (size_t)p.L));
             PHF_TRY(p.arena.alloc(&p.Jr, 2 * b * n2));
         }
     } else if (p.chol) {
@@ -619,9 +621,11 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     } else {
         // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
         PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
-        PHF_TRY(oz_gemm_t(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 0, 1, p.ozerr, st));
+        PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
+                               p.ozerr, st));
         PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, st));
-        PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, 2LL * b, 0, 0, p.ozerr, st));
+        // J^T (2 bc x n^2): transposed output keeps the epilogue's FP64 stores coalesced
+        PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, n2, 0, 1, p.ozerr, st));
     }
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
@@ -644,12 +648,13 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
                                   vo(p.Kvec, 4LL * b, 1), nullptr, st));
         }
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, nullptr, b, p.Kvec, nullptr, 4LL * b, p.Gam, st));
+        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st));
     } else {
         PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
-        PHF_TRY(oz_gemm((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, 8LL * b, 0, p.ozerr, st));
+        // K^T (8 bc x n^2), transposed for coalesced epilogue stores
+        PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, n2, 0, 1, p.ozerr, st));
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, nullptr, p.Jr, 2LL * b, nullptr, p.Dk, 8LL * b, p.Gam, st));
+        PHF_TRY(launch_assemble_gamma(n, bc, nullptr, 0, p.Jr, 1, n2, nullptr, 0, p.Dk, 1, n2, p.Gam, st));
     }
     PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
                           st));

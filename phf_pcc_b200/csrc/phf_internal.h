@@ -79,8 +79,9 @@ int launch_localg(int MM, int nterm, const zc *coef_g, const zc *coef_r, const l
 
 int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStream_t st);
 int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st);
-int launch_assemble_gamma(int n, int b, const zc *J, const double *Jr, long long ldj, const zc *Kc, const double *Kr,
-                          long long ldk, zc *Gam, cudaStream_t st);
+int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
+                          const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
+                          cudaStream_t st);
 
 // ozaki_i8.cu: FP64-accurate GEMM from int8 slices on tcgen05
 long long oz_pad_rows(long long m);
@@ -94,6 +95,9 @@ int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int 
 int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st);
+int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl,
+                   const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
+                   cudaStream_t st);
 int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
             double *D, long long ldd, int accumulate, int *err, cudaStream_t st);
 
@@ -155,7 +159,7 @@ struct PlanImpl {
     // Coulomb term on the tensor cores: d = B vec P, J = B^T d (B = Cholesky vectors as L x n^2)
     signed char *B1sl = nullptr, *B2sl = nullptr, *Psl = nullptr, *dsl = nullptr;
     int *eB1 = nullptr, *eB2 = nullptr, *ePc = nullptr, *edc = nullptr;
-    double *dT = nullptr, *Jr = nullptr;
+    double *dT = nullptr, *Jr = nullptr, *dpart = nullptr;  // dpart: split-k partials of d^T
     SplitWork split;  // tensor-core path workspace (phf_split.cu)
     ~PlanImpl();
 };

@@ -265,11 +265,13 @@ __global__ void gather_kin_kernel(int n, int b, const zc *rho, zc *Kin, long lon
 }
 
 // Gamma_w[2i + sigma][2k + tau] = delta_{sigma tau} J[(i, k), w] - K_{sigma tau}[(i, k), w]
-// J from a complex array J[(i n + k) ldj + w] or real/imaginary pairs Jr[(i n + k) ldj + 2 w + part];
-// K from a complex array Kc[(i n + k) ldk + 4 w + st] or from real/imaginary pairs
-// Kr[(i n + k) ldk + 2 (4 w + st) + part].
-__global__ void assemble_gamma_kernel(int n, int b, const zc *J, const double *Jr, long long ldj, const zc *Kc,
-                                      const double *Kr, long long ldk, zc *Gam) {
+// J: complex J[(i n + k) ldj + w], or real/imaginary pairs with element (ik, c) of Jr at
+//    Jr[ik jrs + c jcs], c = 2 w + part;
+// K: complex Kc[(i n + k) ldk + 4 w + st], or pairs with element (ik, c) of Kr at Kr[ik krs + c kcs],
+//    c = 2 (4 w + st) + part.
+__global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs,
+                                      long long jcs, const zc *Kc, long long ldk, const double *Kr, long long krs,
+                                      long long kcs, zc *Gam) {
     const int M = 2 * n;
     const long long tot = (long long)M * M * b;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
@@ -279,10 +281,17 @@ __global__ void assemble_gamma_kernel(int n, int b, const zc *J, const double *J
         long long ik = (long long)i * n + k;
         int st = sg * 2 + tu;
         zc kv;
-        if (Kc) kv = Kc[ik * ldk + 4 * w + st];
-        else kv = mkz(Kr[ik * ldk + 2 * (4 * w + st)], Kr[ik * ldk + 2 * (4 * w + st) + 1]);
+        if (Kc) {
+            kv = Kc[ik * ldk + 4 * w + st];
+        } else {
+            const long long cc = 2 * (4 * w + st);
+            kv = mkz(Kr[ik * krs + cc * kcs], Kr[ik * krs + (cc + 1) * kcs]);
+        }
         zc g = mkz(-kv.x, -kv.y);
-        if (sg == tu) g = g + (J ? J[ik * ldj + w] : mkz(Jr[ik * ldj + 2 * w], Jr[ik * ldj + 2 * w + 1]));
+        if (sg == tu) {
+            if (J) g = g + J[ik * ldj + w];
+            else g = g + mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
+        }
         Gam[e] = g;
     }
 }
@@ -454,10 +463,12 @@ int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaS
     return PHF_OK;
 }
 
-int launch_assemble_gamma(int n, int b, const zc *J, const double *Jr, long long ldj, const zc *Kc, const double *Kr,
-                          long long ldk, zc *Gam, cudaStream_t st) {
+int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
+                          const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
+                          cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, Jr, ldj, Kc, Kr, ldk, Gam);
+    assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, ldj, Jr, jrs, jcs, Kc, ldk, Kr, krs, kcs,
+                                                                    Gam);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -118,6 +118,10 @@ typedef struct {
     int fp64_library_gemm;                    /* PHF_PREC_FP64, spatial-ERI form: 1 = run the exchange GEMM
                                                  with cuBLAS DGEMM instead of this library's FP64 kernel
                                                  (a library-tuned FP64 comparison form) */
+    int point_begin, point_end;               /* evaluate only grid points [point_begin, point_end) of the
+                                                 flattened order (il*ngrid[1] + iy)*npg + ipg; 0, 0 = all.
+                                                 Partial sums over disjoint ranges add up to the full sums
+                                                 (the rank split of PHFTools.f90:53-57) */
 } phf_plan_desc;
 
 int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);

@@ -44,6 +44,8 @@ class phf_plan_desc(ctypes.Structure):
         ("jk_form", ctypes.c_int),
         ("gradient_mode", ctypes.c_int),
         ("fp64_library_gemm", ctypes.c_int),
+        ("point_begin", ctypes.c_int),
+        ("point_end", ctypes.c_int),
     ]
 
 

@@ -174,8 +174,8 @@ class Plan:
 
     def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
                  rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
-                 workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False, npg=None,
-                 ncipg=None, nso=None):
+                 workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False,
+                 point_range=None, npg=None, ncipg=None, nso=None):
         self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
                         sp, npg, ncipg, nso)
         g = self._g
@@ -200,6 +200,8 @@ class Plan:
         d.jk_form = {"auto": 0, "eri": 1, "factorized": 2}[jk_form]
         d.gradient_mode = {"reference": 0, "exact": 1}[gradient]
         d.fp64_library_gemm = 1 if fp64_library_gemm else 0
+        if point_range is not None:
+            d.point_begin, d.point_end = int(point_range[0]), int(point_range[1])
         self.gradient = gradient
         self.precision = precision
         handle = ctypes.c_void_p()

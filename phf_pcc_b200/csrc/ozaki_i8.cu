@@ -14,19 +14,22 @@
 // (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
 // fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
 //
-// Kernel shape (one CTA per 128 x 256 output tile, 6 warps), with row tiles fastest in the grid so
-// that the CTAs in flight share B column tiles through L2:
-//   warp 0      TMA producer: per 32-byte k-block, boxes of two slices of the A tile (2 x 128 x 32 B)
-//               and of the B tile (2 x 256 x 32 B), SWIZZLE_32B, into a ring of stages guarded by
-//               full/empty mbarriers
-//   warp 1      TMEM allocation (512 columns = two 128 x 256 int32 accumulators) and the
-//               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of two
-//               groups over the whole k range (pass p needs slices 1..2p+2 only); within a stage
-//               every slice pair of the pass's groups is one 128 x 256 x 32 MMA
-//   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of both groups, int32 -> FP64,
-//               2^{-7g} and 2^{ea+eb} scaling, store (first pass) or add into D; then release TMEM
-// With N = 256 an MMA reads 4 KB of A and 8 KB of B from shared memory per 1M MACs, within the
-// shared-memory bandwidth at the full int8 rate (a 64-wide tile needs 1.5x more than available).
+// Slice layout in global memory: slices are grouped four at a time and interleaved per 32-element
+// k-block, so that one 128-byte row segment holds the same 32 k-elements of four slices:
+//   byte ((g * rows_pad + row) * KB + kb) * 128 + q * 32 + kk   for slice t = 4 g + q, k = 32 kb + kk.
+// A TMA box of 128-byte rows then carries four slices at once, and the MMA picks slice q of a
+// stage by a +32 q byte offset of its SWIZZLE_128B K-major descriptor.
+//
+// Kernel shape (one CTA per 128 x 128 output tile, 6 warps), row tiles fastest in the grid so that
+// the CTAs in flight share B column tiles through L2:
+//   warp 0      TMA producer: per 32-element k-block one 128 x 128 B box of A and of B per slice
+//               group the current pass needs, into a ring of stages (full/empty mbarriers)
+//   warp 1      TMEM allocation (512 columns = four 128 x 128 int32 accumulators) and the
+//               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of four
+//               groups over the whole k range; within a stage every slice pair of the pass's
+//               groups is one 128 x 128 x 32 MMA
+//   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of the pass's groups, int32 ->
+//               FP64, 2^{-7g} and 2^{ea+eb} scaling, store (first pass) or add into D
 // Every mbarrier wait gives up after ~2^31 clock cycles, sets *err and lets the CTA finish.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -41,7 +44,8 @@ namespace phf {
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 256, OZ_BK = 32;  // tile rows, tile columns, k-block bytes
+constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 32;  // tile rows, tile columns, k-block (int8 elements)
+constexpr int OZ_GP = 4;                             // slice groups per 128-byte row, accumulators per pass
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_MAX_S = 7;
 
@@ -91,18 +95,18 @@ __device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, SWIZZLE_32B (8 rows x 32 B atoms, SBO = 256 B).
-__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr) {
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B (8 rows x 128 B atoms, SBO = 1024 B).
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
     d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(256 >> 4) << 32;                  // stride byte offset: 8 rows x 32 B
+    d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset: 8 rows x 128 B
     d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
-    d |= (uint64_t)6 << 61;                           // layout: SWIZZLE_32B
+    d |= (uint64_t)2 << 61;                           // layout: SWIZZLE_128B
     return d;
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 256.
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 128.
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
@@ -143,18 +147,18 @@ struct OzArgs {
     int *err;
 };
 
-// slices held per stage (an even count: slices are loaded in pairs)
-__host__ __device__ __forceinline__ int oz_spad(int S) { return (S + 1) & ~1; }
+// slice groups of four (one 128-byte row segment per k-block each)
+__host__ __device__ __forceinline__ int oz_ngroups(int S) { return (S + OZ_GP - 1) / OZ_GP; }
 
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = args.S, STAGES = args.stages, SP = oz_spad(S);
-    const uint32_t a_slice = OZ_BM * OZ_BK, b_slice = OZ_BN * OZ_BK;  // 4 KB, 8 KB
-    const uint32_t a_bytes = (uint32_t)SP * a_slice;
-    const uint32_t stage_bytes = (uint32_t)SP * (a_slice + b_slice);
-    const int npass = (S + 1) / 2;
+    const int S = args.S, STAGES = args.stages, NG = oz_ngroups(S);
+    const uint32_t a_grp = OZ_BM * 128, b_grp = OZ_BN * 128;  // 16 KB each: 4 slices x 32 k-elements per row
+    const uint32_t a_bytes = (uint32_t)NG * a_grp;
+    const uint32_t stage_bytes = (uint32_t)NG * (a_grp + b_grp);
+    const int npass = (S + OZ_GP - 1) / OZ_GP;
     uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)STAGES * stage_bytes);
     uint64_t *empty_bar = full_bar + STAGES;
     uint64_t *pass_bar = empty_bar + STAGES;  // MMAs of a pass complete
@@ -193,8 +197,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         if (lane == 0) {  // TMA producer
             int it = 0;
             for (int p = 0; p < npass && !abort_flag; ++p) {
-                const int npairs = p + 1;  // slice pairs needed by groups 2p+2, 2p+3
-                const uint32_t bytes = (uint32_t)npairs * 2 * (a_slice + b_slice);
+                const int ngl = p + 1;  // slice groups needed by groups 4p+2 .. 4p+5 (slices up to 4p+4)
+                const uint32_t bytes = (uint32_t)ngl * (a_grp + b_grp);
                 for (int kb = 0; kb < KB; ++kb, ++it) {
                     const int s = it % STAGES, use = it / STAGES;
                     if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
@@ -204,10 +208,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     if (abort_flag) break;
                     unsigned char *sa = smem + (size_t)s * stage_bytes;
                     mbar_arrive_expect_tx(&full_bar[s], bytes);
-                    const int kc = (args.kb0 + kz0 + kb) * OZ_BK;
-                    for (int q = 0; q < npairs; ++q) {
-                        tma_load_3d(&tmA, &full_bar[s], sa + (size_t)(2 * q) * a_slice, kc, m0, 2 * q);
-                        tma_load_3d(&tmB, &full_bar[s], sa + a_bytes + (size_t)(2 * q) * b_slice, kc, n0, 2 * q);
+                    const int kc = (args.kb0 + kz0 + kb) * 128;  // byte offset of the k-block in a row
+                    for (int q = 0; q < ngl; ++q) {
+                        tma_load_3d(&tmA, &full_bar[s], sa + (size_t)q * a_grp, kc, m0, q);
+                        tma_load_3d(&tmB, &full_bar[s], sa + a_bytes + (size_t)q * b_grp, kc, n0, q);
                     }
                 }
             }
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
-                const int g0 = 2 + 2 * p, g1 = min(3 + 2 * p, S + 1);
+                const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
                 for (int kb = 0; kb < KB; ++kb, ++it) {
                     const int s = it % STAGES, use = it / STAGES;
                     if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
@@ -239,9 +243,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         const uint32_t dcol = tmem_base + (uint32_t)(g - g0) * OZ_BN;
                         for (int t = 1; t < g; ++t) {
                             const int u = g - t;
-                            const uint64_t da = sdesc_sw32(sa + (uint32_t)(t - 1) * a_slice);
-                            const uint64_t db = sdesc_sw32(sb + (uint32_t)(u - 1) * b_slice);
-                            mma_i8(dcol, da, db, (kb > 0 || t > 1) ? 1u : 0u);
+                            const uint32_t ao = (uint32_t)((t - 1) / OZ_GP) * a_grp + (uint32_t)((t - 1) % OZ_GP) * 32;
+                            const uint32_t bo = (uint32_t)((u - 1) / OZ_GP) * b_grp + (uint32_t)((u - 1) % OZ_GP) * 32;
+                            mma_i8(dcol, sdesc_sw128(sa + ao), sdesc_sw128(sb + bo), (kb > 0 || t > 1) ? 1u : 0u);
                         }
                     }
                     mma_commit(&empty_bar[s]);  // stage reusable once these MMAs have read it
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int p = 0; p < npass; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int g0 = 2 + 2 * p, g1 = min(3 + 2 * p, S + 1);
+            const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
             if (ok && !abort_flag) {
 #pragma unroll 1
                 for (int c = 0; c < OZ_BN / 32; ++c) {
@@ -313,14 +317,18 @@ __device__ __forceinline__ int exp_of_max(double mx) {
     return e;
 }
 
-__device__ __forceinline__ void slice_value(double x, int e, int S, signed char *out, long long stride) {
+// Slices of x (scaled by 2^-e) for element k of a row: row_base points at (group 0, row, k-block 0);
+// group_stride = rows_pad * KB * 128 bytes (see the layout at the top of the file).
+__device__ __forceinline__ void slice_value(double x, int e, int S, signed char *row_base, long long group_stride,
+                                            long long k) {
     double r = ldexp(x, -e);
+    signed char *base = row_base + (k >> 5) * 128 + (k & 31);
     for (int t = 0; t < S; ++t) {
         r *= 128.0;
         double a = (t + 1 < S) ? trunc(r) : rint(r);
         a = fmin(127.0, fmax(-127.0, a));
         r -= a;
-        out[(long long)t * stride] = (signed char)(int)a;
+        base[(long long)(t / OZ_GP) * group_stride + (t % OZ_GP) * 32] = (signed char)(int)a;
     }
 }
 
@@ -350,10 +358,10 @@ __global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const d
     mx = block_max(mx, sh);
     const int e = exp_of_max(mx);
     if (threadIdx.x == 0) ea[row] = e;
-    const long long stride = mpad * kpad;
+    const long long gstride = mpad * kpad * OZ_GP;
     for (long long j = threadIdx.x; j < kpad; j += SL_NT) {
         double x = (j < k) ? a[j * cs] : 0.0;
-        slice_value(x, e, S, out + row * kpad + j, stride);
+        slice_value(x, e, S, out + row * kpad * OZ_GP, gstride, j);
     }
 }
 
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
     mx = block_max(mx, sh);
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
-    const long long stride = npad * kpad;
+    const long long gstride = npad * kpad * OZ_GP;
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
         if (e < k) {
@@ -385,7 +393,7 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
             zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
             x = part ? v.y : v.x;
         }
-        slice_value(x, ex, S, out + c * kpad + e, stride);
+        slice_value(x, ex, S, out + c * kpad * OZ_GP, gstride, e);
     }
 }
 
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
     mx = block_max(mx, sh);
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
-    const long long stride = npad * kpad;
+    const long long gstride = npad * kpad * OZ_GP;
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
         if (e < k) {
@@ -419,7 +427,7 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
             zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
             x = part ? v.y : v.x;
         }
-        slice_value(x, ex, S, out + c * kpad + e, stride);
+        slice_value(x, ex, S, out + c * kpad * OZ_GP, gstride, e);
     }
 }
 
@@ -438,19 +446,20 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 int make_slice_map(CUtensorMap *map, const signed char *base, long long kpad, long long rows_pad, int S, int box_rows) {
-    // boxes of two slices; dimension 2 spans the S slices (a box reaching past slice S - 1 is
-    // zero-filled by the TMA unit and lands in the stage's spare slot)
+    // dimension 0: bytes of a row of one slice group (kpad/32 k-blocks x 128 B), dimension 1: rows,
+    // dimension 2: slice groups; a box is one 128-byte k-block segment of box_rows rows
     auto enc = get_encode();
     if (!enc) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
         return PHF_ERR_CUDA;
     }
-    cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows_pad, (cuuint64_t)S};
-    cuuint64_t strides[2] = {(cuuint64_t)kpad, (cuuint64_t)(kpad * rows_pad)};
-    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 2u};
+    const long long rowb = kpad * OZ_GP;
+    cuuint64_t dims[3] = {(cuuint64_t)rowb, (cuuint64_t)rows_pad, (cuuint64_t)oz_ngroups(S)};
+    cuuint64_t strides[2] = {(cuuint64_t)rowb, (cuuint64_t)(rowb * rows_pad)};
+    cuuint32_t box[3] = {128u, (cuuint32_t)box_rows, 1u};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char *>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -499,8 +508,12 @@ int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *e
     return PHF_OK;
 }
 
+size_t oz_slice_bytes(long long rows_pad, long long k, int S) {
+    return (size_t)oz_ngroups(S) * OZ_GP * (size_t)rows_pad * (size_t)oz_pad_k(k);
+}
+
 int oz_stages(int S) {
-    const size_t stage = (size_t)oz_spad(S) * (OZ_BM + OZ_BN) * OZ_BK;
+    const size_t stage = (size_t)oz_ngroups(S) * (OZ_BM + OZ_BN) * 128;
     const size_t budget = 227 * 1024 - 1024 - 256;
     int st = (int)(budget / stage);
     return st > 6 ? 6 : st;
@@ -508,7 +521,7 @@ int oz_stages(int S) {
 
 size_t oz_smem_bytes(int S) {
     const int STAGES = oz_stages(S);
-    return 1024 + (size_t)STAGES * oz_spad(S) * (OZ_BM + OZ_BN) * OZ_BK + (2 * STAGES + 2) * 8 + 16;
+    return 1024 + (size_t)STAGES * oz_ngroups(S) * (OZ_BM + OZ_BN) * 128 + (2 * STAGES + 2) * 8 + 16;
 }
 
 // D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
@@ -643,7 +656,7 @@ extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA
         return PHF_ERR_ARG;
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n), kp = oz_pad_k(k);
+    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n);
     signed char *As = nullptr, *Bs = nullptr;
     int *ea = nullptr, *eb = nullptr, *err = nullptr;
     int status = PHF_OK;
@@ -655,14 +668,15 @@ extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA
             status = PHF_ERR_OOM;
         }
     };
-    al((void **)&As, (size_t)slices * mp * kp);
-    al((void **)&Bs, (size_t)slices * np * kp);
+    const size_t asz = oz_slice_bytes(mp, k, slices), bsz = oz_slice_bytes(np, k, slices);
+    al((void **)&As, asz);
+    al((void **)&Bs, bsz);
     al((void **)&ea, mp * sizeof(int));
     al((void **)&eb, np * sizeof(int));
     al((void **)&err, sizeof(int));
     if (status == PHF_OK) {
-        cudaMemsetAsync(As, 0, (size_t)slices * mp * kp, st);
-        cudaMemsetAsync(Bs, 0, (size_t)slices * np * kp, st);
+        cudaMemsetAsync(As, 0, asz, st);
+        cudaMemsetAsync(Bs, 0, bsz, st);
         cudaMemsetAsync(err, 0, sizeof(int), st);
         status = oz_slice_rows(m, k, dA, lda, slices, mp, As, ea, st);
         if (status == PHF_OK) status = oz_slice_rows(n, k, dBt, ldb, slices, np, Bs, eb, st);

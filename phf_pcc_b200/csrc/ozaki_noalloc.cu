@@ -61,8 +61,8 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 extern "C" size_t phf_ozaki_dgemm_noalloc_scratch_bytes(int m, int n, int k, int slices) {
     using namespace phf;
-    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n), kp = oz_pad_k(k);
-    return align256((size_t)slices * mp * kp) + align256((size_t)slices * np * kp) + align256(mp * sizeof(int)) +
+    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n);
+    return align256(oz_slice_bytes(mp, k, slices)) + align256(oz_slice_bytes(np, k, slices)) + align256(mp * sizeof(int)) +
            align256(np * sizeof(int)) + align256(sizeof(int));
 }
 
@@ -85,8 +85,8 @@ extern "C" int phf_ozaki_dgemm_noalloc(int m, int n, int k, int slices, const do
     unsigned char *base = nullptr;
     PHF_TRY(scratch_address(&base));
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n), kp = oz_pad_k(k);
-    const size_t a_bytes = (size_t)slices * mp * kp, b_bytes = (size_t)slices * np * kp;
+    const long long mp = oz_pad_rows(m), np = oz_pad_cols(n);
+    const size_t a_bytes = oz_slice_bytes(mp, k, slices), b_bytes = oz_slice_bytes(np, k, slices);
     signed char *As = reinterpret_cast<signed char *>(base);
     signed char *Bs = reinterpret_cast<signed char *>(base + align256(a_bytes));
     int *ea = reinterpret_cast<int *>(base + align256(a_bytes) + align256(b_bytes));

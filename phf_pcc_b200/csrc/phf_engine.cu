@@ -287,6 +287,16 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.ny = d->ngrid[1];
     p.npg = d->npg;
     p.nomega = p.nl * p.ny * p.npg;
+    p.wbeg = 0;
+    p.wend = p.nomega;
+    if (d->point_begin != 0 || d->point_end != 0) {
+        if (d->point_begin < 0 || d->point_end > p.nomega || d->point_begin >= d->point_end) {
+            set_error(PHF_ERR_ARG, "point range outside [0, number of grid points)");
+            return PHF_ERR_ARG;
+        }
+        p.wbeg = d->point_begin;
+        p.wend = d->point_end;
+    }
     p.nci = d->nci;
     p.ncisp = d->ncisp;
     p.ncipg = d->ncipg;
@@ -492,7 +502,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         per += split_bytes_per_point(p);
         long long bmax = (long long)(budget / std::max<size_t>(per, 1));
         bmax = std::max<long long>(1, std::min<long long>(bmax, 1024));
-        p.b = (int)std::min<long long>(bmax, p.nomega);
+        p.b = (int)std::min<long long>(bmax, p.wend - p.wbeg);
         // whole Lebedev-point blocks (ny npg points sharing R1[il]) per chunk when they fit
         const int blk = p.ny * p.npg;
         if (p.b >= blk) p.b = (p.b / blk) * blk;
@@ -535,13 +545,13 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.Kvec, 4 * b * n2));
         } else {
             PHF_TRY(p.arena.alloc(&p.Dk, 8 * b * n2));
-            const size_t bsl = (size_t)p.slices * oz_pad_cols(8 * (long long)b) * oz_pad_k((long long)n2);
+            const size_t bsl = oz_slice_bytes(oz_pad_cols(8 * (long long)b), (long long)n2, p.slices);
             PHF_TRY(p.arena.alloc(&p.Bsl, bsl));
             PHF_CUDA(cudaMemset(p.Bsl, 0, bsl));
             PHF_TRY(p.arena.alloc(&p.eb, (size_t)oz_pad_cols(8 * (long long)b)));
             const long long c2 = oz_pad_cols(2 * (long long)b);
-            const size_t psl = (size_t)p.slices * c2 * oz_pad_k((long long)n2);
-            const size_t dsl = (size_t)p.slices * c2 * oz_pad_k(p.L);
+            const size_t psl = oz_slice_bytes(c2, (long long)n2, p.slices);
+            const size_t dsl = oz_slice_bytes(c2, p.L, p.slices);
             PHF_TRY(p.arena.alloc(&p.Psl, psl));
             PHF_TRY(p.arena.alloc(&p.dsl, dsl));
             PHF_CUDA(cudaMemset(p.Psl, 0, psl));
@@ -580,7 +590,7 @@ int build_exchange_matrix(PlanImpl &p) {
     View Bv = vd(p.Bst, n2, 1, n, 0);
     PHF_TRY(zgemm_strided(n, n, L, n, n, Z1, vd(p.Bst, 1, n2, 0, n), Bv, Z0, o, nullptr, 0));
     if (p.prec == PHF_PREC_OZAKI_I8) {
-        const size_t bytes = (size_t)p.slices * oz_pad_rows(n2) * oz_pad_k(n2);
+        const size_t bytes = oz_slice_bytes(oz_pad_rows(n2), n2, p.slices);
         PHF_TRY(p.arena.alloc(&p.EKsl, bytes));
         PHF_CUDA(cudaMemset(p.EKsl, 0, bytes));
         PHF_TRY(p.arena.alloc(&p.ea, (size_t)oz_pad_rows(n2)));
@@ -588,8 +598,8 @@ int build_exchange_matrix(PlanImpl &p) {
         PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
         PHF_TRY(oz_slice_rows((int)n2, (int)n2, EK, n2, p.slices, oz_pad_rows(n2), p.EKsl, p.ea, 0));
         // Coulomb operands: B (L x n^2, rows of Bst) and B^T (n^2 x L, strided rows of Bst)
-        const size_t b1 = (size_t)p.slices * oz_pad_rows(L) * oz_pad_k(n2);
-        const size_t b2 = (size_t)p.slices * oz_pad_rows(n2) * oz_pad_k(L);
+        const size_t b1 = oz_slice_bytes(oz_pad_rows(L), n2, p.slices);
+        const size_t b2 = oz_slice_bytes(oz_pad_rows(n2), L, p.slices);
         PHF_TRY(p.arena.alloc(&p.B1sl, b1));
         PHF_TRY(p.arena.alloc(&p.B2sl, b2));
         PHF_CUDA(cudaMemset(p.B1sl, 0, b1));
@@ -716,8 +726,8 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
         PHF_TRY(zgemm_strided(L * n, 2 * N, n, 1, 1, Z1, vd(p.Bst, n, 1), vz(p.bra, 2 * N, 1), Z0, vo(p.V, 2 * N, 1),
                               nullptr, st));
     }
-    for (int w0 = 0; w0 < p.nomega; w0 += b) {
-        const int bc = std::min(b, p.nomega - w0);
+    for (int w0 = p.wbeg; w0 < p.wend; w0 += b) {
+        const int bc = std::min(b, p.wend - w0);
         // Y_w = R1[il] T2[iy, ig]: one (M x M) x (M x ny npg N) product per Lebedev point when the
         // chunk holds whole blocks of ny npg points, else per point
         const int blk = p.ny * p.npg;

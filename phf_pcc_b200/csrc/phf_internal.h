@@ -87,6 +87,7 @@ int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double
 long long oz_pad_rows(long long m);
 long long oz_pad_cols(long long n);
 long long oz_pad_k(long long k);
+size_t oz_slice_bytes(long long rows_pad, long long k, int S);  // bytes of an operand's int8 slices
 int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long rows_pad, signed char *out, int *ea,
                   cudaStream_t st);
 int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long long cs, int S, long long rows_pad,
@@ -118,6 +119,7 @@ struct PlanImpl {
     int library_gemm = 0;            // FP64 exchange GEMM through cuBLAS (comparison form)
     void *cublas = nullptr;          // cublasHandle_t when library_gemm
     int nl = 0, ny = 0, npg = 0, nomega = 0;
+    int wbeg = 0, wend = 0;          // grid points evaluated: [wbeg, wend)
     int nci = 0, ncisp = 0, ncipg = 0, cmplxconj = 1, qj = 0, sp = 1, nb = 0;
     std::vector<int> perm;           // working index -> reference index
     std::vector<cd> ref_host;        // Ref row-major (reference order)

@@ -162,3 +162,26 @@ def test_eval_device_matches_oracle():
     R_mo = c["Ref"].conj().T @ (yr[0] @ C.conj().T) @ c["Ref"]
     assert _close(hs[0, 0], c["Hmat"][0, 0]) and _close(hs[0, 1], c["Smat"][0, 0])
     assert _close(G_mo, c["Gradmat"][0, 0]) and _close(R_mo, c["Rdmmat"][0, 0])
+
+
+def test_point_range_plans_sum_to_the_full_grid():
+    """The rank split: plans over disjoint point blocks add up to the full-grid sums."""
+    import torch
+
+    from phf_pcc_b200.distributed import point_range
+
+    p = synth.make_problem(12, 6, 30, ngrid=(14, 5), seed=9, pg="C2v")
+    kw = p.grid_kwargs()
+    akw = dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+               r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+               roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+    C = torch.from_numpy(p.C).cuda()
+    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, **akw) as full:
+        ref = [t.clone() for t in full.eval_device(C)]
+    parts = []
+    for r in range(3):
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, point_range=point_range(p.grid.npoints, r, 3), **akw) as pl:
+            parts.append([t.clone() for t in pl.eval_device(C)])
+    for i in range(3):
+        tot = parts[0][i] + parts[1][i] + parts[2][i]
+        assert torch.allclose(tot, ref[i], rtol=0, atol=1e-12 * float(ref[i].abs().max()))

@@ -23,13 +23,16 @@
 // Kernel shape (one CTA per 128 x 128 output tile, 6 warps), row tiles fastest in the grid so that
 // the CTAs in flight share B column tiles through L2:
 //   warp 0      TMA producer: per 32-element k-block one 128 x 128 B box of A and of B per slice
-//               group the current pass needs, into a ring of stages (full/empty mbarriers)
+//               group the current pass needs, into a ring of six 32 KB slots (full/empty mbarriers)
 //   warp 1      TMEM allocation (512 columns = four 128 x 128 int32 accumulators) and the
 //               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of four
-//               groups over the whole k range; within a stage every slice pair of the pass's
-//               groups is one 128 x 128 x 32 MMA
+//               groups over the whole k range; per k-block every slice pair of the pass's groups
+//               is one 128 x 128 x 32 MMA
 //   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of the pass's groups, int32 ->
-//               FP64, 2^{-7g} and 2^{ea+eb} scaling, store (first pass) or add into D
+//               FP64 with 2^{-7g} scaling.  For S <= 6 the first pass's FP64 sums are parked in
+//               TMEM (columns 0..255, where groups 2 and 3 were) and the second pass, accumulating
+//               in columns 256..511, adds them before the single 2^{ea+eb}-scaled store to D;
+//               for S = 7 the second pass adds into D
 // Every mbarrier wait gives up after ~2^31 clock cycles, sets *err and lets the CTA finish.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -135,8 +138,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]),
+        "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]),
+        "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+
 struct OzArgs {
-    int m, n, kb0, kblocks, S, stages;
+    int m, n, kb0, kblocks, S;
     const int *ea, *eb;  // row / column exponents
     double *D;
     long long ldd;
@@ -150,20 +164,26 @@ struct OzArgs {
 // slice groups of four (one 128-byte row segment per k-block each)
 __host__ __device__ __forceinline__ int oz_ngroups(int S) { return (S + OZ_GP - 1) / OZ_GP; }
 
+// Shared-memory ring: OZ_SLOTS slots of one slice group of the A tile and of the B tile each.
+constexpr int OZ_SLOTS = 6;
+constexpr uint32_t OZ_SLOT_A = OZ_BM * 128, OZ_SLOT = (OZ_BM + OZ_BN) * 128;  // 16 KB + 16 KB
+
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = args.S, STAGES = args.stages, NG = oz_ngroups(S);
-    const uint32_t a_grp = OZ_BM * 128, b_grp = OZ_BN * 128;  // 16 KB each: 4 slices x 32 k-elements per row
-    const uint32_t a_bytes = (uint32_t)NG * a_grp;
-    const uint32_t stage_bytes = (uint32_t)NG * (a_grp + b_grp);
-    const int npass = (S + OZ_GP - 1) / OZ_GP;
-    uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)STAGES * stage_bytes);
-    uint64_t *empty_bar = full_bar + STAGES;
-    uint64_t *pass_bar = empty_bar + STAGES;  // MMAs of a pass complete
-    uint64_t *free_bar = pass_bar + 1;        // epilogue has read the pass's accumulators
+    const int S = args.S;
+    const int npass = oz_ngroups(S);  // pass p: groups 4p+2 .. min(4p+5, S+1), slice groups 0..p
+    // With two passes and at most two groups in the second, the first pass's FP64 partial sums stay
+    // in TMEM columns [0, 256) (high words, then low words, per 32-column chunk) and the second
+    // pass accumulates in columns [256, 512); otherwise the second pass adds into D.
+    const bool keep = (npass == 2) && (S <= 6);
+    uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)OZ_SLOTS * OZ_SLOT);
+    uint64_t *empty_bar = full_bar + OZ_SLOTS;
+    uint64_t *pass_bar = empty_bar + OZ_SLOTS;  // MMAs of a pass complete
+    uint64_t *free_bar = pass_bar + 1;          // epilogue has read the pass's accumulators
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(free_bar + 1);
+    double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} of the tile's columns
     __shared__ int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -174,7 +194,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < OZ_SLOTS; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
@@ -183,6 +203,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+    }
+    if (warp >= 2) {
+        const int c = threadIdx.x - 64;
+        colscale[c] = (n0 + c < args.n) ? ldexp(1.0, args.eb[n0 + c]) : 0.0;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
@@ -194,24 +218,22 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {  // TMA producer
+        if (lane == 0) {  // TMA producer: slot sequence = (pass, k-block, slice group)
             int it = 0;
             for (int p = 0; p < npass && !abort_flag; ++p) {
-                const int ngl = p + 1;  // slice groups needed by groups 4p+2 .. 4p+5 (slices up to 4p+4)
-                const uint32_t bytes = (uint32_t)ngl * (a_grp + b_grp);
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const int s = it % STAGES, use = it / STAGES;
-                    if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
-                        abort_flag = 1;
-                        break;
-                    }
-                    if (abort_flag) break;
-                    unsigned char *sa = smem + (size_t)s * stage_bytes;
-                    mbar_arrive_expect_tx(&full_bar[s], bytes);
+                for (int kb = 0; kb < KB && !abort_flag; ++kb) {
                     const int kc = (args.kb0 + kz0 + kb) * 128;  // byte offset of the k-block in a row
-                    for (int q = 0; q < ngl; ++q) {
-                        tma_load_3d(&tmA, &full_bar[s], sa + (size_t)q * a_grp, kc, m0, q);
-                        tma_load_3d(&tmB, &full_bar[s], sa + a_bytes + (size_t)q * b_grp, kc, n0, q);
+                    for (int q = 0; q <= p; ++q, ++it) {
+                        const int s = it % OZ_SLOTS, use = it / OZ_SLOTS;
+                        if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
+                            abort_flag = 1;
+                            break;
+                        }
+                        if (abort_flag) break;
+                        unsigned char *sa = smem + (size_t)s * OZ_SLOT;
+                        mbar_arrive_expect_tx(&full_bar[s], OZ_SLOT);
+                        tma_load_3d(&tmA, &full_bar[s], sa, kc, m0, q);
+                        tma_load_3d(&tmB, &full_bar[s], sa + OZ_SLOT_A, kc, n0, q);
                     }
                 }
             }
@@ -229,26 +251,33 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
                 const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
-                for (int kb = 0; kb < KB; ++kb, ++it) {
-                    const int s = it % STAGES, use = it / STAGES;
-                    if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
-                        ok = false;
-                        abort_flag = 1;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t sa = smem_u32(smem + (size_t)s * stage_bytes);
-                    const uint32_t sb = sa + a_bytes;
-                    for (int g = g0; g <= g1; ++g) {
-                        const uint32_t dcol = tmem_base + (uint32_t)(g - g0) * OZ_BN;
-                        for (int t = 1; t < g; ++t) {
-                            const int u = g - t;
-                            const uint32_t ao = (uint32_t)((t - 1) / OZ_GP) * a_grp + (uint32_t)((t - 1) % OZ_GP) * 32;
-                            const uint32_t bo = (uint32_t)((u - 1) / OZ_GP) * b_grp + (uint32_t)((u - 1) % OZ_GP) * 32;
-                            mma_i8(dcol, sdesc_sw128(sa + ao), sdesc_sw128(sb + bo), (kb > 0 || t > 1) ? 1u : 0u);
+                const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
+                for (int kb = 0; kb < KB && ok; ++kb) {
+                    // slots of slice groups 0 and (second pass only) 1 of this k-block
+                    const int s0 = it % OZ_SLOTS, s1 = (it + 1) % OZ_SLOTS;
+                    for (int q = 0; q <= p; ++q, ++it) {
+                        const int s = it % OZ_SLOTS, use = it / OZ_SLOTS;
+                        if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
+                            ok = false;
+                            abort_flag = 1;
+                            break;
                         }
                     }
-                    mma_commit(&empty_bar[s]);  // stage reusable once these MMAs have read it
+                    if (!ok) break;
+                    const uint32_t sb0 = smem_u32(smem + (size_t)s0 * OZ_SLOT);
+                    const uint32_t sb1 = smem_u32(smem + (size_t)s1 * OZ_SLOT);
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    for (int g = g0; g <= g1; ++g) {
+                        const uint32_t dcol = acc0 + (uint32_t)(g - g0) * OZ_BN;
+                        for (int t = 1; t < g; ++t) {
+                            const int u = g - t;
+                            const uint32_t ao = (t > OZ_GP ? sb1 : sb0) + (uint32_t)((t - 1) % OZ_GP) * 32;
+                            const uint32_t bo = (u > OZ_GP ? sb1 : sb0) + OZ_SLOT_A + (uint32_t)((u - 1) % OZ_GP) * 32;
+                            mma_i8(dcol, sdesc_sw128(ao), sdesc_sw128(bo), (kb > 0 || t > 1) ? 1u : 0u);
+                        }
+                    }
+                    mma_commit(&empty_bar[s0]);  // slots reusable once these MMAs have read them
+                    if (p > 0) mma_commit(&empty_bar[s1]);
                 }
                 mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
             }
@@ -256,49 +285,71 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     } else {
         // epilogue warps 2..5 cover TMEM lane quarters (warp % 4)
         const int quarter = warp & 3;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
-        const int ea = row_ok ? args.ea[row] : 0;
+        const double rowscale = row_ok ? ldexp(1.0, args.ea[row]) : 0.0;
         double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
         const long long cstride = args.trans ? args.ldd : 1;
         for (int p = 0; p < npass; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!ok || abort_flag) break;
             const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
-            if (ok && !abort_flag) {
+            const uint32_t acc0 = lane_base + ((p > 0 && keep) ? 256u : 0u);
+            const bool last = (p + 1 == npass);
 #pragma unroll 1
-                for (int c = 0; c < OZ_BN / 32; ++c) {
-                    double acc[32];
+            for (int c = 0; c < OZ_BN / 32; ++c) {
+                double acc[32];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 #pragma unroll 1
-                    for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
-                        uint32_t v[32];
-                        const uint32_t taddr =
-                            tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(g - g0) * OZ_BN + c * 32;
-                        tmem_ld32(taddr, v);
-                        const double sc = ldexp(1.0, -7 * g);
+                for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
+                    uint32_t v[32];
+                    tmem_ld32(acc0 + (uint32_t)(g - g0) * OZ_BN + c * 32, v);
+                    const double sc = ldexp(1.0, -7 * g);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                }
+                if (keep && p == 1) {  // add the first pass's partial sums
+                    uint32_t hi[32], lo[32];
+                    tmem_ld32(lane_base + c * 32, hi);
+                    tmem_ld32(lane_base + 128 + c * 32, lo);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] += __hiloint2double((int)hi[j], (int)lo[j]);
+                }
+                if (keep && !last) {  // park the partial sums over groups 2 and 3's chunk c (already read)
+                    uint32_t hi[32], lo[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        hi[j] = (uint32_t)__double2hiint(acc[j]);
+                        lo[j] = (uint32_t)__double2loint(acc[j]);
                     }
-                    if (row_ok) {
-                        const bool add = (p > 0) || args.accumulate;
+                    tmem_st32(lane_base + c * 32, hi);
+                    tmem_st32(lane_base + 128 + c * 32, lo);
+                } else if (row_ok) {
+                    const bool add = (p > 0 && !keep) || args.accumulate;
+                    double old[32];
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = n0 + c * 32 + j;
-                            if (col < args.n) {
-                                const double val = ldexp(acc[j], ea + args.eb[col]);
-                                double *dp = drow + (long long)col * cstride;
-                                *dp = add ? *dp + val : val;
-                            }
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = n0 + c * 32 + j;
+                        old[j] = (add && col < args.n) ? drow[(long long)col * cstride] : 0.0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = n0 + c * 32 + j;
+                        if (col < args.n) {
+                            const double val = acc[j] * rowscale * colscale[c * 32 + j];
+                            drow[(long long)col * cstride] = add ? old[j] + val : val;
                         }
                     }
                 }
-            } else {
-                break;
             }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(free_bar);  // this thread's reads of the pass's accumulators are done
+            if (!last) {
+                if (keep) asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(free_bar);  // this thread's reads of the pass's accumulators are done
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -512,17 +563,8 @@ size_t oz_slice_bytes(long long rows_pad, long long k, int S) {
     return (size_t)oz_ngroups(S) * OZ_GP * (size_t)rows_pad * (size_t)oz_pad_k(k);
 }
 
-int oz_stages(int S) {
-    const size_t stage = (size_t)oz_ngroups(S) * (OZ_BM + OZ_BN) * 128;
-    const size_t budget = 227 * 1024 - 1024 - 256;
-    int st = (int)(budget / stage);
-    return st > 6 ? 6 : st;
-}
-
-size_t oz_smem_bytes(int S) {
-    const int STAGES = oz_stages(S);
-    return 1024 + (size_t)STAGES * oz_ngroups(S) * (OZ_BM + OZ_BN) * 128 + (2 * STAGES + 2) * 8 + 16;
-}
+// alignment slack, the slot ring, 2 OZ_SLOTS + 2 mbarriers, the TMEM address slot, the column scales
+size_t oz_smem_bytes() { return 1024 + (size_t)OZ_SLOTS * OZ_SLOT + (2 * OZ_SLOTS + 2) * 8 + 8 + OZ_BN * 8; }
 
 // D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
 // k is split into passes short enough for exact int32 group sums; later passes add into D.
@@ -551,7 +593,6 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     const long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
     if (nsplit <= 1 || kb_total > kb_pass || kb_total < 2 * nsplit)
         return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, 0, trans, err, st);
-    const int stages = oz_stages(S);
     CUtensorMap ta, tb;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
     PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
@@ -565,7 +606,6 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kblocks = (int)((kb_total + nsplit - 1) / nsplit);
     a.kb_total = (int)kb_total;
     a.S = S;
-    a.stages = stages;
     a.ea = ea;
     a.eb = eb;
     a.D = part;
@@ -574,7 +614,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.trans = trans;
     a.dz = dz;
     a.err = err;
-    const size_t smem = oz_smem_bytes(S);
+    const size_t smem = oz_smem_bytes();
     PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), (unsigned)nsplit);
     {
@@ -598,11 +638,6 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
-    const int stages = oz_stages(S);
-    if (stages < 2) {
-        set_error(PHF_ERR_UNSUPPORTED, "oz_gemm: too many slices for two pipeline stages");
-        return PHF_ERR_UNSUPPORTED;
-    }
     CUtensorMap ta, tb;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
     PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
@@ -611,7 +646,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
     if (kb_pass < 1) kb_pass = 1;
     const long long kb_total = kpad / OZ_BK;
-    const size_t smem = oz_smem_bytes(S);
+    const size_t smem = oz_smem_bytes();
     PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // row tiles fastest
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
@@ -621,7 +656,6 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.kb0 = (int)kb0;
         a.kblocks = (int)std::min(kb_pass, kb_total - kb0);
         a.S = S;
-        a.stages = stages;
         a.ea = ea;
         a.eb = eb;
         a.D = D;

@@ -69,20 +69,26 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait on an mbarrier phase.  Returns false (and sets *err) after ~2^31 cycles.
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false (and sets *err) after ~2^31 cycles.  The first
+// probe takes no clock reading: the MMA issuer calls this once per k-block on its critical path.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
     const uint32_t addr = smem_u32(bar);
+    if (mbar_try(addr, parity)) return true;
     const long long t0 = clock64();
     while (true) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
+        if (mbar_try(addr, parity)) return true;
         if (clock64() - t0 > (1LL << 31)) {
             atomicOr(err, code);
             return false;
@@ -168,11 +174,32 @@ __host__ __device__ __forceinline__ int oz_ngroups(int S) { return (S + OZ_GP - 
 constexpr int OZ_SLOTS = 6;
 constexpr uint32_t OZ_SLOT_A = OZ_BM * 128, OZ_SLOT = (OZ_BM + OZ_BN) * 128;  // 16 KB + 16 KB
 
+// One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
+// so that each descriptor is a slot's base descriptor plus a constant (+2 per 32 bytes): the
+// single issuing thread runs barely ahead of the tensor core, and any latency between two MMAs
+// is tensor-core idle time.  da0 / da1: descriptors of the slots holding slice groups 0 / 1.
+template <int S, int P>
+__device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t da0, uint64_t da1, uint32_t acc_in) {
+    constexpr int g0 = 2 + OZ_GP * P;
+    constexpr int g1 = (1 + OZ_GP * (P + 1) < S + 1) ? 1 + OZ_GP * (P + 1) : S + 1;
+    constexpr uint64_t kB = OZ_SLOT_A >> 4;  // the B tile within a slot, in descriptor address units
+#pragma unroll
+    for (int g = g0; g <= g1; ++g) {
+#pragma unroll
+        for (int t = 1; t < g; ++t) {
+            const int u = g - t;
+            const uint64_t a = (t > OZ_GP ? da1 : da0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
+            const uint64_t b = (u > OZ_GP ? da1 : da0) + kB + (uint64_t)(2 * ((u - 1) % OZ_GP));
+            mma_i8(acc0 + (uint32_t)(g - g0) * OZ_BN, a, b, t > 1 ? 1u : acc_in);
+        }
+    }
+}
+
+template <int S>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = args.S;
     const int npass = oz_ngroups(S);  // pass p: groups 4p+2 .. min(4p+5, S+1), slice groups 0..p
     // With two passes and at most two groups in the second, the first pass's FP64 partial sums stay
     // in TMEM columns [0, 256) (high words, then low words, per 32-column chunk) and the second
@@ -219,13 +246,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer: slot sequence = (pass, k-block, slice group)
-            int it = 0;
+            int s = 0;            // next slot
+            uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
+            bool wrapped = false;
             for (int p = 0; p < npass && !abort_flag; ++p) {
                 for (int kb = 0; kb < KB && !abort_flag; ++kb) {
                     const int kc = (args.kb0 + kz0 + kb) * 128;  // byte offset of the k-block in a row
-                    for (int q = 0; q <= p; ++q, ++it) {
-                        const int s = it % OZ_SLOTS, use = it / OZ_SLOTS;
-                        if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, args.err, 1)) {
+                    for (int q = 0; q <= p; ++q) {
+                        if (wrapped && !mbar_wait(&empty_bar[s], eph, args.err, 1)) {
                             abort_flag = 1;
                             break;
                         }
@@ -234,14 +262,21 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         mbar_arrive_expect_tx(&full_bar[s], OZ_SLOT);
                         tma_load_3d(&tmA, &full_bar[s], sa, kc, m0, q);
                         tma_load_3d(&tmB, &full_bar[s], sa + OZ_SLOT_A, kc, n0, q);
+                        if (++s == OZ_SLOTS) {
+                            s = 0;
+                            if (wrapped) eph ^= 1u;
+                            wrapped = true;
+                        }
                     }
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
-            int it = 0;
+            int s = 0;         // next slot
+            uint32_t ph = 0;   // parity of its full-barrier phase
             bool ok = true;
+            const uint32_t smem_base = smem_u32(smem);
             for (int p = 0; p < npass && ok; ++p) {
                 if (p > 0) {  // accumulators drained by the epilogue
                     if (!mbar_wait(free_bar, (p - 1) & 1, args.err, 8)) {
@@ -250,32 +285,35 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
-                const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
                 const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
-                for (int kb = 0; kb < KB && ok; ++kb) {
+                for (int kb = 0; kb < KB; ++kb) {
                     // slots of slice groups 0 and (second pass only) 1 of this k-block
-                    const int s0 = it % OZ_SLOTS, s1 = (it + 1) % OZ_SLOTS;
-                    for (int q = 0; q <= p; ++q, ++it) {
-                        const int s = it % OZ_SLOTS, use = it / OZ_SLOTS;
-                        if (!mbar_wait(&full_bar[s], use & 1, args.err, 2)) {
-                            ok = false;
-                            abort_flag = 1;
-                            break;
+                    const int s0 = s;
+                    ok = mbar_wait(&full_bar[s], ph, args.err, 2);
+                    if (++s == OZ_SLOTS) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                    int s1 = s0;
+                    if (ok && p > 0) {
+                        s1 = s;
+                        ok = mbar_wait(&full_bar[s], ph, args.err, 2);
+                        if (++s == OZ_SLOTS) {
+                            s = 0;
+                            ph ^= 1u;
                         }
                     }
-                    if (!ok) break;
-                    const uint32_t sb0 = smem_u32(smem + (size_t)s0 * OZ_SLOT);
-                    const uint32_t sb1 = smem_u32(smem + (size_t)s1 * OZ_SLOT);
+                    if (!ok) {
+                        abort_flag = 1;
+                        break;
+                    }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    for (int g = g0; g <= g1; ++g) {
-                        const uint32_t dcol = acc0 + (uint32_t)(g - g0) * OZ_BN;
-                        for (int t = 1; t < g; ++t) {
-                            const int u = g - t;
-                            const uint32_t ao = (t > OZ_GP ? sb1 : sb0) + (uint32_t)((t - 1) % OZ_GP) * 32;
-                            const uint32_t bo = (u > OZ_GP ? sb1 : sb0) + OZ_SLOT_A + (uint32_t)((u - 1) % OZ_GP) * 32;
-                            mma_i8(dcol, sdesc_sw128(ao), sdesc_sw128(bo), (kb > 0 || t > 1) ? 1u : 0u);
-                        }
-                    }
+                    const uint64_t da0 = sdesc_sw128(smem_base + (uint32_t)s0 * OZ_SLOT);
+                    const uint64_t da1 = sdesc_sw128(smem_base + (uint32_t)s1 * OZ_SLOT);
+                    if (p == 0)
+                        issue_kblock<S, 0>(acc0, da0, da1, kb > 0 ? 1u : 0u);
+                    else
+                        issue_kblock<S, 1>(acc0, da0, da1, kb > 0 ? 1u : 0u);
                     mma_commit(&empty_bar[s0]);  // slots reusable once these MMAs have read them
                     if (p > 0) mma_commit(&empty_bar[s1]);
                 }
@@ -574,6 +612,21 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
 }
 
 namespace {
+using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, OzArgs);
+
+OzKernelFn oz_kernel_for(int S) {
+    switch (S) {
+        case 1: return ozaki_i8_gemm_kernel<1>;
+        case 2: return ozaki_i8_gemm_kernel<2>;
+        case 3: return ozaki_i8_gemm_kernel<3>;
+        case 4: return ozaki_i8_gemm_kernel<4>;
+        case 5: return ozaki_i8_gemm_kernel<5>;
+        case 6: return ozaki_i8_gemm_kernel<6>;
+        case 7: return ozaki_i8_gemm_kernel<7>;
+        default: return nullptr;
+    }
+}
+
 __global__ void sum_splits_kernel(long long count, int nsplit, long long dz, const double *part, double *D) {
     for (long long i = blockIdx.x * 256LL + threadIdx.x; i < count; i += (long long)gridDim.x * 256)
     {
@@ -615,11 +668,16 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.dz = dz;
     a.err = err;
     const size_t smem = oz_smem_bytes();
-    PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const OzKernelFn kern = oz_kernel_for(S);
+    if (!kern) {
+        set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
+        return PHF_ERR_ARG;
+    }
+    PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), (unsigned)nsplit);
     {
         ProfScope prof(st, PROF_JK);
-        ozaki_i8_gemm_kernel<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+        kern<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
     }
     ++g_launches;
     PHF_CHECK_LAUNCH();
@@ -647,7 +705,12 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     if (kb_pass < 1) kb_pass = 1;
     const long long kb_total = kpad / OZ_BK;
     const size_t smem = oz_smem_bytes();
-    PHF_CUDA(cudaFuncSetAttribute(ozaki_i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const OzKernelFn kern = oz_kernel_for(S);
+    if (!kern) {
+        set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
+        return PHF_ERR_ARG;
+    }
+    PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // row tiles fastest
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
@@ -667,7 +730,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
-            ozaki_i8_gemm_kernel<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+            kern<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
         }
         ++g_launches;
         PHF_CHECK_LAUNCH();

@@ -408,17 +408,59 @@ __device__ __forceinline__ int exp_of_max(double mx) {
 
 // Slices of x (scaled by 2^-e) for element k of a row: row_base points at (group 0, row, k-block 0);
 // group_stride = rows_pad * KB * 128 bytes (see the layout at the top of the file).
-__device__ __forceinline__ void slice_value(double x, int e, int S, signed char *row_base, long long group_stride,
-                                            long long k) {
-    double r = ldexp(x, -e);
+// Slicing of one value: with r = x 2^-e (|r| < 1), slice t (t < S - 1) is the t-th base-128 digit
+// of |r| with the sign of x, and the last slice is the rounded remainder (clamped to +-127):
+//     T = x 2^{7(S-1) - e},  I = floor(|T|)  (the first S - 1 digits),  last = rint(128 (|T| - I)).
+// Every step is exact (power-of-two scaling, |T| < 2^42), so the digits are those of the
+// step-by-step form  r *= 128; a = trunc(r); r -= a.  I comes from the mantissa of |T| + 2^52 added
+// with round-toward-zero and the rounding of the last digit from adding 1.5 * 2^52 -- plain FP64
+// adds, no integer/floating conversions (those are long-latency and dominated the slicing).
+struct SliceScale {
+    double p1, p2;  // 2^-e and 2^{7(S-1)}
+    int e;
+    bool fast;      // 2^-e is a normal double: two exact multiplications instead of ldexp
+};
+
+__device__ __forceinline__ double pow2_normal(int k) {  // 2^k for -1022 <= k <= 1023
+    return __hiloint2double((1023 + k) << 20, 0);
+}
+
+__device__ __forceinline__ SliceScale slice_scale(int e, int S) {
+    SliceScale sc;
+    sc.e = e;
+    sc.fast = (e >= -1000 && e <= 1000);
+    sc.p1 = sc.fast ? pow2_normal(-e) : 1.0;
+    sc.p2 = pow2_normal(7 * (S - 1));
+    return sc;
+}
+
+__device__ __forceinline__ void slice_digits(double x, const SliceScale &sc, int S, int (&d)[OZ_MAX_S]) {
+    constexpr double kTwo52 = 4503599627370496.0, kRound = 6755399441055744.0;  // 2^52, 1.5 * 2^52
+    const double T = sc.fast ? (x * sc.p1) * sc.p2 : ldexp(x, 7 * (S - 1) - sc.e);
+    const double aT = fabs(T);
+    const double big = __dadd_rz(aT, kTwo52);  // 2^52 + floor(|T|)
+    const unsigned long long mag = (unsigned long long)__double_as_longlong(big) & ((1ull << 52) - 1);
+    const double fr = aT - (big - kTwo52);     // exact fraction
+    const double lastm = fmin(127.0, __dadd_rn(fr * 128.0, kRound) - kRound);
+    const int sg = T < 0.0 ? -1 : 1;
+#pragma unroll
+    for (int t = 0; t < OZ_MAX_S; ++t)
+        d[t] = (t < S - 1) ? sg * (int)((mag >> (7 * (S - 2 - t))) & 127ull) : 0;
+#pragma unroll
+    for (int t = 0; t < OZ_MAX_S; ++t)
+        if (t == S - 1) d[t] = sg * (int)lastm;
+}
+
+// Slices of x for element k of a row: row_base points at (group 0, row, k-block 0);
+// group_stride = rows_pad * KB * 128 bytes (see the layout at the top of the file).
+__device__ __forceinline__ void slice_value(double x, const SliceScale &sc, int S, signed char *row_base,
+                                            long long group_stride, long long k) {
+    int d[OZ_MAX_S];
+    slice_digits(x, sc, S, d);
     signed char *base = row_base + (k >> 5) * 128 + (k & 31);
-    for (int t = 0; t < S; ++t) {
-        r *= 128.0;
-        double a = (t + 1 < S) ? trunc(r) : rint(r);
-        a = fmin(127.0, fmax(-127.0, a));
-        r -= a;
-        base[(long long)(t / OZ_GP) * group_stride + (t % OZ_GP) * 32] = (signed char)(int)a;
-    }
+#pragma unroll
+    for (int t = 0; t < OZ_MAX_S; ++t)
+        if (t < S) base[(long long)(t / OZ_GP) * group_stride + (t % OZ_GP) * 32] = (signed char)d[t];
 }
 
 constexpr int SL_NT = 256;
@@ -448,9 +490,10 @@ __global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const d
     const int e = exp_of_max(mx);
     if (threadIdx.x == 0) ea[row] = e;
     const long long gstride = mpad * kpad * OZ_GP;
+    const SliceScale sc = slice_scale(e, S);
     for (long long j = threadIdx.x; j < kpad; j += SL_NT) {
         double x = (j < k) ? a[j * cs] : 0.0;
-        slice_value(x, e, S, out + row * kpad * OZ_GP, gstride, j);
+        slice_value(x, sc, S, out + row * kpad * OZ_GP, gstride, j);
     }
 }
 
@@ -475,6 +518,7 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
     const long long gstride = npad * kpad * OZ_GP;
+    const SliceScale sc = slice_scale(ex, S);
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
         if (e < k) {
@@ -482,7 +526,7 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
             zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
             x = part ? v.y : v.x;
         }
-        slice_value(x, ex, S, out + c * kpad * OZ_GP, gstride, e);
+        slice_value(x, sc, S, out + c * kpad * OZ_GP, gstride, e);
     }
 }
 
@@ -509,6 +553,7 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
     const long long gstride = npad * kpad * OZ_GP;
+    const SliceScale sc = slice_scale(ex, S);
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
         if (e < k) {
@@ -516,7 +561,214 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
             zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
             x = part ? v.y : v.x;
         }
-        slice_value(x, ex, S, out + c * kpad * OZ_GP, gstride, e);
+        slice_value(x, sc, S, out + c * kpad * OZ_GP, gstride, e);
+    }
+}
+
+
+// ------------------------------------------------------------------ fused density + operand slicing
+// ERI form with n <= 64: the exchange (K) and Coulomb (P) operand columns straight from X_w and
+// bra, without writing the M x M density to HBM.  CTA (w, pair): pair 0 forms rho_aa, rho_bb and
+// P = rho_aa + rho_bb, pair 1 forms rho_ab and rho_ba, each as
+//     rho_st[l][j] = sum_m X_w[2l+s][m] conj(bra[2j+t][m])
+// with the FMA sequence of zgemm_kernel (m ascending), so every column, its exponent and its
+// slices are exactly those of the density GEMM followed by slice_rho_cols / slice_p_cols.
+constexpr int RS_NT = 256, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded row pitch (complex)
+
+// operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
+size_t rs_smem_bytes() { return std::max((size_t)2 * 2 * RS_MC * RS_P * sizeof(zc), (size_t)2 * 64 * 64 * sizeof(double)); }
+
+// Slices of four consecutive k-elements e0..e0+3 (one 32-element block) of a column, S known at
+// compile time: the digits of the four values are cut from the mantissa words of 2^52 + floor(|T|)
+// with constant shifts, packed four to a 32-bit word (byte v = element e0 + v), and the signs are
+// applied to the packed words (per-byte negation, no carries between bytes).  Same digits as
+// slice_digits; one 32-bit store per slice.
+__device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {  // bytes 0..127 -> (-b) mod 256
+    return ((~w & 0x7F7F7F7Fu) + 0x01010101u) ^ 0x80808080u;
+}
+
+template <int S>
+__device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceScale &sc, signed char *row_base,
+                                            long long gstride, long long e0) {
+    constexpr double kTwo52 = 4503599627370496.0, kRound = 6755399441055744.0;
+    uint32_t lo[4], hi[4], last[4], sign = 0u;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const double T = sc.fast ? (x[v] * sc.p1) * sc.p2 : ldexp(x[v], 7 * (S - 1) - sc.e);
+        const double aT = fabs(T);
+        const double big = __dadd_rz(aT, kTwo52);  // 2^52 + floor(|T|)
+        lo[v] = (uint32_t)__double2loint(big);
+        hi[v] = (uint32_t)__double2hiint(big) & 0xFFFFFu;
+        const double fr = aT - (big - kTwo52);
+        // 1.5 * 2^52 + 128 fr rounded to nearest even: its low word is rint(128 fr) (<= 128)
+        last[v] = min((uint32_t)__double2loint(__dadd_rn(fr * 128.0, kRound)), 127u);
+        if (T < 0.0) sign |= 0xFFu << (8 * v);
+    }
+    signed char *base = row_base + (e0 >> 5) * 128 + (e0 & 31);
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+        uint32_t w = 0u;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            uint32_t dg;
+            if (t == S - 1) {
+                dg = last[v];
+            } else {
+                const int off = 7 * (S - 2 - t);
+                if (off >= 32) dg = (hi[v] >> (off - 32)) & 127u;
+                else if (off + 7 > 32) dg = __funnelshift_r(lo[v], hi[v], off) & 127u;
+                else dg = (lo[v] >> off) & 127u;
+            }
+            w |= dg << (8 * v);
+        }
+        w = (w & ~sign) | (neg_bytes(w) & sign);
+        *reinterpret_cast<uint32_t *>(base + (long long)(t / OZ_GP) * gstride + (t % OZ_GP) * 32) = w;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc *__restrict__ Xs, long long ld,
+                                                          const zc *__restrict__ bra, long long npadK,
+                                                          long long npadP, long long kpad, signed char *outK,
+                                                          int *ebK, signed char *outP, int *ebP) {
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    zc *xs = reinterpret_cast<zc *>(rs_smem);  // [s][mm][l]: X_w[2l+s][m0+mm] at (s RS_MC + mm) RS_P + l
+    zc *bs = xs + 2 * RS_MC * RS_P;            // [t][mm][j]: bra[2j+t][m0+mm]
+    double *stage = reinterpret_cast<double *>(rs_smem);  // one column (n^2 values) after the products
+    __shared__ double red[6 * (RS_NT / 32)];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const long long w = blockIdx.x >> 1;
+    const int pair = (int)(blockIdx.x & 1);
+    // thread tile: rows l = ty + 16 i, columns j = tx + 16 jj of both spin blocks q = 0, 1
+    double ar[2][4][4], ai[2][4][4];
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) ar[q][i][jj] = ai[q][i][jj] = 0.0;
+
+    for (int m0 = 0; m0 < N; m0 += RS_MC) {
+        const int mc = min(RS_MC, N - m0);
+        __syncthreads();
+        for (int idx = tid; idx < 2 * 64 * RS_MC; idx += RS_NT) {  // mm fastest: 256-byte row runs
+            const int mm = idx % RS_MC, l = (idx / RS_MC) & 63, sp = idx / (RS_MC * 64);
+            zc xv = {0.0, 0.0}, bv = {0.0, 0.0};
+            if (l < n && mm < mc) {
+                xv = Xs[(long long)(2 * l + sp) * ld + w * N + m0 + mm];
+                bv = bra[(long long)(2 * l + sp) * N + m0 + mm];
+            }
+            xs[(sp * RS_MC + mm) * RS_P + l] = xv;
+            bs[(sp * RS_MC + mm) * RS_P + l] = bv;
+        }
+        __syncthreads();
+        for (int mm = 0; mm < mc; ++mm) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int sg = q, tu = pair ? 1 - q : q;
+                zc a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = xs[(sg * RS_MC + mm) * RS_P + ty + 16 * i];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const zc v = bs[(tu * RS_MC + mm) * RS_P + tx + 16 * jj];
+                    b[jj] = zc{v.x, -v.y};
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) {
+                        ar[q][i][jj] = fma(a[i].x, b[jj].x, ar[q][i][jj]);
+                        ar[q][i][jj] = fma(-a[i].y, b[jj].y, ar[q][i][jj]);
+                        ai[q][i][jj] = fma(a[i].x, b[jj].y, ai[q][i][jj]);
+                        ai[q][i][jj] = fma(a[i].y, b[jj].x, ai[q][i][jj]);
+                    }
+            }
+        }
+    }
+
+    // columns of this CTA: K (q, part) for q = 0, 1; for pair 0 also P (part)
+    const int ncol = pair == 0 ? 6 : 4;
+    const int nn = n * n;
+    auto value = [&](int col, int i, int jj) -> double {
+        const int part = col & 1;
+        if (col < 2) return part ? ai[0][i][jj] : ar[0][i][jj];
+        if (col < 4) return part ? ai[1][i][jj] : ar[1][i][jj];
+        return part ? ai[0][i][jj] + ai[1][i][jj] : ar[0][i][jj] + ar[1][i][jj];
+    };
+    // all column maxima in one reduction: warp shuffles, then the 8 warps through shared memory
+    double mx[6];
+#pragma unroll
+    for (int col = 0; col < 6; ++col) mx[col] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+            if ((ty + 16 * i < n) && (tx + 16 * jj < n)) {
+#pragma unroll
+                for (int col = 0; col < 6; ++col)
+                    if (col < ncol) mx[col] = fmax(mx[col], fabs(value(col, i, jj)));
+            }
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx[col] = fmax(mx[col], __shfl_xor_sync(0xffffffffu, mx[col], off));
+        if (lane == 0) red[col * (RS_NT / 32) + warp] = mx[col];
+    }
+    __syncthreads();  // also orders the last reads of xs / bs before the stage writes
+    long long cidx[6];
+    int ex[6];
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+        double m = 0.0;
+#pragma unroll
+        for (int wv = 0; wv < RS_NT / 32; ++wv) m = fmax(m, red[col * (RS_NT / 32) + wv]);
+        ex[col] = exp_of_max(m);
+        const int part = col & 1;
+        if (col < 4) {
+            const int q = col >> 1, sg = q, tu = pair ? 1 - q : q;
+            cidx[col] = (w * 4 + sg * 2 + tu) * 2 + part;
+        } else {
+            cidx[col] = 2 * w + part;
+        }
+    }
+    if (tid < ncol) {
+#pragma unroll
+        for (int col = 0; col < 6; ++col)
+            if (col == tid) (col < 4 ? ebK : ebP)[cidx[col]] = ex[col];
+    }
+    // two columns per round through the stage (2 n^2 doubles), sliced four k-elements per store
+#pragma unroll
+    for (int c0 = 0; c0 < 6; c0 += 2) {
+        if (c0 >= ncol) break;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const int l = ty + 16 * i, j = tx + 16 * jj;
+                if (l < n && j < n) {
+                    stage[l * n + j] = value(c0, i, jj);
+                    stage[nn + l * n + j] = value(c0 + 1, i, jj);
+                }
+            }
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int col = c0 + h;
+            const bool isK = col < 4;
+            const long long gstride = (isK ? npadK : npadP) * kpad * OZ_GP;
+            signed char *row_base = (isK ? outK : outP) + cidx[col] * kpad * OZ_GP;
+            const SliceScale sc = slice_scale(ex[col], S);
+            const double *src = stage + h * nn;
+            for (long long e0 = 4LL * tid; e0 < kpad; e0 += 4LL * RS_NT) {
+                double x[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) x[u] = (e0 + u < nn) ? src[e0 + u] : 0.0;
+                slice_pack4<S>(x, sc, row_base, gstride, e0);
+            }
+        }
+        __syncthreads();  // the stage is rewritten by the next round
     }
 }
 
@@ -582,6 +834,36 @@ int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int 
     ProfScope prof(st, PROF_MEMORY);
     slice_rho_cols_kernel<<<(unsigned)ncols, SL_NT, 0, st>>>(n, rho, S, oz_pad_cols(ncols), oz_pad_k((long long)n * n),
                                                              out, eb);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+bool oz_rho_slice_ok(int n) { return n >= 1 && n <= 64; }
+
+int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra, int S, signed char *Ksl, int *eK,
+                 signed char *Psl, int *eP, cudaStream_t st) {
+    if (!oz_rho_slice_ok(n) || S < 1 || S > OZ_MAX_S || N < 1) {
+        set_error(PHF_ERR_UNSUPPORTED, "oz_rho_slice: needs 1 <= n <= 64 and 1 <= slices <= 7");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    using RsFn = void (*)(int, int, const zc *, long long, const zc *, long long, long long, long long, signed char *,
+                          int *, signed char *, int *);
+    RsFn fn = nullptr;
+    switch (S) {
+        case 1: fn = rho_slice_kernel<1>; break;
+        case 2: fn = rho_slice_kernel<2>; break;
+        case 3: fn = rho_slice_kernel<3>; break;
+        case 4: fn = rho_slice_kernel<4>; break;
+        case 5: fn = rho_slice_kernel<5>; break;
+        case 6: fn = rho_slice_kernel<6>; break;
+        default: fn = rho_slice_kernel<7>; break;
+    }
+    const size_t smem = rs_smem_bytes();
+    PHF_CUDA(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ProfScope prof(st, PROF_MEMORY);
+    fn<<<(unsigned)(2LL * bc), RS_NT, smem, st>>>(n, N, Xs, ld, bra, oz_pad_cols(8LL * bc), oz_pad_cols(2LL * bc),
+                                                  oz_pad_k((long long)n * n), Ksl, eK, Psl, eP);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

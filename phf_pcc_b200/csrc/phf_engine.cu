@@ -620,8 +620,11 @@ int build_exchange_matrix(PlanImpl &p) {
 int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     const int M = p.M, N = p.N, n = p.n, L = p.L, b = p.b;
     const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
-    PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0, vo(p.Rho, M, 1, MM),
-                          nullptr, st));
+    // int8 path with n <= 64: the operand columns are formed and sliced in one kernel, no density in HBM
+    const bool fused = p.prec != PHF_PREC_FP64 && oz_rho_slice_ok(n);
+    if (!fused)
+        PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0,
+                              vo(p.Rho, M, 1, MM), nullptr, st));
     if (p.prec == PHF_PREC_FP64) {
         PHF_TRY(launch_gather_p(n, bc, p.Rho, p.Pvec, b, st));
         PHF_TRY(zgemm_strided(L, bc, (int)n2, 1, 1, Z1, vd(p.Bst, n2, 1), vz(p.Pvec, b, 1), Z0, vo(p.dvec, b, 1),
@@ -630,7 +633,10 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
                               nullptr, st));
     } else {
         // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
-        PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
+        if (fused)
+            PHF_TRY(oz_rho_slice(n, N, bc, p.Xs, ld, p.bra, p.slices, p.Bsl, p.eb, p.Psl, p.ePc, st));
+        else
+            PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
         PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
                                p.ozerr, st));
         PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, st));
@@ -660,7 +666,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st));
     } else {
-        PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
+        if (!fused) PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
         // K^T (8 bc x n^2), transposed for coalesced epilogue stores
         PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, n2, 0, 1, p.ozerr, st));
         prof_set_class(PROF_GEMM);

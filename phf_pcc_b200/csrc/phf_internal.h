@@ -88,6 +88,10 @@ long long oz_pad_rows(long long m);
 long long oz_pad_cols(long long n);
 long long oz_pad_k(long long k);
 size_t oz_slice_bytes(long long rows_pad, long long k, int S);  // bytes of an operand's int8 slices
+// ERI form, n <= 64: density columns of the K and P operands sliced straight from X and bra
+bool oz_rho_slice_ok(int n);
+int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra, int S, signed char *Ksl, int *eK,
+                 signed char *Psl, int *eP, cudaStream_t st);
 int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long rows_pad, signed char *out, int *ea,
                   cudaStream_t st);
 int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long long cs, int S, long long rows_pad,

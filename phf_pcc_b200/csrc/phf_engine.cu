@@ -674,7 +674,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     }
     PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
                           st));
-    PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st));
+    PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, p.HX));  // then GX <- HX + Gamma X
     return PHF_OK;
 }
 
@@ -785,6 +785,7 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
                 PHF_TRY(split_gamma_x(p, bc, st));
             }
             PHF_TRY(launch_rowsum(bc, L, p.e2part, p.e2, 0.5, st));
+            PHF_TRY(launch_add_inplace(M, N, bc, p.HX, p.GX, ld, st));  // GX <- HX + Gamma X
         } else {
             prof_set_class(PROF_JK);
             // rho_w = X_w bra^H stored as vec: Pv[(l M + j) b + w]
@@ -795,16 +796,14 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
             PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gv, (long long)M * bc, bc, 1), vz(p.Xs, ld, 1, N), Z0,
                                   vo(p.GX, ld, 1, N), nullptr, st));
             prof_set_class(PROF_GEMM);
-            PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st));
+            PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, p.HX));  // then GX <- HX + Gamma X
         }
-        // W = bra^H (HX + GX);  GX <- GX - X W
-        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.HX, ld, 1), Z0, vo(p.W, ld, 1),
-                              nullptr, st));
-        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.GX, ld, 1), Z1, vo(p.W, ld, 1),
+        // GX now holds F X = HX + Gamma X:  W = bra^H F X;  GX <- F X - X W
+        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.GX, ld, 1), Z0, vo(p.W, ld, 1),
                               nullptr, st));
         PHF_TRY(zgemm_strided(M, N, N, bc, 1, ZM1, vz(p.Xs, ld, 1, N), vz(p.W, ld, 1, N), Z1, vo(p.GX, ld, 1, N), nullptr,
                               st));
-        PHF_TRY(launch_epilogue(M, N, bc, p.HX, p.GX, p.Xs, ld, p.det, p.e1, p.e2, p.scal, st));
+        PHF_TRY(launch_epilogue(M, N, bc, p.GX, p.Xs, ld, p.det, p.e1, p.e2, p.scal, st));
         const int nb2 = p.nb * p.nb;
         PHF_TRY(launch_accumulate(nb2, M, N, bc, p.Wt, p.nomega, w0, p.slotmap + (size_t)v * nb2, p.GX, p.Xs, ld, p.scal,
                                   p.accG, p.compG, p.accR, p.compR, p.accHS, p.compHS, p.acc_scratch, st));

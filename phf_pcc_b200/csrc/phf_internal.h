@@ -57,9 +57,11 @@ int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_b
 // phf_kernels.cu
 int launch_tprime(int Ltot, int N, int b, zc *T, long long ldT, zc *e2part, cudaStream_t st);
 int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cudaStream_t st);
-int launch_trace_conj(int M, int N, int b, const zc *C, const zc *X, long long ldX, zc *out, double scale,
-                      cudaStream_t st);
-int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
+// out[w] = scale tr(C^H X_w); with `add`, X_w <- X_w + add_w afterwards (same layout as X)
+int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale,
+                      cudaStream_t st, const zc *add = nullptr);
+int launch_add_inplace(int M, int N, int b, const zc *A, zc *G, long long ldX, cudaStream_t st);
+int launch_epilogue(int M, int N, int b, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
                     const zc *e2, zc *scal, cudaStream_t st);
 size_t accumulate_scratch_bytes(int nslot, int M, int N, int b);
 int launch_accumulate(int nslot, int M, int N, int b, const zc *Wt, long long nomega, long long w0, const int *slotmap,

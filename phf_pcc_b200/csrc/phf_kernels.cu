@@ -59,14 +59,17 @@ __global__ void __launch_bounds__(NT) rowsum_kernel(int ncols, const zc *in, zc 
 }
 
 // out[w] = scale * sum_{r,j} conj(C[r*N + j]) * X[r*ldX + w*N + j]   (tr(C^H X_w))
-__global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *C, const zc *X, long long ldX, zc *out,
-                                                        double scale) {
+__global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *C, zc *X, long long ldX, zc *out,
+                                                        double scale, const zc *add) {
     __shared__ zc sh[NT];
     const long long w = blockIdx.x;
     zc s = mkz(0, 0);
     for (int e = threadIdx.x; e < M * N; e += NT) {
         int r = e / N, j = e - r * N;
-        s = s + conjz(C[e]) * X[(long long)r * ldX + w * N + j];
+        const long long o = (long long)r * ldX + w * N + j;
+        const zc x = X[o];
+        s = s + conjz(C[e]) * x;
+        if (add) X[o] = x + add[o];  // X <- X + add once the trace has read X
     }
     s = block_sum(s, sh);
     if (threadIdx.x == 0) out[w] = scale * s;
@@ -74,10 +77,10 @@ __global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *
 
 // Energy/gradient epilogue over a chunk of b grid points (Gradient, PHFTools.f90:291-308, in
 // the rank-N form): with h_w = e1_w + e2_w and N_w = det S_w,
-//   G <- N_w (HX + G + h_w X)    where G already holds GammaX - X W_w
+//   G <- N_w (G + h_w X)          where G already holds HX + GammaX - X W_w
 //   X <- N_w X
 //   scal[2w] = N_w h_w, scal[2w+1] = N_w
-__global__ void __launch_bounds__(NT) epilogue_kernel(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX,
+__global__ void __launch_bounds__(NT) epilogue_kernel(int M, int N, int b, zc *G, zc *X, long long ldX,
                                                       const zc *det, const zc *e1, const zc *e2, zc *scal) {
     const long long total = (long long)M * b * N;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(NT) epilogue_kernel(int M, int N, int b, const
         zc h = e1[w] + e2[w];
         zc nd = det[w];
         zc x = X[o];
-        G[o] = nd * (HX[o] + G[o] + h * x);
+        G[o] = nd * (G[o] + h * x);
         X[o] = nd * x;
     }
     if (blockIdx.x == 0) {
@@ -349,19 +352,37 @@ int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cud
     return PHF_OK;
 }
 
-int launch_trace_conj(int M, int N, int b, const zc *C, const zc *X, long long ldX, zc *out, double scale,
-                      cudaStream_t st) {
+int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale, cudaStream_t st,
+                      const zc *add) {
     ProfScope prof(st, PROF_MEMORY);
-    trace_conj_kernel<<<b, NT, 0, st>>>(M, N, C, X, ldX, out, scale);
+    trace_conj_kernel<<<b, NT, 0, st>>>(M, N, C, X, ldX, out, scale, add);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
 }
 
-int launch_epilogue(int M, int N, int b, const zc *HX, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
+// G <- G + A over a chunk (M rows x b N columns, row stride ldX)
+__global__ void __launch_bounds__(NT) add_inplace_kernel(long long rows, long long cols, const zc *A, zc *G,
+                                                         long long ldX) {
+    const long long total = rows * cols;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        const long long r = e / cols, c = e - r * cols, o = r * ldX + c;
+        G[o] = G[o] + A[o];
+    }
+}
+
+int launch_add_inplace(int M, int N, int b, const zc *A, zc *G, long long ldX, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    add_inplace_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, (long long)b * N, A, G, ldX);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_epilogue(int M, int N, int b, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
                     const zc *e2, zc *scal, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    epilogue_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, N, b, HX, G, X, ldX, det, e1, e2, scal);
+    epilogue_kernel<<<grid_for((long long)M * b * N), NT, 0, st>>>(M, N, b, G, X, ldX, det, e1, e2, scal);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -37,7 +37,8 @@ __device__ __forceinline__ double load_d(const View &v, long long off) {
 
 // BM x BN output tile, 256 threads in a (BM/4) x (BN/4) grid, 4 x 4 complex accumulators each:
 // thread (ty, tx) owns rows ty + (BM/4) i and columns tx + (BN/4) j.  64 x 64 serves general
-// shapes; 128 x 32 serves the narrow per-point products (N <= 32 columns).
+// shapes; 128 x 32 serves the narrow per-point products (N <= 32 columns), 32 x 128 the
+// N-row products bra^H Y and bra^H F X (m = N <= 32) over all points of a chunk.
 template <bool AREAL, int BM, int BN>
 __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
                                                    zc beta, OutView C, const long long *__restrict__ offs) {
@@ -200,6 +201,7 @@ int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A
         return PHF_ERR_ARG;
     }
     if (n <= 32 && m >= 96) return launch_tile<128, 32>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    if (m <= 32 && n >= 96) return launch_tile<32, 128>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
     return launch_tile<64, 64>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
 }
 

@@ -14,16 +14,18 @@
 // (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
 // fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
 //
-// Slice layout in global memory: slices are grouped four at a time and interleaved per 32-element
-// k-block, so that one 128-byte row segment holds the same 32 k-elements of four slices:
-//   byte ((g * rows_pad + row) * KB + kb) * 128 + q * 32 + kk   for slice t = 4 g + q, k = 32 kb + kk.
-// A TMA box of 128-byte rows then carries four slices at once, and the MMA picks slice q of a
-// stage by a +32 q byte offset of its SWIZZLE_128B K-major descriptor.
+// Slice layout in global memory (per operand, rows padded to 128, k to KB blocks of 32): slices
+// 0..3 (group 0) interleaved per k-block so that one 128-byte row segment holds the same 32
+// k-elements of four slices, byte (row KB + kb) 128 + t 32 + kk; then slices 4..S-1 (group 1) in
+// 64-byte segments for S = 5, 6 (two slices) or 128-byte segments for S = 7.  A TMA box of full
+// segments (SWIZZLE_128B / SWIZZLE_64B) then carries several slices at once, and the MMA picks a
+// slice by a +32-byte offset of its K-major descriptor.
 //
 // Kernel shape (one CTA per 128 x 128 output tile, 6 warps), row tiles fastest in the grid so that
 // the CTAs in flight share B column tiles through L2:
-//   warp 0      TMA producer: per 32-element k-block one 128 x 128 B box of A and of B per slice
-//               group the current pass needs, into a ring of six 32 KB slots (full/empty mbarriers)
+//   warp 0      TMA producer into a ring of fourteen 16 KB units (full/empty mbarrier per unit):
+//               per 32-element k-block the A and B boxes of group 0 (a unit each) and, in the
+//               second pass, of group 1 (one unit holding both 8 KB boxes for S = 5, 6)
 //   warp 1      TMEM allocation (512 columns = four 128 x 128 int32 accumulators) and the
 //               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of four
 //               groups over the whole k range; per k-block every slice pair of the pass's groups
@@ -96,11 +98,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1, int c2) {
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1) {
     asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
             "r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
         : "memory");
 }
 
@@ -112,6 +114,17 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset: 8 rows x 128 B
     d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
     d |= (uint64_t)2 << 61;                           // layout: SWIZZLE_128B
+    return d;
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_64B (8 rows x 64 B atoms, SBO = 512 B).
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(512 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;                           // layout: SWIZZLE_64B
     return d;
 }
 
@@ -167,51 +180,112 @@ struct OzArgs {
     int *err;
 };
 
-// slice groups of four (one 128-byte row segment per k-block each)
+// slice groups: group 0 = slices 0..3, group 1 = slices 4..S-1 (S >= 5)
 __host__ __device__ __forceinline__ int oz_ngroups(int S) { return (S + OZ_GP - 1) / OZ_GP; }
 
-// Shared-memory ring: OZ_SLOTS slots of one slice group of the A tile and of the B tile each.
-constexpr int OZ_SLOTS = 6;
-constexpr uint32_t OZ_SLOT_A = OZ_BM * 128, OZ_SLOT = (OZ_BM + OZ_BN) * 128;  // 16 KB + 16 KB
+// Slices per k-block row of group 1: two (64-byte rows) for S = 5, 6, four (128-byte rows) for S = 7.
+__host__ __device__ constexpr int oz_g1_width(int S) { return S <= OZ_GP ? 0 : (S <= 6 ? 2 : 4); }
+
+// Byte offset of slice t of element (row, k) in an operand's slice buffer with rows_pad rows and KB
+// k-blocks of 32: group 0 in 128-byte k-block rows, then group 1 in (32 x width)-byte rows.
+__host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long row, long long k, long long rows_pad,
+                                                              long long KB, int S) {
+    const long long kb = k >> 5, kk = k & 31;
+    if (t < OZ_GP) return ((row * KB + kb) << 7) + ((long long)t << 5) + kk;
+    return rows_pad * KB * 128 + (row * KB + kb) * (32LL * oz_g1_width(S)) + ((long long)(t - OZ_GP) << 5) + kk;
+}
+
+// Shared-memory ring of OZ_UNITS units of 16 KB: a k-block of the first pass takes two units (A and
+// B tiles of slice group 0), of the second pass three (plus A and B of group 1 at 64-byte rows, 8 KB
+// each) or four (S = 7: group 1 at 128-byte rows).
+constexpr int OZ_UNITS = 14;
+constexpr uint32_t OZ_UNIT = 16384;
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
-// so that each descriptor is a slot's base descriptor plus a constant (+2 per 32 bytes): the
+// so that each descriptor is a tile's base descriptor plus a constant (+2 per 32 bytes): the
 // single issuing thread runs barely ahead of the tensor core, and any latency between two MMAs
-// is tensor-core idle time.  da0 / da1: descriptors of the slots holding slice groups 0 / 1.
+// is tensor-core idle time.  dA0/dB0: group-0 tiles, dA1/dB1: group-1 tiles.
 template <int S, int P>
-__device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t da0, uint64_t da1, uint32_t acc_in) {
+__device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64_t dB0, uint64_t dA1, uint64_t dB1,
+                                             uint32_t acc_in) {
     constexpr int g0 = 2 + OZ_GP * P;
     constexpr int g1 = (1 + OZ_GP * (P + 1) < S + 1) ? 1 + OZ_GP * (P + 1) : S + 1;
-    constexpr uint64_t kB = OZ_SLOT_A >> 4;  // the B tile within a slot, in descriptor address units
 #pragma unroll
     for (int g = g0; g <= g1; ++g) {
 #pragma unroll
         for (int t = 1; t < g; ++t) {
             const int u = g - t;
-            const uint64_t a = (t > OZ_GP ? da1 : da0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
-            const uint64_t b = (u > OZ_GP ? da1 : da0) + kB + (uint64_t)(2 * ((u - 1) % OZ_GP));
+            const uint64_t a = (t > OZ_GP ? dA1 : dA0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
+            const uint64_t b = (u > OZ_GP ? dB1 : dB0) + (uint64_t)(2 * ((u - 1) % OZ_GP));
             mma_i8(acc0 + (uint32_t)(g - g0) * OZ_BN, a, b, t > 1 ? 1u : acc_in);
         }
     }
 }
 
+// Units per k-block of pass P.
+template <int S, int P>
+__host__ __device__ constexpr int oz_units_per_kblock() {
+    return P == 0 ? 2 : (oz_g1_width(S) == 2 ? 3 : 4);
+}
+
+// The MMA issuer's k-block loop of pass P (u, ph: next ring unit and its full-barrier parity).
+template <int S, int P>
+__device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
+                                         uint64_t *full_bar, uint64_t *empty_bar, int *err) {
+    constexpr int NU = oz_units_per_kblock<S, P>();
+    for (int kb = 0; kb < KB; ++kb) {
+        int us[NU];
+#pragma unroll
+        for (int j = 0; j < NU; ++j) {
+            us[j] = u;
+            if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
+            if (++u == OZ_UNITS) {
+                u = 0;
+                ph ^= 1u;
+            }
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t dA0 = sdesc_sw128(smem_base + (uint32_t)us[0] * OZ_UNIT);
+        const uint64_t dB0 = sdesc_sw128(smem_base + (uint32_t)us[1] * OZ_UNIT);
+        uint64_t dA1 = 0, dB1 = 0;
+        if constexpr (NU == 3) {
+            dA1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT);
+            dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_UNIT / 2);
+        } else if constexpr (NU == 4) {
+            dA1 = sdesc_sw128(smem_base + (uint32_t)us[2] * OZ_UNIT);
+            dB1 = sdesc_sw128(smem_base + (uint32_t)us[3] * OZ_UNIT);
+        }
+        issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
+#pragma unroll
+        for (int j = 0; j < NU; ++j) mma_commit(&empty_bar[us[j]]);  // units reusable once these MMAs read them
+    }
+    return true;
+}
+
 template <int S>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-    ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs args) {
+    ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmB0,
+                         const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
+                         OzArgs args) {
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
-    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *smem = oz_smem_raw;
+    if ((smem_u32(oz_smem_raw) & 1023u) != 0u) {  // the swizzled tiles need a 1024-byte aligned base
+        if (threadIdx.x == 0) atomicOr(args.err, 16);
+        return;
+    }
+    constexpr int W1 = oz_g1_width(S);
     const int npass = oz_ngroups(S);  // pass p: groups 4p+2 .. min(4p+5, S+1), slice groups 0..p
     // With two passes and at most two groups in the second, the first pass's FP64 partial sums stay
     // in TMEM columns [0, 256) (high words, then low words, per 32-column chunk) and the second
     // pass accumulates in columns [256, 512); otherwise the second pass adds into D.
     const bool keep = (npass == 2) && (S <= 6);
-    uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)OZ_SLOTS * OZ_SLOT);
-    uint64_t *empty_bar = full_bar + OZ_SLOTS;
-    uint64_t *pass_bar = empty_bar + OZ_SLOTS;  // MMAs of a pass complete
+    uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + (size_t)OZ_UNITS * OZ_UNIT);
+    uint64_t *empty_bar = full_bar + OZ_UNITS;
+    uint64_t *pass_bar = empty_bar + OZ_UNITS;  // MMAs of a pass complete
     uint64_t *free_bar = pass_bar + 1;          // epilogue has read the pass's accumulators
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(free_bar + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
     double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} of the tile's columns
-    __shared__ int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * OZ_BM, n0 = blockIdx.y * OZ_BN;
@@ -220,16 +294,20 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     double *const Dz = args.D + (long long)blockIdx.z * args.dz;
 
     if (threadIdx.x == 0) {
-        abort_flag = 0;
-        for (int s = 0; s < OZ_SLOTS; ++s) {
+        *abort_flag = 0;
+        for (int s = 0; s < OZ_UNITS; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
         mbar_init(pass_bar, 1);
         mbar_init(free_bar, 128);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA0)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB0)) : "memory");
+        if (W1 > 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA1)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB1)) : "memory");
+        }
     }
     if (warp >= 2) {
         const int c = threadIdx.x - 64;
@@ -245,25 +323,35 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {  // TMA producer: slot sequence = (pass, k-block, slice group)
-            int s = 0;            // next slot
+        if (lane == 0) {  // TMA producer: unit sequence = (pass, k-block, tile)
+            int u = 0;            // next unit
             uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
             bool wrapped = false;
-            for (int p = 0; p < npass && !abort_flag; ++p) {
-                for (int kb = 0; kb < KB && !abort_flag; ++kb) {
-                    const int kc = (args.kb0 + kz0 + kb) * 128;  // byte offset of the k-block in a row
-                    for (int q = 0; q <= p; ++q) {
-                        if (wrapped && !mbar_wait(&empty_bar[s], eph, args.err, 1)) {
-                            abort_flag = 1;
+            for (int p = 0; p < npass && !*abort_flag; ++p) {
+                const int nu = p == 0 ? 2 : (W1 == 2 ? 3 : 4);
+                for (int kb = 0; kb < KB && !*abort_flag; ++kb) {
+                    const int kbg = args.kb0 + kz0 + kb;
+                    for (int j = 0; j < nu; ++j) {
+                        if (wrapped && !mbar_wait(&empty_bar[u], eph, args.err, 1)) {
+                            *abort_flag = 1;
                             break;
                         }
-                        if (abort_flag) break;
-                        unsigned char *sa = smem + (size_t)s * OZ_SLOT;
-                        mbar_arrive_expect_tx(&full_bar[s], OZ_SLOT);
-                        tma_load_3d(&tmA, &full_bar[s], sa, kc, m0, q);
-                        tma_load_3d(&tmB, &full_bar[s], sa + OZ_SLOT_A, kc, n0, q);
-                        if (++s == OZ_SLOTS) {
-                            s = 0;
+                        unsigned char *dst = smem + (size_t)u * OZ_UNIT;
+                        mbar_arrive_expect_tx(&full_bar[u], OZ_UNIT);
+                        if (j == 0) {
+                            tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, m0);
+                        } else if (j == 1) {
+                            tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, n0);
+                        } else if (W1 == 2) {  // j == 2: A and B of group 1, 8 KB each
+                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 64, m0);
+                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_UNIT / 2, kbg * 64, n0);
+                        } else if (j == 2) {
+                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, m0);
+                        } else {
+                            tma_load_2d(&tmB1, &full_bar[u], dst, kbg * 128, n0);
+                        }
+                        if (++u == OZ_UNITS) {
+                            u = 0;
                             if (wrapped) eph ^= 1u;
                             wrapped = true;
                         }
@@ -273,50 +361,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
-            int s = 0;         // next slot
+            int u = 0;         // next unit
             uint32_t ph = 0;   // parity of its full-barrier phase
             bool ok = true;
             const uint32_t smem_base = smem_u32(smem);
             for (int p = 0; p < npass && ok; ++p) {
                 if (p > 0) {  // accumulators drained by the epilogue
                     if (!mbar_wait(free_bar, (p - 1) & 1, args.err, 8)) {
-                        abort_flag = 1;
+                        *abort_flag = 1;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
                 const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
-                for (int kb = 0; kb < KB; ++kb) {
-                    // slots of slice groups 0 and (second pass only) 1 of this k-block
-                    const int s0 = s;
-                    ok = mbar_wait(&full_bar[s], ph, args.err, 2);
-                    if (++s == OZ_SLOTS) {
-                        s = 0;
-                        ph ^= 1u;
-                    }
-                    int s1 = s0;
-                    if (ok && p > 0) {
-                        s1 = s;
-                        ok = mbar_wait(&full_bar[s], ph, args.err, 2);
-                        if (++s == OZ_SLOTS) {
-                            s = 0;
-                            ph ^= 1u;
-                        }
-                    }
-                    if (!ok) {
-                        abort_flag = 1;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint64_t da0 = sdesc_sw128(smem_base + (uint32_t)s0 * OZ_SLOT);
-                    const uint64_t da1 = sdesc_sw128(smem_base + (uint32_t)s1 * OZ_SLOT);
-                    if (p == 0)
-                        issue_kblock<S, 0>(acc0, da0, da1, kb > 0 ? 1u : 0u);
-                    else
-                        issue_kblock<S, 1>(acc0, da0, da1, kb > 0 ? 1u : 0u);
-                    mma_commit(&empty_bar[s0]);  // slots reusable once these MMAs have read them
-                    if (p > 0) mma_commit(&empty_bar[s1]);
-                }
+                if (p == 0)
+                    ok = mma_pass<S, 0>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
+                else if constexpr (S > OZ_GP)
+                    ok = mma_pass<S, 1>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
+                if (!ok) *abort_flag = 1;
                 mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
             }
         }
@@ -332,7 +394,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int p = 0; p < npass; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (!ok || abort_flag) break;
+            if (!ok || *abort_flag) break;
             const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
             const uint32_t acc0 = lane_base + ((p > 0 && keep) ? 256u : 0u);
             const bool last = (p + 1 == npass);
@@ -406,8 +468,6 @@ __device__ __forceinline__ int exp_of_max(double mx) {
     return e;
 }
 
-// Slices of x (scaled by 2^-e) for element k of a row: row_base points at (group 0, row, k-block 0);
-// group_stride = rows_pad * KB * 128 bytes (see the layout at the top of the file).
 // Slicing of one value: with r = x 2^-e (|r| < 1), slice t (t < S - 1) is the t-th base-128 digit
 // of |r| with the sign of x, and the last slice is the rounded remainder (clamped to +-127):
 //     T = x 2^{7(S-1) - e},  I = floor(|T|)  (the first S - 1 digits),  last = rint(128 (|T| - I)).
@@ -451,16 +511,14 @@ __device__ __forceinline__ void slice_digits(double x, const SliceScale &sc, int
         if (t == S - 1) d[t] = sg * (int)lastm;
 }
 
-// Slices of x for element k of a row: row_base points at (group 0, row, k-block 0);
-// group_stride = rows_pad * KB * 128 bytes (see the layout at the top of the file).
-__device__ __forceinline__ void slice_value(double x, const SliceScale &sc, int S, signed char *row_base,
-                                            long long group_stride, long long k) {
+// Slices of x for element k of row `row` of an operand slice buffer (rows_pad rows, KB k-blocks).
+__device__ __forceinline__ void slice_value(double x, const SliceScale &sc, int S, signed char *out, long long row,
+                                            long long rows_pad, long long KB, long long k) {
     int d[OZ_MAX_S];
     slice_digits(x, sc, S, d);
-    signed char *base = row_base + (k >> 5) * 128 + (k & 31);
 #pragma unroll
     for (int t = 0; t < OZ_MAX_S; ++t)
-        if (t < S) base[(long long)(t / OZ_GP) * group_stride + (t % OZ_GP) * 32] = (signed char)d[t];
+        if (t < S) out[oz_slice_offset(t, row, k, rows_pad, KB, S)] = (signed char)d[t];
 }
 
 constexpr int SL_NT = 256;
@@ -489,11 +547,10 @@ __global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const d
     mx = block_max(mx, sh);
     const int e = exp_of_max(mx);
     if (threadIdx.x == 0) ea[row] = e;
-    const long long gstride = mpad * kpad * OZ_GP;
     const SliceScale sc = slice_scale(e, S);
     for (long long j = threadIdx.x; j < kpad; j += SL_NT) {
         double x = (j < k) ? a[j * cs] : 0.0;
-        slice_value(x, sc, S, out + row * kpad * OZ_GP, gstride, j);
+        slice_value(x, sc, S, out, row, mpad, kpad >> 5, j);
     }
 }
 
@@ -517,7 +574,6 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
     mx = block_max(mx, sh);
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
-    const long long gstride = npad * kpad * OZ_GP;
     const SliceScale sc = slice_scale(ex, S);
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
@@ -526,7 +582,7 @@ __global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rh
             zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
             x = part ? v.y : v.x;
         }
-        slice_value(x, sc, S, out + c * kpad * OZ_GP, gstride, e);
+        slice_value(x, sc, S, out, c, npad, kpad >> 5, e);
     }
 }
 
@@ -552,7 +608,6 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
     mx = block_max(mx, sh);
     const int ex = exp_of_max(mx);
     if (threadIdx.x == 0) eb[c] = ex;
-    const long long gstride = npad * kpad * OZ_GP;
     const SliceScale sc = slice_scale(ex, S);
     for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
         double x = 0.0;
@@ -561,7 +616,7 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
             zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
             x = part ? v.y : v.x;
         }
-        slice_value(x, sc, S, out + c * kpad * OZ_GP, gstride, e);
+        slice_value(x, sc, S, out, c, npad, kpad >> 5, e);
     }
 }
 
@@ -588,8 +643,8 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {  // bytes 0..127 -> 
 }
 
 template <int S>
-__device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceScale &sc, signed char *row_base,
-                                            long long gstride, long long e0) {
+__device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceScale &sc, signed char *out, long long row,
+                                            long long rows_pad, long long KB, long long e0) {
     constexpr double kTwo52 = 4503599627370496.0, kRound = 6755399441055744.0;
     uint32_t lo[4], hi[4], last[4], sign = 0u;
 #pragma unroll
@@ -604,7 +659,6 @@ __device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceSca
         last[v] = min((uint32_t)__double2loint(__dadd_rn(fr * 128.0, kRound)), 127u);
         if (T < 0.0) sign |= 0xFFu << (8 * v);
     }
-    signed char *base = row_base + (e0 >> 5) * 128 + (e0 & 31);
 #pragma unroll
     for (int t = 0; t < S; ++t) {
         uint32_t w = 0u;
@@ -622,7 +676,7 @@ __device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceSca
             w |= dg << (8 * v);
         }
         w = (w & ~sign) | (neg_bytes(w) & sign);
-        *reinterpret_cast<uint32_t *>(base + (long long)(t / OZ_GP) * gstride + (t % OZ_GP) * 32) = w;
+        *reinterpret_cast<uint32_t *>(out + oz_slice_offset(t, row, e0, rows_pad, KB, S)) = w;
     }
 }
 
@@ -757,15 +811,13 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
         for (int h = 0; h < 2; ++h) {
             const int col = c0 + h;
             const bool isK = col < 4;
-            const long long gstride = (isK ? npadK : npadP) * kpad * OZ_GP;
-            signed char *row_base = (isK ? outK : outP) + cidx[col] * kpad * OZ_GP;
             const SliceScale sc = slice_scale(ex[col], S);
             const double *src = stage + h * nn;
             for (long long e0 = 4LL * tid; e0 < kpad; e0 += 4LL * RS_NT) {
                 double x[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) x[u] = (e0 + u < nn) ? src[e0 + u] : 0.0;
-                slice_pack4<S>(x, sc, row_base, gstride, e0);
+                slice_pack4<S>(x, sc, isK ? outK : outP, cidx[col], isK ? npadK : npadP, kpad >> 5, e0);
             }
         }
         __syncthreads();  // the stage is rewritten by the next round
@@ -786,27 +838,42 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-int make_slice_map(CUtensorMap *map, const signed char *base, long long kpad, long long rows_pad, int S, int box_rows) {
-    // dimension 0: bytes of a row of one slice group (kpad/32 k-blocks x 128 B), dimension 1: rows,
-    // dimension 2: slice groups; a box is one 128-byte k-block segment of box_rows rows
+// 2-D map over one slice group of an operand: dimension 0 = bytes of a row (KB k-block segments of
+// seg_bytes), dimension 1 = rows; a box is one k-block segment of box_rows rows.
+int make_group_map(CUtensorMap *map, const signed char *base, long long KB, int seg_bytes, long long rows_pad,
+                   int box_rows) {
     auto enc = get_encode();
     if (!enc) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
         return PHF_ERR_CUDA;
     }
-    const long long rowb = kpad * OZ_GP;
-    cuuint64_t dims[3] = {(cuuint64_t)rowb, (cuuint64_t)rows_pad, (cuuint64_t)oz_ngroups(S)};
-    cuuint64_t strides[2] = {(cuuint64_t)rowb, (cuuint64_t)(rowb * rows_pad)};
-    cuuint32_t box[3] = {128u, (cuuint32_t)box_rows, 1u};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char *>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const long long rowb = KB * seg_bytes;
+    cuuint64_t dims[2] = {(cuuint64_t)rowb, (cuuint64_t)rows_pad};
+    cuuint64_t strides[1] = {(cuuint64_t)rowb};
+    cuuint32_t box[2] = {(cuuint32_t)seg_bytes, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<signed char *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     seg_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
         return PHF_ERR_CUDA;
     }
     return PHF_OK;
+}
+
+// Group-0 and group-1 maps of an operand's slice buffer (group 1 = group 0 when S <= 4: unused).
+int make_slice_maps(CUtensorMap *g0, CUtensorMap *g1, const signed char *base, long long kpad, long long rows_pad,
+                    int S, int box_rows) {
+    const long long KB = kpad / OZ_BK;
+    PHF_TRY(make_group_map(g0, base, KB, 128, rows_pad, box_rows));
+    const int w = oz_g1_width(S);
+    if (w == 0) {
+        *g1 = *g0;
+        return PHF_OK;
+    }
+    return make_group_map(g1, base + rows_pad * KB * 128, KB, 32 * w, rows_pad, box_rows);
 }
 
 }  // namespace
@@ -880,11 +947,11 @@ int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *e
 }
 
 size_t oz_slice_bytes(long long rows_pad, long long k, int S) {
-    return (size_t)oz_ngroups(S) * OZ_GP * (size_t)rows_pad * (size_t)oz_pad_k(k);
+    return (size_t)(OZ_GP + oz_g1_width(S)) * (size_t)rows_pad * (size_t)oz_pad_k(k);
 }
 
-// alignment slack, the slot ring, 2 OZ_SLOTS + 2 mbarriers, the TMEM address slot, the column scales
-size_t oz_smem_bytes() { return 1024 + (size_t)OZ_SLOTS * OZ_SLOT + (2 * OZ_SLOTS + 2) * 8 + 8 + OZ_BN * 8; }
+// the unit ring, 2 OZ_UNITS + 2 mbarriers, the TMEM address and abort flag, the column scales
+size_t oz_smem_bytes() { return (size_t)OZ_UNITS * OZ_UNIT + (2 * OZ_UNITS + 2) * 8 + 8 + OZ_BN * 8; }
 
 // D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
 // k is split into passes short enough for exact int32 group sums; later passes add into D.
@@ -894,7 +961,7 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
 }
 
 namespace {
-using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, OzArgs);
+using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap, OzArgs);
 
 OzKernelFn oz_kernel_for(int S) {
     switch (S) {
@@ -928,10 +995,10 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     const long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
     if (nsplit <= 1 || kb_total > kb_pass || kb_total < 2 * nsplit)
         return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, 0, trans, err, st);
-    CUtensorMap ta, tb;
+    CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
-    PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
-    PHF_TRY(make_slice_map(&tb, Bsl, kpad, npad, S, OZ_BN));
+    PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, OZ_BN));
     const long long rows = trans ? n : m;
     const long long dz = rows * ldd;
     OzArgs a;
@@ -959,7 +1026,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), (unsigned)nsplit);
     {
         ProfScope prof(st, PROF_JK);
-        kern<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+        kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
     }
     ++g_launches;
     PHF_CHECK_LAUNCH();
@@ -978,10 +1045,10 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
-    CUtensorMap ta, tb;
+    CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
-    PHF_TRY(make_slice_map(&ta, Asl, kpad, mpad, S, OZ_BM));
-    PHF_TRY(make_slice_map(&tb, Bsl, kpad, npad, S, OZ_BN));
+    PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, OZ_BN));
     // k-blocks per pass: S * kpass * 127^2 < 2^31
     long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
     if (kb_pass < 1) kb_pass = 1;
@@ -1012,7 +1079,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
-            kern<<<grid, OZ_THREADS, smem, st>>>(ta, tb, a);
+            kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
         }
         ++g_launches;
         PHF_CHECK_LAUNCH();

@@ -6,9 +6,11 @@
 // batches need no copies.  A may be real (real x complex products: Cholesky vectors and
 // the one-electron matrix applied to complex orbitals).
 //
-// Tiling: 64 x 64 output tile per 256-thread CTA, k-step 16, each thread owns a 4 x 4
-// block of complex accumulators (rows ty + 16 i, columns tx + 16 j); the next k-tile is
-// prefetched into registers while the current one is consumed from shared memory.
+// Tiling: BM x BN output tile per 256-thread CTA (64 x 64, 128 x 32 or 32 x 128), k-step 16; the
+// next k-tile is prefetched into registers while the current one is consumed from shared memory.
+// The products run on the FP64 tensor cores (mma.sync m8n8k4 .f64): each of the 8 warps owns a
+// 32 x 16 block of the tile as 4 x 2 blocks of 8 x 8, and a complex product is four real MMAs
+// (re re, -im im, re im, im re), two for a real A.
 #include <type_traits>
 
 #include "phf_common.cuh"
@@ -35,22 +37,31 @@ __device__ __forceinline__ double load_d(const View &v, long long off) {
     return reinterpret_cast<const double *>(v.p)[off];
 }
 
-// BM x BN output tile, 256 threads in a (BM/4) x (BN/4) grid, 4 x 4 complex accumulators each:
-// thread (ty, tx) owns rows ty + (BM/4) i and columns tx + (BN/4) j.  64 x 64 serves general
-// shapes; 128 x 32 serves the narrow per-point products (N <= 32 columns), 32 x 128 the
-// N-row products bra^H Y and bra^H F X (m = N <= 32) over all points of a chunk.
+// D (8 x 8) += A (8 x 4, row-major) B (4 x 8, column-major), FP64.  Lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2 (l%4) + {0, 1}].
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// BM x BN output tile, 256 threads = 8 warps of 32 x 16 (warp w: rows 32 (w / (BN/16)), columns
+// 16 (w % (BN/16))).  64 x 64 serves general shapes; 128 x 32 the narrow per-point products
+// (N <= 32 columns), 32 x 128 the N-row products bra^H Y and bra^H F X (m = N <= 32) over all
+// points of a chunk.
 template <bool AREAL, int BM, int BN>
 __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
                                                    zc beta, OutView C, const long long *__restrict__ offs) {
     using TA = typename ATile<AREAL>::T;
-    constexpr int TX = BN / 4, TY = BM / 4;
-    static_assert(TX * TY == NT, "tile/thread mismatch");
+    constexpr int WARPS_N = BN / 16;
+    static_assert((BM / 32) * WARPS_N * 32 == NT, "tile/warp mismatch");
     constexpr int LA = (BM * BK) / NT, LB = (BN * BK) / NT;  // elements loaded per thread
     __shared__ TA As[BK][BM + 1];
     __shared__ zc Bs[BK][BN + 1];
 
-    const int tid = threadIdx.x;
-    const int tx = tid % TX, ty = tid / TX;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp / WARPS_N) * 32, wc = (warp % WARPS_N) * 16;  // warp block within the tile
+    const int fr = lane >> 2, fk = lane & 3;                            // fragment row / k of this lane
     const long long bz = blockIdx.x / ntn;
     const int tn = blockIdx.x - bz * ntn;
     const int row0 = blockIdx.y * BM, col0 = tn * BN;
@@ -112,11 +123,11 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
         }
     };
 
-    double accr[4][4], acci[4][4];
+    double cr[4][2][2], ci[4][2][2];  // 8 x 8 blocks (bi, bj): real and imaginary accumulators
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) accr[i][j] = acci[i][j] = 0.0;
+        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
 
     fetch(0);
     for (int k0 = 0; k0 < k; k0 += BK) {
@@ -125,48 +136,49 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
         __syncthreads();
         if (k0 + BK < k) fetch(k0 + BK);
 #pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            TA a[4];
-            zc b[4];
+        for (int kk = 0; kk < BK; kk += 4) {
+            zc b[2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + TY * i];
+            for (int j = 0; j < 2; ++j) b[j] = Bs[kk + fk][wc + 8 * j + fr];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + TX * j];
+            for (int i = 0; i < 4; ++i) {
+                const TA a = As[kk + fk][wr + 8 * i + fr];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
+                for (int j = 0; j < 2; ++j) {
                     if constexpr (AREAL) {
-                        accr[i][j] = fma(a[i], b[j].x, accr[i][j]);
-                        acci[i][j] = fma(a[i], b[j].y, acci[i][j]);
+                        dmma884(cr[i][j], a, b[j].x);
+                        dmma884(ci[i][j], a, b[j].y);
                     } else {
-                        accr[i][j] = fma(a[i].x, b[j].x, accr[i][j]);
-                        accr[i][j] = fma(-a[i].y, b[j].y, accr[i][j]);
-                        acci[i][j] = fma(a[i].x, b[j].y, acci[i][j]);
-                        acci[i][j] = fma(a[i].y, b[j].x, acci[i][j]);
+                        dmma884(cr[i][j], a.x, b[j].x);
+                        dmma884(cr[i][j], -a.y, b[j].y);
+                        dmma884(ci[i][j], a.x, b[j].y);
+                        dmma884(ci[i][j], a.y, b[j].x);
                     }
                 }
+            }
         }
     }
     const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        int gi = row0 + ty + TY * i;
+        const int gi = row0 + wr + 8 * i + fr;
         if (gi >= m) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int gj = col0 + tx + TX * j;
-            if (gj >= n) continue;
-            long long off = oc + (long long)gi * C.rs + (long long)gj * C.cs;
-            zc v = alpha * zc{accr[i][j], acci[i][j]};
-            if (C.real) {
-                double *cp = reinterpret_cast<double *>(C.p);
-                cp[off] = use_beta ? v.x + beta.x * cp[off] : v.x;
-            } else {
-                if (use_beta) v = v + beta * C.p[off];
-                C.p[off] = v;
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = col0 + wc + 8 * j + 2 * fk + h;
+                if (gj >= n) continue;
+                long long off = oc + (long long)gi * C.rs + (long long)gj * C.cs;
+                zc v = alpha * zc{cr[i][j][h], ci[i][j][h]};
+                if (C.real) {
+                    double *cp = reinterpret_cast<double *>(C.p);
+                    cp[off] = use_beta ? v.x + beta.x * cp[off] : v.x;
+                } else {
+                    if (use_beta) v = v + beta * C.p[off];
+                    C.p[off] = v;
+                }
             }
-        }
     }
 }
 

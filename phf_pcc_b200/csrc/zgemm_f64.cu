@@ -45,10 +45,27 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+__device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int bytes_valid, int size) {
+    if (size == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes_valid) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes_valid) : "memory");
+}
+
+constexpr int ZG_STAGES = 3;  // shared-memory stages of the k loop (cp.async pipeline)
+
+template <bool AREAL, int BM, int BN>
+constexpr size_t zg_smem_bytes() {
+    return (size_t)ZG_STAGES * BK * ((BM + 1) * (AREAL ? sizeof(double) : sizeof(zc)) + (BN + 1) * sizeof(zc));
+}
+
 // BM x BN output tile, 256 threads = 8 warps of 32 x 16 (warp w: rows 32 (w / (BN/16)), columns
 // 16 (w % (BN/16))).  64 x 64 serves general shapes; 128 x 32 the narrow per-point products
 // (N <= 32 columns), 32 x 128 the N-row products bra^H Y and bra^H F X (m = N <= 32) over all
-// points of a chunk.
+// points of a chunk.  Tiles of A and B reach shared memory by element-wise cp.async (16 bytes a
+// complex element, 8 a real one; out-of-range elements are zero-filled) through ZG_STAGES stages;
+// conjugation is applied when fragments are read.  A real B (only the exchange-matrix build) is
+// loaded with plain loads into the same stages.
 template <bool AREAL, int BM, int BN>
 __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
                                                    zc beta, OutView C, const long long *__restrict__ offs) {
@@ -56,8 +73,10 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
     constexpr int WARPS_N = BN / 16;
     static_assert((BM / 32) * WARPS_N * 32 == NT, "tile/warp mismatch");
     constexpr int LA = (BM * BK) / NT, LB = (BN * BK) / NT;  // elements loaded per thread
-    __shared__ TA As[BK][BM + 1];
-    __shared__ zc Bs[BK][BN + 1];
+    constexpr int PA = BM + 1, PB = BN + 1;                    // row pitches (elements)
+    extern __shared__ __align__(16) unsigned char zg_smem[];
+    TA *As = reinterpret_cast<TA *>(zg_smem);                                      // [stage][kk][i]
+    zc *Bs = reinterpret_cast<zc *>(zg_smem + (size_t)ZG_STAGES * BK * PA * sizeof(TA));  // [stage][kk][j]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = (warp / WARPS_N) * 32, wc = (warp % WARPS_N) * 16;  // warp block within the tile
@@ -74,52 +93,42 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
     }
     const bool a_mfast = (A.rs == 1);  // element order of the A tile loads
     const bool b_nfast = (B.cs == 1);
+    const double sa = (!AREAL && A.conj) ? -1.0 : 1.0;  // imaginary-part signs (conjugated views)
+    const double sb = B.conj ? -1.0 : 1.0;
+    const uint32_t as_base = (uint32_t)__cvta_generic_to_shared(As);
+    const uint32_t bs_base = (uint32_t)__cvta_generic_to_shared(Bs);
+    const int nkt = (k + BK - 1) / BK;
 
-    TA ra[LA];
-    zc rb[LB];
-    auto fetch = [&](int k0) {
+    auto load_stage = [&](int stage, int kt) {
+        const int k0 = kt * BK;
 #pragma unroll
         for (int r = 0; r < LA; ++r) {
-            int e = tid + NT * r;
+            const int e = tid + NT * r;
             int i, kk;
             if (a_mfast) { i = e % BM; kk = e / BM; }
             else { kk = e % BK; i = e / BK; }
-            int gi = row0 + i, gk = k0 + kk;
-            if (gi < m && gk < k) {
-                long long off = oa + (long long)gi * A.rs + (long long)gk * A.cs;
-                if constexpr (AREAL) ra[r] = load_d(A, off);
-                else ra[r] = load_z(A, off);
+            const int gi = row0 + i, gk = k0 + kk;
+            const bool ok = gi < m && gk < k;
+            const long long off = ok ? oa + (long long)gi * A.rs + (long long)gk * A.cs : 0;
+            cp_async(as_base + (uint32_t)(((stage * BK + kk) * PA + i) * sizeof(TA)),
+                     reinterpret_cast<const unsigned char *>(A.p) + off * (long long)sizeof(TA),
+                     ok ? (int)sizeof(TA) : 0, (int)sizeof(TA));
+        }
+#pragma unroll
+        for (int r = 0; r < LB; ++r) {
+            const int e = tid + NT * r;
+            int j, kk;
+            if (b_nfast) { j = e % BN; kk = e / BN; }
+            else { kk = e % BK; j = e / BK; }
+            const int gj = col0 + j, gk = k0 + kk;
+            const bool ok = gj < n && gk < k;
+            const long long off = ok ? ob + (long long)gk * B.rs + (long long)gj * B.cs : 0;
+            if (B.real) {
+                Bs[(stage * BK + kk) * PB + j] = zc{ok ? reinterpret_cast<const double *>(B.p)[off] : 0.0, 0.0};
             } else {
-                if constexpr (AREAL) ra[r] = 0.0;
-                else ra[r] = zc{0.0, 0.0};
+                cp_async(bs_base + (uint32_t)(((stage * BK + kk) * PB + j) * sizeof(zc)),
+                         reinterpret_cast<const zc *>(B.p) + off, ok ? 16 : 0, 16);
             }
-        }
-#pragma unroll
-        for (int r = 0; r < LB; ++r) {
-            int e = tid + NT * r;
-            int j, kk;
-            if (b_nfast) { j = e % BN; kk = e / BN; }
-            else { kk = e % BK; j = e / BK; }
-            int gj = col0 + j, gk = k0 + kk;
-            rb[r] = (gj < n && gk < k) ? load_z(B, ob + (long long)gk * B.rs + (long long)gj * B.cs) : zc{0.0, 0.0};
-        }
-    };
-    auto stash = [&]() {
-#pragma unroll
-        for (int r = 0; r < LA; ++r) {
-            int e = tid + NT * r;
-            int i, kk;
-            if (a_mfast) { i = e % BM; kk = e / BM; }
-            else { kk = e % BK; i = e / BK; }
-            As[kk][i] = ra[r];
-        }
-#pragma unroll
-        for (int r = 0; r < LB; ++r) {
-            int e = tid + NT * r;
-            int j, kk;
-            if (b_nfast) { j = e % BN; kk = e / BN; }
-            else { kk = e % BK; j = e / BK; }
-            Bs[kk][j] = rb[r];
         }
     };
 
@@ -129,35 +138,48 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0,
 #pragma unroll
         for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
 
-    fetch(0);
-    for (int k0 = 0; k0 < k; k0 += BK) {
-        __syncthreads();
-        stash();
-        __syncthreads();
-        if (k0 + BK < k) fetch(k0 + BK);
+#pragma unroll
+    for (int st = 0; st < ZG_STAGES - 1; ++st) {
+        if (st < nkt) load_stage(st, st);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int kt = 0; kt < nkt; ++kt) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(ZG_STAGES - 2) : "memory");
+        __syncthreads();  // stage kt landed for every thread; stage kt - 1 is no longer read
+        const int stage = kt % ZG_STAGES;
+        const TA *At = As + (size_t)stage * BK * PA;
+        const zc *Bt = Bs + (size_t)stage * BK * PB;
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
             zc b[2];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) b[j] = Bs[kk + fk][wc + 8 * j + fr];
+            for (int j = 0; j < 2; ++j) {
+                b[j] = Bt[(kk + fk) * PB + wc + 8 * j + fr];
+                b[j].y *= sb;
+            }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const TA a = As[kk + fk][wr + 8 * i + fr];
+                TA a = At[(kk + fk) * PA + wr + 8 * i + fr];
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     if constexpr (AREAL) {
                         dmma884(cr[i][j], a, b[j].x);
                         dmma884(ci[i][j], a, b[j].y);
                     } else {
+                        const double ay = a.y * sa;
                         dmma884(cr[i][j], a.x, b[j].x);
-                        dmma884(cr[i][j], -a.y, b[j].y);
+                        dmma884(cr[i][j], -ay, b[j].y);
                         dmma884(ci[i][j], a.x, b[j].y);
-                        dmma884(ci[i][j], a.y, b[j].x);
+                        dmma884(ci[i][j], ay, b[j].x);
                     }
                 }
             }
         }
+        const int kn = kt + ZG_STAGES - 1;  // refill the stage computed in the previous iteration
+        if (kn < nkt) load_stage(kn % ZG_STAGES, kn);
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -193,11 +215,19 @@ int launch_tile(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, 
         return PHF_ERR_ARG;
     }
     dim3 grid((unsigned)gx, (unsigned)ntm, 1);
-    ProfScope prof(st, -1);
-    if (A.real)
-        zgemm_kernel<true, BM, BN><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
-    else
-        zgemm_kernel<false, BM, BN><<<grid, NT, 0, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+    if (A.real) {
+        constexpr size_t smem = zg_smem_bytes<true, BM, BN>();
+        PHF_CUDA(cudaFuncSetAttribute(zgemm_kernel<true, BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        ProfScope prof(st, -1);
+        zgemm_kernel<true, BM, BN><<<grid, NT, smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+    } else {
+        constexpr size_t smem = zg_smem_bytes<false, BM, BN>();
+        PHF_CUDA(cudaFuncSetAttribute(zgemm_kernel<false, BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        ProfScope prof(st, -1);
+        zgemm_kernel<false, BM, BN><<<grid, NT, smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+    }
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -21,8 +21,8 @@
 // segments (SWIZZLE_128B / SWIZZLE_64B) then carries several slices at once, and the MMA picks a
 // slice by a +32-byte offset of its K-major descriptor.
 //
-// Kernel shape (one CTA per 128 x 128 output tile, 6 warps), row tiles fastest in the grid so that
-// the CTAs in flight share B column tiles through L2:
+// Kernel shape (one CTA per 128 x 128 output tile, 6 warps); in launch order the CTAs sweep the
+// column tiles in groups of eight row tiles, so that the A and B tiles in use fit in L2 together:
 //   warp 0      TMA producer into a ring of fourteen 16 KB units (full/empty mbarrier per unit):
 //               per 32-element k-block the A and B boxes of group 0 (a unit each) and, in the
 //               second pass, of group 1 (one unit holding both 8 KB boxes for S = 5, 6)
@@ -199,6 +199,7 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
 // B tiles of slice group 0), of the second pass three (plus A and B of group 1 at 64-byte rows, 8 KB
 // each) or four (S = 7: group 1 at 128-byte rows).
 constexpr int OZ_UNITS = 14;
+constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
 constexpr uint32_t OZ_UNIT = 16384;
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
@@ -288,7 +289,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} of the tile's columns
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * OZ_BM, n0 = blockIdx.y * OZ_BN;
+    // grouped raster: CTAs in launch order sweep the column tiles in groups of OZ_GROUP_M row tiles,
+    // so that the A and B tiles the resident CTAs share fit in L2 together
+    int m0, n0;
+    {
+        const int mt = gridDim.x, nt = gridDim.y;
+        const int L = blockIdx.y * mt + blockIdx.x;
+        const int width = OZ_GROUP_M * nt;
+        const int first = (L / width) * OZ_GROUP_M;
+        const int gm = min(mt - first, OZ_GROUP_M);
+        m0 = (first + (L % width) % gm) * OZ_BM;
+        n0 = ((L % width) / gm) * OZ_BN;
+    }
     const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
     const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
     double *const Dz = args.D + (long long)blockIdx.z * args.dz;
@@ -1060,7 +1072,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         return PHF_ERR_ARG;
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // row tiles fastest
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // mapped to tiles by the grouped raster
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;

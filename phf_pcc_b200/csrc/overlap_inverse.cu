@@ -1,5 +1,6 @@
 // Batched FP64 complex inverse, determinant and log-determinant of the rotated overlaps
-// S_w = bra^H R_w ket (N x N), one CTA per grid point, the matrix resident in shared memory.
+// S_w = bra^H R_w ket (N x N): one warp per grid point for N <= 32, else one CTA per grid point,
+// the matrix resident in shared memory.
 //
 // Replaces InvertC (ZGETRF + ZGETRI) and determinantC (ZGETRF) of PHF_fort/Wrappers.f90:195-336
 // as called from RDM (PHF_fort/PHFTools.f90:259-260).  Algorithm: in-place Gauss-Jordan
@@ -148,12 +149,156 @@ __global__ void __launch_bounds__(NT) gj_inverse_kernel(int N, const zc *__restr
     }
 }
 
+
+// N <= 32: one warp per matrix (lane j owns column j), four matrices per CTA.  The same
+// Gauss-Jordan steps as gj_inverse_kernel -- pivot = first index of the largest |re| + |im| in rows
+// k..N-1 of column k, identical element updates -- but warp-synchronous: the pivot search is a
+// shuffle arg-max and the steps are separated by __syncwarp only.  The pivots are kept and lane 0
+// forms det and log det from them at the end, in pivot order.
+constexpr int WI_WARPS = 4, WI_P = 33;  // matrices per CTA, row pitch (complex) of the shared copy
+
+__host__ __device__ constexpr size_t wi_warp_bytes() { return (size_t)(32 * WI_P + 64) * sizeof(zc) + 32 * sizeof(int); }
+
+__global__ void __launch_bounds__(WI_WARPS * 32) gj_inverse_warp_kernel(
+    int N, int batch, const zc *__restrict__ S, long long s_rs, long long s_bs, zc *__restrict__ Sinv, long long i_rs,
+    long long i_bs, zc *__restrict__ det, zc *__restrict__ logdet, int *__restrict__ flag) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long b = (long long)blockIdx.x * WI_WARPS + warp;
+    if (b >= batch) return;  // the whole warp leaves; nothing below synchronises beyond the warp
+    unsigned char *base = smem_raw + (size_t)warp * wi_warp_bytes();
+    zc *A = reinterpret_cast<zc *>(base);  // N x N, row i at A + i WI_P
+    zc *colk = A + 32 * WI_P;              // saved column k
+    zc *pivs = colk + 32;                  // pivots in order
+    int *perm = reinterpret_cast<int *>(pivs + 32);
+    const unsigned full = 0xffffffffu;
+    const bool own = lane < N;
+
+    const zc *Sb = S + b * s_bs;
+    int bad = 0;
+    for (int i = 0; i < N; ++i)
+        if (own) {
+            const zc v = Sb[(long long)i * s_rs + lane];
+            if (!isfinite(v.x) || !isfinite(v.y)) bad = 2;
+            A[i * WI_P + lane] = v;
+        }
+    bad = __reduce_max_sync(full, bad);
+    __syncwarp();
+
+    for (int k = 0; k < N && bad == 0; ++k) {
+        double a = -1.0;
+        int idx = N;
+        if (lane >= k && lane < N) {
+            const double v = abs1(A[lane * WI_P + k]);
+            if (v > a) {  // NaN never becomes a candidate
+                a = v;
+                idx = lane;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double oa = __shfl_xor_sync(full, a, off);
+            const int oi = __shfl_xor_sync(full, idx, off);
+            if (oa > a || (oa == a && oi < idx)) {
+                a = oa;
+                idx = oi;
+            }
+        }
+        const int p = idx;
+        if (!(a > 0.0)) {  // exactly singular (or NaN pivot)
+            bad = (a == 0.0) ? 1 : 2;
+            break;
+        }
+        if (p != k && own) {
+            const zc t = A[k * WI_P + lane];
+            A[k * WI_P + lane] = A[p * WI_P + lane];
+            A[p * WI_P + lane] = t;
+        }
+        __syncwarp();
+        const zc piv = A[k * WI_P + k];
+        const zc inv = divz(mkz(1.0, 0.0), piv);
+        zc rk = mkz(0.0, 0.0);
+        if (own) {
+            rk = (lane == k) ? inv : A[k * WI_P + lane] * inv;
+            colk[lane] = A[lane * WI_P + k];
+        }
+        if (lane == 0) {
+            pivs[k] = piv;
+            perm[k] = p;
+        }
+        __syncwarp();
+        if (own) {
+            for (int i = 0; i < N; ++i) {
+                if (i == k) {
+                    A[i * WI_P + lane] = rk;
+                } else {
+                    const zc x = (lane == k) ? mkz(0.0, 0.0) : A[i * WI_P + lane];
+                    A[i * WI_P + lane] = x - colk[i] * rk;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (bad == 0) {
+        // undo the row interchanges as column interchanges, in reverse order (lane i swaps row i)
+        for (int k = N - 1; k >= 0; --k) {
+            const int p = perm[k];
+            if (p != k && own) {
+                const zc t = A[lane * WI_P + k];
+                A[lane * WI_P + k] = A[lane * WI_P + p];
+                A[lane * WI_P + p] = t;
+            }
+            __syncwarp();
+        }
+    }
+    zc *Ib = Sinv + b * i_bs;
+    for (int i = 0; i < N; ++i)
+        if (own) Ib[(long long)i * i_rs + lane] = bad ? mkz(0.0, 0.0) : A[i * WI_P + lane];
+    if (lane == 0) {
+        if (bad) {
+            det[b] = mkz(0.0, 0.0);
+            logdet[b] = mkz(-INFINITY, 0.0);
+            atomicOr(flag, bad);
+        } else {
+            zc d = mkz(1.0, 0.0);
+            double logabs = 0.0, phase = 0.0;
+            int nswap = 0;
+            for (int k = 0; k < N; ++k) {
+                const zc piv = pivs[k];
+                d = d * piv;
+                logabs += log(hypot(piv.x, piv.y));
+                phase += atan2(piv.y, piv.x);
+                if (perm[k] != k) {
+                    d = mkz(-d.x, -d.y);
+                    ++nswap;
+                }
+            }
+            det[b] = d;
+            const double pi = 3.14159265358979323846;
+            double ph = fmod(phase + pi * (nswap & 1), 2.0 * pi);
+            if (ph > pi) ph -= 2.0 * pi;
+            if (ph <= -pi) ph += 2.0 * pi;
+            logdet[b] = mkz(logabs, ph);
+        }
+    }
+}
+
 }  // namespace
 
 size_t overlap_inverse_smem(int N) { return (size_t)N * N * sizeof(zc) + 2 * (size_t)N * sizeof(zc) + N * sizeof(int); }
 
 int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_bs, zc *Sinv, long long i_rs,
                     long long i_bs, zc *det, zc *logdet, int *flag, cudaStream_t st) {
+    if (N <= 32) {
+        const size_t smem = WI_WARPS * wi_warp_bytes();
+        PHF_CUDA(cudaFuncSetAttribute(gj_inverse_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ProfScope prof(st, PROF_INVERSE);
+        gj_inverse_warp_kernel<<<(unsigned)((batch + WI_WARPS - 1) / WI_WARPS), WI_WARPS * 32, smem, st>>>(
+            N, batch, S, s_rs, s_bs, Sinv, i_rs, i_bs, det, logdet, flag);
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+        return PHF_OK;
+    }
     size_t smem = overlap_inverse_smem(N);
     PHF_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ProfScope prof(st, PROF_INVERSE);

@@ -176,12 +176,20 @@ __global__ void __launch_bounds__(WI_WARPS * 32) gj_inverse_warp_kernel(
 
     const zc *Sb = S + b * s_bs;
     int bad = 0;
-    for (int i = 0; i < N; ++i)
-        if (own) {
-            const zc v = Sb[(long long)i * s_rs + lane];
-            if (!isfinite(v.x) || !isfinite(v.y)) bad = 2;
-            A[i * WI_P + lane] = v;
+    if (own) {
+        for (int i0 = 0; i0 < N; i0 += 8) {  // eight global loads in flight, then the shared stores
+            zc v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (i0 + u < N) v[u] = Sb[(long long)(i0 + u) * s_rs + lane];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (i0 + u < N) {
+                    if (!isfinite(v[u].x) || !isfinite(v[u].y)) bad = 2;
+                    A[(i0 + u) * WI_P + lane] = v[u];
+                }
         }
+    }
     bad = __reduce_max_sync(full, bad);
     __syncwarp();
 
@@ -227,14 +235,32 @@ __global__ void __launch_bounds__(WI_WARPS * 32) gj_inverse_warp_kernel(
             perm[k] = p;
         }
         __syncwarp();
-        if (own) {
-            for (int i = 0; i < N; ++i) {
-                if (i == k) {
-                    A[i * WI_P + lane] = rk;
-                } else {
-                    const zc x = (lane == k) ? mkz(0.0, 0.0) : A[i * WI_P + lane];
-                    A[i * WI_P + lane] = x - colk[i] * rk;
+        if (own) {  // rows in batches of eight: loads, then arithmetic, then stores (latencies overlap)
+            for (int i0 = 0; i0 < N; i0 += 8) {
+                zc av[8], cv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int i = i0 + u;
+                    if (i < N) {
+                        av[u] = A[i * WI_P + lane];
+                        cv[u] = colk[i];
+                    }
                 }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int i = i0 + u;
+                    if (i < N) {
+                        if (i == k) {
+                            av[u] = rk;
+                        } else {
+                            const zc x = (lane == k) ? mkz(0.0, 0.0) : av[u];
+                            av[u] = x - cv[u] * rk;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (i0 + u < N) A[(i0 + u) * WI_P + lane] = av[u];
             }
         }
         __syncwarp();

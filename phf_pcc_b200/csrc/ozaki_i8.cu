@@ -634,12 +634,20 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
 
 
 // ------------------------------------------------------------------ fused density + operand slicing
+// D (8 x 8) += A (8 x 4, row-major) B (4 x 8, column-major), FP64 tensor cores.
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
 // ERI form with n <= 64: the exchange (K) and Coulomb (P) operand columns straight from X_w and
 // bra, without writing the M x M density to HBM.  CTA (w, pair): pair 0 forms rho_aa, rho_bb and
 // P = rho_aa + rho_bb, pair 1 forms rho_ab and rho_ba, each as
 //     rho_st[l][j] = sum_m X_w[2l+s][m] conj(bra[2j+t][m])
-// with the FMA sequence of zgemm_kernel (m ascending), so every column, its exponent and its
-// slices are exactly those of the density GEMM followed by slice_rho_cols / slice_p_cols.
+// with the tensor-core MMA sequence of zgemm_kernel (m ascending in steps of four), so every
+// column, its exponent and its slices are those of the density GEMM followed by slice_rho_cols /
+// slice_p_cols.
 constexpr int RS_NT = 256, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded row pitch (complex)
 
 // operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
@@ -702,17 +710,21 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
     zc *bs = xs + 2 * RS_MC * RS_P;            // [t][mm][j]: bra[2j+t][m0+mm]
     double *stage = reinterpret_cast<double *>(rs_smem);  // one column (n^2 values) after the products
     __shared__ double red[6 * (RS_NT / 32)];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x;
     const long long w = blockIdx.x >> 1;
     const int pair = (int)(blockIdx.x & 1);
-    // thread tile: rows l = ty + 16 i, columns j = tx + 16 jj of both spin blocks q = 0, 1
-    double ar[2][4][4], ai[2][4][4];
+    // warp tile: rows wr + 8 bi + fr, columns wc + 8 bj + 2 fk + h of both spin blocks q = 0, 1,
+    // as FP64 tensor-core products (mma.sync m8n8k4: lane l holds A[l/4][l%4], B[l%4][l/4],
+    // D[l/4][2 (l%4) + h]), four real MMAs per complex step in the order of zgemm_kernel
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 2) * 32, wc = (warp & 3) * 16, fr = lane >> 2, fk = lane & 3;
+    double cr[2][4][2][2], ci[2][4][2][2];
 #pragma unroll
     for (int q = 0; q < 2; ++q)
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) ar[q][i][jj] = ai[q][i][jj] = 0.0;
+            for (int j = 0; j < 2; ++j) cr[q][i][j][0] = cr[q][i][j][1] = ci[q][i][j][0] = ci[q][i][j][1] = 0.0;
 
     for (int m0 = 0; m0 < N; m0 += RS_MC) {
         const int mc = min(RS_MC, N - m0);
@@ -728,27 +740,27 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
             bs[(sp * RS_MC + mm) * RS_P + l] = bv;
         }
         __syncthreads();
-        for (int mm = 0; mm < mc; ++mm) {
+        for (int kk = 0; kk < mc; kk += 4) {  // zero-padded beyond mc
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int sg = q, tu = pair ? 1 - q : q;
-                zc a[4], b[4];
+                zc b[2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = xs[(sg * RS_MC + mm) * RS_P + ty + 16 * i];
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) {
-                    const zc v = bs[(tu * RS_MC + mm) * RS_P + tx + 16 * jj];
-                    b[jj] = zc{v.x, -v.y};
+                for (int j = 0; j < 2; ++j) {
+                    b[j] = bs[(tu * RS_MC + kk + fk) * RS_P + wc + 8 * j + fr];
+                    b[j].y = -b[j].y;  // conj(bra)
                 }
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i) {
+                    const zc a = xs[(sg * RS_MC + kk + fk) * RS_P + wr + 8 * i + fr];
 #pragma unroll
-                    for (int jj = 0; jj < 4; ++jj) {
-                        ar[q][i][jj] = fma(a[i].x, b[jj].x, ar[q][i][jj]);
-                        ar[q][i][jj] = fma(-a[i].y, b[jj].y, ar[q][i][jj]);
-                        ai[q][i][jj] = fma(a[i].x, b[jj].y, ai[q][i][jj]);
-                        ai[q][i][jj] = fma(a[i].y, b[jj].x, ai[q][i][jj]);
+                    for (int j = 0; j < 2; ++j) {
+                        dmma884(cr[q][i][j], a.x, b[j].x);
+                        dmma884(cr[q][i][j], -a.y, b[j].y);
+                        dmma884(ci[q][i][j], a.x, b[j].y);
+                        dmma884(ci[q][i][j], a.y, b[j].x);
                     }
+                }
             }
         }
     }
@@ -756,11 +768,11 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
     // columns of this CTA: K (q, part) for q = 0, 1; for pair 0 also P (part)
     const int ncol = pair == 0 ? 6 : 4;
     const int nn = n * n;
-    auto value = [&](int col, int i, int jj) -> double {
+    auto value = [&](int col, int i, int j, int h) -> double {
         const int part = col & 1;
-        if (col < 2) return part ? ai[0][i][jj] : ar[0][i][jj];
-        if (col < 4) return part ? ai[1][i][jj] : ar[1][i][jj];
-        return part ? ai[0][i][jj] + ai[1][i][jj] : ar[0][i][jj] + ar[1][i][jj];
+        if (col < 2) return part ? ci[0][i][j][h] : cr[0][i][j][h];
+        if (col < 4) return part ? ci[1][i][j][h] : cr[1][i][j][h];
+        return part ? ci[0][i][j][h] + ci[1][i][j][h] : cr[0][i][j][h] + cr[1][i][j][h];
     };
     // all column maxima in one reduction: warp shuffles, then the 8 warps through shared memory
     double mx[6];
@@ -769,13 +781,14 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-            if ((ty + 16 * i < n) && (tx + 16 * jj < n)) {
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-                for (int col = 0; col < 6; ++col)
-                    if (col < ncol) mx[col] = fmax(mx[col], fabs(value(col, i, jj)));
-            }
-    const int lane = tid & 31, warp = tid >> 5;
+            for (int h = 0; h < 2; ++h)
+                if ((wr + 8 * i + fr < n) && (wc + 8 * j + 2 * fk + h < n)) {
+#pragma unroll
+                    for (int col = 0; col < 6; ++col)
+                        if (col < ncol) mx[col] = fmax(mx[col], fabs(value(col, i, j, h)));
+                }
 #pragma unroll
     for (int col = 0; col < 6; ++col) {
 #pragma unroll
@@ -811,13 +824,15 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) {
-                const int l = ty + 16 * i, j = tx + 16 * jj;
-                if (l < n && j < n) {
-                    stage[l * n + j] = value(c0, i, jj);
-                    stage[nn + l * n + j] = value(c0 + 1, i, jj);
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int l = wr + 8 * i + fr, c = wc + 8 * j + 2 * fk + h;
+                    if (l < n && c < n) {
+                        stage[l * n + c] = value(c0, i, j, h);
+                        stage[nn + l * n + c] = value(c0 + 1, i, j, h);
+                    }
                 }
-            }
         __syncthreads();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {

@@ -880,6 +880,46 @@ bool hermitian_ok(const std::vector<cd> &H, const std::vector<cd> &S, int nci) {
 }  // namespace
 
 // buildhsg semantics: newMO = [I; Z] (MO basis), outputs in Fortran layout on the host.
+// Run `body` (a fixed launch sequence of this plan) as a CUDA graph replayed on `st`: captured once
+// on a private stream at first use, so per call the host submits one graph instead of ~100
+// launches.  Falls back to direct launches while per-launch profiling is on, for the cuBLAS
+// comparison form, or if capture is not possible.
+template <typename F>
+int launch_captured(PlanImpl &p, int key, cudaStream_t st, F &&body) {
+    if (!p.graphs_ok || g_prof.on || p.library_gemm) return body(st);
+    if (!p.gexec[key]) {
+        if (!p.cap_stream && cudaStreamCreateWithFlags(&p.cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            p.graphs_ok = false;
+            return body(st);
+        }
+        const unsigned long long l0 = g_launches;
+        if (cudaStreamBeginCapture(p.cap_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            cudaGetLastError();
+            p.graphs_ok = false;
+            return body(st);
+        }
+        const int rc = body(p.cap_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(p.cap_stream, &g);
+        const unsigned long long nl = g_launches - l0;
+        g_launches = l0;
+        cudaGraphExec_t ex = nullptr;
+        if (rc == PHF_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+            p.gexec[key] = ex;
+            p.glaunch[key] = nl;
+        } else {
+            cudaGetLastError();
+            p.graphs_ok = false;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (!p.gexec[key]) return rc != PHF_OK ? rc : body(st);
+    }
+    PHF_CUDA(cudaGraphLaunch(p.gexec[key], st));
+    g_launches += p.glaunch[key];
+    return PHF_OK;
+}
+
 int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
                   phf_complex *rdmmat) {
     const int M = p.M, N = p.N;
@@ -927,7 +967,7 @@ int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_comp
         const bool cb = (v >= 2), ck = (v == 1 || v == 2);
         PHF_TRY(upload(p.bra, cb ? bw1 : bw0));
         PHF_TRY(upload(p.kety, ck ? ky1 : ky0));
-        PHF_TRY(run_variant(p, v, st));
+        PHF_TRY(launch_captured(p, v, st, [&](cudaStream_t s) -> int { return run_variant(p, v, s); }));
     }
     PHF_TRY(fold_acc(p, st));
     PHF_TRY(read_flag(p, st));
@@ -1004,6 +1044,15 @@ void plan_release(PlanImpl &p) {
         cublasDestroy(reinterpret_cast<cublasHandle_t>(p.cublas));
         p.cublas = nullptr;
     }
+    for (auto &g : p.gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    if (p.cap_stream) {
+        cudaStreamDestroy(p.cap_stream);
+        p.cap_stream = nullptr;
+    }
 }
 
 PlanImpl::~PlanImpl() { plan_release(*this); }
@@ -1028,14 +1077,17 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
         // kety = Ref C (reference AO order)
         PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(p.bra, N, 1), Z0, vo(p.kety, N, 1), nullptr, st));
     }
-    PHF_TRY(zero_acc(p, st));
-    PHF_TRY(run_variant(p, 0, st));
-    PHF_TRY(fold_acc(p, st));
     const long long ns = (long long)p.nci * p.nci;
-    if (p.exact) {  // symmetrised bra + ket derivative
-        PHF_TRY(launch_average(ns * MN, p.accG, p.accKG, p.accG, st));
-        PHF_TRY(launch_average(ns * MN, p.accR, p.accKR, p.accR, st));
-    }
+    PHF_TRY(launch_captured(p, 4, st, [&](cudaStream_t s) -> int {
+        PHF_TRY(zero_acc(p, s));
+        PHF_TRY(run_variant(p, 0, s));
+        PHF_TRY(fold_acc(p, s));
+        if (p.exact) {  // symmetrised bra + ket derivative
+            PHF_TRY(launch_average(ns * MN, p.accG, p.accKG, p.accG, s));
+            PHF_TRY(launch_average(ns * MN, p.accR, p.accKR, p.accR, s));
+        }
+        return PHF_OK;
+    }));
     PHF_CUDA(cudaMemcpyAsync(d_hs, p.accHS, 2 * ns * sizeof(zc), cudaMemcpyDeviceToDevice, st));
     if (p.chol) {
         // back to [alpha; beta] order: out[r] = acc[inv[r]]

@@ -124,6 +124,12 @@ struct PlanImpl {
     int exact = 0;                   // also accumulate the ket-side gradient (gradient_mode 1)
     int library_gemm = 0;            // FP64 exchange GEMM through cuBLAS (comparison form)
     void *cublas = nullptr;          // cublasHandle_t when library_gemm
+    // CUDA graphs of the launch sequences replayed per call (key 0..3: variant of buildhsg, 4: the
+    // whole eval_device pass), captured on first use on a private stream
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec[5] = {};
+    unsigned long long glaunch[5] = {};  // kernels in each graph (for the launch counter)
+    bool graphs_ok = true;
     int nl = 0, ny = 0, npg = 0, nomega = 0;
     int wbeg = 0, wend = 0;          // grid points evaluated: [wbeg, wend)
     int nci = 0, ncisp = 0, ncipg = 0, cmplxconj = 1, qj = 0, sp = 1, nb = 0;

@@ -185,3 +185,26 @@ def test_point_range_plans_sum_to_the_full_grid():
     for i in range(3):
         tot = parts[0][i] + parts[1][i] + parts[2][i]
         assert torch.allclose(tot, ref[i], rtol=0, atol=1e-12 * float(ref[i].abs().max()))
+
+
+def test_graph_replay_matches_direct_launches():
+    """eval_device replays a captured CUDA graph; with per-launch profiling on it launches kernel by
+    kernel.  Both must give bitwise the same sums, call after call."""
+    import torch
+
+    p = synth.make_problem(16, 8, 40, ngrid=(6, 3), seed=4, pg="C2v")
+    kw = p.grid_kwargs()
+    akw = dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+               r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+               roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+    C = torch.from_numpy(p.C).cuda()
+    for prec in ("fp64", "ozaki_i8"):
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, workspace_bytes=400_000, **akw) as plan:
+            graph = [[t.clone() for t in plan.eval_device(C)] for _ in range(2)]
+            _lib.profile_enable(True)
+            try:
+                direct = [t.clone() for t in plan.eval_device(C)]
+            finally:
+                _lib.profile_enable(False)
+        for a, b, c in zip(graph[0], graph[1], direct):
+            assert torch.equal(a, b) and torch.equal(a, c)

@@ -50,6 +50,71 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "fallback": True}
 
 
+class NvmlClockSampler:
+    """SM clock, power and clock-event reasons read through NVML every 2 ms during the timed
+    region (read-only queries; nothing is changed on the GPU)."""
+
+    def __init__(self, index: int):
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = None
+        try:  # NVML numbers all GPUs of the node; find this process's device by its PCI address
+            import torch
+
+            pr = torch.cuda.get_device_properties(index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.samples = []
+        self._stop = threading.Event()
+
+    def _read(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                     int(get_reasons(self.h)), nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        self._stop.clear()
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=5)
+
+    def summary(self):
+        nv = self.nv
+        bits = {"hw_slowdown": nv.nvmlClocksThrottleReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksThrottleReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksThrottleReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksThrottleReasonSwPowerCap}
+        reasons = sorted({nm for _, r, _ in self.samples for nm, b in bits.items() if r & b})
+        sm = [c for c, _, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(sm), "power_w_max": max((w for _, _, w in self.samples), default=None),
+                "source": "NVML, 2 ms period"}
+
+
+def clock_sampler(index: int):
+    """NVML sampler when pynvml works, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return ClockSampler(index)
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -147,9 +212,9 @@ def survey_flops_per_point(p):
 
 
 # ncu capture of the configuration-2 K launch (dram__bytes_read.sum + dram__bytes_write.sum):
-# 3.267 GB + 0.256 GB.  Algorithmic: A slices 134 MB + B slices 268 MB + FP64 output 268 MB.
-K_LAUNCH_DRAM_BYTES = 3.267e9 + 0.256e9
-K_LAUNCH_ALG_BYTES = 0.134e9 + 0.268e9 + 0.268e9
+# 1.436 GB + 0.255 GB.  Algorithmic: A slices 101 MB + B slices 201 MB + FP64 output 268 MB.
+K_LAUNCH_DRAM_BYTES = 1.436e9 + 0.255e9
+K_LAUNCH_ALG_BYTES = 0.101e9 + 0.201e9 + 0.268e9
 
 
 def measure_int8_peak(torch, dev):
@@ -312,7 +377,7 @@ def run_ours(args):
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
 
     plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, **kw)
-    clk = ClockSampler(local)
+    clk = clock_sampler(local)
     step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
     slices = args.slices or 6
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)

@@ -632,16 +632,39 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         PHF_TRY(zgemm_strided((int)n2, bc, L, 1, 1, Z1, vd(p.Bst, 1, n2), vz(p.dvec, b, 1), Z0, vo(p.Jvec, b, 1),
                               nullptr, st));
     } else {
-        // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
         if (fused)
             PHF_TRY(oz_rho_slice(n, N, bc, p.Xs, ld, p.bra, p.slices, p.Bsl, p.eb, p.Psl, p.ePc, st));
         else
             PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
+    }
+    // int8 path: the Coulomb chain runs on a second stream beside the exchange GEMM (independent
+    // operands and outputs; its small, latency-bound launches fill the SMs the exchange GEMM's last
+    // wave leaves idle).  Joined before Gamma is assembled.  Not while per-launch profiling is on:
+    // event times of overlapping kernels would count the shared time twice.
+    cudaStream_t js = st;
+    const bool fork = p.prec != PHF_PREC_FP64 && !g_prof.on;
+    if (p.prec != PHF_PREC_FP64 && !fork) {
         PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
                                p.ozerr, st));
         PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, st));
-        // J^T (2 bc x n^2): transposed output keeps the epilogue's FP64 stores coalesced
         PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, n2, 0, 1, p.ozerr, st));
+    }
+    if (fork) {
+        if (!p.side) {
+            PHF_CUDA(cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking));
+            PHF_CUDA(cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming));
+            PHF_CUDA(cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming));
+        }
+        PHF_CUDA(cudaEventRecord(p.ev_fork, st));
+        PHF_CUDA(cudaStreamWaitEvent(p.side, p.ev_fork, 0));
+        js = p.side;
+        // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
+        PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
+                               p.ozerr, js));
+        PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, js));
+        // J^T (2 bc x n^2): transposed output keeps the epilogue's FP64 stores coalesced
+        PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, n2, 0, 1, p.ozerr, js));
+        PHF_CUDA(cudaEventRecord(p.ev_join, js));
     }
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
@@ -669,6 +692,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         if (!fused) PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
         // K^T (8 bc x n^2), transposed for coalesced epilogue stores
         PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, n2, 0, 1, p.ozerr, st));
+        if (fork) PHF_CUDA(cudaStreamWaitEvent(st, p.ev_join, 0));  // the Coulomb chain is done
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_assemble_gamma(n, bc, nullptr, 0, p.Jr, 1, n2, nullptr, 0, p.Dk, 1, n2, p.Gam, st));
     }
@@ -1049,6 +1073,11 @@ void plan_release(PlanImpl &p) {
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    if (p.ev_fork) cudaEventDestroy(p.ev_fork);
+    if (p.ev_join) cudaEventDestroy(p.ev_join);
+    if (p.side) cudaStreamDestroy(p.side);
+    p.ev_fork = p.ev_join = nullptr;
+    p.side = nullptr;
     if (p.cap_stream) {
         cudaStreamDestroy(p.cap_stream);
         p.cap_stream = nullptr;

@@ -127,6 +127,8 @@ struct PlanImpl {
     // CUDA graphs of the launch sequences replayed per call (key 0..3: variant of buildhsg, 4: the
     // whole eval_device pass), captured on first use on a private stream
     cudaStream_t cap_stream = nullptr;
+    cudaStream_t side = nullptr;             // second stream: the Coulomb GEMMs beside the exchange GEMM
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec[5] = {};
     unsigned long long glaunch[5] = {};  // kernels in each graph (for the launch counter)
     bool graphs_ok = true;

@@ -52,28 +52,33 @@ __device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int byte
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes_valid) : "memory");
 }
 
-constexpr int ZG_STAGES = 3;  // shared-memory stages of the k loop (cp.async pipeline)
+// Shared-memory stages of the k loop (cp.async pipeline): three for the 64 x 64 tile, two for the
+// narrow tiles (their products are mostly k = 32, two k-tiles; two stages let two CTAs share an SM).
+template <int BM, int BN>
+__host__ __device__ constexpr int zg_stages() { return BM == BN ? 3 : 2; }
 
 template <bool AREAL, int BM, int BN>
 constexpr size_t zg_smem_bytes() {
-    return (size_t)ZG_STAGES * BK * ((BM + 1) * (AREAL ? sizeof(double) : sizeof(zc)) + (BN + 1) * sizeof(zc));
+    return (size_t)zg_stages<BM, BN>() * BK *
+           ((BM + 1) * (AREAL ? sizeof(double) : sizeof(zc)) + (BN + 1) * sizeof(zc));
 }
 
 // BM x BN output tile, 256 threads = 8 warps of 32 x 16 (warp w: rows 32 (w / (BN/16)), columns
 // 16 (w % (BN/16))).  64 x 64 serves general shapes; 128 x 32 the narrow per-point products
 // (N <= 32 columns), 32 x 128 the N-row products bra^H Y and bra^H F X (m = N <= 32) over all
 // points of a chunk.  Tiles of A and B reach shared memory by element-wise cp.async (16 bytes a
-// complex element, 8 a real one; out-of-range elements are zero-filled) through ZG_STAGES stages;
+// complex element, 8 a real one; out-of-range elements are zero-filled) through zg_stages stages;
 // conjugation is applied when fragments are read.  A real B (only the exchange-matrix build) is
 // loaded with plain loads into the same stages.
 template <bool AREAL, int BM, int BN>
-__global__ void __launch_bounds__(NT) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
+__global__ void __launch_bounds__(NT, 2) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
                                                    zc beta, OutView C, const long long *__restrict__ offs) {
     using TA = typename ATile<AREAL>::T;
     constexpr int WARPS_N = BN / 16;
     static_assert((BM / 32) * WARPS_N * 32 == NT, "tile/warp mismatch");
     constexpr int LA = (BM * BK) / NT, LB = (BN * BK) / NT;  // elements loaded per thread
     constexpr int PA = BM + 1, PB = BN + 1;                    // row pitches (elements)
+    constexpr int ZG_STAGES = zg_stages<BM, BN>();
     extern __shared__ __align__(16) unsigned char zg_smem[];
     TA *As = reinterpret_cast<TA *>(zg_smem);                                      // [stage][kk][i]
     zc *Bs = reinterpret_cast<zc *>(zg_smem + (size_t)ZG_STAGES * BK * PA * sizeof(TA));  // [stage][kk][j]

@@ -379,7 +379,7 @@ def run_ours(args):
     plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, **kw)
     clk = clock_sampler(local)
     step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
-    slices = args.slices or 6
+    slices = args.slices or 5
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -151,8 +151,9 @@ int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes);
 
 /* FP64-accurate real GEMM on the int8 tensor cores (the arithmetic of PHF_PREC_OZAKI_I8):
  * D (m x n, row-major, ldd) = A (m x k, row-major, lda) * B, with B given transposed as
- * Bt (n x k, row-major, ldb).  `slices` int8 slices per operand (1..7; the error of an entry
- * is below about (slices+1) k 2^(-7 slices) max|A_i.| max|B_.j|).  Device pointers; synchronous on `stream`.
+ * Bt (n x k, row-major, ldb).  `slices` int8 slices per operand (1..7; balanced base-254 digits,
+ * each ~8 bits; the error of an entry is below (slices+1) k 2^(-7 slices) max|A_i.| max|B_.j|, and in
+ * practice near 254^(-slices) sqrt(k) max|A_i.| max|B_.j|).  Device pointers; synchronous on `stream`.
  * No counterpart in the reference (its J/K is a dense FP64 loop, PHFTools.f90:310-337). */
 int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
                     long long ldb, double *dD, long long ldd, void *stream);

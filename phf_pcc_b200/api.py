@@ -167,7 +167,7 @@ class Plan:
 
     Cholesky form: pass ``h`` (n, n) and ``B`` (L, n, n); dense form: ``hone`` and
     ``htwo``.  Grid arguments as buildhsg.  ``precision``: "fp64" or "ozaki_i8" (FP64-accurate
-    int8 tensor-core slices, ``slices`` per operand, default 6); ``jk_form``: "auto", "eri"
+    int8 tensor-core slices, ``slices`` per operand, default 5); ``jk_form``: "auto", "eri"
     (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"; ``gradient``: "reference"
     (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the ket-side term;
     used by autograd)."""

@@ -49,7 +49,7 @@ namespace phf {
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 32;  // tile rows, tile columns, k-block (int8 elements)
+constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 32;  // tile rows, widest tile (row padding of B), k-block
 constexpr int OZ_GP = 4;                             // slice groups per 128-byte row, accumulators per pass
 constexpr int OZ_THREADS = 192;
 constexpr int OZ_MAX_S = 7;
@@ -128,16 +128,18 @@ __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = 128.
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
-                              ((uint32_t)(OZ_BM >> 4) << 24);
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = BN.
+template <int BN>
+__host__ __device__ constexpr uint32_t idesc_i8() {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate));
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -200,6 +202,32 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
 // each) or four (S = 7: group 1 at 128-byte rows).
 constexpr int OZ_UNITS = 14;
 constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
+
+// Tile width and passes per slice count.  S = 5 runs its five groups g = 2..6 in one pass over
+// 96-column tiles (5 x 96 of the 512 TMEM columns); the others use 128-column tiles and passes of
+// up to four groups (S = 6, 7: groups 2..5, then the rest).
+__host__ __device__ constexpr int oz_bn(int S) { return S == 5 ? 96 : 128; }
+__host__ __device__ constexpr int oz_npass(int S) { return S == 5 ? 1 : (S + OZ_GP - 1) / OZ_GP; }
+__host__ __device__ constexpr int oz_g0(int P) { return 2 + OZ_GP * P; }
+__host__ __device__ constexpr int oz_g1(int S, int P) {
+    return S == 5 ? 6 : ((1 + OZ_GP * (P + 1) < S + 1) ? 1 + OZ_GP * (P + 1) : S + 1);
+}
+// 16 KB ring units a k-block of pass P takes: A and B of group 0, plus group 1 when the pass uses
+// slices beyond the fourth (one unit holding both 64-byte-row boxes, or one each for S = 7)
+__host__ __device__ constexpr int oz_units(int S, int P) {
+    return oz_g1(S, P) - 1 > OZ_GP ? (oz_g1_width(S) == 2 ? 3 : 4) : 2;
+}
+// bytes the TMA delivers into unit j of a k-block
+__host__ __device__ constexpr uint32_t oz_unit_bytes(int S, int j) {
+    return j == 0 ? OZ_BM * 128u
+                  : j == 1 ? (uint32_t)oz_bn(S) * 128u
+                           : (oz_g1_width(S) == 2 ? (OZ_BM + (uint32_t)oz_bn(S)) * 64u
+                                                  : (j == 2 ? OZ_BM * 128u : (uint32_t)oz_bn(S) * 128u));
+}
+
+// 254^{-t}: group g = t + 2 of the balanced base-254 digit products
+__constant__ double kPow254[7] = {1.0, 0.003937007874015748, 1.5500031000062e-05, 6.102374409473229e-08,
+                                  2.40250961002883e-10, 9.458699252082008e-13, 3.723897343339373e-15};
 constexpr uint32_t OZ_UNIT = 16384;
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
@@ -209,8 +237,8 @@ constexpr uint32_t OZ_UNIT = 16384;
 template <int S, int P>
 __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64_t dB0, uint64_t dA1, uint64_t dB1,
                                              uint32_t acc_in) {
-    constexpr int g0 = 2 + OZ_GP * P;
-    constexpr int g1 = (1 + OZ_GP * (P + 1) < S + 1) ? 1 + OZ_GP * (P + 1) : S + 1;
+    constexpr int g0 = oz_g0(P), g1 = oz_g1(S, P), BN = oz_bn(S);
+    constexpr uint32_t idesc = idesc_i8<BN>();
 #pragma unroll
     for (int g = g0; g <= g1; ++g) {
 #pragma unroll
@@ -218,22 +246,16 @@ __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64
             const int u = g - t;
             const uint64_t a = (t > OZ_GP ? dA1 : dA0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
             const uint64_t b = (u > OZ_GP ? dB1 : dB0) + (uint64_t)(2 * ((u - 1) % OZ_GP));
-            mma_i8(acc0 + (uint32_t)(g - g0) * OZ_BN, a, b, t > 1 ? 1u : acc_in);
+            mma_i8(acc0 + (uint32_t)(g - g0) * BN, a, b, idesc, t > 1 ? 1u : acc_in);
         }
     }
-}
-
-// Units per k-block of pass P.
-template <int S, int P>
-__host__ __device__ constexpr int oz_units_per_kblock() {
-    return P == 0 ? 2 : (oz_g1_width(S) == 2 ? 3 : 4);
 }
 
 // The MMA issuer's k-block loop of pass P (u, ph: next ring unit and its full-barrier parity).
 template <int S, int P>
 __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
                                          uint64_t *full_bar, uint64_t *empty_bar, int *err) {
-    constexpr int NU = oz_units_per_kblock<S, P>();
+    constexpr int NU = oz_units(S, P);
     for (int kb = 0; kb < KB; ++kb) {
         int us[NU];
 #pragma unroll
@@ -251,7 +273,7 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
         uint64_t dA1 = 0, dB1 = 0;
         if constexpr (NU == 3) {
             dA1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT);
-            dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_UNIT / 2);
+            dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 64);
         } else if constexpr (NU == 4) {
             dA1 = sdesc_sw128(smem_base + (uint32_t)us[2] * OZ_UNIT);
             dB1 = sdesc_sw128(smem_base + (uint32_t)us[3] * OZ_UNIT);
@@ -274,8 +296,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         if (threadIdx.x == 0) atomicOr(args.err, 16);
         return;
     }
-    constexpr int W1 = oz_g1_width(S);
-    const int npass = oz_ngroups(S);  // pass p: groups 4p+2 .. min(4p+5, S+1), slice groups 0..p
+    constexpr int W1 = oz_g1_width(S), BN = oz_bn(S);
+    const int npass = oz_npass(S);  // pass p: groups oz_g0(p) .. oz_g1(S, p)
     // With two passes and at most two groups in the second, the first pass's FP64 partial sums stay
     // in TMEM columns [0, 256) (high words, then low words, per 32-column chunk) and the second
     // pass accumulates in columns [256, 512); otherwise the second pass adds into D.
@@ -286,7 +308,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     uint64_t *free_bar = pass_bar + 1;          // epilogue has read the pass's accumulators
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(free_bar + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-    double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} of the tile's columns
+    double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} / 127 of the tile's columns
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // grouped raster: CTAs in launch order sweep the column tiles in groups of OZ_GROUP_M row tiles,
@@ -299,7 +321,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int first = (L / width) * OZ_GROUP_M;
         const int gm = min(mt - first, OZ_GROUP_M);
         m0 = (first + (L % width) % gm) * OZ_BM;
-        n0 = ((L % width) / gm) * OZ_BN;
+        n0 = ((L % width) / gm) * BN;
     }
     const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
     const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
@@ -323,7 +345,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
     if (warp >= 2) {
         const int c = threadIdx.x - 64;
-        colscale[c] = (n0 + c < args.n) ? ldexp(1.0, args.eb[n0 + c]) : 0.0;
+        colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(1.0 / 127.0, args.eb[n0 + c]) : 0.0;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
@@ -340,7 +362,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
             bool wrapped = false;
             for (int p = 0; p < npass && !*abort_flag; ++p) {
-                const int nu = p == 0 ? 2 : (W1 == 2 ? 3 : 4);
+                const int nu = p == 0 ? oz_units(S, 0) : oz_units(S, 1);
                 for (int kb = 0; kb < KB && !*abort_flag; ++kb) {
                     const int kbg = args.kb0 + kz0 + kb;
                     for (int j = 0; j < nu; ++j) {
@@ -349,14 +371,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                             break;
                         }
                         unsigned char *dst = smem + (size_t)u * OZ_UNIT;
-                        mbar_arrive_expect_tx(&full_bar[u], OZ_UNIT);
+                        const uint32_t ub = j == 0 ? oz_unit_bytes(S, 0)
+                                                   : j == 1 ? oz_unit_bytes(S, 1)
+                                                            : j == 2 ? oz_unit_bytes(S, 2) : oz_unit_bytes(S, 3);
+                        mbar_arrive_expect_tx(&full_bar[u], ub);
                         if (j == 0) {
                             tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, m0);
                         } else if (j == 1) {
                             tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, n0);
-                        } else if (W1 == 2) {  // j == 2: A and B of group 1, 8 KB each
+                        } else if (W1 == 2) {  // j == 2: A and B of group 1 at 64-byte rows
                             tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 64, m0);
-                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_UNIT / 2, kbg * 64, n0);
+                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 64, kbg * 64, n0);
                         } else if (j == 2) {
                             tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, m0);
                         } else {
@@ -388,7 +413,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
                 if (p == 0)
                     ok = mma_pass<S, 0>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
-                else if constexpr (S > OZ_GP)
+                else if constexpr (oz_npass(S) > 1)
                     ok = mma_pass<S, 1>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
                 if (!ok) *abort_flag = 1;
                 mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
@@ -400,26 +425,26 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
-        const double rowscale = row_ok ? ldexp(1.0, args.ea[row]) : 0.0;
+        const double rowscale = row_ok ? ldexp(1.0 / 127.0, args.ea[row]) : 0.0;
         double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
         const long long cstride = args.trans ? args.ldd : 1;
         for (int p = 0; p < npass; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!ok || *abort_flag) break;
-            const int g0 = 2 + OZ_GP * p, g1 = min(1 + OZ_GP * (p + 1), S + 1);
+            const int g0 = p == 0 ? oz_g0(0) : oz_g0(1), g1 = p == 0 ? oz_g1(S, 0) : oz_g1(S, 1);
             const uint32_t acc0 = lane_base + ((p > 0 && keep) ? 256u : 0u);
             const bool last = (p + 1 == npass);
 #pragma unroll 1
-            for (int c = 0; c < OZ_BN / 32; ++c) {
+            for (int c = 0; c < BN / 32; ++c) {
                 double acc[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 #pragma unroll 1
                 for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
                     uint32_t v[32];
-                    tmem_ld32(acc0 + (uint32_t)(g - g0) * OZ_BN + c * 32, v);
-                    const double sc = ldexp(1.0, -7 * g);
+                    tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
+                    const double sc = kPow254[g - 2];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
                 }
@@ -480,17 +505,17 @@ __device__ __forceinline__ int exp_of_max(double mx) {
     return e;
 }
 
-// Slicing of one value: with r = x 2^-e (|r| < 1), slice t (t < S - 1) is the t-th base-128 digit
-// of |r| with the sign of x, and the last slice is the rounded remainder (clamped to +-127):
-//     T = x 2^{7(S-1) - e},  I = floor(|T|)  (the first S - 1 digits),  last = rint(128 (|T| - I)).
-// Every step is exact (power-of-two scaling, |T| < 2^42), so the digits are those of the
-// step-by-step form  r *= 128; a = trunc(r); r -= a.  I comes from the mantissa of |T| + 2^52 added
-// with round-toward-zero and the rounding of the last digit from adding 1.5 * 2^52 -- plain FP64
-// adds, no integer/floating conversions (those are long-latency and dominated the slicing).
+// Slicing of one value (balanced base-254 digits): with r = 127 x 2^-e (|r| < 127), slice t is
+//     d_t = rint(r_t),  r_{t+1} = 254 (r_t - d_t),   r_0 = r,
+// so every digit lies in [-127, 127] (|r_t - d_t| <= 1/2) and carries log2(254) ~ 8 bits:
+//     x = 2^e / 127 * sum_t d_t 254^{-t} + O(2^e 254^{-S}).
+// rint is the round-to-nearest addition of 1.5 * 2^52, whose low mantissa word is the digit as a
+// 32-bit two's-complement integer -- plain FP64 adds, no integer/floating conversions (those are
+// long-latency and dominated the slicing).  r_t - d_t is exact; 254 (r_t - d_t) rounds once.
 struct SliceScale {
-    double p1, p2;  // 2^-e and 2^{7(S-1)}
+    double p1;  // 2^-e
     int e;
-    bool fast;      // 2^-e is a normal double: two exact multiplications instead of ldexp
+    bool fast;  // 2^-e is a normal double: one exact multiplication instead of ldexp
 };
 
 __device__ __forceinline__ double pow2_normal(int k) {  // 2^k for -1022 <= k <= 1023
@@ -498,29 +523,27 @@ __device__ __forceinline__ double pow2_normal(int k) {  // 2^k for -1022 <= k <=
 }
 
 __device__ __forceinline__ SliceScale slice_scale(int e, int S) {
+    (void)S;
     SliceScale sc;
     sc.e = e;
     sc.fast = (e >= -1000 && e <= 1000);
     sc.p1 = sc.fast ? pow2_normal(-e) : 1.0;
-    sc.p2 = pow2_normal(7 * (S - 1));
     return sc;
 }
 
 __device__ __forceinline__ void slice_digits(double x, const SliceScale &sc, int S, int (&d)[OZ_MAX_S]) {
-    constexpr double kTwo52 = 4503599627370496.0, kRound = 6755399441055744.0;  // 2^52, 1.5 * 2^52
-    const double T = sc.fast ? (x * sc.p1) * sc.p2 : ldexp(x, 7 * (S - 1) - sc.e);
-    const double aT = fabs(T);
-    const double big = __dadd_rz(aT, kTwo52);  // 2^52 + floor(|T|)
-    const unsigned long long mag = (unsigned long long)__double_as_longlong(big) & ((1ull << 52) - 1);
-    const double fr = aT - (big - kTwo52);     // exact fraction
-    const double lastm = fmin(127.0, __dadd_rn(fr * 128.0, kRound) - kRound);
-    const int sg = T < 0.0 ? -1 : 1;
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    double r = (sc.fast ? x * sc.p1 : ldexp(x, -sc.e)) * 127.0;
 #pragma unroll
-    for (int t = 0; t < OZ_MAX_S; ++t)
-        d[t] = (t < S - 1) ? sg * (int)((mag >> (7 * (S - 2 - t))) & 127ull) : 0;
-#pragma unroll
-    for (int t = 0; t < OZ_MAX_S; ++t)
-        if (t == S - 1) d[t] = sg * (int)lastm;
+    for (int t = 0; t < OZ_MAX_S; ++t) {
+        if (t < S) {
+            const double big = __dadd_rn(r, kRound);  // 1.5 * 2^52 + rint(r)
+            d[t] = __double2loint(big);
+            r = (r - (big - kRound)) * 254.0;
+        } else {
+            d[t] = 0;
+        }
+    }
 }
 
 // Slices of x for element k of row `row` of an operand slice buffer (rows_pad rows, KB k-blocks).
@@ -653,51 +676,23 @@ constexpr int RS_NT = 256, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded r
 // operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
 size_t rs_smem_bytes() { return std::max((size_t)2 * 2 * RS_MC * RS_P * sizeof(zc), (size_t)2 * 64 * 64 * sizeof(double)); }
 
-// Slices of four consecutive k-elements e0..e0+3 (one 32-element block) of a column, S known at
-// compile time: the digits of the four values are cut from the mantissa words of 2^52 + floor(|T|)
-// with constant shifts, packed four to a 32-bit word (byte v = element e0 + v), and the signs are
-// applied to the packed words (per-byte negation, no carries between bytes).  Same digits as
-// slice_digits; one 32-bit store per slice.
-__device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {  // bytes 0..127 -> (-b) mod 256
-    return ((~w & 0x7F7F7F7Fu) + 0x01010101u) ^ 0x80808080u;
-}
-
+// Slices of four consecutive k-elements e0..e0+3 (one 32-element block) of a column, packed four
+// to a 32-bit word (byte v = element e0 + v), one store per slice.
 template <int S>
 __device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceScale &sc, signed char *out, long long row,
                                             long long rows_pad, long long KB, long long e0) {
-    constexpr double kTwo52 = 4503599627370496.0, kRound = 6755399441055744.0;
-    uint32_t lo[4], hi[4], last[4], sign = 0u;
+    uint32_t wd[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) wd[t] = 0u;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const double T = sc.fast ? (x[v] * sc.p1) * sc.p2 : ldexp(x[v], 7 * (S - 1) - sc.e);
-        const double aT = fabs(T);
-        const double big = __dadd_rz(aT, kTwo52);  // 2^52 + floor(|T|)
-        lo[v] = (uint32_t)__double2loint(big);
-        hi[v] = (uint32_t)__double2hiint(big) & 0xFFFFFu;
-        const double fr = aT - (big - kTwo52);
-        // 1.5 * 2^52 + 128 fr rounded to nearest even: its low word is rint(128 fr) (<= 128)
-        last[v] = min((uint32_t)__double2loint(__dadd_rn(fr * 128.0, kRound)), 127u);
-        if (T < 0.0) sign |= 0xFFu << (8 * v);
+        int d[OZ_MAX_S];
+        slice_digits(x[v], sc, S, d);
+#pragma unroll
+        for (int t = 0; t < S; ++t) wd[t] |= ((uint32_t)d[t] & 0xFFu) << (8 * v);
     }
 #pragma unroll
-    for (int t = 0; t < S; ++t) {
-        uint32_t w = 0u;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            uint32_t dg;
-            if (t == S - 1) {
-                dg = last[v];
-            } else {
-                const int off = 7 * (S - 2 - t);
-                if (off >= 32) dg = (hi[v] >> (off - 32)) & 127u;
-                else if (off + 7 > 32) dg = __funnelshift_r(lo[v], hi[v], off) & 127u;
-                else dg = (lo[v] >> off) & 127u;
-            }
-            w |= dg << (8 * v);
-        }
-        w = (w & ~sign) | (neg_bytes(w) & sign);
-        *reinterpret_cast<uint32_t *>(out + oz_slice_offset(t, row, e0, rows_pad, KB, S)) = w;
-    }
+    for (int t = 0; t < S; ++t) *reinterpret_cast<uint32_t *>(out + oz_slice_offset(t, row, e0, rows_pad, KB, S)) = wd[t];
 }
 
 template <int S>
@@ -1025,7 +1020,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
-    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, OZ_BN));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
     const long long rows = trans ? n : m;
     const long long dz = rows * ldd;
     OzArgs a;
@@ -1050,7 +1045,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
         return PHF_ERR_ARG;
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), (unsigned)nsplit);
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), (unsigned)nsplit);
     {
         ProfScope prof(st, PROF_JK);
         kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
@@ -1075,7 +1070,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
-    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, OZ_BN));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
     // k-blocks per pass: S * kpass * 127^2 < 2^31
     long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
     if (kb_pass < 1) kb_pass = 1;
@@ -1087,7 +1082,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         return PHF_ERR_ARG;
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)(npad / OZ_BN), 1);  // mapped to tiles by the grouped raster
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;

@@ -259,7 +259,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.N = d->nocc;
     p.L = d->nchol;
     p.prec = d->precision;
-    p.slices = d->slices > 0 ? d->slices : 6;
+    p.slices = d->slices > 0 ? d->slices : 5;
     if (p.chol) p.eri = (d->jk_form == 1) || (d->jk_form == 0 && d->nso / 2 <= 128);
     p.exact = d->gradient_mode == 1;
     p.library_gemm = (d->fp64_library_gemm != 0) && p.eri && p.prec == PHF_PREC_FP64;

@@ -458,7 +458,7 @@ def run_ours(args):
             achieved = int8_ops_per_point(p, slices) * pts / (jk_ms * 1e-3) / 1e12
             roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                     "frac": achieved / peak, "traffic": K_LAUNCH_DRAM_BYTES if args.config == "c2" else None,
-                    "traffic_note": ("DRAM read + write of one K launch (4096 x 8192 x 4096, S = 6) from an ncu "
+                    "traffic_note": ("DRAM read + write of one K launch (4096 x 8192 x 4096) from an ncu "
                                      "capture of this workload; algorithmic bytes of that launch: "
                                      f"{K_LAUNCH_ALG_BYTES:.3g}"),
                     "peak_source": ("2 x measured bf16 burst of MEASURED_PEAKS.json (dense int8 rate = 2 x bf16 "

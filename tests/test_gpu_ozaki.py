@@ -1,9 +1,9 @@
 """The int8-sliced tensor-core GEMM (phf_ozaki_dgemm) against FP64 products, and the
 energy/gradient pipeline in that precision against the golden vectors.
 
-Tolerances: a slice is an integer up to 127 ~ 2^7 times 2^{-7t}, so with S slices the dropped
-products and the representation remainder are of order 2^{-7S}; an entry's error is below
-about (S+1) k 2^{-7S} max|A_i.| max|B_.j| (the test bound is 4x that).  Pipeline: |dE| <= 1e-9 Eh relative
+Tolerances: slices are balanced base-254 digits in [-127, 127], so with S slices the dropped
+products and the representation remainder are of order 254^{-S} < 2^{-7S}; an entry's error is
+below (S+1) k 2^{-7S} max|A_i.| max|B_.j| (the test bound is 4x that).  Pipeline: |dE| <= 1e-9 Eh relative
 to FP64, gradient elements <= 1e-8 (the benchmark target is 1e-8 Eh and 1e-7).
 """
 import ctypes

@@ -110,7 +110,8 @@ typedef struct {
     size_t workspace_bytes;                   /* per-chunk workspace budget (0 = default 6 GiB) */
     int jk_form;                              /* Cholesky form only: 0 = automatic, 1 = exchange through the
                                                  spatial ERI matrix (n^2 x n^2, built once per plan),
-                                                 2 = factorized (no n^4 tensor); automatic picks 1 for n <= 128 */
+                                                 2 = factorized (no n^4 tensor); automatic picks 1 for n <= 128
+                                                 and for the int8 precision at every n, else 2 */
     int gradient_mode;                        /* phf_plan_eval_device only: 0 = the reference's gradient
                                                  (bra-side derivative, Gradient/LocalG of PHFTools.f90);
                                                  1 = exact dE/dC* of E = Re H/|Re S|, adding the ket-side

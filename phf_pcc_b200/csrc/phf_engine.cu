@@ -260,7 +260,10 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.L = d->nchol;
     p.prec = d->precision;
     p.slices = d->slices > 0 ? d->slices : 5;
-    if (p.chol) p.eri = (d->jk_form == 1) || (d->jk_form == 0 && d->nso / 2 <= 128);
+    // automatic form: the spatial-ERI exchange matrix for n <= 128, and at every size for the int8
+    // tensor-core path (which needs it); the factorized form for FP64 above n = 128
+    if (p.chol)
+        p.eri = (d->jk_form == 1) || (d->jk_form == 0 && (d->nso / 2 <= 128 || p.prec != PHF_PREC_FP64));
     p.exact = d->gradient_mode == 1;
     p.library_gemm = (d->fp64_library_gemm != 0) && p.eri && p.prec == PHF_PREC_FP64;
     if (p.library_gemm) {

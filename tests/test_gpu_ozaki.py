@@ -104,3 +104,25 @@ def test_int8_pipeline_matches_fp64_on_ragged_sizes(n, N, L):
             res[prec] = [t.cpu().numpy() for t in plan.eval_device(C)]
     for a, b, what in zip(res["ozaki_i8"], res["fp64"], ("HS", "Yg", "Yr")):
         assert _close(a, b, 1e-9), (what, float(np.abs(a - b).max()))
+
+
+def test_automatic_form_above_n128_int8_eri_matches_fp64_factorized():
+    """Above n = 128 the automatic J/K form is the factorized one in FP64 but the spatial-ERI exchange
+    matrix for the int8 path (here n = 130: a 16900 x 16900 exchange matrix); both forms must agree."""
+    import torch
+
+    from phf_pcc_b200 import synth
+
+    p = synth.make_problem(130, 4, 16, ngrid=(6, 3), seed=17, pg="None")
+    kw = p.grid_kwargs()
+    akw = dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+               r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+               roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+    C = torch.from_numpy(p.C).cuda()
+    res = {}
+    for prec in ("fp64", "ozaki_i8"):
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, **akw) as plan:
+            res[prec] = [t.cpu().numpy() for t in plan.eval_device(C)]
+        torch.cuda.empty_cache()
+    for a, b, what in zip(res["ozaki_i8"], res["fp64"], ("HS", "Yg", "Yr")):
+        assert _close(a, b, 1e-9), (what, float(np.abs(a - b).max()))

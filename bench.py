@@ -300,7 +300,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    p = problem_for(args.config, seed=0)
+    if args.config == "c4":  # the batch's rate on its first instance
+        from phf_pcc_b200 import synth
+        p = synth.batch_problems(args.batch, seed=1000)[0]
+    else:
+        p = problem_for(args.config, seed=0)
     vals = []
     desc = ""
     nth = os.cpu_count() or 1
@@ -518,13 +522,165 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """Configuration 4: independent instances of uneven size evaluated together (phf_eval_batch:
+    one CUDA graph over concurrent branches).  value = grid points of all instances / device time
+    of one batch evaluation; the FP64 form is the same batch with FP64 plans."""
+    import torch
+
+    from phf_pcc_b200 import _lib, api, synth
+    from phf_pcc_b200.autograd import _combine
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    probs = synth.batch_problems(args.batch, seed=1000 + rank)
+    pts = sum(p.grid.npoints for p in probs)
+    ws = 512 << 20
+
+    def make(prec):
+        return [api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, slices=args.slices, jk_form="eri",
+                         workspace_bytes=ws, **api_kwargs(p)) for p in probs]
+
+    def energies(outs):
+        res = []
+        for p, (hs, yg, yr) in zip(probs, outs):
+            E, G = _combine(hs, yg, yr, 1, 1, 1)
+            res.append((float(E.item()), G))
+        return res
+
+    Cs = [torch.from_numpy(p.C).to(dev) for p in probs]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)
+
+    def time_batch(plans, steps, warmup, sampler=None):
+        outs = api.eval_batch(plans, Cs)  # captures (and tunes) the batch graph
+        for _ in range(max(0, warmup - 1)):
+            api.eval_batch(plans, Cs, outs)
+        torch.cuda.synchronize()
+        l0 = _lib.kernel_launches()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if sampler:
+            sampler.__enter__()
+        try:
+            for i in range(steps):
+                flush.zero_()
+                ev[i][0].record(stream)
+                api.eval_batch(plans, Cs, outs)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        finally:
+            if sampler:
+                sampler.__exit__(None, None, None)
+        launches = _lib.kernel_launches() - l0
+        return sum(a.elapsed_time(b) for a, b in ev) / steps, outs, launches
+
+    plans = make(args.precision)
+    clk = clock_sampler(local)
+    step_ms, outs, launches = time_batch(plans, args.steps, args.warmup, clk)
+    # per-class device time, kernel by kernel
+    _lib.profile_enable(True)
+    api.eval_batch(plans, Cs, outs)
+    torch.cuda.synchronize()
+    prof = {c: _lib.profile_read(c) for c in range(4)}
+    _lib.profile_enable(False)
+    res = energies(outs)
+    branches = int(_lib.load().phf_batch_branches())
+    # end to end: determinants host -> device, the batch, all accumulators device -> host
+    host_C = [c.cpu().pin_memory() for c in Cs]
+    host_out = [tuple(t.cpu().pin_memory() for t in o) for o in outs]
+    e2e = []
+    for i in range(1 + args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for hc, dc in zip(host_C, Cs):
+            dc.copy_(hc, non_blocking=True)
+        api.eval_batch(plans, Cs, outs)
+        for ho, do in zip(host_out, outs):
+            for a, b in zip(ho, do):
+                a.copy_(b, non_blocking=True)
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e.append(pts / (time.perf_counter() - t0))
+    h2d = sum(c.numel() * 16 for c in Cs)
+    d2h = sum(sum(t.numel() * 16 for t in o) for o in outs)
+    for pl in plans:
+        pl.close()
+    torch.cuda.empty_cache()
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64:
+        plans64 = make("fp64")
+        ms64, outs64, _ = time_batch(plans64, max(1, min(args.steps, 3)), 1)
+        res64 = energies(outs64)
+        for pl in plans64:
+            pl.close()
+        torch.cuda.empty_cache()
+        dE = max(abs(a[0] - b[0]) for a, b in zip(res, res64))
+        dG = max(float((a[1] - b[1]).abs().max().item()) for a, b in zip(res, res64))
+        fp64 = {"own_kernels": {"value": pts / (ms64 * 1e-3), "ms_per_step": ms64, "speedup": ms64 / step_ms,
+                                "max_abs_dE_vs_fp64": dE, "max_abs_dgrad_vs_fp64": dG, "meets_1e-8_Eh": dE <= 1e-8}}
+    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item())
+    if rank == 0:
+        peaks = _peaks()
+        jk_ms = prof[0][0]
+        slices = args.slices or 5
+        ops = sum(int8_ops_per_point(p, slices) * p.grid.npoints for p in probs)
+        bf16 = peaks.get("bf16_tflops")
+        peak = 2.0 * bf16 if bf16 else None
+        achieved = ops / (jk_ms * 1e-3) / 1e12 if args.precision != "fp64" else None
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
+                "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
+                "peak_source": "2 x measured bf16 burst of MEASURED_PEAKS.json",
+                "device_ms_by_class": {k: v[0] for k, v in zip(("jk", "other_gemm", "overlap_inverse", "memory"),
+                                                               prof.values())},
+                "kernel": "ozaki_i8_gemm_kernel (all instances' exchange and Coulomb GEMMs)"}
+        cpu = None
+        if not args.no_cpu:
+            v, nth, desc = cpu_sample(probs[0], seconds_target=args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": f"instance 0: {desc}"}
+        sizes = sorted({p.n for p in probs})
+        line = {"metric": METRIC, "value": world * pts / (step_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else f"int8 x{slices} slices (FP64-accurate emulation) + f64",
+                "data": "synthetic (seeded h, B_L, determinants per instance)",
+                "config": {"workload": f"{len(probs)} independent instances, n in {sizes}, N = n/2, L = 4n, "
+                                       f"grids 112 / 800 points alternating, {pts} points in all",
+                           "precision": args.precision, "jk_form": "eri", "points_per_step": pts,
+                           "batch_branches": branches, "l2": "flushed (256 MB write) between timed steps",
+                           "parallelism": f"{world} independent batch(es), one per GPU"},
+                "max_abs_dE_vs_fp64": fp64["own_kernels"]["max_abs_dE_vs_fp64"] if fp64 else None,
+                "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": statistics.median(e2e) * world if e2e else None, "unit": UNIT,
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "path": "pinned host determinants -> device, phf_eval_batch, accumulators -> pinned host"},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--batch", type=int, default=256, help="instances for --config c4")
     ap.add_argument("--precision", default="ozaki_i8", choices=["fp64", "ozaki_i8"])
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
@@ -534,6 +690,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c4":
+        return run_batch(args)
     return run_ours(args)
 
 

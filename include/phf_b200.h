@@ -147,6 +147,18 @@ int phf_plan_buildhsg(phf_plan *plan, const phf_complex *z, phf_complex *hmat, p
 int phf_plan_eval_device(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
                          phf_complex *d_yr, void *stream);
 
+/* Batched evaluation of independent instances (the many-instance workload of uneven orbital
+ * counts): plans[i] evaluates determinant d_c[i] into d_hs[i], d_yg[i], d_yr[i] exactly as
+ * phf_plan_eval_device.  All instances run as one CUDA graph on `stream`, captured on first use
+ * for this set of plans and buffers (again after any plan is destroyed or a buffer changes) with
+ * the instances spread over 4, 8 or 16 concurrent branches -- the count that timed fastest when the
+ * set was captured.  Synchronous; returns the first failing instance's status.  No counterpart in
+ * the reference (its driver runs one PHF instance at a time). */
+int phf_eval_batch(phf_plan *const *plans, int count, const phf_complex *const *d_c, phf_complex *const *d_hs,
+                   phf_complex *const *d_yg, phf_complex *const *d_yr, void *stream);
+/* Concurrent branches of the batch graph phf_eval_batch captured last (0 before any). */
+int phf_batch_branches(void);
+
 /* Grid points per pipeline chunk chosen by the plan, and its device workspace in bytes. */
 int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes);
 

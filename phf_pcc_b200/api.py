@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import PREC, PHFError, check, phf_complex, phf_plan_desc
 
-__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "PHFError"]
+__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "eval_batch", "PHFError"]
 
 
 def _fz(a):
@@ -275,3 +275,35 @@ class Plan:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def eval_batch(plans, Cs, outs=None, stream=None):
+    """Evaluate independent instances together (phf_eval_batch): plans[i] at the device-resident
+    determinant Cs[i] (complex128 (M_i, N_i) CUDA tensors).  Returns one (hs, yg, yr) triple per
+    instance, as Plan.eval_device.  All instances run as one CUDA graph, captured on the first call
+    for this set of plans and buffers; pass the returned triples back as ``outs`` (and keep the same
+    Cs tensors) to replay it without recapturing."""
+    import torch
+
+    if len(plans) != len(Cs):
+        raise ValueError("one determinant per plan")
+    if outs is None:
+        outs = []
+        for pl, C in zip(plans, Cs):
+            ns = pl.nci * pl.nci
+            yg = torch.empty((ns, pl.nso, pl.nocc), dtype=torch.complex128, device=C.device)
+            outs.append((torch.empty((ns, 2), dtype=torch.complex128, device=C.device), yg, torch.empty_like(yg)))
+    for pl, C in zip(plans, Cs):
+        if C.dtype != torch.complex128 or not C.is_cuda or tuple(C.shape) != (pl.nso, pl.nocc) or \
+                not C.is_contiguous():
+            raise ValueError(f"each C must be a contiguous complex128 CUDA tensor of its plan's shape")
+    n = len(plans)
+    P = ctypes.c_void_p * n
+    ptrs = lambda ts: P(*[ctypes.c_void_p(t.data_ptr()) for t in ts])
+    if stream is None:
+        stream = torch.cuda.current_stream(Cs[0].device if n else None)
+    st = _lib.load().phf_eval_batch(P(*[pl._handle for pl in plans]), n, ptrs(Cs), ptrs([o[0] for o in outs]),
+                                    ptrs([o[1] for o in outs]), ptrs([o[2] for o in outs]),
+                                    ctypes.c_void_p(stream.cuda_stream))
+    check(st, "phf_eval_batch")
+    return outs

@@ -243,8 +243,31 @@ int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan) {
 }
 
 int phf_plan_destroy(phf_plan *plan) {
-    delete plan;  // ~PlanImpl releases the device memory and library handles
+    if (plan) phf::plan_destroyed();  // batch graphs that contain it are recaptured
+    delete plan;                      // ~PlanImpl releases the device memory and library handles
     return PHF_OK;
+}
+
+int phf_batch_branches(void) { return phf::batch_branches(); }
+
+int phf_eval_batch(phf_plan *const *plans, int count, const phf_complex *const *d_c, phf_complex *const *d_hs,
+                   phf_complex *const *d_yg, phf_complex *const *d_yr, void *stream) {
+    phf::set_error(PHF_OK, "");
+    if (count < 0 || (count > 0 && (!plans || !d_c || !d_hs || !d_yg || !d_yr))) {
+        phf::set_error(PHF_ERR_ARG, "phf_eval_batch: null argument");
+        return PHF_ERR_ARG;
+    }
+    std::vector<phf::PlanImpl *> impl((size_t)count);
+    for (int i = 0; i < count; ++i) {
+        if (!plans[i] || !d_c[i] || !d_hs[i] || !d_yg[i] || !d_yr[i]) {
+            phf::set_error(PHF_ERR_ARG, "phf_eval_batch: null plan or buffer at index " + std::to_string(i));
+            return PHF_ERR_ARG;
+        }
+        impl[i] = &plans[i]->impl;
+    }
+    return phf::plan_eval_batch(impl.data(), count, reinterpret_cast<const phf::zc *const *>(d_c),
+                                reinterpret_cast<phf::zc *const *>(d_hs), reinterpret_cast<phf::zc *const *>(d_yg),
+                                reinterpret_cast<phf::zc *const *>(d_yr), reinterpret_cast<cudaStream_t>(stream));
 }
 
 int phf_plan_buildhsg(phf_plan *plan, const phf_complex *z, phf_complex *hmat, phf_complex *smat,

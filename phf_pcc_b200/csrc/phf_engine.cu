@@ -34,6 +34,8 @@
 #include <cublas_v2.h>
 
 #include "phf_common.cuh"
+#include <mutex>
+
 #include "phf_internal.h"
 
 namespace phf {
@@ -613,7 +615,12 @@ int build_exchange_matrix(PlanImpl &p) {
         PHF_TRY(oz_slice_rows_strided((int)n2, L, p.Bst, 1, n2, p.slices, oz_pad_rows(n2), p.B2sl, p.eB2, 0));
     }
     PHF_CUDA(cudaDeviceSynchronize());
-    p.EK = EK;  // kept for the FP64 back-end
+    if (p.prec == PHF_PREC_FP64) {
+        p.EK = EK;  // the FP64 back-end multiplies by it
+    } else {
+        p.arena.free_one(EK);  // the int8 back-end only needs its slices
+        p.EK = nullptr;
+    }
     return PHF_OK;
 }
 
@@ -1089,14 +1096,11 @@ void plan_release(PlanImpl &p) {
 
 PlanImpl::~PlanImpl() { plan_release(*this); }
 
-int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st) {
-    if (p.cmplxconj == 2) {
-        set_error(PHF_ERR_UNSUPPORTED, "phf_plan_eval_device: cmplxconj == 2 needs phf_plan_buildhsg");
-        return PHF_ERR_UNSUPPORTED;
-    }
+// Everything of one eval_device call enqueued on st, without the status check.  in_graph: the
+// caller is capturing a batch graph, so the plan's own graph is not used.
+int eval_enqueue(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st, bool in_graph) {
     const int M = p.M, N = p.N;
     const long long MN = (long long)M * N;
-    PHF_CUDA(cudaSetDevice(p.device));
     if (p.chol) {
         // rows of C from [alpha; beta] order to the working order: bra[r'] = C[perm[r']]
         PHF_TRY(launch_permute_rows(M, N, 1, p.permdev, d_c, N, 0, p.bra, 0, st));
@@ -1110,7 +1114,7 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
         PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(p.bra, N, 1), Z0, vo(p.kety, N, 1), nullptr, st));
     }
     const long long ns = (long long)p.nci * p.nci;
-    PHF_TRY(launch_captured(p, 4, st, [&](cudaStream_t s) -> int {
+    auto body = [&](cudaStream_t s) -> int {
         PHF_TRY(zero_acc(p, s));
         PHF_TRY(run_variant(p, 0, s));
         PHF_TRY(fold_acc(p, s));
@@ -1119,7 +1123,11 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
             PHF_TRY(launch_average(ns * MN, p.accR, p.accKR, p.accR, s));
         }
         return PHF_OK;
-    }));
+    };
+    if (in_graph)
+        PHF_TRY(body(st));
+    else
+        PHF_TRY(launch_captured(p, 4, st, body));
     PHF_CUDA(cudaMemcpyAsync(d_hs, p.accHS, 2 * ns * sizeof(zc), cudaMemcpyDeviceToDevice, st));
     if (p.chol) {
         // back to [alpha; beta] order: out[r] = acc[inv[r]]
@@ -1129,7 +1137,227 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
         PHF_CUDA(cudaMemcpyAsync(d_yg, p.accG, ns * MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
         PHF_CUDA(cudaMemcpyAsync(d_yr, p.accR, ns * MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
     }
+    return PHF_OK;
+}
+
+int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st) {
+    if (p.cmplxconj == 2) {
+        set_error(PHF_ERR_UNSUPPORTED, "phf_plan_eval_device: cmplxconj == 2 needs phf_plan_buildhsg");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    PHF_CUDA(cudaSetDevice(p.device));
+    PHF_TRY(eval_enqueue(p, d_c, d_hs, d_yg, d_yr, st, false));
     return read_flag(p, st);
 }
+
+// ------------------------------------------------------------------ batched evaluation
+namespace {
+
+__global__ void gather_flags_kernel(int *const *ptrs, int n, int *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = ptrs[i] ? *ptrs[i] : 0;
+}
+
+constexpr int kMaxBranches = 16;
+
+// One cached batch graph: the launch sequences of all instances, spread over `branches`
+// concurrent streams, then one kernel copying every plan's status words into `d_flags`.
+struct BatchGraph {
+    std::vector<const void *> key;  // plans and buffers the graph was captured for
+    unsigned long long epoch = 0;
+    int device = -1, count = 0, branches = 0;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;
+    int *d_flags = nullptr;   // 2 per plan: overlap status, tensor-core pipeline status
+    int **d_ptrs = nullptr;   // where those live
+    std::vector<int> h_flags;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (d_flags) cudaFree(d_flags);
+        if (d_ptrs) cudaFree(d_ptrs);
+        exec = nullptr;
+        d_flags = nullptr;
+        d_ptrs = nullptr;
+        key.clear();
+    }
+};
+
+std::mutex g_batch_mu;
+BatchGraph g_batch;
+unsigned long long g_plan_epoch = 0;  // advanced whenever a plan is destroyed
+
+struct BatchStreams {
+    int device = -1;
+    cudaStream_t cap = nullptr, br[kMaxBranches] = {};
+    cudaEvent_t fork = nullptr, join[kMaxBranches] = {};
+} g_bs;
+
+int batch_streams(int device) {
+    if (g_bs.device == device && g_bs.cap) return PHF_OK;
+    PHF_CUDA(cudaStreamCreateWithFlags(&g_bs.cap, cudaStreamNonBlocking));
+    PHF_CUDA(cudaEventCreateWithFlags(&g_bs.fork, cudaEventDisableTiming));
+    for (int i = 0; i < kMaxBranches; ++i) {
+        PHF_CUDA(cudaStreamCreateWithFlags(&g_bs.br[i], cudaStreamNonBlocking));
+        PHF_CUDA(cudaEventCreateWithFlags(&g_bs.join[i], cudaEventDisableTiming));
+    }
+    g_bs.device = device;
+    return PHF_OK;
+}
+
+// Capture the batch with `nb` branches into *exec (and its kernel count into *nl).
+int capture_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *const *d_hs, zc *const *d_yg,
+                  zc *const *d_yr, int nb, int **d_ptrs, int *d_flags, cudaGraphExec_t *exec,
+                  unsigned long long *nl) {
+    const unsigned long long l0 = g_launches;
+    PHF_CUDA(cudaStreamBeginCapture(g_bs.cap, cudaStreamCaptureModeRelaxed));
+    int rc = PHF_OK;
+    cudaError_t e = cudaEventRecord(g_bs.fork, g_bs.cap);
+    for (int b = 0; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(g_bs.br[b], g_bs.fork, 0);
+    for (int i = 0; i < count && rc == PHF_OK && e == cudaSuccess; ++i)
+        rc = eval_enqueue(*plans[i], d_c[i], d_hs[i], d_yg[i], d_yr[i], g_bs.br[i % nb], true);
+    for (int b = 0; b < nb && e == cudaSuccess; ++b) {
+        e = cudaEventRecord(g_bs.join[b], g_bs.br[b]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(g_bs.cap, g_bs.join[b], 0);
+    }
+    if (rc == PHF_OK && e == cudaSuccess) {
+        gather_flags_kernel<<<(2 * count + 255) / 256, 256, 0, g_bs.cap>>>(d_ptrs, 2 * count, d_flags);
+        ++g_launches;
+        e = cudaGetLastError();
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(g_bs.cap, &g);
+    *nl = g_launches - l0;
+    g_launches = l0;
+    if (rc != PHF_OK || e != cudaSuccess || e2 != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (rc != PHF_OK) return rc;
+        set_error(PHF_ERR_CUDA, "phf_eval_batch: graph capture failed");
+        return PHF_ERR_CUDA;
+    }
+    const cudaError_t e3 = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) {
+        cudaGetLastError();
+        set_error(PHF_ERR_CUDA, std::string("phf_eval_batch: graph instantiation failed: ") + cudaGetErrorString(e3));
+        return PHF_ERR_CUDA;
+    }
+    return PHF_OK;
+}
+
+}  // namespace
+
+void plan_destroyed() {
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    ++g_plan_epoch;
+}
+
+// All instances of a batch as one CUDA graph (captured for this set of plans and buffers on first
+// use and replayed after).  The number of concurrent branches is tuned once per captured set:
+// 4, 8 and 16 branches are each captured and timed over one replay, and the fastest is kept.
+int plan_eval_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *const *d_hs, zc *const *d_yg,
+                    zc *const *d_yr, cudaStream_t st) {
+    if (count <= 0) return PHF_OK;
+    const int dev = plans[0]->device;
+    for (int i = 0; i < count; ++i) {
+        if (plans[i]->device != dev) {
+            set_error(PHF_ERR_ARG, "phf_eval_batch: plans on different devices");
+            return PHF_ERR_ARG;
+        }
+        if (plans[i]->cmplxconj == 2) {
+            set_error(PHF_ERR_UNSUPPORTED, "phf_eval_batch: cmplxconj == 2 needs phf_plan_buildhsg");
+            return PHF_ERR_UNSUPPORTED;
+        }
+    }
+    PHF_CUDA(cudaSetDevice(dev));
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    if (g_prof.on) {  // kernel by kernel, one instance after another
+        for (int i = 0; i < count; ++i) {
+            PHF_TRY(eval_enqueue(*plans[i], d_c[i], d_hs[i], d_yg[i], d_yr[i], st, false));
+            PHF_TRY(read_flag(*plans[i], st));
+        }
+        return PHF_OK;
+    }
+    std::vector<const void *> key;
+    key.reserve(5 * (size_t)count);
+    for (int i = 0; i < count; ++i) {
+        key.push_back(plans[i]);
+        key.push_back(d_c[i]);
+        key.push_back(d_hs[i]);
+        key.push_back(d_yg[i]);
+        key.push_back(d_yr[i]);
+    }
+    BatchGraph &bg = g_batch;
+    if (!(bg.exec && bg.key == key && bg.epoch == g_plan_epoch && bg.device == dev)) {
+        bg.release();
+        PHF_TRY(batch_streams(dev));
+        PHF_CUDA(cudaMalloc(&bg.d_flags, 2 * (size_t)count * sizeof(int)));
+        PHF_CUDA(cudaMalloc(&bg.d_ptrs, 2 * (size_t)count * sizeof(int *)));
+        std::vector<int *> ptrs(2 * (size_t)count);
+        for (int i = 0; i < count; ++i) {
+            ptrs[2 * i] = plans[i]->flag;
+            ptrs[2 * i + 1] = plans[i]->ozerr;
+        }
+        PHF_CUDA(cudaMemcpy(bg.d_ptrs, ptrs.data(), ptrs.size() * sizeof(int *), cudaMemcpyHostToDevice));
+        float best = 0.f;
+        for (int nb : {4, 8, 16}) {
+            if (nb > 4 && nb > count) break;
+            const int use = std::min(nb, count);
+            cudaGraphExec_t ex = nullptr;
+            unsigned long long nl = 0;
+            PHF_TRY(capture_batch(plans, count, d_c, d_hs, d_yg, d_yr, use, bg.d_ptrs, bg.d_flags, &ex, &nl));
+            cudaEvent_t e0, e1;
+            PHF_CUDA(cudaEventCreate(&e0));
+            PHF_CUDA(cudaEventCreate(&e1));
+            PHF_CUDA(cudaGraphLaunch(ex, st));  // warm
+            PHF_CUDA(cudaEventRecord(e0, st));
+            PHF_CUDA(cudaGraphLaunch(ex, st));
+            PHF_CUDA(cudaEventRecord(e1, st));
+            PHF_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PHF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (!bg.exec || ms < best) {
+                if (bg.exec) cudaGraphExecDestroy(bg.exec);
+                bg.exec = ex;
+                bg.branches = use;
+                bg.launches = nl;
+                best = ms;
+            } else {
+                cudaGraphExecDestroy(ex);
+            }
+        }
+        bg.key = key;
+        bg.epoch = g_plan_epoch;
+        bg.device = dev;
+        bg.count = count;
+        bg.h_flags.assign(2 * (size_t)count, 0);
+    }
+    PHF_CUDA(cudaGraphLaunch(bg.exec, st));
+    g_launches += bg.launches;
+    PHF_CUDA(cudaMemcpyAsync(bg.h_flags.data(), bg.d_flags, bg.h_flags.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                             st));
+    PHF_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < count; ++i) {
+        const int f = bg.h_flags[2 * i], oz = bg.h_flags[2 * i + 1];
+        if (oz) {
+            set_error(PHF_ERR_CUDA, "phf_eval_batch: instance " + std::to_string(i) +
+                                        ": tensor-core GEMM pipeline wait timed out");
+            return PHF_ERR_CUDA;
+        }
+        if (f & 1) {
+            set_error(PHF_ERR_SINGULAR, "phf_eval_batch: instance " + std::to_string(i) + ": singular rotated overlap");
+            return PHF_ERR_SINGULAR;
+        }
+        if (f & 2) {
+            set_error(PHF_ERR_NONFINITE, "phf_eval_batch: instance " + std::to_string(i) + ": non-finite overlap");
+            return PHF_ERR_NONFINITE;
+        }
+    }
+    return PHF_OK;
+}
+
+int batch_branches() { return g_batch.branches; }
 
 }  // namespace phf

@@ -27,6 +27,16 @@ struct Arena {
         bufs.clear();
         total = 0;
     }
+    // frees one buffer of this arena early (no-op for a pointer it does not own)
+    void free_one(void *ptr) {
+        for (auto it = bufs.begin(); it != bufs.end(); ++it)
+            if (it->p == ptr) {
+                cudaFree(it->p);
+                total -= it->bytes;
+                bufs.erase(it);
+                return;
+            }
+    }
     template <typename T>
     int alloc(T **out, size_t count) {
         size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
@@ -185,6 +195,10 @@ int split_setup(PlanImpl &p);
 int split_gamma_x(PlanImpl &p, int bc, cudaStream_t st);
 
 // phf_engine.cu
+int plan_eval_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *const *d_hs, zc *const *d_yg,
+                    zc *const *d_yr, cudaStream_t st);
+void plan_destroyed();  // invalidates cached batch graphs
+int batch_branches();   // concurrent branches of the last captured batch graph
 int profile_enable(int on);
 int profile_read(int cls, double *ms, unsigned long long *count);
 int plan_create(const phf_plan_desc *d, phf_plan **out);

@@ -206,6 +206,15 @@ def int8_ops_per_point(p, slices):
     return slices * (slices + 1) / 2 * (16.0 * p.n ** 4 + 8.0 * p.L * p.n ** 2)
 
 
+def tc_ops_per_point(p, precision, slices):
+    """Executed tensor-core operations per grid point of the eri-form contractions: int8 slice
+    products (S(S+1)/2 of them), three BF16 products for bf16x3, one TF32 product for tf32."""
+    if precision == "ozaki_i8":
+        return int8_ops_per_point(p, slices)
+    reps = 3 if precision == "bf16x3" else 1
+    return reps * (16.0 * p.n ** 4 + 8.0 * p.L * p.n ** 2)
+
+
 def survey_flops_per_point(p):
     """Per-point work figure of the benchmark description: 32 L n^3 + 8 L n^2 (J/K) plus
     16 M^2 N + 16 M N^2 + 8 N^3 + 16 M^3 (small algebra)."""
@@ -213,9 +222,9 @@ def survey_flops_per_point(p):
     return 32.0 * L * n ** 3 + 8.0 * L * n ** 2 + 16.0 * M * M * N + 16.0 * M * N * N + 8.0 * N ** 3 + 16.0 * M ** 3
 
 
-# ncu capture of the configuration-2 K launch (dram__bytes_read.sum + dram__bytes_write.sum):
-# 1.436 GB + 0.255 GB.  Algorithmic: A slices 101 MB + B slices 201 MB + FP64 output 268 MB.
-K_LAUNCH_DRAM_BYTES = 1.436e9 + 0.255e9
+# ncu capture of the configuration-2 K launch at S = 5 (dram__bytes_read.sum + dram__bytes_write.sum):
+# 1.180 GB + 0.253 GB.  Algorithmic: A slices 101 MB + B slices 201 MB + FP64 output 268 MB.
+K_LAUNCH_DRAM_BYTES = 1.180e9 + 0.253e9
 K_LAUNCH_ALG_BYTES = 0.101e9 + 0.201e9 + 0.268e9
 
 
@@ -405,6 +414,7 @@ def run_ours(args):
     # the plain FP64 form on the same problem (comparison and error reference): with this
     # library's FP64 GEMM kernels, and with cuBLAS DGEMM for the exchange GEMM
     fp64 = None
+    ref64 = None
     if args.precision != "fp64" and not args.no_fp64:
         fp64 = {}
         forms = [("own_kernels", False, "eri"), ("cublas_exchange", True, "eri")]
@@ -417,12 +427,39 @@ def run_ours(args):
             ms64, E64, G64, _, prof64 = time_plan(torch, plan64, C, stream, n64, 1, flush, _lib)
             plan64.close()
             torch.cuda.empty_cache()
+            if label == "own_kernels":
+                ref64 = (E64, G64)
             dE = abs(E.item() - E64.item())
             dG = float((G - G64).abs().max().item())
             fp64[label] = {"value": p.grid.npoints / (ms64 * 1e-3), "ms_per_step": ms64, "energy": E64.item(),
                            "jk_form": jf, "exchange_ms_per_step": prof64[0][0] / n64,
                            "abs_dE_vs_fp64": dE, "max_abs_dgrad_vs_fp64": dG, "speedup": ms64 / step_ms,
                            "meets_1e-8_Eh": dE <= 1e-8}
+
+    # precision study: the other tensor-core precisions on the same problem, timed the same way,
+    # with their energy and gradient errors against the FP64 form
+    study = None
+    if (args.study or args.config == "c3") and ref64 is not None:
+        study = {args.precision: {"ms_per_step": step_ms, "value": p.grid.npoints / (step_ms * 1e-3),
+                                  "abs_dE_vs_fp64": abs(E.item() - ref64[0].item()),
+                                  "max_abs_dgrad_vs_fp64": float((G - ref64[1]).abs().max().item()),
+                                  "jk_ms_per_step": prof[0][0] / args.steps}}
+        for prec in ("ozaki_i8", "bf16x3", "tf32"):
+            if prec == args.precision:
+                continue
+            plan_s = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, slices=args.slices, jk_form=form, **kw)
+            ms_s, E_s, G_s, _, prof_s = time_plan(torch, plan_s, C, stream, max(1, min(args.steps, 3)), 2, flush,
+                                                  _lib)
+            plan_s.close()
+            torch.cuda.empty_cache()
+            study[prec] = {"ms_per_step": ms_s, "value": p.grid.npoints / (ms_s * 1e-3),
+                           "abs_dE_vs_fp64": abs(E_s.item() - ref64[0].item()),
+                           "max_abs_dgrad_vs_fp64": float((G_s - ref64[1]).abs().max().item()),
+                           "jk_ms_per_step": prof_s[0][0] / max(1, min(args.steps, 3))}
+        for prec, r in study.items():
+            r["meets_1e-8_Eh"] = r["abs_dE_vs_fp64"] <= 1e-8
+            r["meets_1e-7_grad"] = r["max_abs_dgrad_vs_fp64"] <= 1e-7
+            r["tc_tops"] = tc_ops_per_point(p, prec, slices) * p.grid.npoints / (r["jk_ms_per_step"] * 1e-3) / 1e12
 
     # end to end with host buffers: (1) the plan API an optimiser loop uses (Hamiltonian set up once,
     # per call: Z host -> device, the grid pass, Hmat/Smat/Gradmat/Rdmmat device -> host); (2) the
@@ -474,9 +511,13 @@ def run_ours(args):
             i8 = measure_int8_peak(torch, dev)
             bf16 = peaks.get("bf16_tflops")
             peak = 2.0 * bf16 if bf16 else i8
-            achieved = int8_ops_per_point(p, slices) * pts / (jk_ms * 1e-3) / 1e12
-            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
-                    "frac": achieved / peak, "traffic": K_LAUNCH_DRAM_BYTES if args.config == "c2" else None,
+            if args.precision != "ozaki_i8":  # dense bf16 rate; TF32 runs at half of it
+                peak = bf16 * (0.5 if args.precision == "tf32" else 1.0) if bf16 else None
+            achieved = tc_ops_per_point(p, args.precision, slices) * pts / (jk_ms * 1e-3) / 1e12
+            unit = {"ozaki_i8": "TOP/s (int8)", "bf16x3": "TFLOP/s (bf16)", "tf32": "TFLOP/s (tf32)"}[args.precision]
+            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
+                    "frac": achieved / peak if peak else None,
+                    "traffic": K_LAUNCH_DRAM_BYTES if (args.config == "c2" and args.precision == "ozaki_i8") else None,
                     "traffic_note": ("DRAM read + write of one K launch (4096 x 8192 x 4096) from an ncu "
                                      "capture of this workload; algorithmic bytes of that launch: "
                                      f"{K_LAUNCH_ALG_BYTES:.3g}"),
@@ -485,7 +526,8 @@ def run_ours(args):
                     "int8_cublaslt_tops_measured": i8,
                     "frac_of_cublaslt_int8": achieved / i8 if i8 else None,
                     "bf16_tflops_measured": bf16,
-                    "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::i8, exchange and Coulomb GEMMs)",
+                    "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::%s, exchange and Coulomb GEMMs)"
+                              % {"ozaki_i8": "i8", "bf16x3": "f16 (bf16)", "tf32": "tf32"}[args.precision],
                     "fp64_equivalent_tflops": alg * pts / (jk_ms * 1e-3) / 1e12,
                     "fp64_dgemm_peak_tflops": fp64_peak}
         roof.update({"jk_form": form, "jk_launches": jk_n, "jk_ms_per_step": jk_ms / args.steps,
@@ -497,7 +539,9 @@ def run_ours(args):
         if not args.no_cpu:
             v, nth, desc = cpu_sample(p, seconds_target=args.cpu_seconds)
             cpu = {"value": v, "unit": UNIT, "cores": nth, "kind": "port", "sample": desc}
-        dtype = "f64" if args.precision == "fp64" else f"int8 x{slices} slices (FP64-accurate emulation) + f64"
+        dtype = {"fp64": "f64", "ozaki_i8": f"int8 x{slices} slices (FP64-accurate emulation) + f64",
+                 "bf16x3": "bf16 hi+lo x3 products, f32 accumulation + f64",
+                 "tf32": "tf32, f32 accumulation + f64"}[args.precision]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded h, B_L, determinant)",
@@ -505,7 +549,7 @@ def run_ours(args):
                            "points_per_step": p.grid.npoints, "chunk": chunk,
                            "l2": "flushed (256 MB write) between timed steps",
                            "parallelism": f"{world} independent instance(s), one per GPU"},
-                "energy": float(E.item()), "fp64_gpu": fp64,
+                "energy": float(E.item()), "fp64_gpu": fp64, "precision_study": study,
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "path": "phf_plan_buildhsg (C ABI, host Z in, host Hmat/Smat/Gradmat/Rdmmat out; "
@@ -616,6 +660,7 @@ def run_batch(args):
         pl.close()
     torch.cuda.empty_cache()
     fp64 = None
+    ref64 = None
     if args.precision != "fp64" and not args.no_fp64:
         plans64 = make("fp64")
         ms64, outs64, _ = time_batch(plans64, max(1, min(args.steps, 3)), 1)
@@ -681,7 +726,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--batch", type=int, default=256, help="instances for --config c4")
-    ap.add_argument("--precision", default="ozaki_i8", choices=["fp64", "ozaki_i8"])
+    ap.add_argument("--precision", default="ozaki_i8", choices=["fp64", "ozaki_i8", "bf16x3", "tf32"])
+    ap.add_argument("--study", action="store_true",
+                    help="also run the other tensor-core precisions and report their errors against FP64 "
+                         "(on by default for --config c3)")
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
     ap.add_argument("--e2e-steps", type=int, default=3)

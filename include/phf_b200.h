@@ -56,8 +56,8 @@ enum phf_status {
 enum phf_precision {
     PHF_PREC_FP64 = 0,      /* FP64 CUDA-core GEMMs (the plain FP64 form) */
     PHF_PREC_OZAKI_I8 = 1,  /* FP64-accurate emulation: int8 slices on tcgen05 tensor cores */
-    PHF_PREC_BF16X3 = 2,    /* split-BF16, 3 products, FP32 accumulation (tcgen05) */
-    PHF_PREC_TF32 = 3       /* TF32, FP32 accumulation (tcgen05) */
+    PHF_PREC_BF16X3 = 2,    /* split-BF16 (hi + lo: ~16 significant bits), 3 products, FP32 accumulation (tcgen05) */
+    PHF_PREC_TF32 = 3       /* TF32 (11 significant bits), FP32 accumulation (tcgen05) */
 };
 
 /* ---------------------------------------------------------------- drop-in entry points */
@@ -170,6 +170,17 @@ int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes);
  * No counterpart in the reference (its J/K is a dense FP64 loop, PHFTools.f90:310-337). */
 int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
                     long long ldb, double *dD, long long ldd, void *stream);
+
+/* The real GEMM of phf_ozaki_dgemm in each tensor-core precision that plans offer for their J/K
+ * contractions, with the same arithmetic: PHF_PREC_OZAKI_I8 with `slices` int8 slices
+ * (0 = 5); PHF_PREC_BF16X3: each row of A and column of B scaled by a power of two, split into
+ * BF16 high and low parts (about 16 significant bits), hi*hi + hi*lo + lo*hi on the tensor cores
+ * with FP32 accumulation (hi*hi and the cross terms in separate accumulators, summed in FP64);
+ * PHF_PREC_TF32: TF32 operands (10 fraction bits, round to nearest), FP32 accumulation.  `slices`
+ * is ignored for the floating-point precisions; PHF_PREC_FP64 is PHF_ERR_ARG.  Device pointers;
+ * synchronous on `stream`.  No counterpart in the reference. */
+int phf_tc_dgemm(int m, int n, int k, int precision, int slices, const double *dA, long long lda, const double *dBt,
+                 long long ldb, double *dD, long long ldd, void *stream);
 
 /* The same product as phf_ozaki_dgemm for callers that cannot allocate device memory at the
  * point of the call: code that runs while another component is capturing a CUDA graph,

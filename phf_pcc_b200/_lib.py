@@ -71,6 +71,8 @@ SIGNATURES = {
     "phf_version": (ctypes.c_char_p, []),
     "phf_profile_enable": (_I, [_I]),
     "phf_ozaki_dgemm": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P]),
+    "phf_tc_dgemm": (_I, [_I, _I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong,
+                          _P]),
     "phf_ozaki_dgemm_noalloc": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P,
                                      ctypes.c_longlong, _P]),
     "phf_ozaki_dgemm_noalloc_scratch_bytes": (ctypes.c_size_t, [_I, _I, _I, _I]),

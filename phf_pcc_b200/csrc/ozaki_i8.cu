@@ -1,15 +1,14 @@
 // FP64-accurate GEMM on the tcgen05 int8 tensor cores (Ozaki-style error-free slicing).
 //
 // D = A B with A (m x k) and B (k x n) given as FP64.  Each row of A is scaled by a power of
-// two 2^ea so that |a| < 1 and cut into S signed 7-bit slices, a = sum_t a_t 2^{-7t}
-// (a_t in [-127, 127], truncation, the last slice rounded); each column of B likewise with
-// 2^eb.  Then
-//     D_ij = 2^{ea_i + eb_j} sum_{g=2}^{S+1} 2^{-7g} sum_{t+u=g} (A_t B_u)_ij
-// where every A_t B_u is an exact int8 x int8 -> int32 product on the tensor cores, the
-// products of one group g share one int32 accumulator (exact while (g-1) k 127^2 < 2^31),
-// and the S group sums are combined in FP64 in the epilogue.  Terms with t + u > S + 1 are
-// dropped; since a slice is an integer up to 127 ~ 2^7 (times 2^{-7t}), the dropped terms and
-// the slicing remainder are of order 2^{-7S}: an entry's error is below about
+// two so that r = 127 a 2^-ea lies in (-127, 127) and cut into S balanced base-254 digits,
+// r = sum_t d_t 254^{-t} (d_t in [-127, 127]); each column of B likewise with 2^eb.  Then
+//     D_ij = 2^{ea_i + eb_j} / 127^2 sum_{g=2}^{S+1} 254^{2-g} sum_{t+u=g} (A_t B_u)_ij
+// (slices numbered from 1) where every A_t B_u is an exact int8 x int8 -> int32 product on the
+// tensor cores, the products of one group g share one int32 accumulator (exact while
+// (g-1) k 127^2 < 2^31; longer k runs in several launches that add into D), and the S group sums
+// are combined in FP64 in the epilogue.  Terms with t + u > S + 1 are dropped; the dropped terms
+// and the digit remainder are of order 254^{-S} < 2^{-7S}: an entry's error is below about
 // (S+1) k 2^{-7S} max|A_i.| max|B_.j| (random-sign errors grow like sqrt(k) in practice).
 // (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix multiplication by using
 // fast routines of matrix multiplication and its applications", Numer. Algorithms 59 (2012).)
@@ -17,26 +16,34 @@
 // Slice layout in global memory (per operand, rows padded to 128, k to KB blocks of 32): slices
 // 0..3 (group 0) interleaved per k-block so that one 128-byte row segment holds the same 32
 // k-elements of four slices, byte (row KB + kb) 128 + t 32 + kk; then slices 4..S-1 (group 1) in
-// 64-byte segments for S = 5, 6 (two slices) or 128-byte segments for S = 7.  A TMA box of full
-// segments (SWIZZLE_128B / SWIZZLE_64B) then carries several slices at once, and the MMA picks a
-// slice by a +32-byte offset of its K-major descriptor.
+// 32-byte segments for S = 5, 64-byte segments for S = 6 or 128-byte segments for S = 7.  A TMA
+// box of full segments (SWIZZLE_128B / 64B / 32B) carries several slices at once, and the MMA
+// picks a slice by a +32-byte offset of its K-major descriptor.
 //
-// Kernel shape (one CTA per 128 x 128 output tile, 6 warps); in launch order the CTAs sweep the
-// column tiles in groups of eight row tiles, so that the A and B tiles in use fit in L2 together:
+// Kernel shape (one CTA per output tile, 6 warps); in launch order the CTAs sweep the column
+// tiles in groups of eight row tiles, so that the A and B tiles in use fit in L2 together:
 //   warp 0      TMA producer into a ring of fourteen 16 KB units (full/empty mbarrier per unit):
-//               per 32-element k-block the A and B boxes of group 0 (a unit each) and, in the
-//               second pass, of group 1 (one unit holding both 8 KB boxes for S = 5, 6)
-//   warp 1      TMEM allocation (512 columns = four 128 x 128 int32 accumulators) and the
-//               single-thread tcgen05.mma issuer.  The S groups g = 2..S+1 run in passes of four
-//               groups over the whole k range; per k-block every slice pair of the pass's groups
-//               is one 128 x 128 x 32 MMA
+//               per 32-element k-block the A and B boxes of group 0 (a unit each) and, in a pass
+//               that uses group 1, its A and B boxes (one unit for S = 5, 6, two for S = 7)
+//   warp 1      TMEM allocation (512 columns) and the single-thread tcgen05.mma issuer.  S = 5
+//               runs all five groups g = 2..6 in one pass over 128 x 96 tiles (five int32
+//               accumulators, 480 columns); otherwise the tile is 128 x 128 and the groups run in
+//               passes of four over the whole k range.  Per k-block every slice pair of the
+//               pass's groups is one 128 x BN x 32 MMA
 //   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of the pass's groups, int32 ->
-//               FP64 with 2^{-7g} scaling.  For S <= 6 the first pass's FP64 sums are parked in
+//               FP64 with 254^{2-g} scaling.  For S = 6 the first pass's FP64 sums are parked in
 //               TMEM (columns 0..255, where groups 2 and 3 were) and the second pass, accumulating
-//               in columns 256..511, adds them before the single 2^{ea+eb}-scaled store to D;
-//               for S = 7 the second pass adds into D
+//               in columns 256..511, adds them before the single scaled store to D; for S = 7 the
+//               second pass adds into D
 // Every mbarrier wait gives up after ~2^31 clock cycles, sets *err and lets the CTA finish.
+//
+// The same kernel contracts two floating-point operand formats (slice-count codes OZ_FMT_BF16X3
+// and OZ_FMT_TF32): a row (column) scaled by 2^-ea is held as BF16 high and low parts, or as one
+// TF32 value, in one 128-byte segment per 32-element k-block; the MMAs are kind::f16 (BF16 x BF16)
+// or kind::tf32 with FP32 accumulators in TMEM.  BF16X3 adds hi*hi into one accumulator and the
+// two cross products hi*lo + lo*hi into a second, and the epilogue sums the two in FP64.
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
@@ -117,6 +124,17 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     return d;
 }
 
+// Shared-memory matrix descriptor: K-major, SWIZZLE_32B (8 rows x 32 B atoms, SBO = 256 B).
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(256 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)6 << 61;                           // layout: SWIZZLE_32B
+    return d;
+}
+
 // Shared-memory matrix descriptor: K-major, SWIZZLE_64B (8 rows x 64 B atoms, SBO = 512 B).
 __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
     uint64_t d = 0;
@@ -139,6 +157,33 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, 
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// Instruction descriptors with FP32 accumulation, K-major A and B, M = 128, N = BN: kind::f16 with
+// A = B = BF16, and kind::tf32.
+template <int BN>
+__host__ __device__ constexpr uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
+template <int BN>
+__host__ __device__ constexpr uint32_t idesc_tf32() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
@@ -182,11 +227,25 @@ struct OzArgs {
     int *err;
 };
 
-// slice groups: group 0 = slices 0..3, group 1 = slices 4..S-1 (S >= 5)
-__host__ __device__ __forceinline__ int oz_ngroups(int S) { return (S + OZ_GP - 1) / OZ_GP; }
+// floating-point operand formats (slice-count codes beyond the int8 range 1..7)
+__host__ __device__ constexpr bool oz_float(int S) { return S == OZ_FMT_BF16X3 || S == OZ_FMT_TF32; }
 
-// Slices per k-block row of group 1: two (64-byte rows) for S = 5, 6, four (128-byte rows) for S = 7.
-__host__ __device__ constexpr int oz_g1_width(int S) { return S <= OZ_GP ? 0 : (S <= 6 ? 2 : 4); }
+// Slices per k-block row of group 1: one (32-byte rows) for S = 5, two (64-byte rows) for S = 6,
+// four (128-byte rows) for S = 7; none for S <= 4 and the floating-point formats (one 128-byte
+// segment per k-block).
+__host__ __device__ constexpr int oz_g1_width(int S) {
+    return (S <= OZ_GP || oz_float(S)) ? 0 : (S == 5 ? 1 : (S == 6 ? 2 : 4));
+}
+
+// Byte offset of element (row, k) of a floating-point-format operand (KB k-blocks of 32): the
+// 128-byte segment of (row, k-block) holds, for BF16X3, the high parts of its 32 elements in bytes
+// [0, 64) and the low parts in [64, 128) (part = 0, 1); for TF32 the 32 four-byte values.  Each
+// 32-byte quarter is the K-chunk of one MMA (16 BF16 or 8 TF32 values).
+__host__ __device__ __forceinline__ long long oz_float_offset(int part, long long row, long long k, long long KB,
+                                                              int S) {
+    const long long base = (row * KB + (k >> 5)) << 7, kk = k & 31;
+    return S == OZ_FMT_BF16X3 ? base + 64 * part + 2 * kk : base + 4 * kk;
+}
 
 // Byte offset of slice t of element (row, k) in an operand's slice buffer with rows_pad rows and KB
 // k-blocks of 32: group 0 in 128-byte k-block rows, then group 1 in (32 x width)-byte rows.
@@ -197,9 +256,9 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
     return rows_pad * KB * 128 + (row * KB + kb) * (32LL * oz_g1_width(S)) + ((long long)(t - OZ_GP) << 5) + kk;
 }
 
-// Shared-memory ring of OZ_UNITS units of 16 KB: a k-block of the first pass takes two units (A and
-// B tiles of slice group 0), of the second pass three (plus A and B of group 1 at 64-byte rows, 8 KB
-// each) or four (S = 7: group 1 at 128-byte rows).
+// Shared-memory ring of OZ_UNITS units of 16 KB: a k-block takes two units (A and B tiles of slice
+// group 0), plus, in a pass that uses group 1, one unit holding its A and B boxes at 32-byte (S = 5)
+// or 64-byte (S = 6) rows, or two units (S = 7: group 1 at 128-byte rows).
 constexpr int OZ_UNITS = 14;
 constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
 
@@ -207,21 +266,21 @@ constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
 // 96-column tiles (5 x 96 of the 512 TMEM columns); the others use 128-column tiles and passes of
 // up to four groups (S = 6, 7: groups 2..5, then the rest).
 __host__ __device__ constexpr int oz_bn(int S) { return S == 5 ? 96 : 128; }
-__host__ __device__ constexpr int oz_npass(int S) { return S == 5 ? 1 : (S + OZ_GP - 1) / OZ_GP; }
+__host__ __device__ constexpr int oz_npass(int S) { return (S == 5 || oz_float(S)) ? 1 : (S + OZ_GP - 1) / OZ_GP; }
 __host__ __device__ constexpr int oz_g0(int P) { return 2 + OZ_GP * P; }
 __host__ __device__ constexpr int oz_g1(int S, int P) {
     return S == 5 ? 6 : ((1 + OZ_GP * (P + 1) < S + 1) ? 1 + OZ_GP * (P + 1) : S + 1);
 }
 // 16 KB ring units a k-block of pass P takes: A and B of group 0, plus group 1 when the pass uses
-// slices beyond the fourth (one unit holding both 64-byte-row boxes, or one each for S = 7)
+// slices beyond the fourth (one unit holding both 32- or 64-byte-row boxes, or one each for S = 7)
 __host__ __device__ constexpr int oz_units(int S, int P) {
-    return oz_g1(S, P) - 1 > OZ_GP ? (oz_g1_width(S) == 2 ? 3 : 4) : 2;
+    return oz_float(S) ? 2 : (oz_g1(S, P) - 1 > OZ_GP ? (oz_g1_width(S) <= 2 ? 3 : 4) : 2);
 }
 // bytes the TMA delivers into unit j of a k-block
 __host__ __device__ constexpr uint32_t oz_unit_bytes(int S, int j) {
     return j == 0 ? OZ_BM * 128u
                   : j == 1 ? (uint32_t)oz_bn(S) * 128u
-                           : (oz_g1_width(S) == 2 ? (OZ_BM + (uint32_t)oz_bn(S)) * 64u
+                           : (oz_g1_width(S) <= 2 ? (OZ_BM + (uint32_t)oz_bn(S)) * 32u * (uint32_t)oz_g1_width(S)
                                                   : (j == 2 ? OZ_BM * 128u : (uint32_t)oz_bn(S) * 128u));
 }
 
@@ -251,6 +310,29 @@ __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64
     }
 }
 
+// One k-block of a floating-point format (one 128-byte segment per operand row, +2 in a descriptor
+// = +32 bytes = the next quarter).  TF32: four K = 8 MMAs into acc0.  BF16X3 (quarters 0, 1 = high
+// parts of k 0..15 and 16..31, quarters 2, 3 = low parts): hi*hi into acc0, hi*lo and lo*hi into
+// acc0 + BN.
+template <int S>
+__device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, uint64_t dB, uint32_t acc_in) {
+    constexpr int BN = oz_bn(S);
+    if constexpr (S == OZ_FMT_TF32) {
+        constexpr uint32_t idesc = idesc_tf32<BN>();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mma_tf32(acc0, dA + 2 * q, dB + 2 * q, idesc, q > 0 ? 1u : acc_in);
+    } else {
+        constexpr uint32_t idesc = idesc_bf16<BN>();
+        const uint32_t acc1 = acc0 + BN;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) mma_bf16(acc0, dA + 2 * h, dB + 2 * h, idesc, h > 0 ? 1u : acc_in);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) mma_bf16(acc1, dA + 2 * h, dB + 4 + 2 * h, idesc, h > 0 ? 1u : acc_in);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) mma_bf16(acc1, dA + 4 + 2 * h, dB + 2 * h, idesc, 1u);
+    }
+}
+
 // The MMA issuer's k-block loop of pass P (u, ph: next ring unit and its full-barrier parity).
 template <int S, int P>
 __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
@@ -271,14 +353,20 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
         const uint64_t dA0 = sdesc_sw128(smem_base + (uint32_t)us[0] * OZ_UNIT);
         const uint64_t dB0 = sdesc_sw128(smem_base + (uint32_t)us[1] * OZ_UNIT);
         uint64_t dA1 = 0, dB1 = 0;
-        if constexpr (NU == 3) {
+        if constexpr (NU == 3 && oz_g1_width(S) == 1) {
+            dA1 = sdesc_sw32(smem_base + (uint32_t)us[2] * OZ_UNIT);
+            dB1 = sdesc_sw32(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 32);
+        } else if constexpr (NU == 3) {
             dA1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT);
             dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 64);
         } else if constexpr (NU == 4) {
             dA1 = sdesc_sw128(smem_base + (uint32_t)us[2] * OZ_UNIT);
             dB1 = sdesc_sw128(smem_base + (uint32_t)us[3] * OZ_UNIT);
         }
-        issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
+        if constexpr (oz_float(S))
+            issue_kblock_float<S>(acc0, dA0, dB0, kb > 0 ? 1u : 0u);
+        else
+            issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
 #pragma unroll
         for (int j = 0; j < NU; ++j) mma_commit(&empty_bar[us[j]]);  // units reusable once these MMAs read them
     }
@@ -297,6 +385,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         return;
     }
     constexpr int W1 = oz_g1_width(S), BN = oz_bn(S);
+    constexpr double kUnit = oz_float(S) ? 1.0 : 1.0 / 127.0;  // value of one slice unit at exponent 0
     const int npass = oz_npass(S);  // pass p: groups oz_g0(p) .. oz_g1(S, p)
     // With two passes and at most two groups in the second, the first pass's FP64 partial sums stay
     // in TMEM columns [0, 256) (high words, then low words, per 32-column chunk) and the second
@@ -345,7 +434,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
     if (warp >= 2) {
         const int c = threadIdx.x - 64;
-        colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(1.0 / 127.0, args.eb[n0 + c]) : 0.0;
+        colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(kUnit, args.eb[n0 + c]) : 0.0;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
@@ -379,9 +468,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                             tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, m0);
                         } else if (j == 1) {
                             tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, n0);
-                        } else if (W1 == 2) {  // j == 2: A and B of group 1 at 64-byte rows
-                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 64, m0);
-                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 64, kbg * 64, n0);
+                        } else if (W1 <= 2) {  // j == 2: A and B of group 1 at 32- or 64-byte rows
+                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 32 * W1, m0);
+                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 32 * W1, kbg * 32 * W1, n0);
                         } else if (j == 2) {
                             tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, m0);
                         } else {
@@ -425,7 +514,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
-        const double rowscale = row_ok ? ldexp(1.0 / 127.0, args.ea[row]) : 0.0;
+        const double rowscale = row_ok ? ldexp(kUnit, args.ea[row]) : 0.0;
         double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
         const long long cstride = args.trans ? args.ldd : 1;
         for (int p = 0; p < npass; ++p) {
@@ -440,13 +529,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 double acc[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                if constexpr (oz_float(S)) {
+                    // FP32 accumulators (BF16X3: the cross-product sum, then hi*hi), summed in FP64
 #pragma unroll 1
-                for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
-                    uint32_t v[32];
-                    tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
-                    const double sc = kPow254[g - 2];
+                    for (int g = (S == OZ_FMT_BF16X3 ? 1 : 0); g >= 0 && KB > 0; --g) {
+                        uint32_t v[32];
+                        tmem_ld32(acc0 + (uint32_t)g * BN + c * 32, v);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                        for (int j = 0; j < 32; ++j) acc[j] += (double)__uint_as_float(v[j]);
+                    }
+                } else {
+#pragma unroll 1
+                    for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
+                        uint32_t v[32];
+                        tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
+                        const double sc = kPow254[g - 2];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                    }
                 }
                 if (keep && p == 1) {  // add the first pass's partial sums
                     uint32_t hi[32], lo[32];
@@ -546,9 +646,35 @@ __device__ __forceinline__ void slice_digits(double x, const SliceScale &sc, int
     }
 }
 
+// Floating-point formats of r = x 2^-e (|r| < 1).  BF16X3: hi = the BF16 nearest to (float) r,
+// lo = the BF16 nearest to r - hi (exact in FP64), so that r - hi - lo = O(2^-17 |r|).  TF32: the
+// FP32 value of r rounded to 10 fraction bits, ties away from zero (cvt.rna.tf32.f32), whose
+// low 13 bits are zero.  Returned as raw bits: hi | lo << 16, or the TF32 word.
+__device__ __forceinline__ uint32_t float_format_bits(double x, const SliceScale &sc, int S) {
+    const double r = sc.fast ? x * sc.p1 : ldexp(x, -sc.e);
+    if (S == OZ_FMT_TF32) {
+        uint32_t t;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)r));
+        return t;
+    }
+    const __nv_bfloat16 hi = __float2bfloat16_rn((float)r);
+    const __nv_bfloat16 lo = __float2bfloat16_rn((float)(r - (double)__bfloat162float(hi)));
+    return (uint32_t)__bfloat16_as_ushort(hi) | ((uint32_t)__bfloat16_as_ushort(lo) << 16);
+}
+
 // Slices of x for element k of row `row` of an operand slice buffer (rows_pad rows, KB k-blocks).
 __device__ __forceinline__ void slice_value(double x, const SliceScale &sc, int S, signed char *out, long long row,
                                             long long rows_pad, long long KB, long long k) {
+    if (oz_float(S)) {
+        const uint32_t bits = float_format_bits(x, sc, S);
+        if (S == OZ_FMT_TF32) {
+            *reinterpret_cast<uint32_t *>(out + oz_float_offset(0, row, k, KB, S)) = bits;
+        } else {
+            *reinterpret_cast<unsigned short *>(out + oz_float_offset(0, row, k, KB, S)) = (unsigned short)bits;
+            *reinterpret_cast<unsigned short *>(out + oz_float_offset(1, row, k, KB, S)) = (unsigned short)(bits >> 16);
+        }
+        return;
+    }
     int d[OZ_MAX_S];
     slice_digits(x, sc, S, d);
 #pragma unroll
@@ -671,28 +797,45 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
 // with the tensor-core MMA sequence of zgemm_kernel (m ascending in steps of four), so every
 // column, its exponent and its slices are those of the density GEMM followed by slice_rho_cols /
 // slice_p_cols.
-constexpr int RS_NT = 256, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded row pitch (complex)
+constexpr int RS_NT = 512, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded row pitch (complex)
+constexpr int RS_WI = 2;  // 8-row fragments per warp: 16 warps of 16 x 16 cover the 64 x 64 blocks
 
 // operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
 size_t rs_smem_bytes() { return std::max((size_t)2 * 2 * RS_MC * RS_P * sizeof(zc), (size_t)2 * 64 * 64 * sizeof(double)); }
 
 // Slices of four consecutive k-elements e0..e0+3 (one 32-element block) of a column, packed four
-// to a 32-bit word (byte v = element e0 + v), one store per slice.
+// to a 32-bit word (byte v = element e0 + v), one store per slice; for the floating-point formats
+// one 16-byte store (TF32) or two 8-byte stores (BF16 high parts, low parts).
 template <int S>
 __device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceScale &sc, signed char *out, long long row,
                                             long long rows_pad, long long KB, long long e0) {
-    uint32_t wd[S];
+    if constexpr (oz_float(S)) {
+        uint32_t b[4];
 #pragma unroll
-    for (int t = 0; t < S; ++t) wd[t] = 0u;
+        for (int v = 0; v < 4; ++v) b[v] = float_format_bits(x[v], sc, S);
+        if constexpr (S == OZ_FMT_TF32) {
+            *reinterpret_cast<uint4 *>(out + oz_float_offset(0, row, e0, KB, S)) = make_uint4(b[0], b[1], b[2], b[3]);
+        } else {
+            *reinterpret_cast<uint2 *>(out + oz_float_offset(0, row, e0, KB, S)) =
+                make_uint2((b[0] & 0xFFFFu) | (b[1] << 16), (b[2] & 0xFFFFu) | (b[3] << 16));
+            *reinterpret_cast<uint2 *>(out + oz_float_offset(1, row, e0, KB, S)) =
+                make_uint2((b[0] >> 16) | (b[1] & 0xFFFF0000u), (b[2] >> 16) | (b[3] & 0xFFFF0000u));
+        }
+    } else {
+        uint32_t wd[S];
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        int d[OZ_MAX_S];
-        slice_digits(x[v], sc, S, d);
+        for (int t = 0; t < S; ++t) wd[t] = 0u;
 #pragma unroll
-        for (int t = 0; t < S; ++t) wd[t] |= ((uint32_t)d[t] & 0xFFu) << (8 * v);
+        for (int v = 0; v < 4; ++v) {
+            int d[OZ_MAX_S];
+            slice_digits(x[v], sc, S, d);
+#pragma unroll
+            for (int t = 0; t < S; ++t) wd[t] |= ((uint32_t)d[t] & 0xFFu) << (8 * v);
+        }
+#pragma unroll
+        for (int t = 0; t < S; ++t)
+            *reinterpret_cast<uint32_t *>(out + oz_slice_offset(t, row, e0, rows_pad, KB, S)) = wd[t];
     }
-#pragma unroll
-    for (int t = 0; t < S; ++t) *reinterpret_cast<uint32_t *>(out + oz_slice_offset(t, row, e0, rows_pad, KB, S)) = wd[t];
 }
 
 template <int S>
@@ -712,12 +855,12 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
     // as FP64 tensor-core products (mma.sync m8n8k4: lane l holds A[l/4][l%4], B[l%4][l/4],
     // D[l/4][2 (l%4) + h]), four real MMAs per complex step in the order of zgemm_kernel
     const int lane = tid & 31, warp = tid >> 5;
-    const int wr = (warp >> 2) * 32, wc = (warp & 3) * 16, fr = lane >> 2, fk = lane & 3;
-    double cr[2][4][2][2], ci[2][4][2][2];
+    const int wr = (warp >> 2) * (8 * RS_WI), wc = (warp & 3) * 16, fr = lane >> 2, fk = lane & 3;
+    double cr[2][RS_WI][2][2], ci[2][RS_WI][2][2];
 #pragma unroll
     for (int q = 0; q < 2; ++q)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < RS_WI; ++i)
 #pragma unroll
             for (int j = 0; j < 2; ++j) cr[q][i][j][0] = cr[q][i][j][1] = ci[q][i][j][0] = ci[q][i][j][1] = 0.0;
 
@@ -746,7 +889,7 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
                     b[j].y = -b[j].y;  // conj(bra)
                 }
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < RS_WI; ++i) {
                     const zc a = xs[(sg * RS_MC + kk + fk) * RS_P + wr + 8 * i + fr];
 #pragma unroll
                     for (int j = 0; j < 2; ++j) {
@@ -774,7 +917,7 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
 #pragma unroll
     for (int col = 0; col < 6; ++col) mx[col] = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < RS_WI; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -817,7 +960,7 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
     for (int c0 = 0; c0 < 6; c0 += 2) {
         if (c0 >= ncol) break;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < RS_WI; ++i)
 #pragma unroll
             for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -876,7 +1019,8 @@ int make_group_map(CUtensorMap *map, const signed char *base, long long KB, int 
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<signed char *>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     seg_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     seg_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                      : (seg_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B),
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -932,8 +1076,8 @@ bool oz_rho_slice_ok(int n) { return n >= 1 && n <= 64; }
 
 int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra, int S, signed char *Ksl, int *eK,
                  signed char *Psl, int *eP, cudaStream_t st) {
-    if (!oz_rho_slice_ok(n) || S < 1 || S > OZ_MAX_S || N < 1) {
-        set_error(PHF_ERR_UNSUPPORTED, "oz_rho_slice: needs 1 <= n <= 64 and 1 <= slices <= 7");
+    if (!oz_rho_slice_ok(n) || !oz_format_ok(S) || N < 1) {
+        set_error(PHF_ERR_UNSUPPORTED, "oz_rho_slice: needs 1 <= n <= 64 and a valid operand format");
         return PHF_ERR_UNSUPPORTED;
     }
     using RsFn = void (*)(int, int, const zc *, long long, const zc *, long long, long long, long long, signed char *,
@@ -946,7 +1090,9 @@ int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra
         case 4: fn = rho_slice_kernel<4>; break;
         case 5: fn = rho_slice_kernel<5>; break;
         case 6: fn = rho_slice_kernel<6>; break;
-        default: fn = rho_slice_kernel<7>; break;
+        case 7: fn = rho_slice_kernel<7>; break;
+        case OZ_FMT_BF16X3: fn = rho_slice_kernel<OZ_FMT_BF16X3>; break;
+        default: fn = rho_slice_kernel<OZ_FMT_TF32>; break;
     }
     const size_t smem = rs_smem_bytes();
     PHF_CUDA(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -967,6 +1113,10 @@ int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *e
     PHF_CHECK_LAUNCH();
     return PHF_OK;
 }
+
+bool oz_format_ok(int S) { return (S >= 1 && S <= OZ_MAX_S) || oz_float(S); }
+
+int oz_slots(int S) { return OZ_GP + oz_g1_width(S); }
 
 size_t oz_slice_bytes(long long rows_pad, long long k, int S) {
     return (size_t)(OZ_GP + oz_g1_width(S)) * (size_t)rows_pad * (size_t)oz_pad_k(k);
@@ -994,8 +1144,18 @@ OzKernelFn oz_kernel_for(int S) {
         case 5: return ozaki_i8_gemm_kernel<5>;
         case 6: return ozaki_i8_gemm_kernel<6>;
         case 7: return ozaki_i8_gemm_kernel<7>;
+        case OZ_FMT_BF16X3: return ozaki_i8_gemm_kernel<OZ_FMT_BF16X3>;
+        case OZ_FMT_TF32: return ozaki_i8_gemm_kernel<OZ_FMT_TF32>;
         default: return nullptr;
     }
+}
+
+// k-blocks one launch may accumulate: int8 group sums stay exact while S kpass 127^2 < 2^31; the
+// FP32 accumulators of the floating-point formats take the whole k range.
+long long oz_kb_pass(int S) {
+    if (oz_float(S)) return 1LL << 40;
+    const long long kb = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
+    return kb < 1 ? 1 : kb;
 }
 
 __global__ void sum_splits_kernel(long long count, int nsplit, long long dz, const double *part, double *D) {
@@ -1014,8 +1174,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
                    const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
                    cudaStream_t st) {
     const long long kpad = oz_pad_k(k), kb_total = kpad / OZ_BK;
-    const long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
-    if (nsplit <= 1 || kb_total > kb_pass || kb_total < 2 * nsplit)
+    if (nsplit <= 1 || kb_total > oz_kb_pass(S) || kb_total < 2 * nsplit)
         return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, 0, trans, err, st);
     CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
@@ -1063,7 +1222,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st) {
-    if (S < 1 || S > OZ_MAX_S) {
+    if (!oz_format_ok(S)) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
@@ -1071,9 +1230,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
     PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
-    // k-blocks per pass: S * kpass * 127^2 < 2^31
-    long long kb_pass = (long long)(2147483647.0 / ((double)S * 127.0 * 127.0)) / OZ_BK;
-    if (kb_pass < 1) kb_pass = 1;
+    const long long kb_pass = oz_kb_pass(S);
     const long long kb_total = kpad / OZ_BK;
     const size_t smem = oz_smem_bytes();
     const OzKernelFn kern = oz_kernel_for(S);
@@ -1111,19 +1268,11 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
 
 }  // namespace phf
 
-extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
-                               long long ldb, double *dD, long long ldd, void *stream) {
-    using namespace phf;
-    set_error(PHF_OK, "");
-    if (m <= 0 || n <= 0 || k <= 0 || !dA || !dBt || !dD || lda < k || ldb < k || ldd < n) {
-        set_error(PHF_ERR_ARG, "phf_ozaki_dgemm: bad sizes or null pointer");
-        return PHF_ERR_ARG;
-    }
-    if (slices < 1 || slices > OZ_MAX_S) {
-        set_error(PHF_ERR_ARG, "phf_ozaki_dgemm: slices must be 1..7");
-        return PHF_ERR_ARG;
-    }
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+namespace phf {
+namespace {
+// Slices both operands into freshly allocated scratch, multiplies and frees (synchronous on st).
+int tc_dgemm(const char *who, int m, int n, int k, int S, const double *dA, long long lda, const double *dBt,
+             long long ldb, double *dD, long long ldd, cudaStream_t st) {
     const long long mp = oz_pad_rows(m), np = oz_pad_cols(n);
     signed char *As = nullptr, *Bs = nullptr;
     int *ea = nullptr, *eb = nullptr, *err = nullptr;
@@ -1132,11 +1281,11 @@ extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA
         if (status != PHF_OK) return;
         if (cudaMalloc(p, bytes) != cudaSuccess) {
             cudaGetLastError();
-            set_error(PHF_ERR_OOM, "phf_ozaki_dgemm: cudaMalloc failed");
+            set_error(PHF_ERR_OOM, std::string(who) + ": cudaMalloc failed");
             status = PHF_ERR_OOM;
         }
     };
-    const size_t asz = oz_slice_bytes(mp, k, slices), bsz = oz_slice_bytes(np, k, slices);
+    const size_t asz = oz_slice_bytes(mp, k, S), bsz = oz_slice_bytes(np, k, S);
     al((void **)&As, asz);
     al((void **)&Bs, bsz);
     al((void **)&ea, mp * sizeof(int));
@@ -1146,17 +1295,17 @@ extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA
         cudaMemsetAsync(As, 0, asz, st);
         cudaMemsetAsync(Bs, 0, bsz, st);
         cudaMemsetAsync(err, 0, sizeof(int), st);
-        status = oz_slice_rows(m, k, dA, lda, slices, mp, As, ea, st);
-        if (status == PHF_OK) status = oz_slice_rows(n, k, dBt, ldb, slices, np, Bs, eb, st);
-        if (status == PHF_OK) status = oz_gemm(m, n, k, slices, As, ea, Bs, eb, dD, ldd, 0, err, st);
+        status = oz_slice_rows(m, k, dA, lda, S, mp, As, ea, st);
+        if (status == PHF_OK) status = oz_slice_rows(n, k, dBt, ldb, S, np, Bs, eb, st);
+        if (status == PHF_OK) status = oz_gemm(m, n, k, S, As, ea, Bs, eb, dD, ldd, 0, err, st);
         int herr = 0;
         if (status == PHF_OK) {
             cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
             if (cudaStreamSynchronize(st) != cudaSuccess) {
-                set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm: stream synchronize failed");
+                set_error(PHF_ERR_CUDA, std::string(who) + ": stream synchronize failed");
                 status = PHF_ERR_CUDA;
             } else if (herr) {
-                set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm: pipeline wait timed out");
+                set_error(PHF_ERR_CUDA, std::string(who) + ": pipeline wait timed out");
                 status = PHF_ERR_CUDA;
             }
         }
@@ -1168,4 +1317,51 @@ extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA
     cudaFree(eb);
     cudaFree(err);
     return status;
+}
+
+bool gemm_args_ok(const char *who, int m, int n, int k, const double *dA, long long lda, const double *dBt,
+                  long long ldb, double *dD, long long ldd) {
+    if (m <= 0 || n <= 0 || k <= 0 || !dA || !dBt || !dD || lda < k || ldb < k || ldd < n) {
+        set_error(PHF_ERR_ARG, std::string(who) + ": bad sizes or null pointer");
+        return false;
+    }
+    return true;
+}
+}  // namespace
+}  // namespace phf
+
+extern "C" int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
+                               long long ldb, double *dD, long long ldd, void *stream) {
+    using namespace phf;
+    set_error(PHF_OK, "");
+    if (!gemm_args_ok("phf_ozaki_dgemm", m, n, k, dA, lda, dBt, ldb, dD, ldd)) return PHF_ERR_ARG;
+    if (slices < 1 || slices > OZ_MAX_S) {
+        set_error(PHF_ERR_ARG, "phf_ozaki_dgemm: slices must be 1..7");
+        return PHF_ERR_ARG;
+    }
+    return tc_dgemm("phf_ozaki_dgemm", m, n, k, slices, dA, lda, dBt, ldb, dD, ldd,
+                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int phf_tc_dgemm(int m, int n, int k, int precision, int slices, const double *dA, long long lda,
+                            const double *dBt, long long ldb, double *dD, long long ldd, void *stream) {
+    using namespace phf;
+    set_error(PHF_OK, "");
+    if (!gemm_args_ok("phf_tc_dgemm", m, n, k, dA, lda, dBt, ldb, dD, ldd)) return PHF_ERR_ARG;
+    int S = 0;
+    if (precision == PHF_PREC_OZAKI_I8) {
+        S = slices == 0 ? 5 : slices;
+        if (S < 1 || S > OZ_MAX_S) {
+            set_error(PHF_ERR_ARG, "phf_tc_dgemm: slices must be 0..7");
+            return PHF_ERR_ARG;
+        }
+    } else if (precision == PHF_PREC_BF16X3) {
+        S = OZ_FMT_BF16X3;
+    } else if (precision == PHF_PREC_TF32) {
+        S = OZ_FMT_TF32;
+    } else {
+        set_error(PHF_ERR_ARG, "phf_tc_dgemm: precision must be PHF_PREC_OZAKI_I8, PHF_PREC_BF16X3 or PHF_PREC_TF32");
+        return PHF_ERR_ARG;
+    }
+    return tc_dgemm("phf_tc_dgemm", m, n, k, S, dA, lda, dBt, ldb, dD, ldd, reinterpret_cast<cudaStream_t>(stream));
 }

@@ -261,9 +261,12 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.N = d->nocc;
     p.L = d->nchol;
     p.prec = d->precision;
-    p.slices = d->slices > 0 ? d->slices : 5;
-    // automatic form: the spatial-ERI exchange matrix for n <= 128, and at every size for the int8
-    // tensor-core path (which needs it); the factorized form for FP64 above n = 128
+    // operand format of the tensor-core GEMMs: int8 slice count, or a floating-point format code
+    p.slices = p.prec == PHF_PREC_BF16X3 ? OZ_FMT_BF16X3
+             : p.prec == PHF_PREC_TF32  ? OZ_FMT_TF32
+                                        : (d->slices > 0 ? d->slices : 5);
+    // automatic form: the spatial-ERI exchange matrix for n <= 128, and at every size for the
+    // tensor-core precisions (which need it); the factorized form for FP64 above n = 128
     if (p.chol)
         p.eri = (d->jk_form == 1) || (d->jk_form == 0 && (d->nso / 2 <= 128 || p.prec != PHF_PREC_FP64));
     p.exact = d->gradient_mode == 1;
@@ -280,12 +283,8 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs the spatial-ERI exchange form (n <= 128 or jk_form 1)");
         return PHF_ERR_UNSUPPORTED;
     }
-    if (p.prec == PHF_PREC_OZAKI_I8 && !p.eri) {
-        set_error(PHF_ERR_UNSUPPORTED, "the int8 tensor-core path needs the spatial-ERI exchange form (jk_form 0/1)");
-        return PHF_ERR_UNSUPPORTED;
-    }
-    if (p.prec == PHF_PREC_BF16X3 || p.prec == PHF_PREC_TF32) {
-        set_error(PHF_ERR_UNSUPPORTED, "BF16x3 and TF32 contractions are not built into this library version");
+    if (p.prec != PHF_PREC_FP64 && !p.eri) {
+        set_error(PHF_ERR_UNSUPPORTED, "the tensor-core precisions need the spatial-ERI exchange form (jk_form 0/1)");
         return PHF_ERR_UNSUPPORTED;
     }
     p.nl = d->ngrid[0];
@@ -494,8 +493,8 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         if (p.chol && p.eri) {
             per += 2 * MM + 2 * n2 + p.L;                       // Rho, Gam, Pvec, Jvec, dvec
             if (p.prec == PHF_PREC_FP64) per += 8 * n2;         // Kin, Kvec
-            else per += 4 * n2 + (8 * n2 * p.slices) / sizeof(zc) + 1  // Dk, exchange slices
-                        + (2 * n2 + 2 * (size_t)p.L) * p.slices / sizeof(zc) + 1    // Coulomb slices
+            else per += 4 * n2 + (8 * n2 * oz_slots(p.slices)) / sizeof(zc) + 1  // Dk, exchange slices
+                        + (2 * n2 + 2 * (size_t)p.L) * oz_slots(p.slices) / sizeof(zc) + 1    // Coulomb slices
                         + p.L + n2;                                                // d^T, J pairs
         } else if (p.chol) {
             per += (size_t)p.L * N * N + (size_t)p.L * MN + p.L;
@@ -584,7 +583,7 @@ namespace {
 
 // EK[(i n + k) n^2 + (l n + j)] = sum_L B_L[i][l] B_L[k][j] = (il|kj): the exchange operator
 // K(rho)_ik = sum_{lj} (il|jk) rho_lj as an n^2 x n^2 matrix acting on vec(rho) (built as n^2
-// batched n x n x L products); sliced to int8 for the tensor-core back-end.
+// batched n x n x L products); sliced (int8 digits, BF16 pairs or TF32) for the tensor-core back-end.
 int build_exchange_matrix(PlanImpl &p) {
     const int n = p.n, L = p.L;
     const long long n2 = (long long)n * n;
@@ -594,7 +593,7 @@ int build_exchange_matrix(PlanImpl &p) {
     o.real = 1;
     View Bv = vd(p.Bst, n2, 1, n, 0);
     PHF_TRY(zgemm_strided(n, n, L, n, n, Z1, vd(p.Bst, 1, n2, 0, n), Bv, Z0, o, nullptr, 0));
-    if (p.prec == PHF_PREC_OZAKI_I8) {
+    if (p.prec != PHF_PREC_FP64) {
         const size_t bytes = oz_slice_bytes(oz_pad_rows(n2), n2, p.slices);
         PHF_TRY(p.arena.alloc(&p.EKsl, bytes));
         PHF_CUDA(cudaMemset(p.EKsl, 0, bytes));
@@ -618,7 +617,7 @@ int build_exchange_matrix(PlanImpl &p) {
     if (p.prec == PHF_PREC_FP64) {
         p.EK = EK;  // the FP64 back-end multiplies by it
     } else {
-        p.arena.free_one(EK);  // the int8 back-end only needs its slices
+        p.arena.free_one(EK);  // the tensor-core back-end only needs its slices
         p.EK = nullptr;
     }
     return PHF_OK;
@@ -630,7 +629,7 @@ int build_exchange_matrix(PlanImpl &p) {
 int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     const int M = p.M, N = p.N, n = p.n, L = p.L, b = p.b;
     const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
-    // int8 path with n <= 64: the operand columns are formed and sliced in one kernel, no density in HBM
+    // tensor-core path with n <= 64: the operand columns are formed and sliced in one kernel, no density in HBM
     const bool fused = p.prec != PHF_PREC_FP64 && oz_rho_slice_ok(n);
     if (!fused)
         PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0,
@@ -647,7 +646,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         else
             PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
     }
-    // int8 path: the Coulomb chain runs on a second stream beside the exchange GEMM (independent
+    // tensor-core path: the Coulomb chain runs on a second stream beside the exchange GEMM (independent
     // operands and outputs; its small, latency-bound launches fill the SMs the exchange GEMM's last
     // wave leaves idle).  Joined before Gamma is assembled.  Not while per-launch profiling is on:
     // event times of overlapping kernels would count the shared time twice.

@@ -95,7 +95,12 @@ int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
                           cudaStream_t st);
 
-// ozaki_i8.cu: FP64-accurate GEMM from int8 slices on tcgen05
+// ozaki_i8.cu: FP64-accurate GEMM from int8 slices on tcgen05.  The slice-count argument S is 1..7
+// int8 slices, or one of two floating-point operand formats contracted by the same kernel:
+constexpr int OZ_FMT_BF16X3 = 8;  // BF16 high + low parts, hi*hi + hi*lo + lo*hi, FP32 accumulation
+constexpr int OZ_FMT_TF32 = 9;    // TF32 values, FP32 accumulation
+bool oz_format_ok(int S);
+int oz_slots(int S);  // bytes per operand element in the slice buffers
 long long oz_pad_rows(long long m);
 long long oz_pad_cols(long long n);
 long long oz_pad_k(long long k);

@@ -36,7 +36,7 @@ def _bound_units(A, Bt):
 
 
 @pytest.mark.parametrize("m,n,k", [(128, 64, 64), (200, 150, 333), (256, 192, 1000), (64, 40, 17)])
-@pytest.mark.parametrize("S", [6, 3])
+@pytest.mark.parametrize("S", [7, 6, 5, 3])
 def test_ozaki_dgemm_matches_fp64(m, n, k, S):
     rng = np.random.default_rng(m * 7 + n * 3 + k + S)
     A = rng.normal(size=(m, k)) * 10.0 ** rng.uniform(-3, 3, size=(m, 1))

@@ -174,9 +174,10 @@ int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long
 /* The real GEMM of phf_ozaki_dgemm in each tensor-core precision that plans offer for their J/K
  * contractions, with the same arithmetic: PHF_PREC_OZAKI_I8 with `slices` int8 slices
  * (0 = 5); PHF_PREC_BF16X3: each row of A and column of B scaled by a power of two, split into
- * BF16 high and low parts (about 16 significant bits), hi*hi + hi*lo + lo*hi on the tensor cores
- * with FP32 accumulation (hi*hi and the cross terms in separate accumulators, summed in FP64);
- * PHF_PREC_TF32: TF32 operands (10 fraction bits, round to nearest), FP32 accumulation.  `slices`
+ * BF16 high and low parts (about 16 significant bits), hi*hi + hi*lo + lo*hi on the tensor cores;
+ * PHF_PREC_TF32: TF32 operands (10 fraction bits, round to nearest).  Both accumulate in FP32 over
+ * segments of 512 k-elements whose results are summed in FP64 (the tensor core's FP32 sums round
+ * towards zero, which over long same-sign sums is the dominant error).  `slices`
  * is ignored for the floating-point precisions; PHF_PREC_FP64 is PHF_ERR_ARG.  Device pointers;
  * synchronous on `stream`.  No counterpart in the reference. */
 int phf_tc_dgemm(int m, int n, int k, int precision, int slices, const double *dA, long long lda, const double *dBt,

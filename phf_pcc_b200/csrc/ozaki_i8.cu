@@ -40,8 +40,12 @@
 // The same kernel contracts two floating-point operand formats (slice-count codes OZ_FMT_BF16X3
 // and OZ_FMT_TF32): a row (column) scaled by 2^-ea is held as BF16 high and low parts, or as one
 // TF32 value, in one 128-byte segment per 32-element k-block; the MMAs are kind::f16 (BF16 x BF16)
-// or kind::tf32 with FP32 accumulators in TMEM.  BF16X3 adds hi*hi into one accumulator and the
-// two cross products hi*lo + lo*hi into a second, and the epilogue sums the two in FP64.
+// or kind::tf32 with FP32 accumulators in TMEM.  The k range runs in segments of args.kseg
+// k-blocks that alternate between two FP32 accumulators (TMEM columns 0..127 and 128..255); the
+// epilogue warps add each finished segment into FP64 sums parked in columns 256..511 (high and low
+// words) while the MMAs fill the other accumulator, and store the FP64 total after the last one.
+// The tensor core's FP32 accumulation rounds towards zero, so its error grows with the length of a
+// same-sign sum; FP64 sums of short segments keep it at the level of one segment.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -224,6 +228,7 @@ struct OzArgs {
     int trans;           // write D^T: element (i, j) at D[j * ldd + i]
     long long dz;        // split-k: CTA z covers k-blocks [z kblocks, (z+1) kblocks) and writes D + z dz
     int kb_total;        // k-blocks of this launch over all splits
+    int kseg;            // floating-point formats: k-blocks per FP32 accumulation segment (>= 1)
     int *err;
 };
 
@@ -261,6 +266,7 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
 // or 64-byte (S = 6) rows, or two units (S = 7: group 1 at 128-byte rows).
 constexpr int OZ_UNITS = 14;
 constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
+constexpr int OZ_KSEG = 16;    // floating-point formats: k-blocks (512 k-elements) per FP32 accumulation segment
 
 // Tile width and passes per slice count.  S = 5 runs its five groups g = 2..6 in one pass over
 // 96-column tiles (5 x 96 of the 512 TMEM columns); the others use 128-column tiles and passes of
@@ -311,9 +317,9 @@ __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64
 }
 
 // One k-block of a floating-point format (one 128-byte segment per operand row, +2 in a descriptor
-// = +32 bytes = the next quarter).  TF32: four K = 8 MMAs into acc0.  BF16X3 (quarters 0, 1 = high
-// parts of k 0..15 and 16..31, quarters 2, 3 = low parts): hi*hi into acc0, hi*lo and lo*hi into
-// acc0 + BN.
+// = +32 bytes = the next quarter), all into the accumulator acc0.  TF32: four K = 8 MMAs.  BF16X3
+// (quarters 0, 1 = high parts of k 0..15 and 16..31, quarters 2, 3 = low parts): hi*hi, hi*lo and
+// lo*hi of each half, six K = 16 MMAs.
 template <int S>
 __device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, uint64_t dB, uint32_t acc_in) {
     constexpr int BN = oz_bn(S);
@@ -323,13 +329,12 @@ __device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, u
         for (int q = 0; q < 4; ++q) mma_tf32(acc0, dA + 2 * q, dB + 2 * q, idesc, q > 0 ? 1u : acc_in);
     } else {
         constexpr uint32_t idesc = idesc_bf16<BN>();
-        const uint32_t acc1 = acc0 + BN;
 #pragma unroll
         for (int h = 0; h < 2; ++h) mma_bf16(acc0, dA + 2 * h, dB + 2 * h, idesc, h > 0 ? 1u : acc_in);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) mma_bf16(acc1, dA + 2 * h, dB + 4 + 2 * h, idesc, h > 0 ? 1u : acc_in);
+        for (int h = 0; h < 2; ++h) mma_bf16(acc0, dA + 2 * h, dB + 4 + 2 * h, idesc, 1u);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) mma_bf16(acc1, dA + 4 + 2 * h, dB + 2 * h, idesc, 1u);
+        for (int h = 0; h < 2; ++h) mma_bf16(acc0, dA + 4 + 2 * h, dB + 2 * h, idesc, 1u);
     }
 }
 
@@ -398,6 +403,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(free_bar + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
     double *colscale = reinterpret_cast<double *>(free_bar + 2);  // 2^{eb} / 127 of the tile's columns
+    // floating-point formats: accumulator b holds a finished segment (acc_full[b], one arrival by
+    // the MMA commit) / has been drained by the epilogue (acc_empty[b], 128 arrivals)
+    uint64_t *acc_full = reinterpret_cast<uint64_t *>(colscale + OZ_BN);
+    uint64_t *acc_empty = acc_full + 2;
+    const int kseg = max(1, args.kseg);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // grouped raster: CTAs in launch order sweep the column tiles in groups of OZ_GROUP_M row tiles,
@@ -424,6 +434,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
         mbar_init(pass_bar, 1);
         mbar_init(free_bar, 128);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 128);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA0)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB0)) : "memory");
@@ -491,7 +505,25 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             uint32_t ph = 0;   // parity of its full-barrier phase
             bool ok = true;
             const uint32_t smem_base = smem_u32(smem);
-            for (int p = 0; p < npass && ok; ++p) {
+            if constexpr (oz_float(S)) {  // segments s into accumulator s & 1
+                const int nseg = max(1, (KB + kseg - 1) / kseg);
+                for (int sg = 0; sg < nseg && ok; ++sg) {
+                    const int b = sg & 1;
+                    if (sg >= 2) {  // wait until the epilogue has drained segment sg - 2
+                        if (!mbar_wait(&acc_empty[b], ((sg >> 1) - 1) & 1, args.err, 8)) {
+                            *abort_flag = 1;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    }
+                    const int nkb = max(0, min(kseg, KB - sg * kseg));
+                    ok = mma_pass<S, 0>(tmem_base + (uint32_t)b * BN, nkb, u, ph, smem_base, full_bar, empty_bar,
+                                        args.err);
+                    if (!ok) *abort_flag = 1;
+                    mma_commit(&acc_full[b]);
+                }
+            }
+            for (int p = 0; p < npass && ok && !oz_float(S); ++p) {
                 if (p > 0) {  // accumulators drained by the epilogue
                     if (!mbar_wait(free_bar, (p - 1) & 1, args.err, 8)) {
                         *abort_flag = 1;
@@ -517,7 +549,66 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const double rowscale = row_ok ? ldexp(kUnit, args.ea[row]) : 0.0;
         double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
         const long long cstride = args.trans ? args.ldd : 1;
-        for (int p = 0; p < npass; ++p) {
+        if constexpr (oz_float(S)) {
+            // segment sums: FP32 accumulator -> FP64, added to the parked sums (columns 256 + c 32
+            // high words, 384 + c 32 low words), stored to D after the last segment
+            const int nseg = max(1, (KB + kseg - 1) / kseg);
+            for (int sg = 0; sg < nseg; ++sg) {
+                const int b = sg & 1;
+                const bool ok = mbar_wait(&acc_full[b], (sg >> 1) & 1, args.err, 4);
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (!ok || *abort_flag) break;
+                const bool filled = sg * kseg < KB, last = (sg + 1 == nseg);
+#pragma unroll 1
+                for (int c = 0; c < BN / 32; ++c) {
+                    double acc[32];
+                    uint32_t v[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                    if (filled) {
+                        tmem_ld32(lane_base + (uint32_t)b * BN + c * 32, v);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] = (double)__uint_as_float(v[j]);
+                    }
+                    if (sg > 0) {
+                        uint32_t hi[32], lo[32];
+                        tmem_ld32(lane_base + 256 + c * 32, hi);
+                        tmem_ld32(lane_base + 384 + c * 32, lo);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] += __hiloint2double((int)hi[j], (int)lo[j]);
+                    }
+                    if (!last) {
+                        uint32_t hi[32], lo[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            hi[j] = (uint32_t)__double2hiint(acc[j]);
+                            lo[j] = (uint32_t)__double2loint(acc[j]);
+                        }
+                        tmem_st32(lane_base + 256 + c * 32, hi);
+                        tmem_st32(lane_base + 384 + c * 32, lo);
+                    } else if (row_ok) {
+                        double old[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = n0 + c * 32 + j;
+                            old[j] = (args.accumulate && col < args.n) ? drow[(long long)col * cstride] : 0.0;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = n0 + c * 32 + j;
+                            if (col < args.n) {
+                                const double val = acc[j] * rowscale * colscale[c * 32 + j];
+                                drow[(long long)col * cstride] = args.accumulate ? old[j] + val : val;
+                            }
+                        }
+                    }
+                }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(&acc_empty[b]);  // accumulator b may take segment sg + 2
+            }
+        }
+        for (int p = 0; p < npass && !oz_float(S); ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!ok || *abort_flag) break;
@@ -529,24 +620,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 double acc[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-                if constexpr (oz_float(S)) {
-                    // FP32 accumulators (BF16X3: the cross-product sum, then hi*hi), summed in FP64
 #pragma unroll 1
-                    for (int g = (S == OZ_FMT_BF16X3 ? 1 : 0); g >= 0 && KB > 0; --g) {
-                        uint32_t v[32];
-                        tmem_ld32(acc0 + (uint32_t)g * BN + c * 32, v);
+                for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
+                    uint32_t v[32];
+                    tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
+                    const double sc = kPow254[g - 2];
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] += (double)__uint_as_float(v[j]);
-                    }
-                } else {
-#pragma unroll 1
-                    for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
-                        uint32_t v[32];
-                        tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
-                        const double sc = kPow254[g - 2];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
-                    }
+                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
                 }
                 if (keep && p == 1) {  // add the first pass's partial sums
                     uint32_t hi[32], lo[32];
@@ -1122,8 +1202,9 @@ size_t oz_slice_bytes(long long rows_pad, long long k, int S) {
     return (size_t)(OZ_GP + oz_g1_width(S)) * (size_t)rows_pad * (size_t)oz_pad_k(k);
 }
 
-// the unit ring, 2 OZ_UNITS + 2 mbarriers, the TMEM address and abort flag, the column scales
-size_t oz_smem_bytes() { return (size_t)OZ_UNITS * OZ_UNIT + (2 * OZ_UNITS + 2) * 8 + 8 + OZ_BN * 8; }
+// the unit ring, 2 OZ_UNITS + 2 mbarriers, the TMEM address and abort flag, the column scales, the
+// four accumulator mbarriers of the floating-point formats
+size_t oz_smem_bytes() { return (size_t)OZ_UNITS * OZ_UNIT + (2 * OZ_UNITS + 2) * 8 + 8 + OZ_BN * 8 + 4 * 8; }
 
 // D (m x n, ldd) (+)= A_slices (S x mpad x kpad) * B_slices (S x npad x kpad)^T with exponents ea, eb.
 // k is split into passes short enough for exact int32 group sums; later passes add into D.
@@ -1188,6 +1269,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kb0 = 0;
     a.kblocks = (int)((kb_total + nsplit - 1) / nsplit);
     a.kb_total = (int)kb_total;
+    a.kseg = OZ_KSEG;
     a.S = S;
     a.ea = ea;
     a.eb = eb;
@@ -1255,6 +1337,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.trans = trans;
         a.dz = 0;
         a.kb_total = a.kblocks;
+        a.kseg = OZ_KSEG;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);

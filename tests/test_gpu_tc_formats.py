@@ -64,6 +64,20 @@ def test_tc_dgemm_long_k_against_fp64(fmt, rel):
     assert emu.max() <= 1.0, emu.max()
 
 
+@pytest.mark.parametrize("fmt,rel", [("bf16x3", 1e-5), ("tf32", 3e-5)])
+def test_tc_dgemm_same_sign_sums_keep_the_error_of_one_segment(fmt, rel):
+    """Same-sign data with k = 16384 (the exchange GEMM's k at n = 128): the tensor core's FP32
+    accumulation rounds towards zero, so one FP32 sum over the whole k range is off by ~1e-4 of the
+    result (7.5e-5 for BF16x3, 1.2e-4 for TF32, measured); FP64 sums of 512-element segments keep
+    the accumulation error at the level of one segment."""
+    rng = np.random.default_rng(13)
+    A = np.abs(rng.normal(size=(128, 16384))) + 0.5
+    Bt = np.abs(rng.normal(size=(96, 16384))) + 0.5
+    D = _tc_dgemm(A, Bt, fmt)
+    acc = np.abs(D - tf.emulate(A, Bt, fmt)).max() / np.abs(A @ Bt.T).max()
+    assert acc <= rel, acc
+
+
 def test_tc_dgemm_int8_is_ozaki_dgemm():
     import torch
 

@@ -486,10 +486,8 @@ def run_ours(args):
             if i > 0:
                 e2e_vals.append(p.grid.npoints / (t1 - t0))
         planh.close()
-        nvar = 4 if kw["cmplxconj"] == 2 else 1
-        nci = int(kw["nci"])
-        # per call the plan uploads bra and ket per conjugation variant and newMO per slot
-        h2d = (2 * nvar + nci * nci) * p.M * p.N * 16
+        # per call the plan uploads newMO and its conjugate (the AO vectors are formed on the device)
+        h2d = 2 * p.M * p.N * 16
         d2h = sum(x.nbytes for x in out)
         for i in range(1 + args.e2e_steps):
             torch.cuda.synchronize()
@@ -580,7 +578,8 @@ def run_ours(args):
 def run_batch(args):
     """Configuration 4: independent instances of uneven size evaluated together (phf_eval_batch:
     one CUDA graph over concurrent branches).  value = grid points of all instances / device time
-    of one batch evaluation; the FP64 form is the same batch with FP64 plans."""
+    of one batch evaluation; the FP64 and split-BF16 forms are the same batch with FP64 and BF16x3
+    plans."""
     import torch
 
     from phf_pcc_b200 import _lib, api, synth
@@ -683,6 +682,19 @@ def run_batch(args):
         dG = max(float((a[1] - b[1]).abs().max().item()) for a, b in zip(res, res64))
         fp64 = {"own_kernels": {"value": pts / (ms64 * 1e-3), "ms_per_step": ms64, "speedup": ms64 / step_ms,
                                 "max_abs_dE_vs_fp64": dE, "max_abs_dgrad_vs_fp64": dG, "meets_1e-8_Eh": dE <= 1e-8}}
+        # the split-BF16 form of the same batch (three BF16 products, FP32 accumulation, FP64 segment sums)
+        if args.precision != "bf16x3":
+            plansb = make("bf16x3")
+            msb, outsb, _ = time_batch(plansb, max(1, min(args.steps, 3)), 1)
+            resb = energies(outsb)
+            for pl in plansb:
+                pl.close()
+            torch.cuda.empty_cache()
+            fp64["split_bf16"] = {
+                "value": pts / (msb * 1e-3), "ms_per_step": msb, "speedup_vs_fp64": ms64 / msb,
+                "max_abs_dE_vs_fp64": max(abs(a[0] - b[0]) for a, b in zip(resb, res64)),
+                "max_rel_dE_vs_fp64": max(abs(a[0] - b[0]) / abs(b[0]) for a, b in zip(resb, res64)),
+                "max_abs_dgrad_vs_fp64": max(float((a[1] - b[1]).abs().max().item()) for a, b in zip(resb, res64))}
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -691,7 +703,7 @@ def run_batch(args):
         peaks = _peaks()
         jk_ms = prof[0][0]
         slices = args.slices or 5
-        ops = sum(int8_ops_per_point(p, slices) * p.grid.npoints for p in probs)
+        ops = sum(tc_ops_per_point(p, args.precision, slices) * p.grid.npoints for p in probs)
         bf16 = peaks.get("bf16_tflops")
         peak = 2.0 * bf16 if bf16 else None
         achieved = ops / (jk_ms * 1e-3) / 1e12 if args.precision != "fp64" else None

@@ -166,8 +166,10 @@ class Plan:
     """A reusable evaluation plan (Hamiltonian, grid and workspace resident on the GPU).
 
     Cholesky form: pass ``h`` (n, n) and ``B`` (L, n, n); dense form: ``hone`` and
-    ``htwo``.  Grid arguments as buildhsg.  ``precision``: "fp64" or "ozaki_i8" (FP64-accurate
-    int8 tensor-core slices, ``slices`` per operand, default 5); ``jk_form``: "auto", "eri"
+    ``htwo``.  Grid arguments as buildhsg.  ``precision`` of the J/K contractions: "fp64",
+    "ozaki_i8" (FP64-accurate int8 tensor-core slices, ``slices`` per operand, default 5),
+    "bf16x3" (split BF16, three products) or "tf32" (both FP32-accumulated in 512-element segments
+    summed in FP64; about 1e-6 relative, far from FP64); ``jk_form``: "auto", "eri"
     (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"; ``gradient``: "reference"
     (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the ket-side term;
     used by autograd)."""

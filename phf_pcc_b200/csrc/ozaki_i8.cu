@@ -877,7 +877,10 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
 // with the tensor-core MMA sequence of zgemm_kernel (m ascending in steps of four), so every
 // column, its exponent and its slices are those of the density GEMM followed by slice_rho_cols /
 // slice_p_cols.
-constexpr int RS_NT = 512, RS_MC = 16, RS_P = 65;  // threads, m-chunk, padded row pitch (complex)
+// threads, m-chunk, padded row pitch (complex).  A 16-byte fragment load is served eight lanes at a
+// time; lanes (fk, fr) of one such group read row kk + fk, column c + fr, so with a pitch of 2 mod 8
+// (complex) the eight land on distinct bank quadruples.
+constexpr int RS_NT = 512, RS_MC = 16, RS_P = 66;
 constexpr int RS_WI = 2;  // 8-row fragments per warp: 16 warps of 16 x 16 cover the 64 x 64 blocks
 
 // operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
@@ -1058,10 +1061,20 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
             const bool isK = col < 4;
             const SliceScale sc = slice_scale(ex[col], S);
             const double *src = stage + h * nn;
+            const bool pairs = (reinterpret_cast<uintptr_t>(src) & 15u) == 0;  // 16-byte loads possible
             for (long long e0 = 4LL * tid; e0 < kpad; e0 += 4LL * RS_NT) {
                 double x[4];
+                if (pairs && e0 + 3 < nn) {
+                    const double2 a = *reinterpret_cast<const double2 *>(src + e0);
+                    const double2 b = *reinterpret_cast<const double2 *>(src + e0 + 2);
+                    x[0] = a.x;
+                    x[1] = a.y;
+                    x[2] = b.x;
+                    x[3] = b.y;
+                } else {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) x[u] = (e0 + u < nn) ? src[e0 + u] : 0.0;
+                    for (int u = 0; u < 4; ++u) x[u] = (e0 + u < nn) ? src[e0 + u] : 0.0;
+                }
                 slice_pack4<S>(x, sc, isK ? outK : outP, cidx[col], isK ? npadK : npadP, kpad >> 5, e0);
             }
         }

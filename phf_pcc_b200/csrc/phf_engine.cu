@@ -464,6 +464,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(p.arena.alloc(&p.ket, MN));
     PHF_TRY(p.arena.alloc(&p.kety, MN));
     PHF_TRY(p.arena.alloc(&p.newmo, MN));
+    PHF_TRY(p.arena.alloc(&p.newmoc, MN));
     PHF_TRY(p.arena.alloc(&p.T1, (size_t)p.npg * MN));
     PHF_TRY(p.arena.alloc(&p.T2, (size_t)p.ny * p.npg * MN));
     if (p.chol) PHF_TRY(p.arena.alloc(&p.V, (size_t)p.L * MN));
@@ -475,7 +476,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(p.arena.alloc(&p.accHS, 2 * nslot));
     PHF_TRY(p.arena.alloc(&p.compHS, 2 * nslot));
     PHF_TRY(p.arena.alloc(&p.tmpG, MN));
-    PHF_TRY(p.arena.alloc(&p.outMM, MM));
+    PHF_TRY(p.arena.alloc(&p.outMM, 2 * nslot * MM));  // every slot's Gradmat and Rdmmat block
     if (p.exact) {
         PHF_TRY(p.arena.alloc(&p.Hb, MN));
         PHF_TRY(p.arena.alloc(&p.accKG, nslot * MN));
@@ -875,11 +876,8 @@ int fold_acc(PlanImpl &p, cudaStream_t st) {
     return PHF_OK;
 }
 
-int read_flag(PlanImpl &p, cudaStream_t st) {
-    int flag = 0, oz = 0;
-    PHF_CUDA(cudaMemcpyAsync(&flag, p.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (p.ozerr) PHF_CUDA(cudaMemcpyAsync(&oz, p.ozerr, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PHF_CUDA(cudaStreamSynchronize(st));
+// Status of an evaluation from its flag word and the tensor-core GEMM error word (host copies).
+int flag_status(int flag, int oz) {
     if (oz) {
         set_error(PHF_ERR_CUDA, "tensor-core GEMM pipeline wait timed out (code " + std::to_string(oz) + ")");
         return PHF_ERR_CUDA;
@@ -893,6 +891,22 @@ int read_flag(PlanImpl &p, cudaStream_t st) {
         return PHF_ERR_NONFINITE;
     }
     return PHF_OK;
+}
+
+// Queues the device-to-host copies of the two status words on st (read after a synchronisation).
+int enqueue_flags(PlanImpl &p, int *flag, int *oz, cudaStream_t st) {
+    *flag = 0;
+    *oz = 0;
+    PHF_CUDA(cudaMemcpyAsync(flag, p.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (p.ozerr) PHF_CUDA(cudaMemcpyAsync(oz, p.ozerr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return PHF_OK;
+}
+
+int read_flag(PlanImpl &p, cudaStream_t st) {
+    int flag = 0, oz = 0;
+    PHF_TRY(enqueue_flags(p, &flag, &oz, st));
+    PHF_CUDA(cudaStreamSynchronize(st));
+    return flag_status(flag, oz);
 }
 
 // Hermiticity check of PHFTools.f90:195-200 on host copies
@@ -968,50 +982,38 @@ int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_comp
             if (p.cmplxconj == 0) v = cd(v.real(), 0.0);
             mo[(size_t)(N + a) * N + i] = v;
         }
-    auto to_work = [&](const std::vector<cd> &m_mo, std::vector<cd> &bra_w, std::vector<cd> &kety) {
-        // AO vector Ref m (reference order) and its working-order copy
-        std::vector<cd> ao(MN, cd(0, 0));
-        for (int r = 0; r < M; ++r)
-            for (int k = 0; k < M; ++k) {
-                cd rv = p.ref_host[(size_t)r * M + k];
-                if (rv == cd(0, 0)) continue;
-                for (int j = 0; j < N; ++j) ao[(size_t)r * N + j] += rv * m_mo[(size_t)k * N + j];
-            }
-        bra_w.assign(MN, cd(0, 0));
-        if (p.chol) {
-            for (int r = 0; r < M; ++r)
-                for (int j = 0; j < N; ++j) bra_w[(size_t)r * N + j] = ao[(size_t)p.perm[r] * N + j];
-            kety = bra_w;
-        } else {
-            bra_w = m_mo;
-            kety = ao;
-        }
-    };
     std::vector<cd> moc(MN);
     for (size_t i = 0; i < MN; ++i) moc[i] = std::conj(mo[i]);
-    std::vector<cd> bw0, ky0, bw1, ky1;
-    to_work(mo, bw0, ky0);
-    to_work(moc, bw1, ky1);
+    PHF_TRY(upload(p.newmo, mo));
+    PHF_TRY(upload(p.newmoc, moc));
 
     PHF_TRY(zero_acc(p, st));
     const int nvar = p.cmplxconj == 2 ? 4 : 1;
-    // variants (bra, ket): 0 (C, C), 1 (C, C*), 2 (C*, C*), 3 (C*, C)   -- RDM / RDMConj calls of :91-107
+    // variants (bra, ket): 0 (C, C), 1 (C, C*), 2 (C*, C*), 3 (C*, C)   -- RDM / RDMConj calls of :91-107.
+    // The AO vectors Ref m are formed on the device (Refw holds Ref's rows in working order): in the
+    // Cholesky form bra and ket are both Ref m in working order; in the dense form the bra stays in
+    // the MO basis and the ket is Ref m in the reference order.
     for (int v = 0; v < nvar; ++v) {
         const bool cb = (v >= 2), ck = (v == 1 || v == 2);
-        PHF_TRY(upload(p.bra, cb ? bw1 : bw0));
-        PHF_TRY(upload(p.kety, ck ? ky1 : ky0));
+        const zc *mb = cb ? p.newmoc : p.newmo, *mk = ck ? p.newmoc : p.newmo;
+        if (p.chol)
+            PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(mb, N, 1), Z0, vo(p.bra, N, 1), nullptr, st));
+        else
+            PHF_CUDA(cudaMemcpyAsync(p.bra, mb, MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+        PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(mk, N, 1), Z0, vo(p.kety, N, 1), nullptr, st));
         PHF_TRY(launch_captured(p, v, st, [&](cudaStream_t s) -> int { return run_variant(p, v, s); }));
     }
     PHF_TRY(fold_acc(p, st));
-    PHF_TRY(read_flag(p, st));
 
-    // Gradmat_a = T Yg_a bra_a^H, Rdmmat likewise (T = Ref^H in the Cholesky form)
+    // Gradmat_a = T Yg_a bra_a^H, Rdmmat likewise (T = Ref^H in the Cholesky form); every block is
+    // formed on the device first, then all blocks and H, S come back in one synchronisation
     const int nci = p.nci, nb = p.nb;
     const long long ns = (long long)nci * nci;
+    const size_t MMs = (size_t)M * M;
     for (int a = 0; a < nci * nci; ++a) {
         const int m = a % nci;
         const bool conj_bra = (p.cmplxconj == 2) && (m >= nb);
-        PHF_TRY(upload(p.newmo, conj_bra ? moc : mo));
+        const zc *nmo = conj_bra ? p.newmoc : p.newmo;
         for (int which = 0; which < 2; ++which) {
             zc *acc = (which == 0 ? p.accG : p.accR) + (size_t)a * MN;
             const zc *src = acc;
@@ -1020,23 +1022,29 @@ int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_comp
                                       nullptr, st));
                 src = p.tmpG;
             }
-            zc *outp = p.outMM;
-            PHF_TRY(zgemm_strided(M, M, N, 1, 1, Z1, vz(src, N, 1), vz(p.newmo, 1, N, 0, 0, 1), Z0, vo(outp, 1, M),
+            // the M x M block in column-major order
+            zc *outp = p.outMM + (2 * (size_t)a + which) * MMs;
+            PHF_TRY(zgemm_strided(M, M, N, 1, 1, Z1, vz(src, N, 1), vz(nmo, 1, N, 0, 0, 1), Z0, vo(outp, 1, M),
                                   nullptr, st));
-            // outp holds the M x M block in column-major order; scatter into the (nci, nci, M, M) array on the host
-            std::vector<cd> blk((size_t)M * M);
-            PHF_CUDA(cudaMemcpyAsync(blk.data(), outp, blk.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
-            PHF_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+    std::vector<cd> blocks(2 * (size_t)ns * MMs), hs(2 * (size_t)ns);
+    PHF_CUDA(cudaMemcpyAsync(blocks.data(), p.outMM, blocks.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
+    PHF_CUDA(cudaMemcpyAsync(hs.data(), p.accHS, hs.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
+    int flag = 0, oz = 0;
+    PHF_TRY(enqueue_flags(p, &flag, &oz, st));
+    PHF_CUDA(cudaStreamSynchronize(st));
+    PHF_TRY(flag_status(flag, oz));  // on failure the host outputs are left untouched
+    // scatter into the (nci, nci, M, M) Fortran-ordered arrays
+    for (long long a = 0; a < ns; ++a)
+        for (int which = 0; which < 2; ++which) {
+            const cd *blk = blocks.data() + (2 * (size_t)a + which) * MMs;
             phf_complex *dst = which == 0 ? gradmat : rdmmat;
-            for (size_t ij = 0; ij < (size_t)M * M; ++ij) {
+            for (size_t ij = 0; ij < MMs; ++ij) {
                 dst[(size_t)a + (size_t)ns * ij].re = blk[ij].real();
                 dst[(size_t)a + (size_t)ns * ij].im = blk[ij].imag();
             }
         }
-    }
-    std::vector<cd> hs(2 * (size_t)ns);
-    PHF_CUDA(cudaMemcpyAsync(hs.data(), p.accHS, hs.size() * sizeof(zc), cudaMemcpyDeviceToHost, st));
-    PHF_CUDA(cudaStreamSynchronize(st));
     std::vector<cd> H(ns), S(ns);
     for (int a = 0; a < ns; ++a) {
         H[a] = hs[2 * a];

@@ -164,7 +164,7 @@ struct PlanImpl {
     double *h = nullptr, *Bst = nullptr;               // Cholesky form
     zc *H1 = nullptr, *H2r = nullptr;                  // dense form
     // per evaluation
-    zc *bra = nullptr, *ket = nullptr, *kety = nullptr, *newmo = nullptr;
+    zc *bra = nullptr, *ket = nullptr, *kety = nullptr, *newmo = nullptr, *newmoc = nullptr;
     zc *T1 = nullptr, *T2 = nullptr, *V = nullptr;
     // chunk workspace
     int b = 0;

@@ -261,9 +261,10 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
     return rows_pad * KB * 128 + (row * KB + kb) * (32LL * oz_g1_width(S)) + ((long long)(t - OZ_GP) << 5) + kk;
 }
 
-// Shared-memory ring of OZ_UNITS units of 16 KB: a k-block takes two units (A and B tiles of slice
-// group 0), plus, in a pass that uses group 1, one unit holding its A and B boxes at 32-byte (S = 5)
-// or 64-byte (S = 6) rows, or two units (S = 7: group 1 at 128-byte rows).
+// Shared-memory ring of OZ_UNITS units of 16 KB for the two-pass slice counts S = 6, 7: a k-block
+// takes two units (A and B tiles of slice group 0), plus, in the second pass, one unit holding group
+// 1's A and B boxes at 64-byte rows (S = 6) or two units (S = 7: group 1 at 128-byte rows).  The
+// single-pass formats use the same bytes as a ring of packed k-block stages (oz_stage_bytes).
 constexpr int OZ_UNITS = 14;
 constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
 constexpr int OZ_KSEG = 16;    // floating-point formats: k-blocks (512 k-elements) per FP32 accumulation segment
@@ -294,6 +295,19 @@ __host__ __device__ constexpr uint32_t oz_unit_bytes(int S, int j) {
 __constant__ double kPow254[7] = {1.0, 0.003937007874015748, 1.5500031000062e-05, 6.102374409473229e-08,
                                   2.40250961002883e-10, 9.458699252082008e-13, 3.723897343339373e-15};
 constexpr uint32_t OZ_UNIT = 16384;
+
+// Single-pass formats (S <= 5 and the floating-point formats) pack all boxes of one k-block into one
+// stage of the ring instead of whole 16 KB units: A (BM x 128 B) at 0, B (BN x 128 B) at BM 128 and,
+// for S = 5, the fifth slice's A (BM x 32 B) and B (BN x 32 B) behind them.  For S = 5 that is 35 KB
+// per k-block (6 stages in flight instead of 4.7 k-blocks of three units); the ring's depth, not its
+// bandwidth, is what keeps the MMAs fed.
+__host__ __device__ constexpr bool oz_staged(int S) { return oz_npass(S) == 1; }
+__host__ __device__ constexpr uint32_t oz_stage_bytes(int S) {
+    return (OZ_BM + (uint32_t)oz_bn(S)) * 128u + (oz_g1_width(S) == 1 ? (OZ_BM + (uint32_t)oz_bn(S)) * 32u : 0u);
+}
+// stage footprint in the ring, a multiple of 1024 bytes (the SWIZZLE_128B atom)
+__host__ __device__ constexpr uint32_t oz_stage_pitch(int S) { return (oz_stage_bytes(S) + 1023u) / 1024u * 1024u; }
+__host__ __device__ constexpr int oz_stages(int S) { return (int)((OZ_UNITS * OZ_UNIT) / oz_stage_pitch(S)); }
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
 // so that each descriptor is a tile's base descriptor plus a constant (+2 per 32 bytes): the
@@ -338,44 +352,67 @@ __device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, u
     }
 }
 
-// The MMA issuer's k-block loop of pass P (u, ph: next ring unit and its full-barrier parity).
+// The MMA issuer's k-block loop of pass P (u, ph: next ring unit -- or stage, for the single-pass
+// formats -- and its full-barrier parity).
 template <int S, int P>
 __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
                                          uint64_t *full_bar, uint64_t *empty_bar, int *err) {
-    constexpr int NU = oz_units(S, P);
-    for (int kb = 0; kb < KB; ++kb) {
-        int us[NU];
-#pragma unroll
-        for (int j = 0; j < NU; ++j) {
-            us[j] = u;
+    if constexpr (oz_staged(S)) {
+        constexpr int NS = oz_stages(S), BN = oz_bn(S);
+        constexpr uint32_t PITCH = oz_stage_pitch(S);
+        for (int kb = 0; kb < KB; ++kb) {
             if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
-            if (++u == OZ_UNITS) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = smem_base + (uint32_t)u * PITCH;
+            const uint64_t dA0 = sdesc_sw128(base);
+            const uint64_t dB0 = sdesc_sw128(base + OZ_BM * 128);
+            if constexpr (oz_float(S)) {
+                issue_kblock_float<S>(acc0, dA0, dB0, kb > 0 ? 1u : 0u);
+            } else {
+                uint64_t dA1 = 0, dB1 = 0;
+                if constexpr (oz_g1_width(S) == 1) {
+                    dA1 = sdesc_sw32(base + (OZ_BM + BN) * 128);
+                    dB1 = sdesc_sw32(base + (OZ_BM + BN) * 128 + OZ_BM * 32);
+                }
+                issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
+            }
+            mma_commit(&empty_bar[u]);  // the stage is reusable once these MMAs have read it
+            if (++u == NS) {
                 u = 0;
                 ph ^= 1u;
             }
         }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint64_t dA0 = sdesc_sw128(smem_base + (uint32_t)us[0] * OZ_UNIT);
-        const uint64_t dB0 = sdesc_sw128(smem_base + (uint32_t)us[1] * OZ_UNIT);
-        uint64_t dA1 = 0, dB1 = 0;
-        if constexpr (NU == 3 && oz_g1_width(S) == 1) {
-            dA1 = sdesc_sw32(smem_base + (uint32_t)us[2] * OZ_UNIT);
-            dB1 = sdesc_sw32(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 32);
-        } else if constexpr (NU == 3) {
-            dA1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT);
-            dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 64);
-        } else if constexpr (NU == 4) {
-            dA1 = sdesc_sw128(smem_base + (uint32_t)us[2] * OZ_UNIT);
-            dB1 = sdesc_sw128(smem_base + (uint32_t)us[3] * OZ_UNIT);
-        }
-        if constexpr (oz_float(S))
-            issue_kblock_float<S>(acc0, dA0, dB0, kb > 0 ? 1u : 0u);
-        else
+        return true;
+    } else {
+        constexpr int NU = oz_units(S, P);
+        for (int kb = 0; kb < KB; ++kb) {
+            int us[NU];
+#pragma unroll
+            for (int j = 0; j < NU; ++j) {
+                us[j] = u;
+                if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
+                if (++u == OZ_UNITS) {
+                    u = 0;
+                    ph ^= 1u;
+                }
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t dA0 = sdesc_sw128(smem_base + (uint32_t)us[0] * OZ_UNIT);
+            const uint64_t dB0 = sdesc_sw128(smem_base + (uint32_t)us[1] * OZ_UNIT);
+            uint64_t dA1 = 0, dB1 = 0;
+            if constexpr (NU == 3) {  // S = 6: group 1 at 64-byte rows in one unit
+                dA1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT);
+                dB1 = sdesc_sw64(smem_base + (uint32_t)us[2] * OZ_UNIT + OZ_BM * 64);
+            } else if constexpr (NU == 4) {
+                dA1 = sdesc_sw128(smem_base + (uint32_t)us[2] * OZ_UNIT);
+                dB1 = sdesc_sw128(smem_base + (uint32_t)us[3] * OZ_UNIT);
+            }
             issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
 #pragma unroll
-        for (int j = 0; j < NU; ++j) mma_commit(&empty_bar[us[j]]);  // units reusable once these MMAs read them
+            for (int j = 0; j < NU; ++j) mma_commit(&empty_bar[us[j]]);  // units reusable once these MMAs read them
+        }
+        return true;
     }
-    return true;
 }
 
 template <int S>
@@ -460,7 +497,33 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {  // TMA producer: unit sequence = (pass, k-block, tile)
+        if (lane == 0 && oz_staged(S)) {  // TMA producer, one stage per k-block
+            constexpr int NS = oz_stages(S);
+            constexpr uint32_t PITCH = oz_stage_pitch(S), BYTES = oz_stage_bytes(S);
+            int sg = 0;           // next stage
+            uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
+            bool wrapped = false;
+            for (int kb = 0; kb < KB && !*abort_flag; ++kb) {
+                const int kbg = args.kb0 + kz0 + kb;
+                if (wrapped && !mbar_wait(&empty_bar[sg], eph, args.err, 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                unsigned char *dst = smem + (size_t)sg * PITCH;
+                mbar_arrive_expect_tx(&full_bar[sg], BYTES);
+                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, m0);
+                tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
+                if constexpr (W1 == 1) {
+                    tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, m0);
+                    tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
+                }
+                if (++sg == NS) {
+                    sg = 0;
+                    if (wrapped) eph ^= 1u;
+                    wrapped = true;
+                }
+            }
+        } else if (lane == 0) {  // TMA producer: unit sequence = (pass, k-block, tile)
             int u = 0;            // next unit
             uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
             bool wrapped = false;

@@ -22,9 +22,11 @@
 //
 // Kernel shape (one CTA per output tile, 6 warps); in launch order the CTAs sweep the column
 // tiles in groups of eight row tiles, so that the A and B tiles in use fit in L2 together:
-//   warp 0      TMA producer into a ring of fourteen 16 KB units (full/empty mbarrier per unit):
-//               per 32-element k-block the A and B boxes of group 0 (a unit each) and, in a pass
-//               that uses group 1, its A and B boxes (one unit for S = 5, 6, two for S = 7)
+//   warp 0      TMA producer into a 224 KB shared-memory ring (full/empty mbarrier per slot): for
+//               the single-pass formats (S <= 5, BF16X3, TF32) one packed stage per 32-element
+//               k-block holding its A and B boxes (35 KB for S = 5, six stages); for S = 6, 7
+//               fourteen 16 KB units, a k-block taking the A and B boxes of group 0 (a unit
+//               each) and, in the second pass, group 1's boxes (one unit for S = 6, two for S = 7)
 //   warp 1      TMEM allocation (512 columns) and the single-thread tcgen05.mma issuer.  S = 5
 //               runs all five groups g = 2..6 in one pass over 128 x 96 tiles (five int32
 //               accumulators, 480 columns); otherwise the tile is 128 x 128 and the groups run in

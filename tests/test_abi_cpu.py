@@ -60,3 +60,24 @@ def test_shim_checks_shapes_before_calling_the_library():
     with pytest.raises(ValueError):  # wrong z shape
         phftools.buildhsg(np.eye(M), np.zeros((M, M, M, M)), np.eye(M), np.zeros((M, N)), [1, 1], 1, 1, 1, N,
                           eye, eye, eye, np.ones((1, 1)), np.ones((1, 1, 1)), [0.0], [0.0], [0.0], 0, 1, 0)
+
+
+def test_tensor_core_gemm_entries_validate_arguments_before_any_device_call():
+    """phf_tc_dgemm and phf_ozaki_dgemm reject bad precisions, slice counts and sizes with
+    PHF_ERR_ARG before touching device memory (the pointers here are never dereferenced)."""
+    import ctypes
+
+    lib = _lib.load()
+    p = ctypes.c_void_p(8)
+    null = ctypes.c_void_p(0)
+    # precision FP64 (0) and unknown (7) are not tensor-core precisions
+    for prec in (0, 7):
+        assert lib.phf_tc_dgemm(8, 8, 8, prec, 0, p, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+    # int8 slice counts outside 0..7
+    for slices in (-1, 8):
+        assert lib.phf_tc_dgemm(8, 8, 8, 1, slices, p, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_ozaki_dgemm(8, 8, 8, 0, p, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+    # leading dimensions below the row length, empty sizes, null operands
+    assert lib.phf_tc_dgemm(8, 8, 8, 2, 0, p, 4, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_tc_dgemm(0, 8, 8, 3, 0, p, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_tc_dgemm(8, 8, 8, 2, 0, null, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG

@@ -332,6 +332,28 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(rot(d->r1, p.nl, &p.R1));
     PHF_TRY(rot(d->r2, p.ny, &p.R2));
     PHF_TRY(rot(d->rpg, p.npg, &p.Rpg));
+    // Cholesky forms: a spin rotation R1 is block diagonal in the interleaved order (one 2 x 2 block
+    // per spatial orbital); when every R1[il] is exactly that, Y = R1 T2 needs two terms per element
+    // instead of an M x M product (the dropped terms are exact zeros)
+    if (p.chol) {
+        std::vector<cd> blocks((size_t)p.nl * p.n * 4);
+        bool spin_blocks = true;
+        for (int g = 0; g < p.nl && spin_blocks; ++g)
+            for (int i = 0; i < M && spin_blocks; ++i)
+                for (int j = 0; j < M; ++j) {
+                    const cd v = fz(d->r1, (size_t)g + (size_t)p.nl * ((size_t)p.perm[i] + (size_t)M * p.perm[j]));
+                    if ((i >> 1) == (j >> 1)) {
+                        blocks[((size_t)g * p.n + (i >> 1)) * 4 + 2 * (i & 1) + (j & 1)] = v;
+                    } else if (v != cd(0, 0)) {
+                        spin_blocks = false;
+                        break;
+                    }
+                }
+        if (spin_blocks) {
+            PHF_TRY(p.arena.alloc(&p.R1b, blocks.size()));
+            PHF_TRY(upload(p.R1b, blocks));
+        }
+    }
 
     // Ref (row-major, reference order kept on the host; rows in working order on the device)
     p.ref_host.resize(MM);
@@ -771,7 +793,9 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
         // Y_w = R1[il] T2[iy, ig]: one (M x M) x (M x ny npg N) product per Lebedev point when the
         // chunk holds whole blocks of ny npg points, else per point
         const int blk = p.ny * p.npg;
-        if (w0 % blk == 0 && bc % blk == 0)
+        if (p.R1b)
+            PHF_TRY(launch_spin_block_y(n, N, bc, w0, blk, p.R1b, p.T2, ld2, p.Ys, ld, st));
+        else if (w0 % blk == 0 && bc % blk == 0)
             PHF_TRY(zgemm_strided(M, (int)ld2, M, bc / blk, 1, Z1, vz(p.R1 + (size_t)(w0 / blk) * MM, M, 1, MM),
                                   vz(p.T2, ld2, 1), Z0, vo(p.Ys, ld, 1, ld2), nullptr, st));
         else

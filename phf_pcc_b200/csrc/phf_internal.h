@@ -71,6 +71,8 @@ int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cud
 int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale,
                       cudaStream_t st, const zc *add = nullptr);
 int launch_add_inplace(int M, int N, int b, const zc *A, zc *G, long long ldX, cudaStream_t st);
+int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, const zc *T2, long long ld2, zc *Ys,
+                        long long ld, cudaStream_t st);
 int launch_epilogue(int M, int N, int b, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
                     const zc *e2, zc *scal, cudaStream_t st);
 size_t accumulate_scratch_bytes(int nslot, int M, int N, int b);
@@ -156,6 +158,7 @@ struct PlanImpl {
     Arena arena;
     // persistent device data
     zc *R1 = nullptr, *R2 = nullptr, *Rpg = nullptr;  // working order, row-major
+    zc *R1b = nullptr;  // Cholesky forms: R1's 2 x 2 spin blocks when R1 has no other nonzeros (nl x n x 4)
     zc *Refw = nullptr;                                // Ref with rows in working order, row-major
     zc *Wt = nullptr;                                  // nb^2 x nomega
     long long *offs = nullptr;                         // 3 * nomega

@@ -327,6 +327,26 @@ __global__ void average_kernel(long long n, const zc *a, const zc *b, zc *out) {
         out[i] = 0.5 * (a[i] + b[i]);
 }
 
+// Y_w = R1[il] T2[:, rem] for a spin rotation R1 that is block diagonal with one 2 x 2 block per
+// spatial orbital in the interleaved order r = 2p + sigma (R1b[(il n + p) 4 + 2 sigma + tau] =
+// R1[il][2p + sigma][2p + tau]): row r of Y takes two rows of T2.  Point w = w0 + wl of the chunk
+// belongs to Lebedev point il = w / blk and takes column block rem = w % blk of T2; Y is row-major
+// M x (bc N) with leading dimension ld, as the GEMM form writes it.
+__global__ void spin_block_y_kernel(int n, int N, int bc, int w0, int blk, const zc *__restrict__ R1b,
+                                    const zc *__restrict__ T2, long long ld2, zc *__restrict__ Ys, long long ld) {
+    const long long cols = (long long)bc * N, total = 2LL * n * cols;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        const int r = (int)(e / cols);
+        const long long c = e - (long long)r * cols;
+        const int wl = (int)(c / N), j = (int)(c - (long long)wl * N);
+        const int w = w0 + wl, il = w / blk, rem = w - il * blk;
+        const int pp = r >> 1, sg = r & 1;
+        const zc *B = R1b + ((long long)il * n + pp) * 4 + 2 * sg;
+        const long long tc = (long long)rem * N + j;
+        Ys[(long long)r * ld + c] = B[0] * T2[(long long)(2 * pp) * ld2 + tc] + B[1] * T2[(long long)(2 * pp + 1) * ld2 + tc];
+    }
+}
+
 inline int grid_for(long long n) {
     long long g = (n + NT - 1) / NT;
     if (g > 148LL * 16) g = 148LL * 16;
@@ -479,6 +499,15 @@ int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStrea
 int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     gather_kin_kernel<<<grid_for((long long)n * n * b * 4), NT, 0, st>>>(n, b, rho, Kin, ldk);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, const zc *T2, long long ld2, zc *Ys,
+                        long long ld, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    spin_block_y_kernel<<<grid_for(2LL * n * bc * N), NT, 0, st>>>(n, N, bc, w0, blk, R1b, T2, ld2, Ys, ld);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -208,3 +208,29 @@ def test_graph_replay_matches_direct_launches():
                 _lib.profile_enable(False)
         for a, b, c in zip(graph[0], graph[1], direct):
             assert torch.equal(a, b) and torch.equal(a, c)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "ozaki_i8"])
+def test_spin_block_rotations_match_the_general_product(precision):
+    """Spin rotations R1 are 2 x 2 block diagonal in the interleaved spin order, and a Cholesky plan
+    then forms Y = R1 T2 from the blocks; a single extra entry of 1e-300 outside the blocks sends the
+    same problem through the general M x M product.  Both must agree (the tiny entry changes the
+    products by far less than the tolerance)."""
+    import torch
+
+    p = synth.make_problem(20, 10, 40, ngrid=(6, 3), seed=3, pg="C2v")
+    kw = p.grid_kwargs()
+    akw = dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+               r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+               roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+    C = torch.from_numpy(p.C).cuda()
+    res = []
+    for tweak in (False, True):
+        r1 = np.array(akw["r1"], dtype=np.complex128, copy=True)
+        if tweak:
+            r1[0, 0, p.M - 1] = 1e-300  # reference order: alpha orbital 0 -> beta orbital n - 1
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, jk_form="eri", precision=precision,
+                      **dict(akw, r1=r1)) as plan:
+            res.append([t.cpu().numpy() for t in plan.eval_device(C)])
+    for a, b in zip(*res):
+        assert _close(a, b, 1e-12), float(np.abs(a - b).max())

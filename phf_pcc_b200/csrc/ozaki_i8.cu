@@ -231,8 +231,55 @@ struct OzArgs {
     long long dz;        // split-k: CTA z covers k-blocks [z kblocks, (z+1) kblocks) and writes D + z dz
     int kb_total;        // k-blocks of this launch over all splits
     int kseg;            // floating-point formats: k-blocks per FP32 accumulation segment (>= 1)
+    int gamma_n;         // > 0: exchange-to-Gamma output (see store_row_chunk), n spatial orbitals
     int *err;
 };
+
+// Stores one epilogue thread's 32 consecutive columns col0 .. col0 + 31 of output row `row` (values
+// acc * rowscale * cs): element (row, col) at D[row ldd + col], or D[col ldd + row] when args.trans,
+// added to what is there when `add`.  Exchange-to-Gamma mode (args.gamma_n = n > 0): the product is
+// K^T of the exchange GEMM, row = i n + k, col = (4 w + 2 sigma + tau) 2 + part, and -K goes
+// straight into the complex M x M matrix Gamma_w (D = Gamma as doubles) at [2i + sigma][2k + tau];
+// the Coulomb term is added to the diagonal spin blocks afterwards.
+__device__ __forceinline__ void store_row_chunk(const OzArgs &args, double *Dz, int row, int col0,
+                                                const double (&acc)[32], double rowscale, const double *cs,
+                                                bool add) {
+    if (args.gamma_n > 0) {
+        const int gn = args.gamma_n, M = 2 * gn, i = row / gn, k = row - i * gn;
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const int col = col0 + j;
+            if (col < args.n) {
+                const int w = col >> 3, sg = (col >> 2) & 1, tu = (col >> 1) & 1;
+                double2 *g = reinterpret_cast<double2 *>(Dz) + ((long long)w * M + 2 * i + sg) * M + 2 * k + tu;
+                double2 v = make_double2(-(acc[j] * rowscale * cs[j]), -(acc[j + 1] * rowscale * cs[j + 1]));
+                if (add) {
+                    const double2 o = *g;
+                    v.x = o.x + v.x;
+                    v.y = o.y + v.y;
+                }
+                *g = v;
+            }
+        }
+        return;
+    }
+    double *drow = Dz + (args.trans ? (long long)row : (long long)row * args.ldd);
+    const long long cstride = args.trans ? args.ldd : 1;
+    double old[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int col = col0 + j;
+        old[j] = (add && col < args.n) ? drow[(long long)col * cstride] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int col = col0 + j;
+        if (col < args.n) {
+            const double val = acc[j] * rowscale * cs[j];
+            drow[(long long)col * cstride] = add ? old[j] + val : val;
+        }
+    }
+}
 
 // floating-point operand formats (slice-count codes beyond the int8 range 1..7)
 __host__ __device__ constexpr bool oz_float(int S) { return S == OZ_FMT_BF16X3 || S == OZ_FMT_TF32; }
@@ -612,8 +659,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
         const double rowscale = row_ok ? ldexp(kUnit, args.ea[row]) : 0.0;
-        double *drow = Dz + (args.trans ? (long long)(row_ok ? row : 0) : (long long)(row_ok ? row : 0) * args.ldd);
-        const long long cstride = args.trans ? args.ldd : 1;
         if constexpr (oz_float(S)) {
             // segment sums: FP32 accumulator -> FP64, added to the parked sums (columns 256 + c 32
             // high words, 384 + c 32 low words), stored to D after the last segment
@@ -652,20 +697,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         tmem_st32(lane_base + 256 + c * 32, hi);
                         tmem_st32(lane_base + 384 + c * 32, lo);
                     } else if (row_ok) {
-                        double old[32];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = n0 + c * 32 + j;
-                            old[j] = (args.accumulate && col < args.n) ? drow[(long long)col * cstride] : 0.0;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = n0 + c * 32 + j;
-                            if (col < args.n) {
-                                const double val = acc[j] * rowscale * colscale[c * 32 + j];
-                                drow[(long long)col * cstride] = args.accumulate ? old[j] + val : val;
-                            }
-                        }
+                        store_row_chunk(args, Dz, row, n0 + c * 32, acc, rowscale, colscale + c * 32,
+                                        args.accumulate != 0);
                     }
                 }
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -710,21 +743,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     tmem_st32(lane_base + c * 32, hi);
                     tmem_st32(lane_base + 128 + c * 32, lo);
                 } else if (row_ok) {
-                    const bool add = (p > 0 && !keep) || args.accumulate;
-                    double old[32];
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = n0 + c * 32 + j;
-                        old[j] = (add && col < args.n) ? drow[(long long)col * cstride] : 0.0;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = n0 + c * 32 + j;
-                        if (col < args.n) {
-                            const double val = acc[j] * rowscale * colscale[c * 32 + j];
-                            drow[(long long)col * cstride] = add ? old[j] + val : val;
-                        }
-                    }
+                    store_row_chunk(args, Dz, row, n0 + c * 32, acc, rowscale, colscale + c * 32,
+                                    (p > 0 && !keep) || args.accumulate);
                 }
             }
             if (!last) {
@@ -1348,6 +1368,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kblocks = (int)((kb_total + nsplit - 1) / nsplit);
     a.kb_total = (int)kb_total;
     a.kseg = OZ_KSEG;
+    a.gamma_n = 0;
     a.S = S;
     a.ea = ea;
     a.eb = eb;
@@ -1381,7 +1402,11 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
 }
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
-              double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st) {
+              double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n) {
+    if (gamma_n > 0 && (m != gamma_n * gamma_n || n % 8 != 0)) {
+        set_error(PHF_ERR_ARG, "oz_gemm: the Gamma output needs m = n^2 rows and 8 columns per point");
+        return PHF_ERR_ARG;
+    }
     if (!oz_format_ok(S)) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
@@ -1416,6 +1441,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.dz = 0;
         a.kb_total = a.kblocks;
         a.kseg = OZ_KSEG;
+        a.gamma_n = gamma_n;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);

@@ -516,7 +516,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         if (p.chol && p.eri) {
             per += 2 * MM + 2 * n2 + p.L;                       // Rho, Gam, Pvec, Jvec, dvec
             if (p.prec == PHF_PREC_FP64) per += 8 * n2;         // Kin, Kvec
-            else per += 4 * n2 + (8 * n2 * oz_slots(p.slices)) / sizeof(zc) + 1  // Dk, exchange slices
+            else per += (8 * n2 * oz_slots(p.slices)) / sizeof(zc) + 1  // exchange slices
                         + (2 * n2 + 2 * (size_t)p.L) * oz_slots(p.slices) / sizeof(zc) + 1    // Coulomb slices
                         + p.L + n2;                                                // d^T, J pairs
         } else if (p.chol) {
@@ -571,7 +571,6 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.Kin, 4 * b * n2));
             PHF_TRY(p.arena.alloc(&p.Kvec, 4 * b * n2));
         } else {
-            PHF_TRY(p.arena.alloc(&p.Dk, 8 * b * n2));
             const size_t bsl = oz_slice_bytes(oz_pad_cols(8 * (long long)b), (long long)n2, p.slices);
             PHF_TRY(p.arena.alloc(&p.Bsl, bsl));
             PHF_CUDA(cudaMemset(p.Bsl, 0, bsl));
@@ -722,11 +721,12 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st));
     } else {
         if (!fused) PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
-        // K^T (8 bc x n^2), transposed for coalesced epilogue stores
-        PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, p.Dk, n2, 0, 1, p.ozerr, st));
+        // K (as K^T, 8 bc x n^2) written by the GEMM epilogue as -K into Gamma's complex M x M blocks
+        PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, reinterpret_cast<double *>(p.Gam),
+                          0, 0, 0, p.ozerr, st, n));
         if (fork) PHF_CUDA(cudaStreamWaitEvent(st, p.ev_join, 0));  // the Coulomb chain is done
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, nullptr, 0, p.Jr, 1, n2, nullptr, 0, p.Dk, 1, n2, p.Gam, st));
+        PHF_TRY(launch_add_coulomb_diag(n, bc, p.Jr, 1, n2, p.Gam, st));
     }
     PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
                           st));

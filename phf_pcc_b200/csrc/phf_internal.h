@@ -71,6 +71,7 @@ int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cud
 int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale,
                       cudaStream_t st, const zc *add = nullptr);
 int launch_add_inplace(int M, int N, int b, const zc *A, zc *G, long long ldX, cudaStream_t st);
+int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st);
 int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, const zc *T2, long long ld2, zc *Ys,
                         long long ld, cudaStream_t st);
 int launch_epilogue(int M, int N, int b, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
@@ -118,7 +119,8 @@ int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long lon
 int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
 int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
-              double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st);
+              double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st,
+              int gamma_n = 0);  // gamma_n > 0: -K^T written into Gamma (exchange GEMM, m = n^2)
 int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl,
                    const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
                    cudaStream_t st);
@@ -188,7 +190,6 @@ struct PlanImpl {
     signed char *EKsl = nullptr;       // its int8 slices, Ozaki back-end
     int *ea = nullptr, *eb = nullptr, *ozerr = nullptr;
     zc *Rho = nullptr, *Pvec = nullptr, *dvec = nullptr, *Jvec = nullptr, *Kin = nullptr, *Kvec = nullptr, *Gam = nullptr;
-    double *Dk = nullptr;
     signed char *Bsl = nullptr;
     // Coulomb term on the tensor cores: d = B vec P, J = B^T d (B = Cholesky vectors as L x n^2)
     signed char *B1sl = nullptr, *B2sl = nullptr, *Psl = nullptr, *dsl = nullptr;

@@ -347,6 +347,23 @@ __global__ void spin_block_y_kernel(int n, int N, int bc, int w0, int blk, const
     }
 }
 
+// Coulomb term of the tensor-core path: Gamma_w[2i + s][2k + s] += J_w(i, k) for both spins s, with
+// J_w's real and imaginary parts at Jr[ik jrs + (2w) jcs] and Jr[ik jrs + (2w + 1) jcs] (Gamma already
+// holds -K from the exchange GEMM).
+__global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam) {
+    const int M = 2 * n;
+    const long long nn = (long long)n * n, tot = 2LL * nn * b;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        const long long w = e / (2 * nn), rem = e - w * 2 * nn;
+        const int sg = (int)(rem / nn);
+        const long long ik = rem - (long long)sg * nn;
+        const int i = (int)(ik / n), k = (int)(ik - (long long)i * n);
+        zc *g = Gam + (w * M + 2 * i + sg) * M + 2 * k + sg;
+        const zc jv = mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
+        *g = *g + jv;
+    }
+}
+
 inline int grid_for(long long n) {
     long long g = (n + NT - 1) / NT;
     if (g > 148LL * 16) g = 148LL * 16;
@@ -508,6 +525,14 @@ int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, co
                         long long ld, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     spin_block_y_kernel<<<grid_for(2LL * n * bc * N), NT, 0, st>>>(n, N, bc, w0, blk, R1b, T2, ld2, Ys, ld);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    add_coulomb_diag_kernel<<<grid_for(2LL * n * n * b), NT, 0, st>>>(n, b, Jr, jrs, jcs, Gam);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

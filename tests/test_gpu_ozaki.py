@@ -106,14 +106,17 @@ def test_int8_pipeline_matches_fp64_on_ragged_sizes(n, N, L):
         assert _close(a, b, 1e-9), (what, float(np.abs(a - b).max()))
 
 
-def test_automatic_form_above_n128_int8_eri_matches_fp64_factorized():
+@pytest.mark.parametrize("n", [130, 170])
+def test_automatic_form_above_n128_int8_eri_matches_fp64_factorized(n):
     """Above n = 128 the automatic J/K form is the factorized one in FP64 but the spatial-ERI exchange
-    matrix for the int8 path (here n = 130: a 16900 x 16900 exchange matrix); both forms must agree."""
+    matrix for the int8 path (n = 130: a 16900 x 16900 exchange matrix); both forms must agree.  At
+    n = 170 (k = n^2 = 28900) the exchange GEMM needs two launches for exact int32 group sums, the
+    second adding into Gamma."""
     import torch
 
     from phf_pcc_b200 import synth
 
-    p = synth.make_problem(130, 4, 16, ngrid=(6, 3), seed=17, pg="None")
+    p = synth.make_problem(n, 4, 16, ngrid=(6, 3), seed=17, pg="None")
     kw = p.grid_kwargs()
     akw = dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
                r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],

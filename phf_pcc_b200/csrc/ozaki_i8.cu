@@ -210,18 +210,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// tcgen05.ld of 32 columns without the wait (the caller issues tcgen05.wait::ld before reading v)
-__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-}
-
 __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -730,22 +718,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 double acc[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-                // groups g1 down to g0 (an empty k range contributes zero), two TMEM loads per wait
 #pragma unroll 1
-                for (int g = g1; g >= g0 && KB > 0; g -= 2) {
-                    uint32_t v0[32], v1[32];
-                    const bool two = g - 1 >= g0;
-                    tmem_ld32_nowait(acc0 + (uint32_t)(g - g0) * BN + c * 32, v0);
-                    if (two) tmem_ld32_nowait(acc0 + (uint32_t)(g - 1 - g0) * BN + c * 32, v1);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                    const double sc0 = kPow254[g - 2];
+                for (int g = g1; g >= g0 && KB > 0; --g) {  // an empty k range contributes zero
+                    uint32_t v[32];
+                    tmem_ld32(acc0 + (uint32_t)(g - g0) * BN + c * 32, v);
+                    const double sc = kPow254[g - 2];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v0[j], sc0, acc[j]);
-                    if (two) {
-                        const double sc1 = kPow254[g - 3];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v1[j], sc1, acc[j]);
-                    }
+                    for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
                 }
                 if (keep && p == 1) {  // add the first pass's partial sums
                     uint32_t hi[32], lo[32];

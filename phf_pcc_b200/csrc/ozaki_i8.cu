@@ -961,15 +961,22 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
 //     rho_st[l][j] = sum_m X_w[2l+s][m] conj(bra[2j+t][m])
 // with the tensor-core MMA sequence of zgemm_kernel (m ascending in steps of four), so every
 // column, its exponent and its slices are those of the density GEMM followed by slice_rho_cols /
-// slice_p_cols.
+// slice_p_cols.  A cluster of two CTAs shares each (w, pair): CTA rank r forms rows
+// l in [32 r, 32 r + 32) and slices that part of every column; the column maxima (one exponent per
+// column) are combined through distributed shared memory.  Two such CTAs fit on an SM, so one
+// CTA's FP64 MMAs overlap another's slicing.
 // threads, m-chunk, padded row pitch (complex).  A 16-byte fragment load is served eight lanes at a
 // time; lanes (fk, fr) of one such group read row kk + fk, column c + fr, so with a pitch of 2 mod 8
 // (complex) the eight land on distinct bank quadruples.
-constexpr int RS_NT = 512, RS_MC = 16, RS_P = 66;
-constexpr int RS_WI = 2;  // 8-row fragments per warp: 16 warps of 16 x 16 cover the 64 x 64 blocks
+constexpr int RS_NT = 256, RS_MC = 16, RS_P = 66;
+constexpr int RS_WI = 2;     // 8-row fragments per warp: 8 warps of 16 x 16 cover 32 rows x 64 columns
+constexpr int RS_ROWS = 32;  // density rows l per CTA: the two CTAs of a cluster take l < 32 and l >= 32
 
-// operand staging (2 x 2 x RS_MC x RS_P complex), reused for two density columns (2 x 64^2 doubles)
-size_t rs_smem_bytes() { return std::max((size_t)2 * 2 * RS_MC * RS_P * sizeof(zc), (size_t)2 * 64 * 64 * sizeof(double)); }
+// operand staging (2 x 2 x RS_MC x RS_P complex), reused for two half density columns (2 x 32 x 64
+// doubles)
+size_t rs_smem_bytes() {
+    return std::max((size_t)2 * 2 * RS_MC * RS_P * sizeof(zc), (size_t)2 * RS_ROWS * 64 * sizeof(double));
+}
 
 // Slices of four consecutive k-elements e0..e0+3 (one 32-element block) of a column, packed four
 // to a 32-bit word (byte v = element e0 + v), one store per slice; for the floating-point formats
@@ -1007,19 +1014,23 @@ __device__ __forceinline__ void slice_pack4(const double (&x)[4], const SliceSca
 }
 
 template <int S>
-__global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc *__restrict__ Xs, long long ld,
-                                                          const zc *__restrict__ bra, long long npadK,
-                                                          long long npadP, long long kpad, signed char *outK,
-                                                          int *ebK, signed char *outP, int *ebP) {
+__global__ void __launch_bounds__(RS_NT, 2) rho_slice_kernel(int n, int N, const zc *__restrict__ Xs, long long ld,
+                                                             const zc *__restrict__ bra, long long npadK,
+                                                             long long npadP, long long kpad, signed char *outK,
+                                                             int *ebK, signed char *outP, int *ebP) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
-    zc *xs = reinterpret_cast<zc *>(rs_smem);  // [s][mm][l]: X_w[2l+s][m0+mm] at (s RS_MC + mm) RS_P + l
+    zc *xs = reinterpret_cast<zc *>(rs_smem);  // [s][mm][l - r0]: X_w[2l+s][m0+mm] at (s RS_MC + mm) RS_P + l - r0
     zc *bs = xs + 2 * RS_MC * RS_P;            // [t][mm][j]: bra[2j+t][m0+mm]
-    double *stage = reinterpret_cast<double *>(rs_smem);  // one column (n^2 values) after the products
+    double *stage = reinterpret_cast<double *>(rs_smem);  // this CTA's part of two columns after the products
     __shared__ double red[6 * (RS_NT / 32)];
+    __shared__ double cmax[6];  // this CTA's column maxima, read by the other CTA of the cluster
     const int tid = threadIdx.x;
-    const long long w = blockIdx.x >> 1;
-    const int pair = (int)(blockIdx.x & 1);
-    // warp tile: rows wr + 8 bi + fr, columns wc + 8 bj + 2 fk + h of both spin blocks q = 0, 1,
+    uint32_t rank;
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const long long w = blockIdx.x >> 2;
+    const int pair = (int)((blockIdx.x >> 1) & 1);
+    const int r0 = (int)rank * RS_ROWS;  // first density row of this CTA
+    // warp tile: rows r0 + wr + 8 bi + fr, columns wc + 8 bj + 2 fk + h of both spin blocks q = 0, 1,
     // as FP64 tensor-core products (mma.sync m8n8k4: lane l holds A[l/4][l%4], B[l%4][l/4],
     // D[l/4][2 (l%4) + h]), four real MMAs per complex step in the order of zgemm_kernel
     const int lane = tid & 31, warp = tid >> 5;
@@ -1037,13 +1048,16 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
         __syncthreads();
         for (int idx = tid; idx < 2 * 64 * RS_MC; idx += RS_NT) {  // mm fastest: 256-byte row runs
             const int mm = idx % RS_MC, l = (idx / RS_MC) & 63, sp = idx / (RS_MC * 64);
-            zc xv = {0.0, 0.0}, bv = {0.0, 0.0};
-            if (l < n && mm < mc) {
-                xv = Xs[(long long)(2 * l + sp) * ld + w * N + m0 + mm];
-                bv = bra[(long long)(2 * l + sp) * N + m0 + mm];
-            }
-            xs[(sp * RS_MC + mm) * RS_P + l] = xv;
+            zc bv = {0.0, 0.0};
+            if (l < n && mm < mc) bv = bra[(long long)(2 * l + sp) * N + m0 + mm];
             bs[(sp * RS_MC + mm) * RS_P + l] = bv;
+        }
+        for (int idx = tid; idx < 2 * RS_ROWS * RS_MC; idx += RS_NT) {
+            const int mm = idx % RS_MC, ll = (idx / RS_MC) % RS_ROWS, sp = idx / (RS_MC * RS_ROWS);
+            const int l = r0 + ll;
+            zc xv = {0.0, 0.0};
+            if (l < n && mm < mc) xv = Xs[(long long)(2 * l + sp) * ld + w * N + m0 + mm];
+            xs[(sp * RS_MC + mm) * RS_P + ll] = xv;
         }
         __syncthreads();
         for (int kk = 0; kk < mc; kk += 4) {  // zero-padded beyond mc
@@ -1080,7 +1094,7 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
         if (col < 4) return part ? ci[1][i][j][h] : cr[1][i][j][h];
         return part ? ci[0][i][j][h] + ci[1][i][j][h] : cr[0][i][j][h] + cr[1][i][j][h];
     };
-    // all column maxima in one reduction: warp shuffles, then the 8 warps through shared memory
+    // column maxima over this CTA's rows: warp shuffles, then the 8 warps through shared memory
     double mx[6];
 #pragma unroll
     for (int col = 0; col < 6; ++col) mx[col] = 0.0;
@@ -1090,7 +1104,7 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
         for (int j = 0; j < 2; ++j)
 #pragma unroll
             for (int h = 0; h < 2; ++h)
-                if ((wr + 8 * i + fr < n) && (wc + 8 * j + 2 * fk + h < n)) {
+                if ((r0 + wr + 8 * i + fr < n) && (wc + 8 * j + 2 * fk + h < n)) {
 #pragma unroll
                     for (int col = 0; col < 6; ++col)
                         if (col < ncol) mx[col] = fmax(mx[col], fabs(value(col, i, j, h)));
@@ -1102,14 +1116,24 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
         if (lane == 0) red[col * (RS_NT / 32) + warp] = mx[col];
     }
     __syncthreads();  // also orders the last reads of xs / bs before the stage writes
+    if (tid < 6) {
+        double m = 0.0;
+#pragma unroll
+        for (int wv = 0; wv < RS_NT / 32; ++wv) m = fmax(m, red[tid * (RS_NT / 32) + wv]);
+        cmax[tid] = m;
+    }
+    // exchange the maxima with the other CTA of the cluster (every thread of both CTAs arrives)
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+    uint32_t peer_cmax;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(peer_cmax) : "r"(smem_u32(cmax)), "r"(rank ^ 1u));
     long long cidx[6];
     int ex[6];
 #pragma unroll
     for (int col = 0; col < 6; ++col) {
-        double m = 0.0;
-#pragma unroll
-        for (int wv = 0; wv < RS_NT / 32; ++wv) m = fmax(m, red[col * (RS_NT / 32) + wv]);
-        ex[col] = exp_of_max(m);
+        double other;
+        asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(other) : "r"(peer_cmax + 8u * col) : "memory");
+        ex[col] = exp_of_max(fmax(cmax[col], other));
         const int part = col & 1;
         if (col < 4) {
             const int q = col >> 1, sg = q, tu = pair ? 1 - q : q;
@@ -1118,12 +1142,20 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
             cidx[col] = 2 * w + part;
         }
     }
-    if (tid < ncol) {
+    // the peer's maxima have been read: neither CTA leaves (or reuses cmax) before both have
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+    if (rank == 0 && tid < ncol) {
 #pragma unroll
         for (int col = 0; col < 6; ++col)
             if (col == tid) (col < 4 ? ebK : ebP)[cidx[col]] = ex[col];
     }
-    // two columns per round through the stage (2 n^2 doubles), sliced four k-elements per store
+    // this CTA slices elements [e_lo, e_hi) of every column (element e = l n + c); rows l >= 32 and the
+    // zero padding up to kpad belong to rank 1 unless n <= 32, when rank 0 covers the whole column
+    const long long split = (RS_ROWS * n >= nn) ? kpad : (long long)RS_ROWS * n;
+    const long long e_lo = rank ? split : 0, e_hi = rank ? kpad : split;
+    const long long part_len = (long long)RS_ROWS * n;  // stage pitch of one column part
+    // two columns per round through the stage, sliced four k-elements per store
 #pragma unroll
     for (int c0 = 0; c0 < 6; c0 += 2) {
         if (c0 >= ncol) break;
@@ -1133,10 +1165,10 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
             for (int j = 0; j < 2; ++j)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int l = wr + 8 * i + fr, c = wc + 8 * j + 2 * fk + h;
-                    if (l < n && c < n) {
-                        stage[l * n + c] = value(c0, i, j, h);
-                        stage[nn + l * n + c] = value(c0 + 1, i, j, h);
+                    const int ll = wr + 8 * i + fr, c = wc + 8 * j + 2 * fk + h;
+                    if (r0 + ll < n && c < n) {
+                        stage[ll * n + c] = value(c0, i, j, h);
+                        stage[part_len + ll * n + c] = value(c0 + 1, i, j, h);
                     }
                 }
         __syncthreads();
@@ -1145,9 +1177,9 @@ __global__ void __launch_bounds__(RS_NT) rho_slice_kernel(int n, int N, const zc
             const int col = c0 + h;
             const bool isK = col < 4;
             const SliceScale sc = slice_scale(ex[col], S);
-            const double *src = stage + h * nn;
-            const bool pairs = (reinterpret_cast<uintptr_t>(src) & 15u) == 0;  // 16-byte loads possible
-            for (long long e0 = 4LL * tid; e0 < kpad; e0 += 4LL * RS_NT) {
+            const double *src = stage + h * part_len - (long long)r0 * n;  // indexed by the element e
+            const bool pairs = (reinterpret_cast<uintptr_t>(stage + h * part_len) & 15u) == 0;  // 16-byte loads
+            for (long long e0 = e_lo + 4LL * tid; e0 < e_hi; e0 += 4LL * RS_NT) {
                 double x[4];
                 if (pairs && e0 + 3 < nn) {
                     const double2 a = *reinterpret_cast<const double2 *>(src + e0);
@@ -1274,9 +1306,22 @@ int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra
     }
     const size_t smem = rs_smem_bytes();
     PHF_CUDA(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // one cluster of two CTAs per (grid point, spin-block pair)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(4LL * bc), 1, 1);
+    cfg.blockDim = dim3(RS_NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const long long npadK = oz_pad_cols(8LL * bc), npadP = oz_pad_cols(2LL * bc), kpad = oz_pad_k((long long)n * n);
     ProfScope prof(st, PROF_MEMORY);
-    fn<<<(unsigned)(2LL * bc), RS_NT, smem, st>>>(n, N, Xs, ld, bra, oz_pad_cols(8LL * bc), oz_pad_cols(2LL * bc),
-                                                  oz_pad_k((long long)n * n), Ksl, eK, Psl, eP);
+    PHF_CUDA(cudaLaunchKernelEx(&cfg, fn, n, N, Xs, ld, bra, npadK, npadP, kpad, Ksl, eK, Psl, eP));
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -528,7 +528,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         per *= sizeof(zc);
         per += split_bytes_per_point(p);
         long long bmax = (long long)(budget / std::max<size_t>(per, 1));
-        bmax = std::max<long long>(1, std::min<long long>(bmax, 1024));
+        bmax = std::max<long long>(1, std::min<long long>(bmax, 4096));
         p.b = (int)std::min<long long>(bmax, p.wend - p.wbeg);
         // whole Lebedev-point blocks (ny npg points sharing R1[il]) per chunk when they fit
         const int blk = p.ny * p.npg;

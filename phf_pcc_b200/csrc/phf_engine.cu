@@ -648,6 +648,8 @@ int build_exchange_matrix(PlanImpl &p) {
 // Gamma(rho_w) X_w through the spatial ERI matrix:
 //   rho_w = X_w bra^H;  J = B^T (B vec P), P = rho_aa + rho_bb;  K_st = EK vec(rho_st);
 //   Gamma_w = I (x) J - K;  GX_w = Gamma_w X_w;  e2_w = tr(bra^H GX_w) / 2
+// FP64 form: J and K in FP64 GEMMs, Gamma assembled from both.  Tensor-core forms: the exchange
+// GEMM's epilogue writes -K into Gamma and J is then added to the diagonal spin blocks.
 int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     const int M = p.M, N = p.N, n = p.n, L = p.L, b = p.b;
     const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
@@ -670,7 +672,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     }
     // tensor-core path: the Coulomb chain runs on a second stream beside the exchange GEMM (independent
     // operands and outputs; its small, latency-bound launches fill the SMs the exchange GEMM's last
-    // wave leaves idle).  Joined before Gamma is assembled.  Not while per-launch profiling is on:
+    // wave leaves idle).  Joined before J is added to Gamma.  Not while per-launch profiling is on:
     // event times of overlapping kernels would count the shared time twice.
     cudaStream_t js = st;
     const bool fork = p.prec != PHF_PREC_FP64 && !g_prof.on;

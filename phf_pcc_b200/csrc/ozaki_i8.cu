@@ -119,15 +119,6 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
-// Prefetch of one box of a 2-D tensor map into L2 (no shared memory, no barrier): issued a ring
-// length ahead of the load that will need it, so that the load finds the box in L2.
-__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap *map, int c0, int c1) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(c0), "r"(c1)
-                 : "memory");
-}
-
 // Shared-memory matrix descriptor: K-major, SWIZZLE_128B (8 rows x 128 B atoms, SBO = 1024 B).
 __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     uint64_t d = 0;
@@ -574,14 +565,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 if constexpr (W1 == 1) {
                     tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, m0);
                     tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
-                }
-                if (kb + NS < KB) {  // the k-block one ring length ahead, into L2
-                    tma_prefetch_2d(&tmA0, (kbg + NS) * 128, m0);
-                    tma_prefetch_2d(&tmB0, (kbg + NS) * 128, n0);
-                    if constexpr (W1 == 1) {
-                        tma_prefetch_2d(&tmA1, (kbg + NS) * 32, m0);
-                        tma_prefetch_2d(&tmB1, (kbg + NS) * 32, n0);
-                    }
                 }
                 if (++sg == NS) {
                     sg = 0;

@@ -232,8 +232,6 @@ struct OzArgs {
     int kb_total;        // k-blocks of this launch over all splits
     int kseg;            // floating-point formats: k-blocks per FP32 accumulation segment (>= 1)
     int gamma_n;         // > 0: exchange-to-Gamma output (see store_row_chunk), n spatial orbitals
-    int persistent;      // single-pass int8 formats: each CTA loops over tiles L = blockIdx.x + t gridDim.x
-    int mt, nt;          // row and column tiles of the output (persistent launches)
     int *err;
 };
 
@@ -547,121 +545,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
 
-    // Persistent launches (single-pass int8 formats, no split-k): one CTA per SM loops over the
-    // tiles in raster order, so the producer loads the next tile's first stages while the epilogue
-    // drains this tile's accumulators, and the CTA start-up is paid once.  The MMAs of tile t + 1
-    // wait until the epilogue has read tile t (free_bar, phase t); the epilogue waits for tile t's
-    // MMAs (pass_bar, phase t).  Each epilogue thread computes its own column scales.
-    bool persistent_done = false;
-    if constexpr (oz_staged(S) && !oz_float(S)) {
-        if (args.persistent) {
-            persistent_done = true;
-            const int mt = args.mt, nt = args.nt, ntiles = mt * nt;
-            auto tile_origin = [&](int L, int &tm0, int &tn0) {
-                const int width = OZ_GROUP_M * nt;
-                const int first = (L / width) * OZ_GROUP_M;
-                const int gm = min(mt - first, OZ_GROUP_M);
-                tm0 = (first + (L % width) % gm) * OZ_BM;
-                tn0 = ((L % width) / gm) * BN;
-            };
-            if (warp == 0) {
-                if (lane == 0) {  // TMA producer over (tile, k-block), one stage per k-block
-                    constexpr int NS = oz_stages(S);
-                    constexpr uint32_t PITCH = oz_stage_pitch(S), BYTES = oz_stage_bytes(S);
-                    int sg = 0;
-                    uint32_t eph = 0;
-                    bool wrapped = false;
-                    for (int L = blockIdx.x; L < ntiles && !*abort_flag; L += gridDim.x) {
-                        int tm0, tn0;
-                        tile_origin(L, tm0, tn0);
-                        for (int kb = 0; kb < KB && !*abort_flag; ++kb) {
-                            const int kbg = args.kb0 + kb;
-                            if (wrapped && !mbar_wait(&empty_bar[sg], eph, args.err, 1)) {
-                                *abort_flag = 1;
-                                break;
-                            }
-                            unsigned char *dst = smem + (size_t)sg * PITCH;
-                            mbar_arrive_expect_tx(&full_bar[sg], BYTES);
-                            tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, tm0);
-                            tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, tn0);
-                            if constexpr (W1 == 1) {
-                                tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, tm0);
-                                tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32,
-                                            tn0);
-                            }
-                            if (++sg == NS) {
-                                sg = 0;
-                                if (wrapped) eph ^= 1u;
-                                wrapped = true;
-                            }
-                        }
-                    }
-                }
-            } else if (warp == 1) {
-                if (lane == 0) {  // MMA issuer
-                    int u = 0;
-                    uint32_t ph = 0;
-                    bool ok = true;
-                    const uint32_t smem_base = smem_u32(smem);
-                    int t = 0;
-                    for (int L = blockIdx.x; L < ntiles && ok; L += gridDim.x, ++t) {
-                        if (t > 0) {  // the epilogue has read tile t - 1's accumulators
-                            if (!mbar_wait(free_bar, (t - 1) & 1, args.err, 8)) {
-                                *abort_flag = 1;
-                                break;
-                            }
-                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                        }
-                        ok = mma_pass<S, 0>(tmem_base, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
-                        if (!ok) *abort_flag = 1;
-                        mma_commit(pass_bar);  // tile t's accumulators are final once its MMAs complete
-                    }
-                }
-            } else {
-                const int quarter = warp & 3;
-                const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
-                constexpr int g0 = oz_g0(0), g1 = oz_g1(S, 0);
-                int t = 0;
-                for (int L = blockIdx.x; L < ntiles; L += gridDim.x, ++t) {
-                    int tm0, tn0;
-                    tile_origin(L, tm0, tn0);
-                    const int row = tm0 + quarter * 32 + lane;
-                    const bool row_ok = row < args.m;
-                    const double rowscale = row_ok ? ldexp(kUnit, args.ea[row]) : 0.0;
-                    const bool ok = mbar_wait(pass_bar, t & 1, args.err, 4);
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    if (!ok || *abort_flag) break;
-#pragma unroll 1
-                    for (int c = 0; c < BN / 32; ++c) {
-                        double acc[32];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-#pragma unroll 1
-                        for (int g = g1; g >= g0 && KB > 0; --g) {
-                            uint32_t v[32];
-                            tmem_ld32(lane_base + (uint32_t)(g - g0) * BN + c * 32, v);
-                            const double sc = kPow254[g - 2];
-#pragma unroll
-                            for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
-                        }
-                        if (row_ok) {
-                            double cs[32];
-#pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                const int col = tn0 + c * 32 + j;
-                                cs[j] = col < args.n ? ldexp(kUnit, args.eb[col]) : 0.0;
-                            }
-                            store_row_chunk(args, args.D, row, tn0 + c * 32, acc, rowscale, cs, args.accumulate != 0);
-                        }
-                    }
-                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    mbar_arrive(free_bar);  // this thread's reads of tile t's accumulators are done
-                }
-            }
-        }
-    }
-
-    if (!persistent_done && warp == 0) {
+    if (warp == 0) {
         if (lane == 0 && oz_staged(S)) {  // TMA producer, one stage per k-block
             constexpr int NS = oz_stages(S);
             constexpr uint32_t PITCH = oz_stage_pitch(S), BYTES = oz_stage_bytes(S);
@@ -727,7 +611,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 }
             }
         }
-    } else if (!persistent_done && warp == 1) {
+    } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
             int u = 0;         // next unit
             uint32_t ph = 0;   // parity of its full-barrier phase
@@ -768,7 +652,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
             }
         }
-    } else if (!persistent_done) {
+    } else {
         // epilogue warps 2..5 cover TMEM lane quarters (warp % 4)
         const int quarter = warp & 3;
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
@@ -1475,17 +1359,6 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
 namespace {
 using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap, OzArgs);
 
-// SMs of the current device (persistent grid size)
-int sm_count() {
-    int dev = 0, n = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        n < 1) {
-        cudaGetLastError();
-        return 148;
-    }
-    return n;
-}
-
 OzKernelFn oz_kernel_for(int S) {
     switch (S) {
         case 1: return ozaki_i8_gemm_kernel<1>;
@@ -1541,9 +1414,6 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kb_total = (int)kb_total;
     a.kseg = OZ_KSEG;
     a.gamma_n = 0;
-    a.persistent = 0;
-    a.mt = 0;
-    a.nt = 0;
     a.S = S;
     a.ea = ea;
     a.eb = eb;
@@ -1600,13 +1470,6 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
-    // single-pass int8 formats run persistent CTAs, one per SM, over the same raster
-    const bool persist = oz_staged(S) && !oz_float(S);
-    dim3 launch_grid = grid;
-    if (persist) {
-        const long long tiles = (long long)grid.x * grid.y;
-        launch_grid = dim3((unsigned)std::min<long long>(tiles, sm_count()), 1, 1);
-    }
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;
@@ -1624,13 +1487,10 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.kb_total = a.kblocks;
         a.kseg = OZ_KSEG;
         a.gamma_n = gamma_n;
-        a.persistent = persist ? 1 : 0;
-        a.mt = (int)grid.x;
-        a.nt = (int)grid.y;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
-            kern<<<launch_grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
+            kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
         }
         ++g_launches;
         PHF_CHECK_LAUNCH();

@@ -684,7 +684,10 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     }
     if (fork) {
         if (!p.side) {
-            PHF_CUDA(cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking));
+            // highest priority: its few small launches get SMs as the exchange GEMM's CTAs retire
+            int lo = 0, hi = 0;
+            PHF_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            PHF_CUDA(cudaStreamCreateWithPriority(&p.side, cudaStreamNonBlocking, hi));
             PHF_CUDA(cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming));
             PHF_CUDA(cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming));
         }
@@ -978,7 +981,8 @@ int launch_captured(PlanImpl &p, int key, cudaStream_t st, F &&body) {
         const unsigned long long nl = g_launches - l0;
         g_launches = l0;
         cudaGraphExec_t ex = nullptr;
-        if (rc == PHF_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+        if (rc == PHF_OK && e == cudaSuccess && g &&
+            cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority) == cudaSuccess) {
             p.gexec[key] = ex;
             p.glaunch[key] = nl;
         } else {
@@ -1268,7 +1272,7 @@ int capture_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *c
         set_error(PHF_ERR_CUDA, "phf_eval_batch: graph capture failed");
         return PHF_ERR_CUDA;
     }
-    const cudaError_t e3 = cudaGraphInstantiate(exec, g, 0);
+    const cudaError_t e3 = cudaGraphInstantiate(exec, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e3 != cudaSuccess) {
         cudaGetLastError();

@@ -222,7 +222,7 @@ def tc_ops_per_point(p, precision, slices):
     return reps * (16.0 * p.n ** 4 + 8.0 * p.L * p.n ** 2)
 
 
-def survey_flops_per_point(p):
+def quoted_flops_per_point(p):
     """Per-point work figure of the benchmark description: 32 L n^3 + 8 L n^2 (J/K) plus
     16 M^2 N + 16 M N^2 + 8 N^3 + 16 M^3 (small algebra)."""
     n, N, M, L = p.n, p.N, p.M, p.L
@@ -543,7 +543,7 @@ def run_ours(args):
                      "jk_share_of_device_time": jk_ms / all_ms if all_ms else None,
                      "device_ms_by_class": {k: v[0] / args.steps for k, v in
                                             zip(("jk", "other_gemm", "overlap_inverse", "memory"), prof.values())},
-                     "alg_flops_per_point": alg, "survey_flops_per_point": survey_flops_per_point(p)})
+                     "alg_flops_per_point": alg, "quoted_flops_per_point": quoted_flops_per_point(p)})
         cpu = None
         if not args.no_cpu:
             v, nth, desc = cpu_sample(p, seconds_target=args.cpu_seconds)

@@ -16,8 +16,12 @@
  *                       Lebedev index, :79-84), each thread with private accumulators, reduced in
  *                       thread order.
  *   oracle_localg    -- LocalG (PHFTools.f90:203-247).
- * Gamma comes either from the dense HTwo(M,M,M,M) (the reference form) or from MO-basis
- * Cholesky vectors Bt(M,M,L) with (ik|jl) = sum_L Bt[ik] Bt[jl] (identical J - K).
+ * Gamma comes either from the dense HTwo(M,M,M,M) (the reference form), from MO-basis
+ * Cholesky vectors Bt(M,M,L) with (ik|jl) = sum_L Bt[ik] Bt[jl] (identical J - K), or
+ * (oracle_buildhsg_ex) from the spatial AO-basis vectors B(n,n,L) with the spin blocks of
+ * Main_PHF.py:22-29 written out (the same J - K at a quarter of the work; used where the dense
+ * HTwo would not fit in host memory).  With fewer grid points than threads the points run one
+ * after another and the work inside each point is split over the threads.
  * CmplxConj == 2 is supported.
  *
  * All arrays use the reference's Fortran (column-major) layouts:
@@ -37,9 +41,15 @@ typedef double complex zc;
 
 #define IDX2(i, j, ld) ((size_t)(i) + (size_t)(ld) * (size_t)(j))
 
+/* Threads that share the work of ONE grid point: > 1 only when fewer grid points than threads are
+ * evaluated (then the points run one after another and the products and the Cholesky sum inside a
+ * point are split over the threads); 1 while the points themselves run in parallel. */
+static int g_inner = 1;
+
 /* C = op(A) * B, column-major; A is m x k (opA: 0 none, 2 conj-transpose of a k x m array) */
 static void zgemm_cm(int m, int n, int k, const zc *A, int lda, int opA, const zc *B, int ldb, zc *C, int ldc)
 {
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int j = 0; j < n; ++j) {
         zc *cj = C + (size_t)ldc * j;
         for (int i = 0; i < m; ++i) cj[i] = 0;
@@ -143,7 +153,97 @@ static zc wignerfac(int j, int n, int m, double alpha, double beta, double gamma
 typedef struct {
     int M, N, L;
     const zc *hone, *htwo, *bt;
+    const double *bs; /* spatial Cholesky vectors B(p,q,L) = bs[p + n*(q + n*L)] in the AO basis */
+    const zc *ref;    /* Ref (M x M): MO = AO Ref, for the spatial form */
 } ham_t;
+
+/* C (n x n complex) = A (n x n real) * B (n x n complex, leading dimension ldb), column-major */
+static void dz_gemm(int n, const double *A, const zc *B, int ldb, zc *C)
+{
+    for (int j = 0; j < n; ++j) {
+        zc *cj = C + (size_t)n * j;
+        for (int i = 0; i < n; ++i) cj[i] = 0;
+        for (int p = 0; p < n; ++p) {
+            const zc b = B[(size_t)p + (size_t)ldb * j];
+            const double *ap = A + (size_t)n * p;
+            for (int i = 0; i < n; ++i) cj[i] += ap[i] * b;
+        }
+    }
+}
+
+/* Gamma from spatial Cholesky vectors (the same J - K as the MO-basis form, with the spin
+ * structure B~_L = blockdiag(B_L, B_L) of Main_PHF.py:22-29 used explicitly):
+ *   rho_AO = Ref rho Ref^H;  P = rho_aa + rho_bb;  d_L = tr(B_L P)
+ *   J = sum_L d_L B_L on both spin diagonal blocks;  K_st = sum_L B_L rho_st B_L (four spin blocks)
+ *   gama = Ref^H (J - K) Ref
+ * The L sum is split over g_inner threads in contiguous ranges, added in thread order. */
+static void make_gamma_spatial(const ham_t *H, const zc *rho, zc *gama, zc *tmp)
+{
+    const int M = H->M, n = M / 2, L = H->L, nt = g_inner;
+    const size_t MM = (size_t)M * M, nn = (size_t)n * n;
+    const zc *ref = H->ref;
+    zc *rao = malloc(sizeof(zc) * MM), *part = calloc((size_t)nt * 5 * nn, sizeof(zc));
+    zgemm_cm(M, M, M, ref, M, 0, rho, M, tmp, M); /* Ref rho */
+#pragma omp parallel for schedule(static) num_threads(nt) if (nt > 1)
+    for (int j = 0; j < M; ++j) /* rao = (Ref rho) Ref^H */
+        for (int i = 0; i < M; ++i) {
+            zc a = 0;
+            for (int p = 0; p < M; ++p) a += tmp[IDX2(i, p, M)] * conj(ref[IDX2(j, p, M)]);
+            rao[IDX2(i, j, M)] = a;
+        }
+#pragma omp parallel num_threads(nt) if (nt > 1)
+    {
+        int t = 0;
+#ifdef _OPENMP
+        if (nt > 1) t = omp_get_thread_num();
+#endif
+        const int l0 = (int)((long long)L * t / nt), l1 = (int)((long long)L * (t + 1) / nt);
+        zc *Jp = part + (size_t)t * 5 * nn, *Kp = Jp + nn;
+        zc *T = malloc(sizeof(zc) * nn), *U = malloc(sizeof(zc) * nn);
+        for (int l = l0; l < l1; ++l) {
+            const double *b = H->bs + (size_t)l * nn;
+            zc d = 0;
+            for (int q = 0; q < n; ++q)
+                for (int p = 0; p < n; ++p) d += b[IDX2(p, q, n)] * (rao[IDX2(q, p, M)] + rao[IDX2(n + q, n + p, M)]);
+            for (size_t e = 0; e < nn; ++e) Jp[e] += d * b[e];
+            for (int st = 0; st < 4; ++st) {
+                const int sg = st >> 1, tu = st & 1;
+                dz_gemm(n, b, rao + (size_t)sg * n + (size_t)M * tu * n, M, T); /* B rho_st */
+                for (int j = 0; j < n; ++j)                                    /* (B rho_st) B */
+                    for (int i = 0; i < n; ++i) U[IDX2(i, j, n)] = 0;
+                for (int j = 0; j < n; ++j)
+                    for (int p = 0; p < n; ++p) {
+                        const double bpj = b[IDX2(p, j, n)];
+                        const zc *tp = T + (size_t)n * p;
+                        zc *uj = U + (size_t)n * j;
+                        for (int i = 0; i < n; ++i) uj[i] += tp[i] * bpj;
+                    }
+                zc *Ks = Kp + (size_t)st * nn;
+                for (size_t e = 0; e < nn; ++e) Ks[e] += U[e];
+            }
+        }
+        free(T);
+        free(U);
+    }
+    /* Gamma_AO = blockdiag(J, J) - K, partial sums added in thread order */
+    for (size_t e = 0; e < MM; ++e) rao[e] = 0;
+    for (int t = 0; t < nt; ++t) {
+        const zc *Jp = part + (size_t)t * 5 * nn, *Kp = Jp + nn;
+        for (int st = 0; st < 4; ++st) {
+            const int sg = st >> 1, tu = st & 1;
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    zc v = -Kp[(size_t)st * nn + IDX2(i, j, n)];
+                    if (sg == tu) v += Jp[IDX2(i, j, n)];
+                    rao[IDX2(sg * n + i, tu * n + j, M)] += v;
+                }
+        }
+    }
+    zgemm_cm(M, M, M, rao, M, 0, ref, M, tmp, M); /* Gamma_AO Ref */
+    zgemm_cm(M, M, M, ref, M, 2, tmp, M, gama, M); /* Ref^H Gamma_AO Ref */
+    free(rao);
+    free(part);
+}
 
 /* gama_ik = sum_jl H2_ijkl rho_lj (MakeGamma) or the J - K Cholesky form */
 static void make_gamma(const ham_t *H, const zc *rho, zc *gama, zc *tmp)
@@ -160,6 +260,10 @@ static void make_gamma(const ham_t *H, const zc *rho, zc *gama, zc *tmp)
                 }
                 gama[IDX2(i, k, M)] = s;
             }
+        return;
+    }
+    if (H->bs) {
+        make_gamma_spatial(H, rho, gama, tmp);
         return;
     }
     /* Cholesky: J_ik = sum_L Bt_L[ik] tr(Bt_L rho); K = sum_L Bt_L rho Bt_L */
@@ -209,6 +313,7 @@ static int rdm(int M, int N, const zc *R, const zc *mo, int conj_bra, int conj_k
     if (zinv_det(N, s->Mm, s->Minv, det, s->work, s->piv)) return 1;
     zc *t3 = s->Rt2;                                          /* M x N */
     zgemm_cm(M, N, N, s->tmp, M, 0, s->Minv, N, t3, M);      /* tmp Minv */
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int j = 0; j < M; ++j)                               /* rho = t3 bra^H */
         for (int i = 0; i < M; ++i) {
             zc acc = 0;
@@ -226,6 +331,7 @@ static void gradient(const ham_t *H, const zc *gama, const zc *rho, zc det, scra
     zc *F = s->Rt, *FR = s->R;
     for (size_t i = 0; i < (size_t)M * M; ++i) F[i] = H->hone[i] + gama[i];
     zgemm_cm(M, M, M, F, M, 0, rho, M, FR, M);                /* F rho */
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int j = 0; j < M; ++j)
         for (int i = 0; i < M; ++i) {
             zc acc = FR[IDX2(i, j, M)];
@@ -234,18 +340,20 @@ static void gradient(const ham_t *H, const zc *gama, const zc *rho, zc det, scra
         }
 }
 
-int oracle_buildhsg(const zc *hone, const zc *htwo, const zc *bt, int nchol, const zc *ref, const zc *z,
-                    const int *ngrid, int nci, int cmplxconj, int ncisp, int nocc, const zc *r1, const zc *r2,
-                    const zc *rpg, const double *weightsp, const double *weightpg, const double *roota,
-                    const double *rootb, const double *rooty, int qj, int sp, int npg, int ncipg, int nso,
-                    const int *omega_list, int n_omega, int nthreads, zc *hmat, zc *smat, zc *gradmat,
-                    zc *rdmmat)
+/* bs != NULL: Gamma from the spatial Cholesky vectors bs (AO basis, n = nso/2, nchol of them)
+ * through make_gamma_spatial, with the MO basis given by ref; else from htwo or bt. */
+int oracle_buildhsg_ex(const zc *hone, const zc *htwo, const zc *bt, const double *bs, int nchol, const zc *ref,
+                       const zc *z, const int *ngrid, int nci, int cmplxconj, int ncisp, int nocc, const zc *r1,
+                       const zc *r2, const zc *rpg, const double *weightsp, const double *weightpg,
+                       const double *roota, const double *rootb, const double *rooty, int qj, int sp, int npg,
+                       int ncipg, int nso, const int *omega_list, int n_omega, int nthreads, zc *hmat, zc *smat,
+                       zc *gradmat, zc *rdmmat)
 {
     const int M = nso, N = nocc, nl = ngrid[0], ny = ngrid[1];
     const size_t MM = (size_t)M * M;
     const int nw = 2 * qj + 1;
     if (nw != ncisp && sp == 1) return -1;
-    ham_t H = {M, N, nchol, hone, htwo, bt};
+    ham_t H = {M, N, nchol, hone, htwo, bt, bs, ref};
     zc *newmo = calloc((size_t)M * N, sizeof(zc));
     for (int i = 0; i < N; ++i) newmo[IDX2(i, i, M)] = 1.0;
     for (int j = 0; j < N; ++j)
@@ -260,6 +368,9 @@ int oracle_buildhsg(const zc *hone, const zc *htwo, const zc *bt, int nchol, con
 #ifdef _OPENMP
     nth = nthreads > 0 ? nthreads : omp_get_max_threads();
 #endif
+    /* fewer points than threads: the points run one after another, each split over the threads */
+    g_inner = (npts < nth) ? nth : 1;
+    if (g_inner > 1) nth = 1;
     zc *th_h = calloc(acc_scalar * nth, sizeof(zc)), *th_s = calloc(acc_scalar * nth, sizeof(zc));
     zc *th_g = calloc(acc_mat * nth, sizeof(zc)), *th_r = calloc(acc_mat * nth, sizeof(zc));
     int status = 0;
@@ -366,7 +477,20 @@ int oracle_buildhsg(const zc *hone, const zc *htwo, const zc *bt, int nchol, con
             }
     }
     free(th_h); free(th_s); free(th_g); free(th_r); free(newmo);
+    g_inner = 1;
     return status;
+}
+
+int oracle_buildhsg(const zc *hone, const zc *htwo, const zc *bt, int nchol, const zc *ref, const zc *z,
+                    const int *ngrid, int nci, int cmplxconj, int ncisp, int nocc, const zc *r1, const zc *r2,
+                    const zc *rpg, const double *weightsp, const double *weightpg, const double *roota,
+                    const double *rootb, const double *rooty, int qj, int sp, int npg, int ncipg, int nso,
+                    const int *omega_list, int n_omega, int nthreads, zc *hmat, zc *smat, zc *gradmat,
+                    zc *rdmmat)
+{
+    return oracle_buildhsg_ex(hone, htwo, bt, NULL, nchol, ref, z, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg,
+                              weightsp, weightpg, roota, rootb, rooty, qj, sp, npg, ncipg, nso, omega_list, n_omega,
+                              nthreads, hmat, smat, gradmat, rdmmat);
 }
 
 /* LocalG (PHFTools.f90:203-247) */

@@ -28,6 +28,7 @@ def lib():
         build()
         _lib = ctypes.CDLL(LIB_PATH)
         _lib.oracle_buildhsg.restype = ctypes.c_int
+        _lib.oracle_buildhsg_ex.restype = ctypes.c_int
         _lib.oracle_localg.restype = ctypes.c_int
         _lib.oracle_num_threads.restype = ctypes.c_int
     return _lib
@@ -42,16 +43,19 @@ def _p(a):
 
 
 def buildhsg(HOne, HTwo, Ref, Z, ngrid, nci, CmplxConj, ncisp, NOcc, R1, R2, Rpg, weightsp, weightpg,
-             roota, rootb, rooty, QJ, SP, npg, ncipg, NSO, Bt=None, omega_list=None, nthreads=0):
+             roota, rootb, rooty, QJ, SP, npg, ncipg, NSO, Bt=None, Bs=None, omega_list=None, nthreads=0):
     """Same contract as oracle.phf_oracle.buildhsg.  ``Bt`` (M, M, L) are MO-basis Cholesky
-    vectors used instead of HTwo when HTwo is None.  ``omega_list``: flattened grid-point
-    indices ((il*ny + iy)*npg + ipg) to restrict the sum."""
+    vectors used instead of HTwo when HTwo is None; ``Bs`` (L, n, n) are the real spatial
+    Cholesky vectors in the AO basis (the MO basis is Ref), used instead of both.  ``omega_list``:
+    flattened grid-point indices ((il*ny + iy)*npg + ipg) to restrict the sum.  With fewer
+    points than threads each point's work is split over the threads."""
     M = NSO
     keep = []
     hone = _f(HOne)
     htwo = _f(HTwo) if HTwo is not None else None
     bt = _f(Bt) if Bt is not None else None
-    nchol = 0 if Bt is None else Bt.shape[2]
+    bs = _f(np.transpose(Bs, (1, 2, 0)), np.float64) if Bs is not None else None
+    nchol = Bt.shape[2] if Bt is not None else (Bs.shape[0] if Bs is not None else 0)
     ref, z = _f(Ref), _f(Z)
     r1, r2, rpg = _f(R1), _f(R2), _f(Rpg)
     wsp, wpg = _f(weightsp, np.float64), _f(weightpg, np.float64)
@@ -62,9 +66,9 @@ def buildhsg(HOne, HTwo, Ref, Z, ngrid, nci, CmplxConj, ncisp, NOcc, R1, R2, Rpg
     smat = np.zeros((nci, nci), dtype=np.complex128, order="F")
     gmat = np.zeros((nci, nci, M, M), dtype=np.complex128, order="F")
     rmat = np.zeros((nci, nci, M, M), dtype=np.complex128, order="F")
-    keep += [hone, htwo, bt, ref, z, r1, r2, rpg, wsp, wpg, ra, rb, ry, ng, ol]
-    st = lib().oracle_buildhsg(
-        _p(hone), _p(htwo), _p(bt), ctypes.c_int(nchol), _p(ref), _p(z), _p(ng), ctypes.c_int(nci),
+    keep += [hone, htwo, bt, bs, ref, z, r1, r2, rpg, wsp, wpg, ra, rb, ry, ng, ol]
+    st = lib().oracle_buildhsg_ex(
+        _p(hone), _p(htwo), _p(bt), _p(bs), ctypes.c_int(nchol), _p(ref), _p(z), _p(ng), ctypes.c_int(nci),
         ctypes.c_int(CmplxConj), ctypes.c_int(ncisp), ctypes.c_int(NOcc), _p(r1), _p(r2), _p(rpg), _p(wsp),
         _p(wpg), _p(ra), _p(rb), _p(ry), ctypes.c_int(QJ), ctypes.c_int(SP), ctypes.c_int(npg), ctypes.c_int(ncipg),
         ctypes.c_int(NSO), _p(ol), ctypes.c_int(0 if ol is None else len(ol)), ctypes.c_int(nthreads),

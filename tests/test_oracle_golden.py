@@ -76,3 +76,24 @@ def test_c_oracle_cholesky_mode(name):
     for x, key in zip((Hm, Sm, Gm, Rm), ("Hmat", "Smat", "Gradmat", "Rdmmat")):
         ref = c[key]
         assert np.abs(x - ref).max() <= 1e-11 * max(1.0, np.abs(ref).max()), key
+
+
+@pytest.mark.parametrize("name", ["tiny_sp1", "cmplx2", "j1_c2v_b1", "c1"])
+def test_c_oracle_spatial_cholesky_mode(name):
+    """The spatial (AO-basis, real B_L) Cholesky form of the C oracle, with the grid points in
+    parallel and with one point at a time split over the threads, against the golden vectors."""
+    from oracle import phf_oracle_c as corc
+    c = load(name)
+    kw = grid_kwargs(c)
+    npts = kw["ngrid"][0] * kw["ngrid"][1] * kw["npg"]
+    sub = np.arange(0, npts, max(1, npts // 3))[:3]
+    full = corc.buildhsg(c["HOne"], None, c["Ref"], c["Z"], Bs=c["B"], nthreads=2, **kw)
+    for x, key in zip(full, ("Hmat", "Smat", "Gradmat", "Rdmmat")):
+        ref = c[key]
+        assert np.abs(x - ref).max() <= 1e-11 * max(1.0, np.abs(ref).max()), key
+    # a 3-point subset on 4 threads (one point at a time, split inside) against the MO-basis form
+    Bt = np.transpose(orc.chol_spin_orbital(c["B"], c["Ref"]), (1, 2, 0))
+    a = corc.buildhsg(c["HOne"], None, c["Ref"], c["Z"], Bs=c["B"], omega_list=sub, nthreads=4, **kw)
+    b = corc.buildhsg(c["HOne"], None, c["Ref"], c["Z"], Bt=Bt, omega_list=sub, nthreads=1, **kw)
+    for x, y in zip(a, b):
+        assert np.abs(x - y).max() <= 1e-12 * max(1.0, np.abs(y).max())

@@ -107,11 +107,15 @@ typedef struct {
     const double *weightsp, *weightpg, *roota, *rootb, *rooty;
     int precision;                            /* enum phf_precision */
     int slices;                               /* int8 slices per operand for PHF_PREC_OZAKI_I8 (0 = default) */
-    size_t workspace_bytes;                   /* per-chunk workspace budget (0 = default 6 GiB) */
+    size_t workspace_bytes;                   /* per-chunk workspace budget (0 = default: 6 GiB, or 45 % of
+                                                 the free device memory for jk_form 3 when that is more) */
     int jk_form;                              /* Cholesky form only: 0 = automatic, 1 = exchange through the
-                                                 spatial ERI matrix (n^2 x n^2, built once per plan),
-                                                 2 = factorized (no n^4 tensor); automatic picks 1 for n <= 128
-                                                 and for the int8 precision at every n, else 2 */
+                                                 spatial ERI matrix (n^2 x n^2, built once per plan and kept),
+                                                 2 = factorized (rank-N, no n^4 tensor, FP64 only),
+                                                 3 = streamed: the exchange rows regenerated from the Cholesky
+                                                 vectors panel by panel in every chunk, each panel used
+                                                 against the whole chunk (no n^4 tensor; memory of one panel);
+                                                 automatic picks 1 for n <= 128, else 3 */
     int gradient_mode;                        /* phf_plan_eval_device only: 0 = the reference's gradient
                                                  (bra-side derivative, Gradient/LocalG of PHFTools.f90);
                                                  1 = exact dE/dC* of E = Re H/|Re S|, adding the ket-side
@@ -123,6 +127,9 @@ typedef struct {
                                                  flattened order (il*ngrid[1] + iy)*npg + ipg; 0, 0 = all.
                                                  Partial sums over disjoint ranges add up to the full sums
                                                  (the rank split of PHFTools.f90:53-57) */
+    int exchange_panel;                       /* jk_form 3: spatial indices i per exchange panel (rows (i, k)
+                                                 of the exchange matrix formed at once); 0 = automatic
+                                                 (at most 4096 rows, fewest padded rows) */
 } phf_plan_desc;
 
 int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);
@@ -184,20 +191,22 @@ int phf_tc_dgemm(int m, int n, int k, int precision, int slices, const double *d
                  long long ldb, double *dD, long long ldd, void *stream);
 
 /* The same product as phf_ozaki_dgemm for callers that cannot allocate device memory at the
- * point of the call: code that runs while another component is capturing a CUDA graph,
- * programs whose device memory is owned by another allocator (a framework's caching pool, a
- * fixed arena reserved at start-up), and loops that must never enter the driver's allocator.
- * No counterpart in the reference.  Scratch (int8 slices, exponents, error flag) lives in one
- * static device array of 32 MiB that every GPU loading this library holds until exit; sizes
- * needing more (see phf_ozaki_dgemm_noalloc_scratch_bytes) return PHF_ERR_UNSUPPORTED.  No
- * cudaMalloc/cudaFree or allocating library call is made.  All calls share the array and it
- * keeps the last call's contents (the parts that must start at zero are cleared on each call):
- * calls that overlap on the GPU race.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress, with that device current); make that first call before any
- * stream capture.  Synchronous on `stream`. */
+ * point of the call: programs whose device memory belongs to another allocator (a framework's
+ * caching pool, or a fixed arena reserved at start-up, where a cudaMalloc of this library's own
+ * would fail or split the pool), and loops that must never enter the driver's allocator (cudaMalloc
+ * and cudaFree can synchronize the device).  No counterpart in the reference.  Scratch (int8
+ * slices, exponents, error flag) lives in one static device array of 32 MiB that every GPU loading
+ * this library holds until exit; sizes needing more (see phf_ozaki_dgemm_noalloc_scratch_bytes)
+ * return PHF_ERR_UNSUPPORTED.  No cudaMalloc/cudaFree or allocating library call is made.  All
+ * calls share the array and it keeps the last call's contents (the parts that must start at zero
+ * are cleared on each call): calls that overlap on the GPU race.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture.  Synchronous on `stream`; a failed synchronisation is reported
+ * as PHF_ERR_CUDA with the message "stream synchronize failed", as for phf_ozaki_dgemm. */
 int phf_ozaki_dgemm_noalloc(int m, int n, int k, int slices, const double *dA, long long lda, const double *dBt,
                             long long ldb, double *dD, long long ldd, void *stream);
-/* Scratch bytes phf_ozaki_dgemm_noalloc needs for these sizes. */
+/* Scratch bytes phf_ozaki_dgemm_noalloc needs for these sizes; 0 for arguments it rejects
+ * (m, n or k below 1, slices outside 1..7). */
 size_t phf_ozaki_dgemm_noalloc_scratch_bytes(int m, int n, int k, int slices);
 
 /* ---------------------------------------------------------------- diagnostics */

@@ -46,6 +46,7 @@ class phf_plan_desc(ctypes.Structure):
         ("fp64_library_gemm", ctypes.c_int),
         ("point_begin", ctypes.c_int),
         ("point_end", ctypes.c_int),
+        ("exchange_panel", ctypes.c_int),
     ]
 
 

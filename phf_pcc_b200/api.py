@@ -170,14 +170,17 @@ class Plan:
     "ozaki_i8" (FP64-accurate int8 tensor-core slices, ``slices`` per operand, default 5),
     "bf16x3" (split BF16, three products) or "tf32" (both FP32-accumulated in 512-element segments
     summed in FP64; about 1e-6 relative, far from FP64); ``jk_form``: "auto", "eri"
-    (exchange through the n^2 x n^2 spatial ERI matrix) or "factorized"; ``gradient``: "reference"
-    (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the ket-side term;
-    used by autograd)."""
+    (exchange through the n^2 x n^2 spatial ERI matrix, built once and kept), "streamed" (the same
+    exchange rows regenerated from the Cholesky vectors panel by panel in every chunk: no n^4
+    tensor, ``exchange_panel`` spatial indices per panel, 0 = automatic) or "factorized" (rank-N
+    J/K, FP64 only); "auto" takes "eri" up to n = 128 and "streamed" above.  ``gradient``:
+    "reference" (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the
+    ket-side term; used by autograd)."""
 
     def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
                  rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
                  workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False,
-                 point_range=None, npg=None, ncipg=None, nso=None):
+                 point_range=None, npg=None, ncipg=None, nso=None, exchange_panel=0):
         self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
                         sp, npg, ncipg, nso)
         g = self._g
@@ -199,7 +202,9 @@ class Plan:
         d.precision = PREC[precision]
         d.slices = int(slices)
         d.workspace_bytes = int(workspace_bytes)
-        d.jk_form = {"auto": 0, "eri": 1, "factorized": 2}[jk_form]
+        d.jk_form = {"auto": 0, "eri": 1, "factorized": 2, "streamed": 3}[jk_form]
+        d.exchange_panel = int(exchange_panel)
+        self.jk_form = jk_form
         d.gradient_mode = {"reference": 0, "exact": 1}[gradient]
         d.fp64_library_gemm = 1 if fp64_library_gemm else 0
         if point_range is not None:

@@ -232,6 +232,8 @@ struct OzArgs {
     int kb_total;        // k-blocks of this launch over all splits
     int kseg;            // floating-point formats: k-blocks per FP32 accumulation segment (>= 1)
     int gamma_n;         // > 0: exchange-to-Gamma output (see store_row_chunk), n spatial orbitals
+    int g_row0;          // exchange-to-Gamma output: global row of output row 0 (a panel of the exchange rows)
+    int a_row0;          // A tiles are read from row a_row0 + m0 of the A slice buffer (a row range of it)
     int *err;
 };
 
@@ -245,7 +247,7 @@ __device__ __forceinline__ void store_row_chunk(const OzArgs &args, double *Dz, 
                                                 const double (&acc)[32], double rowscale, const double *cs,
                                                 bool add) {
     if (args.gamma_n > 0) {
-        const int gn = args.gamma_n, M = 2 * gn, i = row / gn, k = row - i * gn;
+        const int gn = args.gamma_n, M = 2 * gn, grow = args.g_row0 + row, i = grow / gn, k = grow - i * gn;
 #pragma unroll
         for (int j = 0; j < 32; j += 2) {
             const int col = col0 + j;
@@ -508,6 +510,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         m0 = (first + (L % width) % gm) * OZ_BM;
         n0 = ((L % width) / gm) * BN;
     }
+    const int am0 = m0 + args.a_row0;           // first row of the A tile in the A slice buffer
     const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
     const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
     double *const Dz = args.D + (long long)blockIdx.z * args.dz;
@@ -560,10 +563,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 }
                 unsigned char *dst = smem + (size_t)sg * PITCH;
                 mbar_arrive_expect_tx(&full_bar[sg], BYTES);
-                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, m0);
+                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
                 tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
                 if constexpr (W1 == 1) {
-                    tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, m0);
+                    tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
                     tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
                 }
                 if (++sg == NS) {
@@ -591,14 +594,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                                                             : j == 2 ? oz_unit_bytes(S, 2) : oz_unit_bytes(S, 3);
                         mbar_arrive_expect_tx(&full_bar[u], ub);
                         if (j == 0) {
-                            tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, m0);
+                            tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, am0);
                         } else if (j == 1) {
                             tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, n0);
                         } else if (W1 <= 2) {  // j == 2: A and B of group 1 at 32- or 64-byte rows
-                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 32 * W1, m0);
+                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 32 * W1, am0);
                             tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 32 * W1, kbg * 32 * W1, n0);
                         } else if (j == 2) {
-                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, m0);
+                            tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, am0);
                         } else {
                             tma_load_2d(&tmB1, &full_bar[u], dst, kbg * 128, n0);
                         }
@@ -946,6 +949,36 @@ __global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *
     }
 }
 
+// Rows of one panel of the exchange matrix, EK[(i, k), (l, j)] = (il|kj) for i in [i0, i0 + I),
+// from the panel's Gram block G[(i - i0) n + l][k n + j] = sum_L B_L[i][l] B_L[k][j] (row stride ldg):
+// slice row r = (i - i0) n + k holds EK[(i, k), (l, j)] at k-index l n + j.  For fixed l the n
+// values j are contiguous in G, so the reads run in coalesced segments of n doubles.
+__global__ void __launch_bounds__(SL_NT) slice_ek_panel_kernel(int n, const double *G, long long ldg, int S,
+                                                               long long rows_pad, long long kpad, signed char *out,
+                                                               int *ea) {
+    __shared__ double sh[SL_NT];
+    const long long r = blockIdx.x;
+    const int il = (int)(r / n), k = (int)(r - (long long)il * n);
+    const double *g = G + (long long)il * n * ldg + (long long)k * n;  // + l ldg + j
+    const int kk = n * n;
+    double mx = 0.0;
+    for (int e = threadIdx.x; e < kk; e += SL_NT) {
+        const int l = e / n, j = e - l * n;
+        mx = fmax(mx, fabs(g[(long long)l * ldg + j]));
+    }
+    mx = block_max(mx, sh);
+    const int ex = exp_of_max(mx);
+    if (threadIdx.x == 0) ea[r] = ex;
+    const SliceScale sc = slice_scale(ex, S);
+    for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
+        double x = 0.0;
+        if (e < kk) {
+            const int l = (int)(e / n), j = (int)(e - (long long)l * n);
+            x = g[(long long)l * ldg + j];
+        }
+        slice_value(x, sc, S, out, r, rows_pad, kpad >> 5, e);
+    }
+}
 
 // ------------------------------------------------------------------ fused density + operand slicing
 // D (8 x 8) += A (8 x 4, row-major) B (4 x 8, column-major), FP64 tensor cores.
@@ -1282,6 +1315,21 @@ int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int 
     return PHF_OK;
 }
 
+int oz_slice_ek_panel(int n, int ipanel, const double *G, long long ldg, int S, long long rows_pad, signed char *out,
+                      int *ea, cudaStream_t st) {
+    const long long rows = (long long)ipanel * n;
+    if (rows <= 0 || rows > rows_pad) {
+        set_error(PHF_ERR_ARG, "oz_slice_ek_panel: panel rows outside the slice buffer");
+        return PHF_ERR_ARG;
+    }
+    ProfScope prof(st, PROF_MEMORY);
+    slice_ek_panel_kernel<<<(unsigned)rows, SL_NT, 0, st>>>(n, G, ldg, S, rows_pad, oz_pad_k((long long)n * n), out,
+                                                            ea);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 bool oz_rho_slice_ok(int n) { return n >= 1 && n <= 64; }
 
 int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra, int S, signed char *Ksl, int *eK,
@@ -1414,6 +1462,8 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kb_total = (int)kb_total;
     a.kseg = OZ_KSEG;
     a.gamma_n = 0;
+    a.g_row0 = 0;
+    a.a_row0 = 0;
     a.S = S;
     a.ea = ea;
     a.eb = eb;
@@ -1448,8 +1498,18 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n) {
-    if (gamma_n > 0 && (m != gamma_n * gamma_n || n % 8 != 0)) {
-        set_error(PHF_ERR_ARG, "oz_gemm: the Gamma output needs m = n^2 rows and 8 columns per point");
+    return oz_gemm_ex(m, n, k, S, Asl, oz_pad_rows(m), 0, ea, Bsl, eb, D, ldd, accumulate, trans, err, st, gamma_n, 0);
+}
+
+int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,
+               const signed char *Bsl, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
+               cudaStream_t st, int gamma_n, int g_row0) {
+    if (gamma_n > 0 && (g_row0 < 0 || (long long)g_row0 + m > (long long)gamma_n * gamma_n || n % 8 != 0)) {
+        set_error(PHF_ERR_ARG, "oz_gemm: the Gamma output needs rows within [0, n^2) and 8 columns per point");
+        return PHF_ERR_ARG;
+    }
+    if (a_row0 < 0 || (long long)a_row0 + m > a_rows_pad) {
+        set_error(PHF_ERR_ARG, "oz_gemm: A row range outside its slice buffer");
         return PHF_ERR_ARG;
     }
     if (!oz_format_ok(S)) {
@@ -1458,7 +1518,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
     }
     CUtensorMap ta0, ta1, tb0, tb1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
-    PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
+    PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, a_rows_pad, S, OZ_BM));
     PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
     const long long kb_pass = oz_kb_pass(S);
     const long long kb_total = kpad / OZ_BK;
@@ -1477,7 +1537,7 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.kb0 = (int)kb0;
         a.kblocks = (int)std::min(kb_pass, kb_total - kb0);
         a.S = S;
-        a.ea = ea;
+        a.ea = ea + a_row0;
         a.eb = eb;
         a.D = D;
         a.ldd = ldd;
@@ -1487,6 +1547,8 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
         a.kb_total = a.kblocks;
         a.kseg = OZ_KSEG;
         a.gamma_n = gamma_n;
+        a.g_row0 = g_row0;
+        a.a_row0 = a_row0;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);

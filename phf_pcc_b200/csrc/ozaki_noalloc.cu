@@ -1,10 +1,11 @@
 // FP64-accurate int8 GEMM for callers that cannot allocate device memory.
 //
 // Some callers of this library cannot call cudaMalloc at the point where they need a product:
-// code running while a CUDA graph is being captured by someone else, applications whose
-// device-memory pool is owned by another allocator (a framework caching allocator, a
-// fixed arena set up at start), and latency-critical loops that must not enter the driver's
-// allocator.  phf_ozaki_dgemm_noalloc computes the same product as phf_ozaki_dgemm but keeps
+// applications whose device-memory pool is owned by another allocator (a framework caching
+// allocator, a fixed arena set up at start, where an allocation of this library's own would
+// fail or split the pool), and latency-critical loops that must not enter the driver's
+// allocator (cudaMalloc and cudaFree can synchronize the device).  phf_ozaki_dgemm_noalloc
+// computes the same product as phf_ozaki_dgemm but keeps
 // its scratch (the int8 slices of both operands, their power-of-two exponents and the
 // pipeline error flag) in one file-scope device array of kNoAllocScratchBytes, which every
 // GPU that loads this library holds until the process exits.  The caller still provides A, B
@@ -61,6 +62,7 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 extern "C" size_t phf_ozaki_dgemm_noalloc_scratch_bytes(int m, int n, int k, int slices) {
     using namespace phf;
+    if (m <= 0 || n <= 0 || k <= 0 || slices < 1 || slices > 7) return 0;
     const long long mp = oz_pad_rows(m), np = oz_pad_cols(n);
     return align256(oz_slice_bytes(mp, k, slices)) + align256(oz_slice_bytes(np, k, slices)) + align256(mp * sizeof(int)) +
            align256(np * sizeof(int)) + align256(sizeof(int));
@@ -101,9 +103,12 @@ extern "C" int phf_ozaki_dgemm_noalloc(int m, int n, int k, int slices, const do
     PHF_TRY(oz_gemm(m, n, k, slices, As, ea, Bs, eb, dD, ldd, 0, err, st));
     int herr = 0;
     PHF_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PHF_CUDA(cudaStreamSynchronize(st));
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm_noalloc: stream synchronize failed");
+        return PHF_ERR_CUDA;
+    }
     if (herr) {
-        set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm_noalloc: tensor-core pipeline wait timed out");
+        set_error(PHF_ERR_CUDA, "phf_ozaki_dgemm_noalloc: pipeline wait timed out");
         return PHF_ERR_CUDA;
     }
     return PHF_OK;

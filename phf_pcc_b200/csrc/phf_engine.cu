@@ -232,11 +232,16 @@ int validate(const phf_plan_desc *d) {
         return PHF_ERR_ARG;
     }
     if (d->gradient_mode == 1 && (d->nchol <= 0 || d->jk_form == 2 || d->nci != 1 || d->cmplxconj == 2)) {
-        set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs the spatial-ERI form, nci == 1 and cmplxconj 0/1");
+        set_error(PHF_ERR_UNSUPPORTED,
+                  "the exact gradient needs an exchange-matrix form (stored or streamed), nci == 1 and cmplxconj 0/1");
         return PHF_ERR_UNSUPPORTED;
     }
-    if (d->jk_form < 0 || d->jk_form > 2) {
-        set_error(PHF_ERR_ARG, "jk_form must be 0, 1 or 2");
+    if (d->jk_form < 0 || d->jk_form > 3) {
+        set_error(PHF_ERR_ARG, "jk_form must be 0, 1, 2 or 3");
+        return PHF_ERR_ARG;
+    }
+    if (d->exchange_panel < 0) {
+        set_error(PHF_ERR_ARG, "exchange_panel must be >= 0");
         return PHF_ERR_ARG;
     }
     return PHF_OK;
@@ -247,6 +252,23 @@ int validate(const phf_plan_desc *d) {
 namespace {
 int build_exchange_matrix(PlanImpl &p);
 constexpr int kDSplit = 4;  // split-k of the Coulomb GEMM d = B vec P (small output, k = n^2)
+
+// Spatial indices i per exchange panel of the streamed form: panels of at most 4096 exchange rows
+// (i, k), with the fewest padded rows over all panels (GEMM tiles are 128 rows), ties to the larger
+// panel (fewer launches).  n = 200: 16 (12 panels of 3200 rows and one of 1600).
+int choose_ipanel(int n) {
+    int best = 1;
+    long long best_rows = -1;
+    for (int I = 1; I <= n && (long long)I * n <= std::max<long long>(4096, n); ++I) {
+        const long long full = n / I, rest = n % I;
+        const long long rows = full * oz_pad_rows((long long)I * n) + (rest ? oz_pad_rows(rest * n) : 0);
+        if (best_rows < 0 || rows <= best_rows) {
+            best_rows = rows;
+            best = I;
+        }
+    }
+    return best;
+}
 }  // namespace
 
 int plan_create(const phf_plan_desc *d, phf_plan **out) {
@@ -265,10 +287,15 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     p.slices = p.prec == PHF_PREC_BF16X3 ? OZ_FMT_BF16X3
              : p.prec == PHF_PREC_TF32  ? OZ_FMT_TF32
                                         : (d->slices > 0 ? d->slices : 5);
-    // automatic form: the spatial-ERI exchange matrix for n <= 128, and at every size for the
-    // tensor-core precisions (which need it); the factorized form for FP64 above n = 128
-    if (p.chol)
-        p.eri = (d->jk_form == 1) || (d->jk_form == 0 && (d->nso / 2 <= 128 || p.prec != PHF_PREC_FP64));
+    // automatic form: the stored spatial-ERI exchange matrix for n <= 128 (n^4 doubles: 2.1 GB at
+    // n = 128); above, the streamed form, which regenerates the exchange rows panel by panel from the
+    // Cholesky vectors instead of holding the n^4 matrix (the factorized form has ~3L/(4n) times the
+    // flops of either and is chosen only explicitly)
+    if (p.chol) {
+        const int form = d->jk_form != 0 ? d->jk_form : (d->nso / 2 <= 128 ? 1 : 3);
+        p.eri = (form == 1 || form == 3);
+        p.streamed = (form == 3);
+    }
     p.exact = d->gradient_mode == 1;
     p.library_gemm = (d->fp64_library_gemm != 0) && p.eri && p.prec == PHF_PREC_FP64;
     if (p.library_gemm) {
@@ -280,12 +307,17 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         p.cublas = h;
     }
     if (p.exact && !p.eri) {
-        set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs the spatial-ERI exchange form (n <= 128 or jk_form 1)");
+        set_error(PHF_ERR_UNSUPPORTED, "the exact gradient needs an exchange-matrix form (jk_form 0, 1 or 3)");
         return PHF_ERR_UNSUPPORTED;
     }
     if (p.prec != PHF_PREC_FP64 && !p.eri) {
-        set_error(PHF_ERR_UNSUPPORTED, "the tensor-core precisions need the spatial-ERI exchange form (jk_form 0/1)");
+        set_error(PHF_ERR_UNSUPPORTED, "the tensor-core precisions need an exchange-matrix form (jk_form 0, 1 or 3)");
         return PHF_ERR_UNSUPPORTED;
+    }
+    if (p.streamed) {
+        const int n = d->nso / 2;
+        p.ek_ipanel = d->exchange_panel > 0 ? std::min(d->exchange_panel, n) : choose_ipanel(n);
+        p.ek_npanel = (n + p.ek_ipanel - 1) / p.ek_ipanel;
     }
     p.nl = d->ngrid[0];
     p.ny = d->ngrid[1];
@@ -508,9 +540,16 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     }
     PHF_TRY(p.arena.alloc(&p.flag, 1));
 
-    // chunk size from the workspace budget
+    // chunk size from the workspace budget.  The streamed form regenerates its exchange rows once
+    // per chunk (2 n^4 L flops against 16 n^4 per point), so by default it takes up to 45 % of the
+    // free device memory to keep the chunk (and the regeneration's share, L / (8 b)) large.
     {
-        const size_t budget = d->workspace_bytes ? d->workspace_bytes : ((size_t)6 << 30);
+        size_t budget = d->workspace_bytes ? d->workspace_bytes : ((size_t)6 << 30);
+        if (!d->workspace_bytes && p.streamed) {
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) budget = std::max(budget, (size_t)(0.45 * (double)fr));
+            cudaGetLastError();
+        }
         size_t per = 5 * MN + 3 * (size_t)N * N + 8;
         const size_t n2 = (size_t)n * n;
         if (p.chol && p.eri) {
@@ -526,7 +565,6 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         }
         if (p.exact) per += 5 * MN;
         per *= sizeof(zc);
-        per += split_bytes_per_point(p);
         long long bmax = (long long)(budget / std::max<size_t>(per, 1));
         bmax = std::max<long long>(1, std::min<long long>(bmax, 4096));
         p.b = (int)std::min<long long>(bmax, p.wend - p.wbeg);
@@ -596,7 +634,6 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         PHF_TRY(p.arena.alloc(&p.Pv, (size_t)p.b * MM));
         PHF_TRY(p.arena.alloc(&p.Gv, (size_t)p.b * MM));
     }
-    PHF_TRY(split_setup(p));
     *out = P.release();
     return PHF_OK;
 }
@@ -606,9 +643,45 @@ namespace {
 // EK[(i n + k) n^2 + (l n + j)] = sum_L B_L[i][l] B_L[k][j] = (il|kj): the exchange operator
 // K(rho)_ik = sum_{lj} (il|jk) rho_lj as an n^2 x n^2 matrix acting on vec(rho) (built as n^2
 // batched n x n x L products); sliced (int8 digits, BF16 pairs or TF32) for the tensor-core back-end.
+// Coulomb operands of the tensor-core path: B (L x n^2, rows of Bst) and B^T (n^2 x L, strided rows of
+// Bst).  B^T's slices are also both operands of the streamed form's Gram blocks.
+int build_coulomb_slices(PlanImpl &p) {
+    const int n = p.n, L = p.L;
+    const long long n2 = (long long)n * n;
+    PHF_TRY(p.arena.alloc(&p.ozerr, 1));
+    PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
+    const size_t b1 = oz_slice_bytes(oz_pad_rows(L), n2, p.slices);
+    const size_t b2 = oz_slice_bytes(oz_pad_rows(n2), L, p.slices);
+    PHF_TRY(p.arena.alloc(&p.B1sl, b1));
+    PHF_TRY(p.arena.alloc(&p.B2sl, b2));
+    PHF_CUDA(cudaMemset(p.B1sl, 0, b1));
+    PHF_CUDA(cudaMemset(p.B2sl, 0, b2));
+    PHF_TRY(p.arena.alloc(&p.eB1, (size_t)oz_pad_rows(L)));
+    PHF_TRY(p.arena.alloc(&p.eB2, (size_t)oz_pad_rows(n2)));
+    PHF_TRY(oz_slice_rows_strided(L, (int)n2, p.Bst, n2, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
+    PHF_TRY(oz_slice_rows_strided((int)n2, L, p.Bst, 1, n2, p.slices, oz_pad_rows(n2), p.B2sl, p.eB2, 0));
+    return PHF_OK;
+}
+
 int build_exchange_matrix(PlanImpl &p) {
     const int n = p.n, L = p.L;
     const long long n2 = (long long)n * n;
+    if (p.streamed) {  // buffers of one exchange panel; the rows themselves are formed per chunk
+        const long long rows = (long long)p.ek_ipanel * n;
+        PHF_TRY(p.arena.alloc(&p.Gp, (size_t)(rows * n2)));
+        if (p.prec == PHF_PREC_FP64) {
+            PHF_TRY(p.arena.alloc(&p.EKp, (size_t)(rows * n2)));
+        } else {
+            const size_t bytes = oz_slice_bytes(oz_pad_rows(rows), n2, p.slices);
+            PHF_TRY(p.arena.alloc(&p.EKpsl, bytes));
+            PHF_CUDA(cudaMemset(p.EKpsl, 0, bytes));
+            PHF_TRY(p.arena.alloc(&p.eEKp, (size_t)oz_pad_rows(rows)));
+            PHF_CUDA(cudaMemset(p.eEKp, 0, (size_t)oz_pad_rows(rows) * sizeof(int)));
+            PHF_TRY(build_coulomb_slices(p));
+        }
+        PHF_CUDA(cudaDeviceSynchronize());
+        return PHF_OK;
+    }
     double *EK = nullptr;
     PHF_TRY(p.arena.alloc(&EK, (size_t)(n2 * n2)));
     OutView o = vo(reinterpret_cast<zc *>(EK), n, 1, n2, n2 * n);
@@ -620,20 +693,8 @@ int build_exchange_matrix(PlanImpl &p) {
         PHF_TRY(p.arena.alloc(&p.EKsl, bytes));
         PHF_CUDA(cudaMemset(p.EKsl, 0, bytes));
         PHF_TRY(p.arena.alloc(&p.ea, (size_t)oz_pad_rows(n2)));
-        PHF_TRY(p.arena.alloc(&p.ozerr, 1));
-        PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
         PHF_TRY(oz_slice_rows((int)n2, (int)n2, EK, n2, p.slices, oz_pad_rows(n2), p.EKsl, p.ea, 0));
-        // Coulomb operands: B (L x n^2, rows of Bst) and B^T (n^2 x L, strided rows of Bst)
-        const size_t b1 = oz_slice_bytes(oz_pad_rows(L), n2, p.slices);
-        const size_t b2 = oz_slice_bytes(oz_pad_rows(n2), L, p.slices);
-        PHF_TRY(p.arena.alloc(&p.B1sl, b1));
-        PHF_TRY(p.arena.alloc(&p.B2sl, b2));
-        PHF_CUDA(cudaMemset(p.B1sl, 0, b1));
-        PHF_CUDA(cudaMemset(p.B2sl, 0, b2));
-        PHF_TRY(p.arena.alloc(&p.eB1, (size_t)oz_pad_rows(L)));
-        PHF_TRY(p.arena.alloc(&p.eB2, (size_t)oz_pad_rows(n2)));
-        PHF_TRY(oz_slice_rows_strided(L, (int)n2, p.Bst, n2, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
-        PHF_TRY(oz_slice_rows_strided((int)n2, L, p.Bst, 1, n2, p.slices, oz_pad_rows(n2), p.B2sl, p.eB2, 0));
+        PHF_TRY(build_coulomb_slices(p));
     }
     PHF_CUDA(cudaDeviceSynchronize());
     if (p.prec == PHF_PREC_FP64) {
@@ -641,6 +702,64 @@ int build_exchange_matrix(PlanImpl &p) {
     } else {
         p.arena.free_one(EK);  // the tensor-core back-end only needs its slices
         p.EK = nullptr;
+    }
+    return PHF_OK;
+}
+
+// Exchange term of the streamed form for one chunk.  For each panel of ek_ipanel spatial indices i:
+// the Gram block G[(i, l)][(k, j)] = sum_L B_L[i][l] B_L[k][j] (rows (i, l) of B^T times B, k-dim L),
+// its rows rearranged into the exchange rows EK[(i, k)][(l, j)] = (il|kj), and those rows times the
+// chunk's density columns.  FP64 form: the panel's exchange rows times the gathered density blocks
+// Kin into the matching rows of Kvec.  Tensor-core forms: the panel is sliced, and the product's
+// epilogue writes -K of the panel's rows straight into Gamma.  The Gram block costs 2 n^2 ipanel L
+// flops per panel (2 n^4 L per chunk against 16 n^4 per grid point).
+int exchange_streamed(PlanImpl &p, int bc, cudaStream_t st) {
+    const int n = p.n, L = p.L, b = p.b;
+    const long long n2 = (long long)n * n, prow = (long long)p.ek_ipanel * n;
+    for (int pi = 0; pi < p.ek_npanel; ++pi) {
+        const int i0 = pi * p.ek_ipanel, ip = std::min(p.ek_ipanel, n - i0);
+        const int rows = ip * n;
+        if (p.prec == PHF_PREC_FP64) {
+            if (p.library_gemm) {
+                cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
+                const double one = 1.0, zero = 0.0;
+                ProfScope prof(st, PROF_JK);
+                // column-major: G^T (n^2 x rows) = (B^T) (n^2 x L) * (rows of B^T)^T
+                if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS ||
+                    cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)n2, rows, L, &one, p.Bst, (int)n2,
+                                p.Bst + (size_t)i0 * n, (int)n2, &zero, p.Gp, (int)n2) != CUBLAS_STATUS_SUCCESS) {
+                    set_error(PHF_ERR_CUDA, "cublasDgemm (exchange panel) failed");
+                    return PHF_ERR_CUDA;
+                }
+            } else {
+                OutView o = vo(reinterpret_cast<zc *>(p.Gp), n2, 1);
+                o.real = 1;
+                PHF_TRY(zgemm_strided(rows, (int)n2, L, 1, 1, Z1, vd(p.Bst + (size_t)i0 * n, 1, n2), vd(p.Bst, n2, 1),
+                                      Z0, o, nullptr, st));
+            }
+            PHF_TRY(launch_ek_panel(n, ip, p.Gp, n2, p.EKp, n2, st));
+            if (p.library_gemm) {
+                cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
+                const double one = 1.0, zero = 0.0;
+                ProfScope prof(st, PROF_JK);
+                if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, 8 * bc, rows, (int)n2, &one,
+                                reinterpret_cast<const double *>(p.Kin), 8 * b, p.EKp, (int)n2, &zero,
+                                reinterpret_cast<double *>(p.Kvec) + (size_t)i0 * n * 8 * b, 8 * b) !=
+                    CUBLAS_STATUS_SUCCESS) {
+                    set_error(PHF_ERR_CUDA, "cublasDgemm (exchange rows) failed");
+                    return PHF_ERR_CUDA;
+                }
+            } else {
+                PHF_TRY(zgemm_strided(rows, 4 * bc, (int)n2, 1, 1, Z1, vd(p.EKp, n2, 1), vz(p.Kin, 4LL * b, 1), Z0,
+                                      vo(p.Kvec + (size_t)i0 * n * 4 * b, 4LL * b, 1), nullptr, st));
+            }
+        } else {
+            PHF_TRY(oz_gemm_ex(rows, (int)n2, L, p.slices, p.B2sl, oz_pad_rows(n2), i0 * n, p.eB2, p.B2sl, p.eB2, p.Gp,
+                               n2, 0, 0, p.ozerr, st, 0, 0));
+            PHF_TRY(oz_slice_ek_panel(n, ip, p.Gp, n2, p.slices, oz_pad_rows(prow), p.EKpsl, p.eEKp, st));
+            PHF_TRY(oz_gemm_ex(rows, 8 * bc, (int)n2, p.slices, p.EKpsl, oz_pad_rows(prow), 0, p.eEKp, p.Bsl, p.eb,
+                               reinterpret_cast<double *>(p.Gam), 0, 0, 0, p.ozerr, st, n, i0 * n));
+        }
     }
     return PHF_OK;
 }
@@ -705,7 +824,9 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
         PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
-        if (p.library_gemm) {
+        if (p.streamed) {
+            PHF_TRY(exchange_streamed(p, bc, st));
+        } else if (p.library_gemm) {
             // row-major Kvec (n^2 x 8bc reals) = EK (n^2 x n^2) Kin (n^2 x 8bc reals), i.e. column-major
             // Kvec^T = Kin^T EK^T
             cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
@@ -727,8 +848,11 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     } else {
         if (!fused) PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
         // K (as K^T, 8 bc x n^2) written by the GEMM epilogue as -K into Gamma's complex M x M blocks
-        PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb, reinterpret_cast<double *>(p.Gam),
-                          0, 0, 0, p.ozerr, st, n));
+        if (p.streamed)
+            PHF_TRY(exchange_streamed(p, bc, st));
+        else
+            PHF_TRY(oz_gemm_t((int)n2, 8 * bc, (int)n2, p.slices, p.EKsl, p.ea, p.Bsl, p.eb,
+                              reinterpret_cast<double *>(p.Gam), 0, 0, 0, p.ozerr, st, n));
         if (fork) PHF_CUDA(cudaStreamWaitEvent(st, p.ev_join, 0));  // the Coulomb chain is done
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_add_coulomb_diag(n, bc, p.Jr, 1, n2, p.Gam, st));
@@ -830,8 +954,8 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
         // Gamma(rho_w) X_w and e2
         if (p.chol && p.eri) {
             PHF_TRY(gamma_x_eri(p, bc, st));
-        } else if (p.chol) {
-            if (p.prec == PHF_PREC_FP64) {
+        } else if (p.chol) {  // factorized form (FP64 only: plan_create rejects the others)
+            {
                 prof_set_class(PROF_JK);
                 // T_Lw = V_L^H X_w : batched over L, (N x M) x (M x bN)
                 PHF_TRY(zgemm_strided(N, bc * N, M, L, 1, Z1, vz(p.V, 1, N, MN, 0, 1), vz(p.Xs, ld, 1), Z0,
@@ -844,8 +968,6 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
                 PHF_TRY(zgemm_strided(n, bc * N, L * n, 2, 1, Z1, vd(p.Bst, 1, n), vz(p.Q, 2 * ld, 1, ld), Z0,
                                       vo(p.GX, 2 * ld, 1, ld), nullptr, st));
                 prof_set_class(PROF_GEMM);
-            } else {
-                PHF_TRY(split_gamma_x(p, bc, st));
             }
             PHF_TRY(launch_rowsum(bc, L, p.e2part, p.e2, 0.5, st));
             PHF_TRY(launch_add_inplace(M, N, bc, p.HX, p.GX, ld, st));  // GX <- HX + Gamma X

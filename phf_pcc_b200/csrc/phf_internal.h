@@ -94,6 +94,8 @@ int launch_localg(int MM, int nterm, const zc *coef_g, const zc *coef_r, const l
 
 int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStream_t st);
 int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st);
+// streamed FP64 form: EKp[(i - i0) n + k][l n + j] = G[(i - i0) n + l][k n + j] for one panel of ipanel i's
+int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *EKp, long long lde, cudaStream_t st);
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
                           cudaStream_t st);
@@ -121,17 +123,20 @@ int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *e
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st,
               int gamma_n = 0);  // gamma_n > 0: -K^T written into Gamma (exchange GEMM, m = n^2)
+// oz_gemm_t with A rows [a_row0, a_row0 + m) of a slice buffer of a_rows_pad rows (ea indexed by that
+// buffer's rows) and, in the Gamma mode, output row 0 at exchange row g_row0 (a panel of the exchange rows)
+int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,
+               const signed char *Bsl, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
+               cudaStream_t st, int gamma_n, int g_row0);
+// slices of the exchange rows (i, k), i in [i0, i0 + ipanel), from the panel's Gram block G
+// (G[(i - i0) n + l][k n + j] = sum_L B_L[i][l] B_L[k][j], row stride ldg); k-index l n + j
+int oz_slice_ek_panel(int n, int ipanel, const double *G, long long ldg, int S, long long rows_pad, signed char *out,
+                      int *ea, cudaStream_t st);
 int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl,
                    const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
                    cudaStream_t st);
 int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
             double *D, long long ldd, int accumulate, int *err, cudaStream_t st);
-
-// phf_split.cu: tensor-core (tcgen05) J/K contraction workspace
-struct SplitWork {
-    void *ws = nullptr;
-    size_t bytes = 0;
-};
 
 // Everything a plan owns: sizes, grid tables, Hamiltonian and the chunk workspace.
 struct PlanImpl {
@@ -140,6 +145,10 @@ struct PlanImpl {
     int n = 0, M = 0, N = 0, L = 0;
     int prec = PHF_PREC_FP64, slices = 0;
     int eri = 0;                     // exchange via the spatial ERI matrix (1) or factorized Cholesky (0)
+    int streamed = 0;                // ERI form without the stored n^4 matrix: its rows are regenerated
+                                     // from the Cholesky vectors in panels of ek_ipanel spatial indices i,
+                                     // each used against the whole chunk and then overwritten
+    int ek_ipanel = 0, ek_npanel = 0;
     int exact = 0;                   // also accumulate the ket-side gradient (gradient_mode 1)
     int library_gemm = 0;            // FP64 exchange GEMM through cuBLAS (comparison form)
     void *cublas = nullptr;          // cublasHandle_t when library_gemm
@@ -187,6 +196,10 @@ struct PlanImpl {
     long long *offs_k = nullptr;       // 3 x 3 x nomega: GEMM offsets of R1^H, R2^H, Rpg^H per point
     // spatial-ERI exchange form
     double *EK = nullptr;              // EK[(i n + k) n^2 + l n + j] = (il|kj), FP64 back-end
+    double *Gp = nullptr;              // streamed form: Gram block of one panel, G[(i - i0) n + l][k n + j]
+    double *EKp = nullptr;             // streamed FP64 form: the panel's exchange rows (ipanel n x n^2)
+    signed char *EKpsl = nullptr;      // streamed tensor-core form: the panel's exchange rows, sliced
+    int *eEKp = nullptr;
     signed char *EKsl = nullptr;       // its int8 slices, Ozaki back-end
     int *ea = nullptr, *eb = nullptr, *ozerr = nullptr;
     zc *Rho = nullptr, *Pvec = nullptr, *dvec = nullptr, *Jvec = nullptr, *Kin = nullptr, *Kvec = nullptr, *Gam = nullptr;
@@ -195,13 +208,9 @@ struct PlanImpl {
     signed char *B1sl = nullptr, *B2sl = nullptr, *Psl = nullptr, *dsl = nullptr;
     int *eB1 = nullptr, *eB2 = nullptr, *ePc = nullptr, *edc = nullptr;
     double *dT = nullptr, *Jr = nullptr, *dpart = nullptr;  // dpart: split-k partials of d^T
-    SplitWork split;  // tensor-core path workspace (phf_split.cu)
     ~PlanImpl();
 };
 
-size_t split_bytes_per_point(const PlanImpl &p);
-int split_setup(PlanImpl &p);
-int split_gamma_x(PlanImpl &p, int bc, cudaStream_t st);
 
 // phf_engine.cu
 int plan_eval_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *const *d_hs, zc *const *d_yg,

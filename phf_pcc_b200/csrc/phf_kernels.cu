@@ -364,6 +364,22 @@ __global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long lon
     }
 }
 
+// One panel of the FP64 exchange matrix from its Gram block (streamed form): for r = (i - i0) n + k,
+// EKp[r][l n + j] = G[(i - i0) n + l][k n + j] (ldg, lde: row strides), i.e. (il|kj) for the panel's i.
+// One CTA per output row; for fixed l the n values j are contiguous on both sides.
+__global__ void ek_panel_kernel(int n, const double *__restrict__ G, long long ldg, double *__restrict__ EKp,
+                                long long lde) {
+    const long long r = blockIdx.x;
+    const int il = (int)(r / n), k = (int)(r - (long long)il * n);
+    const double *g = G + (long long)il * n * ldg + (long long)k * n;
+    double *e = EKp + r * lde;
+    const int kk = n * n;
+    for (int t = threadIdx.x; t < kk; t += NT) {
+        const int l = t / n, j = t - l * n;
+        e[t] = g[(long long)l * ldg + j];
+    }
+}
+
 inline int grid_for(long long n) {
     long long g = (n + NT - 1) / NT;
     if (g > 148LL * 16) g = 148LL * 16;
@@ -533,6 +549,14 @@ int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, co
 int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     add_coulomb_diag_kernel<<<grid_for(2LL * n * n * b), NT, 0, st>>>(n, b, Jr, jrs, jcs, Gam);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *EKp, long long lde, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    ek_panel_kernel<<<(unsigned)((long long)ipanel * n), NT, 0, st>>>(n, G, ldg, EKp, lde);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -71,13 +71,18 @@ def _close(a, b, rel):
 
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("form,precision", [("factorized", "fp64"), ("eri", "fp64"), ("eri", "fp64-cublas"),
-                                            ("eri", "ozaki_i8")])
+                                            ("eri", "ozaki_i8"), ("streamed", "fp64"), ("streamed", "fp64-cublas"),
+                                            ("streamed", "ozaki_i8"), ("streamed-3", "fp64"),
+                                            ("streamed-3", "ozaki_i8")])
 def test_forms_and_precisions_match_golden(name, form, precision):
+    """Every J/K form and precision against the golden vectors.  "streamed-3": the exchange rows
+    regenerated in panels of three spatial indices (c1, n = 20: six panels of 60 rows and one of 40)."""
     c = load(name)
     rel = 1e-10 if precision.startswith("fp64") else 1e-9
     lib_gemm = precision == "fp64-cublas"
-    with api.Plan(ref=c["Ref"], h=c["h"], B=c["B"], jk_form=form, precision=precision.split("-")[0],
-                  fp64_library_gemm=lib_gemm, **_api_kwargs(c)) as plan:
+    panel = int(form.split("-")[1]) if "-" in form else 0
+    with api.Plan(ref=c["Ref"], h=c["h"], B=c["B"], jk_form=form.split("-")[0], precision=precision.split("-")[0],
+                  fp64_library_gemm=lib_gemm, exchange_panel=panel, **_api_kwargs(c)) as plan:
         out = plan.buildhsg(c["Z"], check_hermitian=False)
     for x, key in zip(out, ("Hmat", "Smat", "Gradmat", "Rdmmat")):
         assert _close(x, c[key], rel), (key, float(np.abs(x - c[key]).max()))
@@ -107,11 +112,12 @@ def test_int8_pipeline_matches_fp64_on_ragged_sizes(n, N, L):
 
 
 @pytest.mark.parametrize("n", [130, 170])
-def test_automatic_form_above_n128_int8_eri_matches_fp64_factorized(n):
-    """Above n = 128 the automatic J/K form is the factorized one in FP64 but the spatial-ERI exchange
-    matrix for the int8 path (n = 130: a 16900 x 16900 exchange matrix); both forms must agree.  At
-    n = 170 (k = n^2 = 28900) the exchange GEMM needs two launches for exact int32 group sums, the
-    second adding into Gamma."""
+def test_automatic_form_above_n128_streamed_matches_fp64_factorized(n):
+    """Above n = 128 the automatic J/K form is the streamed one (no n^4 matrix; n = 130: panels of
+    the 16900 x 16900 exchange matrix regenerated from the Cholesky vectors) in every precision; it
+    must agree with the rank-N factorized FP64 form, which shares none of its exchange arithmetic.  At
+    n = 170 (k = n^2 = 28900) each panel's exchange GEMM needs two launches for exact int32 group
+    sums, the second adding into Gamma."""
     import torch
 
     from phf_pcc_b200 import synth
@@ -123,9 +129,10 @@ def test_automatic_form_above_n128_int8_eri_matches_fp64_factorized(n):
                roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
     C = torch.from_numpy(p.C).cuda()
     res = {}
-    for prec in ("fp64", "ozaki_i8"):
-        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, **akw) as plan:
-            res[prec] = [t.cpu().numpy() for t in plan.eval_device(C)]
+    for label, prec, form in (("fact", "fp64", "factorized"), ("fp64", "fp64", "auto"), ("i8", "ozaki_i8", "auto")):
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, jk_form=form, **akw) as plan:
+            res[label] = [t.cpu().numpy() for t in plan.eval_device(C)]
         torch.cuda.empty_cache()
-    for a, b, what in zip(res["ozaki_i8"], res["fp64"], ("HS", "Yg", "Yr")):
-        assert _close(a, b, 1e-9), (what, float(np.abs(a - b).max()))
+    for label, rel in (("fp64", 1e-11), ("i8", 1e-9)):
+        for a, b, what in zip(res[label], res["fact"], ("HS", "Yg", "Yr")):
+            assert _close(a, b, rel), (label, what, float(np.abs(a - b).max()))

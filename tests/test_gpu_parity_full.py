@@ -1,0 +1,110 @@
+"""Parity at the benchmark sizes: the CUDA path against the C oracle on fixed blocks of grid points.
+
+The full grids take the oracle hours, so each case evaluates two contiguous blocks of the flattened
+grid (w = (il ny + iy) npg + ipg) that contain the Lebedev poles -- il = 4 is beta = 0 (overlaps near
+one) and il = 5 is beta = pi (spin-flipped, the smallest overlaps) -- with a plan restricted to that
+block (point_range) and the oracle on the same indices (omega_list).  Partial sums over a block are
+what a rank of the reference's grid split would hold (PHFTools.f90:53-57), so they compare directly.
+
+  n = 64  (M = 128, L = 400, 3200-point C2v grid): 2 x 32 points; the oracle contracts the dense
+          antisymmetrised HTwo (MakeGamma, PHFTools.f90:310-337) with Ref = I and the determinant in
+          Thouless form; the GPU runs the dense drop-in form and the Cholesky forms
+  n = 128 (M = 256, L = 800, 800 points): 2 x 8 points, spatial Cholesky oracle, Ref = the unitary
+          whose first N columns are the determinant, Z = 0
+  n = 200 (M = 400, L = 1000, 3200-point C2v grid): 2 x 4 points, as n = 128; the GPU forms are the
+          streamed exchange rows (no n^4 tensor) in FP64 and in int8 slices
+
+Tolerances: Hmat, Smat, Gradmat, Rdmmat within 1e-10 (FP64 forms) or 1e-9 (int8 slices, S = 5) of
+the largest element of each; the energy E = Re H / |Re S| of the two blocks together within 1e-8 Eh
+and the LocalG gradient elements G[N:, :N] within 1e-7 (the benchmark's targets).
+"""
+import numpy as np
+import pytest
+
+from oracle import phf_oracle as orc
+from oracle import phf_oracle_c as corc
+from phf_pcc_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("Hmat", "Smat", "Gradmat", "Rdmmat")
+
+
+def _blocks(p, size):
+    """Two blocks of `size` consecutive points starting at the beta = 0 and beta = pi Lebedev points."""
+    g = p.grid
+    per_l = g.ngrid[1] * g.npg
+    out = []
+    for beta in (0.0, np.pi):
+        il = int(np.argmin(np.abs(np.asarray(g.rootb) - beta)))
+        out.append((il * per_l, il * per_l + size))
+    return out
+
+
+def _akw(p):
+    kw = p.grid_kwargs()
+    return dict(ngrid=kw["ngrid"], nci=kw["nci"], cmplxconj=kw["CmplxConj"], ncisp=kw["ncisp"], nocc=p.N,
+                r1=kw["R1"], r2=kw["R2"], rpg=kw["Rpg"], weightsp=kw["weightsp"], weightpg=kw["weightpg"],
+                roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
+
+
+def _energy_grad(p, H, S, G, R):
+    e = H[0, 0].real / abs(S[0, 0].real)
+    Gl = orc.localg(G, R, S, e, [1.0 / np.sqrt(abs(S[0, 0].real))], [1.0], [1.0], 1, p.M, 1, 1, 1)
+    return e, Gl[p.N:, :p.N]
+
+
+def _compare(p, gpu, ora, rel, label):
+    for x, y, key in zip(gpu, ora, KEYS):
+        err = float(np.abs(x - y).max())
+        assert err <= rel * max(float(np.abs(y).max()), 1e-300), (label, key, err, float(np.abs(y).max()))
+
+
+def _check_forms(p, Ref, Z, blocks, oracle_kw, forms):
+    """Oracle partial sums per block; every GPU form per block; energy and gradient of the summed blocks."""
+    ora = [corc.buildhsg(omega_list=np.arange(b0, b1), **oracle_kw) for b0, b1 in blocks]
+    ora_tot = [sum(o[i] for o in ora) for i in range(4)]
+    e_o, g_o = _energy_grad(p, *ora_tot)
+    for label, plan_kw, rel in forms:
+        parts = []
+        for (b0, b1), o in zip(blocks, ora):
+            with api.Plan(ref=Ref, point_range=(b0, b1), **plan_kw) as plan:
+                out = plan.buildhsg(Z, check_hermitian=False)
+            _compare(p, out, o, rel, (label, b0))
+            parts.append(out)
+        tot = [sum(o[i] for o in parts) for i in range(4)]
+        e, g = _energy_grad(p, *tot)
+        assert abs(e - e_o) <= 1e-8, (label, e, e_o)
+        assert float(np.abs(g - g_o).max()) <= 1e-7, (label, float(np.abs(g - g_o).max()))
+
+
+def test_n64_c2v_grid_blocks_against_dense_oracle():
+    p = synth.config_problem("c2", seed=0)
+    M, N = p.M, p.N
+    Z = p.C[N:] @ np.linalg.inv(p.C[:N])          # Ref = I: the determinant [I; Z] spans C
+    H2 = orc.dense_htwo_from_chol(p.B).astype(np.complex128)
+    kw = p.grid_kwargs()
+    oracle_kw = dict(HOne=p.hone_ao(), HTwo=H2, Ref=np.eye(M), Z=Z, **kw)
+    akw = _akw(p)
+    forms = [("dense fp64", dict(hone=p.hone_ao(), htwo=H2, **akw), 1e-10),
+             ("eri fp64", dict(h=p.h, B=p.B, jk_form="eri", **akw), 1e-10),
+             ("eri int8", dict(h=p.h, B=p.B, jk_form="eri", precision="ozaki_i8", **akw), 1e-9),
+             ("streamed int8", dict(h=p.h, B=p.B, jk_form="streamed", precision="ozaki_i8", exchange_panel=8, **akw),
+              1e-9)]
+    _check_forms(p, np.eye(M), Z, _blocks(p, 32), oracle_kw, forms)
+
+
+@pytest.mark.parametrize("name,size", [("c3", 8), ("c5", 4)])
+def test_large_grid_blocks_against_spatial_cholesky_oracle(name, size):
+    p = synth.config_problem(name, seed=0)
+    Ref, Z = p.ref_and_z()
+    kw = p.grid_kwargs()
+    H1 = orc.mo_transform_1(p.hone_ao(), Ref)
+    oracle_kw = dict(HOne=H1, HTwo=None, Ref=Ref, Z=Z, Bs=p.B, **kw)
+    akw = _akw(p)
+    forms = [("auto fp64", dict(h=p.h, B=p.B, **akw), 1e-10),
+             ("auto int8", dict(h=p.h, B=p.B, precision="ozaki_i8", **akw), 1e-9)]
+    if name == "c5":  # the FP64 comparison form of the benchmark: cuBLAS DGEMM for the exchange rows
+        forms.append(("streamed fp64 cublas", dict(h=p.h, B=p.B, jk_form="streamed", fp64_library_gemm=True, **akw),
+                      1e-10))
+    _check_forms(p, Ref, Z, _blocks(p, size), oracle_kw, forms)

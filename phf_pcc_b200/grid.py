@@ -10,6 +10,11 @@ produces the arrays that the reference passes to ``phftools.buildhsg``:
 * ``wigner_D``          -- WignerMat.py:8-27 and PHF_fort/PHFTools.f90:350-376
 * ``c2v_projector``     -- PG_irrep.py:6-28 (signed-diagonal C2v operations) with the
                            C2v characters of PGSymm.py:87-107, assembled as PG_Proj.py:17-26
+* ``c4v_projector``     -- C4vTable (PGSymm.py:109-137): eight operations E, C4, C2, C4^3, sigma_xz,
+                           sigma_yz, sigma_d, sigma_d' with the 1-D characters or, for the 2-D
+                           irrep E (ncipg = 2), the 2 x 2 representation matrices as weights; the
+                           orbital operations are block diagonal over synthetic orbital blocks
+                           that carry the irreps of C4v (the reference takes them from pyscf AOs)
 * ``no_pg``             -- PG_Proj.py:12-16
 
 Spin-orbital order is [alpha block; beta block] (M = 2n), as BuildRotMat uses.
@@ -28,7 +33,8 @@ import numpy as np
 
 __all__ = [
     "lebedev", "root_weight", "root_weight_sy", "build_rot_mat", "spin_rotation_2x2",
-    "spin_proj", "wigner_D", "c2v_projector", "no_pg", "ProjectionGrid", "make_grid",
+    "spin_proj", "wigner_D", "c2v_projector", "c4v_projector", "c4v_orbital_ops", "no_pg", "ProjectionGrid",
+    "make_grid",
 ]
 
 _SUPPORTED_NL = (1, 6, 14, 26, 38, 50)
@@ -326,6 +332,62 @@ def c2v_projector(n: int, irrep: str = "A1", labels=None):
     return 1, weightpg, Rpg
 
 
+# C4v in the operation order of PGSymm.py:109-137: E, C4, C2, C4^3, sigma_xz, sigma_yz, sigma_d, sigma_d'
+_C4V_CHARACTERS = {
+    "A1": (1.0,) * 8,
+    "A2": (1.0, 1.0, 1.0, 1.0, -1.0, -1.0, -1.0, -1.0),
+    "B1": (1.0, -1.0, 1.0, -1.0, 1.0, 1.0, -1.0, -1.0),
+    "B2": (1.0, -1.0, 1.0, -1.0, -1.0, -1.0, 1.0, 1.0),
+}
+
+
+def c4v_e_matrices() -> np.ndarray:
+    """The 2 x 2 matrices of the C4v irrep E in the operation order above: C4^k is the rotation by
+    -k 90 degrees, and the reflections are rot(j) sigma_xz with j = 0, 2, 1, 3 for sigma_xz, sigma_yz,
+    sigma_d, sigma_d' (sigma_xz = diag(1, -1)) -- the matrices of PGSymm.py:127-135."""
+    def rot(k):
+        c, s_ = round(math.cos(-k * math.pi / 2)), round(math.sin(-k * math.pi / 2))
+        return np.array([[c, -s_], [s_, c]], dtype=np.float64)
+
+    sxz = np.diag([1.0, -1.0])
+    return np.stack([rot(0), rot(1), rot(2), rot(3)] + [rot(j) @ sxz for j in (0, 2, 1, 3)])
+
+
+def c4v_orbital_ops(n: int) -> np.ndarray:
+    """Eight n x n orbital operations of C4v (a representation of the group): orbitals fill blocks
+    that transform as A1, E (a pair), B1, E, A2, B2, A1, ... in turn (a last single orbital that
+    would start an E pair is A1)."""
+    E2 = c4v_e_matrices()
+    ops = np.zeros((8, n, n))
+    kinds = ("A1", "E", "B1", "E", "A2", "B2")
+    i = t = 0
+    while i < n:
+        kind = kinds[t % len(kinds)]
+        t += 1
+        if kind == "E" and i + 1 < n:
+            ops[:, i:i + 2, i:i + 2] = E2
+            i += 2
+        else:
+            ops[:, i, i] = _C4V_CHARACTERS["A1" if kind == "E" else kind]
+            i += 1
+    return ops
+
+
+def c4v_projector(n: int, irrep: str = "A1"):
+    """C4v point-group projector data (ncipg, weightpg (8, ncipg, ncipg), Rpg (8, M, M)) as
+    C4vTable (PGSymm.py:109-137) and PG_Proj.py:17-26 assemble it: the weights are the irrep's
+    characters, or the E matrices (ncipg = 2); Rpg[i] = blockdiag(op_i, op_i)."""
+    if irrep == "E":
+        ncipg, weightpg = 2, c4v_e_matrices()
+    elif irrep in _C4V_CHARACTERS:
+        ncipg, weightpg = 1, np.array(_C4V_CHARACTERS[irrep], dtype=np.float64).reshape(8, 1, 1)
+    else:
+        raise ValueError(f"unknown C4v irrep {irrep!r}")
+    ops = c4v_orbital_ops(n)
+    Rpg = np.stack([np.kron(np.eye(2), ops[i]) for i in range(8)]).astype(np.complex128)
+    return ncipg, weightpg, Rpg
+
+
 def no_pg(n: int):
     """Identity point group (PG_Proj.py:12-16): ncipg=1, weightpg=ones(1,1,1), Rpg=[I]."""
     M = 2 * n
@@ -366,14 +428,16 @@ class ProjectionGrid:
 
 def make_grid(n: int, ngrid=(14, 8), SP: int = 1, J: int = 0, pg: str = "None", irrep: str = "A1",
               CmplxConj: int = 1) -> ProjectionGrid:
-    """Build the spin (and optional C2v) projection grid for n spatial orbitals."""
+    """Build the spin (and optional C2v or C4v) projection grid for n spatial orbitals."""
     ncisp, roota, rootb, rooty, w, R1, R2 = spin_proj(SP, ngrid, n, J)
     if pg == "None":
         ncipg, wpg, Rpg = no_pg(n)
     elif pg == "C2v":
         ncipg, wpg, Rpg = c2v_projector(n, irrep)
+    elif pg == "C4v":
+        ncipg, wpg, Rpg = c4v_projector(n, irrep)
     else:
-        raise ValueError(f"point group {pg!r} is not supported (None, C2v)")
+        raise ValueError(f"point group {pg!r} is not supported (None, C2v, C4v)")
     return ProjectionGrid(SP=SP, ngrid=tuple(int(g) for g in ngrid), J=J, ncisp=ncisp, ncipg=ncipg,
                           npg=Rpg.shape[0], roota=roota, rootb=rootb, rooty=rooty, weightsp=w,
                           weightpg=wpg, R1=R1, R2=R2, Rpg=Rpg, CmplxConj=CmplxConj)

@@ -6,7 +6,8 @@ import numpy as np
 from oracle import phf_oracle as orc
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["tiny_sp1", "c1", "j1_c2v_b1", "j2_c2v_a1", "suhf_sp2_real", "cmplx2", "tiny_dense_htwo"]
+CASES = ["tiny_sp1", "c1", "j1_c2v_b1", "j2_c2v_a1", "suhf_sp2_real", "cmplx2", "tiny_dense_htwo", "e_c4v",
+         "j1_e_c4v"]
 
 
 def load(name):

@@ -93,6 +93,25 @@ def _c2v_ops(n, irrep):
     return wpg, Rpg
 
 
+def _c4v_ops(ref_dir, n, irrep):
+    """The reference's C4vTable (PGSymm.py:109-137) -- its character or E-matrix weights -- with its
+    pyscf-based orbital operations (SymmMat) replaced by synthetic block-diagonal ones that carry the
+    C4v irreps (phf_pcc_b200.grid.c4v_orbital_ops), assembled as PG_Proj.py:21-25."""
+    if ref_dir not in sys.path:
+        sys.path.insert(0, ref_dir)
+    sys.modules.pop("PGSymm", None)
+    import PGSymm  # noqa: E402
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from phf_pcc_b200.grid import c4v_orbital_ops  # noqa: E402
+
+    PGSymm.SymmMat = lambda pg, nrot, mol: c4v_orbital_ops(mol.nao)
+    ID, nci, ops = PGSymm.C4vTable(types.SimpleNamespace(nao=n), irrep)
+    weightpg = np.asarray(ID, dtype=np.float64)
+    Rpg = np.stack([np.kron(np.eye(2), ops[i]) for i in range(ops.shape[0])]).astype(np.complex128)
+    return weightpg, Rpg
+
+
 def make_case(ref_dir, name, n, N, L, ngrid, seed, SP=1, J=0, CmplxConj=1, pg="None", irrep="A1",
               z_scale=0.1, store_htwo=False):
     M = 2 * n
@@ -105,10 +124,12 @@ def make_case(ref_dir, name, n, N, L, ngrid, seed, SP=1, J=0, CmplxConj=1, pg="N
     ncisp = 2 * J + 1 if SP == 1 else 1
     if pg == "C2v":
         weightpg, Rpg = _c2v_ops(n, irrep)
+    elif pg == "C4v":
+        weightpg, Rpg = _c4v_ops(ref_dir, n, irrep)
     else:
         weightpg, Rpg = np.ones((1, 1, 1)), np.eye(M, dtype=np.complex128)[None]
     npg = Rpg.shape[0]
-    ncipg = 1
+    ncipg = weightpg.shape[1]
     ncik = 2 if CmplxConj == 2 else 1
     nci = ncisp * ncipg * ncik
     params = dict(NSO=M, NOccSO=N, ncisp=ncisp, ncipg=ncipg, ncik=ncik, CmplxConj=CmplxConj, SP=SP, J=J,
@@ -277,6 +298,9 @@ def main():
     # SP = 3 is not generated: RootWeight fails for nl = 1 (1-D loadtxt), and for nl > 1
     # Spin_Proj.py:126 leaves R1[1:] = 0, which makes every overlap singular.
     make_case(ref_dir, "tiny_dense_htwo", n=3, N=2, L=4, ngrid=(6, 3), seed=17, store_htwo=True)
+    # two-dimensional irrep (C4v E, ncipg = 2), alone and with J = 1 spin projection (nci = 6)
+    make_case(ref_dir, "e_c4v", n=6, N=4, L=9, ngrid=(6, 4), seed=18, pg="C4v", irrep="E")
+    make_case(ref_dir, "j1_e_c4v", n=5, N=3, L=6, ngrid=(6, 3), seed=19, J=1, pg="C4v", irrep="E")
 
 
 if __name__ == "__main__":

@@ -66,3 +66,19 @@ def test_c2v_projector_characters():
         assert np.allclose(Rpg[1] @ Rpg[2], Rpg[3])
         for g in Rpg:
             assert np.allclose(g @ g, np.eye(2 * n))
+
+
+@pytest.mark.parametrize("name", ["e_c4v", "j1_e_c4v"])
+def test_c4v_projector_matches_reference_table(name):
+    """grid.c4v_projector's E-irrep weights and operations against the golden cases, whose weights
+    came from the reference's own C4vTable (PGSymm.py:109-137)."""
+    c = load(name)
+    ncipg, w, R = grid.c4v_projector(int(c["n"]), "E")
+    assert ncipg == int(c["ncipg"]) == 2
+    assert np.array_equal(w, c["weightpg"])
+    assert np.array_equal(R, c["Rpg"])
+    # a representation: the orbital operations multiply like the E matrices (C4 C4 = C2, C4 sigma_xz = sigma_d)
+    ops = grid.c4v_orbital_ops(int(c["n"]))
+    E = grid.c4v_e_matrices()
+    for a, b, ab in ((1, 1, 2), (1, 4, 6), (2, 4, 5), (3, 4, 7)):
+        assert np.allclose(ops[a] @ ops[b], ops[ab]) and np.allclose(E[a] @ E[b], E[ab])

@@ -40,7 +40,7 @@ def test_cholesky_gamma_equals_dense(name):
 # Cases whose grids integrate exactly enough for the reference's Hermiticity check
 # (PHFTools.f90:195-200); the Fortran would STOP "Not Hermitian" on the others.
 HERMITIAN = {"c1": True, "cmplx2": True, "tiny_dense_htwo": True, "tiny_sp1": False, "j1_c2v_b1": False,
-             "j2_c2v_a1": False, "suhf_sp2_real": False}
+             "j2_c2v_a1": False, "suhf_sp2_real": False, "e_c4v": False, "j1_e_c4v": False}
 
 
 @pytest.mark.parametrize("name", CASES)

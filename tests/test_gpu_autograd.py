@@ -76,31 +76,70 @@ def test_exact_and_reference_gradients_agree_on_fine_symmetric_grid():
     assert diff <= 1e-6 * out["reference"][1].abs().max().item(), diff
 
 
-def test_gradient_fd_at_config2_orbital_rotation_steps():
-    """Configuration 2 adjoint check: seeded orbital-rotation steps C <- exp(kappa) C, forward +
-    autograd backward, directional derivative against central differences (h = 1e-5)."""
+def test_config2_adjoint_twenty_rotation_steps_against_fd_and_reference_gradient():
+    """Configuration-2 adjoint protocol (n = 64, M = 128, N = 32, L = 400, 50 x 16 x 4 C2v grid, int8
+    slices): 20 seeded orbital-rotation steps C <- exp(kappa) C (anti-Hermitian kappa, N(0, 1e-2)).
+    At each step the autograd gradient (exact-gradient plan, forward + backward) is checked
+
+    * against central finite differences (h = 1e-5) along a random direction, to 1e-6 relative;
+    * against the reference's gradient: with Ref = I and the determinant in Thouless form
+      [I; Z] = C C_occ^-1, LocalG's G[N:, :N] = dE/dZ* (PHF_fort/PHFTools.f90:203-247) from the
+      reference-mode plan on the full grid equals the autograd gradient's rows N: at [I; Z] (the
+      bra-side and exact gradients differ only by the grid's Hermiticity defect), to 1e-5 of max|G|;
+    * and that reference gradient against the C oracle on a block of 4 grid points (the beta = 0
+      Lebedev point): the block's LocalG gradient from the GPU plan and from the oracle within 1e-7,
+      the block's energy within 1e-8 Eh."""
     import torch
 
+    from oracle import phf_oracle_c as corc
+
     p = synth.config_problem("c2", seed=2)
+    M, N = p.M, p.N
+    kw = p.grid_kwargs()
+    akw = _plan_kwargs_from_grid(kw, N)
+    g = p.grid
+    w0 = int(np.argmin(np.abs(np.asarray(g.rootb)))) * g.ngrid[1] * g.npg
+    block = (w0, w0 + 4)
     rng = np.random.default_rng(11)
-    with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="ozaki_i8", gradient="exact",
-                  **_plan_kwargs_from_grid(p.grid_kwargs(), p.N)) as plan:
+
+    def block_e_g(H, S, Gm, Rm):
+        e = H[0, 0].real / abs(S[0, 0].real)
+        G = api.localg(Gm, Rm, S, e, [1.0 / np.sqrt(abs(S[0, 0].real))], [1.0], [1.0], 1)
+        return e, G[N:, :N]
+
+    with api.Plan(ref=np.eye(M), h=p.h, B=p.B, precision="ozaki_i8", gradient="exact", **akw) as pe, \
+            api.Plan(ref=np.eye(M), h=p.h, B=p.B, precision="ozaki_i8", **akw) as pr, \
+            api.Plan(ref=np.eye(M), h=p.h, B=p.B, precision="ozaki_i8", point_range=block, **akw) as pb:
         C0 = p.C
-        for step in range(3):
+        for step in range(20):
             C0 = synth.orbital_rotation(C0, 1e-2, rng)
-            C = torch.from_numpy(C0).cuda().requires_grad_(True)
-            E = projected_energy(C, plan)
+            Z = C0[N:] @ np.linalg.inv(C0[:N])
+            Ct = np.vstack([np.eye(N), Z])                 # the same determinant, Thouless form
+            C = torch.from_numpy(Ct).cuda().requires_grad_(True)
+            E = projected_energy(C, pe)
             E.backward()
-            g = C.grad
-            d = rng.normal(size=C0.shape) + 1j * rng.normal(size=C0.shape)
+            grad = C.grad
+            d = rng.normal(size=Ct.shape) + 1j * rng.normal(size=Ct.shape)
             d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
             h = 1e-5
             with torch.no_grad():
-                ep = projected_energy(C.detach() + h * d, plan)
-                em = projected_energy(C.detach() - h * d, plan)
+                ep = projected_energy(C.detach() + h * d, pe)
+                em = projected_energy(C.detach() - h * d, pe)
             fd = (ep - em).item() / (2 * h)
-            an = torch.real(torch.sum(torch.conj(g) * d)).item()
+            an = torch.real(torch.sum(torch.conj(grad) * d)).item()
             assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (step, fd, an)
+            # the reference's gradient on the full grid (bra side, LocalG), dE/dZ*
+            H, S, Gm, Rm = pr.buildhsg(Z, check_hermitian=False)
+            e_ref, G_ref = block_e_g(H, S, Gm, Rm)
+            gz = (grad.cpu().numpy() / 2.0)[N:, :]
+            assert abs(e_ref - E.item()) <= 1e-9 * abs(E.item()), (step, e_ref, E.item())
+            assert np.abs(gz - G_ref).max() <= 1e-5 * np.abs(G_ref).max(), (step, np.abs(gz - G_ref).max())
+            # that gradient's machinery against the oracle on a block of grid points
+            eb, gb = block_e_g(*pb.buildhsg(Z, check_hermitian=False))
+            ora = corc.buildhsg(p.hone_ao(), None, np.eye(M), Z, Bs=p.B, omega_list=np.arange(*block), **kw)
+            eo, go = block_e_g(*ora)
+            assert abs(eb - eo) <= 1e-8, (step, eb, eo)
+            assert np.abs(gb - go).max() <= 1e-7, (step, np.abs(gb - go).max())
 
 
 def test_recompute_mode_equals_fused_mode():

@@ -154,6 +154,18 @@ int phf_plan_buildhsg(phf_plan *plan, const phf_complex *z, phf_complex *hmat, p
 int phf_plan_eval_device(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
                          phf_complex *d_yr, void *stream);
 
+/* phf_plan_eval_device without its synchronisation, for device-resident loops (one optimiser step
+ * per host round trip): the evaluation is queued on `stream` and returns at once; the two status
+ * words -- d_status[0]: bit 0 a rotated overlap was exactly singular, bit 1 non-finite; d_status[1]:
+ * tensor-core pipeline error code (0 = none) -- are copied to device memory on the same stream, to
+ * be read by the caller with its own results (PHF_ERR_SINGULAR / PHF_ERR_NONFINITE / PHF_ERR_CUDA
+ * where phf_plan_eval_device would return them).  Returns only errors found while queueing.  The
+ * plan's buffers are in use until the stream reaches the end of the evaluation: do not queue a
+ * second evaluation of the same plan on another stream before then.  No counterpart in the
+ * reference (its driver synchronises every call). */
+int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
+                               phf_complex *d_yr, int *d_status, void *stream);
+
 /* Batched evaluation of independent instances (the many-instance workload of uneven orbital
  * counts): plans[i] evaluates determinant d_c[i] into d_hs[i], d_yg[i], d_yr[i] exactly as
  * phf_plan_eval_device.  All instances run as one CUDA graph on `stream`, captured on first use

@@ -63,6 +63,7 @@ SIGNATURES = {
     "phf_plan_destroy": (_I, [_P]),
     "phf_plan_buildhsg": (_I, [_P, _P, _P, _P, _P, _P]),
     "phf_plan_eval_device": (_I, [_P, _P, _P, _P, _P, _P]),
+    "phf_plan_eval_device_async": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "phf_eval_batch": (_I, [_P, _I, _P, _P, _P, _P, _P]),
     "phf_batch_branches": (_I, []),
     "phf_plan_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_size_t)]),

@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import PREC, PHFError, check, phf_complex, phf_plan_desc
 
-__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "eval_batch", "PHFError"]
+__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "eval_batch", "check_status", "PHFError"]
 
 
 def _fz(a):
@@ -266,6 +266,28 @@ class Plan:
         check(st, "phf_plan_eval_device")
         return hs, yg, yr
 
+    def eval_device_async(self, C, out, status, stream=None):
+        """eval_device without the host synchronisation (phf_plan_eval_device_async): queues the
+        evaluation on ``stream`` and returns at once; ``out`` = (hs, yg, yr) as eval_device returns
+        them and ``status`` an int32 CUDA tensor of 2 that receives the status words (see
+        ``check_status``) on the same stream."""
+        import torch
+
+        if C.dtype != torch.complex128 or not C.is_cuda or tuple(C.shape) != (self.nso, self.nocc) or \
+                not C.is_contiguous():
+            raise ValueError(f"C must be a contiguous complex128 CUDA tensor of shape {(self.nso, self.nocc)}")
+        if status.dtype != torch.int32 or not status.is_cuda or status.numel() < 2:
+            raise ValueError("status must be an int32 CUDA tensor of at least 2 elements")
+        hs, yg, yr = out
+        if stream is None:
+            stream = torch.cuda.current_stream(C.device)
+        st = _lib.load().phf_plan_eval_device_async(
+            self._handle, ctypes.c_void_p(C.data_ptr()), ctypes.c_void_p(hs.data_ptr()),
+            ctypes.c_void_p(yg.data_ptr()), ctypes.c_void_p(yr.data_ptr()), ctypes.c_void_p(status.data_ptr()),
+            ctypes.c_void_p(stream.cuda_stream))
+        check(st, "phf_plan_eval_device_async")
+        return hs, yg, yr
+
     def close(self):
         if getattr(self, "_handle", None):
             _lib.load().phf_plan_destroy(self._handle)
@@ -282,6 +304,17 @@ class Plan:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def check_status(words):
+    """Raise PHFError for the status words of phf_plan_eval_device_async (host ints)."""
+    flag, oz = int(words[0]), int(words[1])
+    if oz:
+        raise PHFError(_lib.PHF_ERR_CUDA, f"tensor-core GEMM pipeline wait timed out (code {oz})")
+    if flag & 1:
+        raise PHFError(_lib.PHF_ERR_SINGULAR, "a rotated overlap bra^H R ket is exactly singular")
+    if flag & 2:
+        raise PHFError(_lib.PHF_ERR_NONFINITE, "non-finite rotated overlap")
 
 
 def eval_batch(plans, Cs, outs=None, stream=None):

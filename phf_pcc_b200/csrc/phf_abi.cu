@@ -292,6 +292,19 @@ int phf_plan_eval_device(phf_plan *plan, const phf_complex *d_c, phf_complex *d_
                                  reinterpret_cast<cudaStream_t>(stream));
 }
 
+int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_complex *d_hs, phf_complex *d_yg,
+                               phf_complex *d_yr, int *d_status, void *stream) {
+    phf::set_error(PHF_OK, "");
+    if (!plan || !d_c || !d_hs || !d_yg || !d_yr || !d_status) {
+        phf::set_error(PHF_ERR_ARG, "null argument");
+        return PHF_ERR_ARG;
+    }
+    return phf::plan_eval_device_async(plan->impl, reinterpret_cast<const phf::zc *>(d_c),
+                                       reinterpret_cast<phf::zc *>(d_hs), reinterpret_cast<phf::zc *>(d_yg),
+                                       reinterpret_cast<phf::zc *>(d_yr), d_status,
+                                       reinterpret_cast<cudaStream_t>(stream));
+}
+
 int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes) {
     if (!plan) return PHF_ERR_ARG;
     if (chunk) *chunk = plan->impl.b;

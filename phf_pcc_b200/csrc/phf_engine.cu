@@ -1309,6 +1309,23 @@ int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, c
     return read_flag(p, st);
 }
 
+// phf_plan_eval_device without the host synchronisation: the status words are copied to device
+// memory on the same stream for the caller to read together with its own results.
+int plan_eval_device_async(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, int *d_status, cudaStream_t st) {
+    if (p.cmplxconj == 2) {
+        set_error(PHF_ERR_UNSUPPORTED, "phf_plan_eval_device_async: cmplxconj == 2 needs phf_plan_buildhsg");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    PHF_CUDA(cudaSetDevice(p.device));
+    PHF_TRY(eval_enqueue(p, d_c, d_hs, d_yg, d_yr, st, false));
+    PHF_CUDA(cudaMemcpyAsync(d_status, p.flag, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (p.ozerr)
+        PHF_CUDA(cudaMemcpyAsync(d_status + 1, p.ozerr, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    else
+        PHF_CUDA(cudaMemsetAsync(d_status + 1, 0, sizeof(int), st));
+    return PHF_OK;
+}
+
 // ------------------------------------------------------------------ batched evaluation
 namespace {
 

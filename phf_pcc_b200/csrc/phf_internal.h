@@ -224,6 +224,8 @@ void plan_release(PlanImpl &p);
 int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_complex *smat, phf_complex *gradmat,
                   phf_complex *rdmmat);
 int plan_eval_device(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaStream_t st);
+int plan_eval_device_async(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, int *d_status,
+                           cudaStream_t st);
 
 }  // namespace phf
 

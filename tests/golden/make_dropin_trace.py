@@ -8,12 +8,13 @@ It imports the reference's unmodified PHF.py (with stub modules for ``parameter_
 ``solve_ci``, ``FixGauge`` and ``pyscf``, which only carry module globals or need absent
 packages, and with ``PHFTools_F`` replaced by a recorder) and calls its ``EandG`` (PHF.py:55-91)
 twice on the c1 golden problem (n = 20, M = 40, N = 10, Lebedev 14 x 8 grid): at the golden Z
-and at a perturbed Z, as two optimiser steps would.  The recorder's ``buildhsg`` and ``localg``
+and at a perturbed Z, as two optimiser steps would; then it runs five iterations of the BFGS
+optimiser of PHF.py:23 on that EandG from z = 0 and records every function call (x, E, g).  The recorder's ``buildhsg`` and ``localg``
 compute with the numpy oracle (itself pinned to the reference's functions by the golden tests)
 and store every positional argument the driver passed and every result.  The fixture
 ``dropin_trace.npz`` holds, per call, the arguments (arrays that equal a field of c1.npz are
 stored by that field's name; HTwo is rebuilt from c1's Cholesky vectors), the results, and
-EandG's own returned (E, gradient vector).  The replay test (tests/test_gpu_dropin.py) feeds the
+EandG's own returned (E, gradient vector), and the BFGS trajectory.  The replay test (tests/test_gpu_dropin.py) feeds the
 same arguments to the drop-in module on the GPU.
 """
 from __future__ import annotations
@@ -105,6 +106,22 @@ def main():
                 x = np.concatenate([z.real, z.imag])
                 E, g = PHF.EandG(x, c["HOne"], HTwo, c["Ref"], 0)
                 results.append((x, E, g))
+            ncalls_eandg = len(rec.calls)
+            # the reference's optimiser on its EandG (PHF.py:23's BFGS, started from z = 0 as optPHF
+            # does without a saved solution), five iterations; every function call recorded
+            from scipy.optimize import minimize
+
+            traj = []
+
+            def fun(x, *args):
+                E, g = PHF.EandG(x, *args)
+                traj.append((np.array(x), E, np.array(g)))
+                return E, g
+
+            M, N = int(c["M"]), int(c["N"])
+            minimize(fun, np.zeros(2 * (M - N) * N), args=(c["HOne"], HTwo, c["Ref"], 0), method="BFGS", jac=True,
+                     options={"gtol": 1e-4, "maxiter": 5})
+            del rec.calls[ncalls_eandg:]
         finally:
             os.chdir(cwd)
     out = {"ncalls": len(rec.calls)}
@@ -136,6 +153,9 @@ def main():
         out[f"step{s}_x"] = x
         out[f"step{s}_E"] = E
         out[f"step{s}_g"] = g
+    out["bfgs_x"] = np.array([t[0] for t in traj])
+    out["bfgs_E"] = np.array([t[1] for t in traj])
+    out["bfgs_g"] = np.array([t[2] for t in traj])
     path = os.path.join(HERE, "dropin_trace.npz")
     np.savez_compressed(path, **out)
     print(f"{len(rec.calls)} calls, E = {[r[1] for r in results]} -> {path}")

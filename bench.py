@@ -46,6 +46,13 @@ METRIC = "projected E+grad grid-pts/s, split-prec vs FP64 GPU @|ΔE|≤1e-8 Eh; 
 UNIT = "grid-pts/s"
 
 
+def _json_default(o):
+    """numpy scalars (bools, floats, ints) in the bench line as their Python values."""
+    if isinstance(o, np.generic):
+        return o.item()
+    raise TypeError(f"{type(o).__name__} is not JSON serializable")
+
+
 def _peak_source(peaks, what):
     """Where the bf16 denominator came from: the measured file, or the fallback figure."""
     if peaks.get("fallback"):
@@ -392,7 +399,7 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nth, "cpu_model": cpu_model(), "kind": "port",
                              "sample": desc + "; rate scaled to the full grid (per-point work is independent)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
     return 0
 
 
@@ -681,7 +688,7 @@ def run_ours(args):
                                      "path": "phf_buildhsg_chol (plan set-up from h, B, Ref and the grid "
                                              "inside every call)"}},
                 "gpu_launches": launches, "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_default), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -848,7 +855,7 @@ def run_batch(args):
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "path": "pinned host determinants -> device, phf_eval_batch, accumulators -> pinned host"},
                 "gpu_launches": launches, "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_default), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

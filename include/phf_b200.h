@@ -130,6 +130,11 @@ typedef struct {
     int exchange_panel;                       /* jk_form 3: spatial indices i per exchange panel (rows (i, k)
                                                  of the exchange matrix formed at once); 0 = automatic
                                                  (at most 4096 rows, fewest padded rows) */
+    int autotune;                             /* 1: at the plan's first evaluation, time the candidate launch
+                                                 choices of every GEMM shape the plan uses (FP64 GEMM tile
+                                                 shape, int8 GEMM raster group) and keep the fastest; the table
+                                                 is shared by all plans of the process.  Results are bitwise
+                                                 those of the untuned plan */
 } phf_plan_desc;
 
 int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);
@@ -233,6 +238,8 @@ unsigned long long phf_kernel_launches(void);
  * launches recorded since (it waits for their end events). */
 int phf_profile_enable(int on);
 int phf_profile_read(int kernel_class, double *total_ms, unsigned long long *launches);
+/* GEMM shapes the launch tuner has timed so far in this process (plans created with autotune). */
+int phf_tuned_shapes(void);
 /* Library version string. */
 const char *phf_version(void);
 

@@ -47,6 +47,7 @@ class phf_plan_desc(ctypes.Structure):
         ("point_begin", ctypes.c_int),
         ("point_end", ctypes.c_int),
         ("exchange_panel", ctypes.c_int),
+        ("autotune", ctypes.c_int),
     ]
 
 
@@ -71,6 +72,7 @@ SIGNATURES = {
     "phf_last_error": (ctypes.c_char_p, []),
     "phf_kernel_launches": (ctypes.c_ulonglong, []),
     "phf_version": (ctypes.c_char_p, []),
+    "phf_tuned_shapes": (_I, []),
     "phf_profile_enable": (_I, [_I]),
     "phf_ozaki_dgemm": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P]),
     "phf_tc_dgemm": (_I, [_I, _I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong,

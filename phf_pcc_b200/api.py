@@ -175,12 +175,13 @@ class Plan:
     tensor, ``exchange_panel`` spatial indices per panel, 0 = automatic) or "factorized" (rank-N
     J/K, FP64 only); "auto" takes "eri" up to n = 128 and "streamed" above.  ``gradient``:
     "reference" (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the
-    ket-side term; used by autograd)."""
+    ket-side term; used by autograd).  ``autotune``: time the launch choices of the plan's GEMM shapes
+    at its first evaluation (bitwise the same results)."""
 
     def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
                  rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
                  workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False,
-                 point_range=None, npg=None, ncipg=None, nso=None, exchange_panel=0):
+                 point_range=None, npg=None, ncipg=None, nso=None, exchange_panel=0, autotune=False):
         self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
                         sp, npg, ncipg, nso)
         g = self._g
@@ -204,6 +205,7 @@ class Plan:
         d.workspace_bytes = int(workspace_bytes)
         d.jk_form = {"auto": 0, "eri": 1, "factorized": 2, "streamed": 3}[jk_form]
         d.exchange_panel = int(exchange_panel)
+        d.autotune = 1 if autotune else 0
         self.jk_form = jk_form
         d.gradient_mode = {"reference": 0, "exact": 1}[gradient]
         d.fp64_library_gemm = 1 if fp64_library_gemm else 0

@@ -234,6 +234,7 @@ struct OzArgs {
     int gamma_n;         // > 0: exchange-to-Gamma output (see store_row_chunk), n spatial orbitals
     int g_row0;          // exchange-to-Gamma output: global row of output row 0 (a panel of the exchange rows)
     int a_row0;          // A tiles are read from row a_row0 + m0 of the A slice buffer (a row range of it)
+    int group_m;         // row tiles per column sweep of the raster
     int *err;
 };
 
@@ -317,7 +318,7 @@ __host__ __device__ __forceinline__ long long oz_slice_offset(int t, long long r
 // 1's A and B boxes at 64-byte rows (S = 6) or two units (S = 7: group 1 at 128-byte rows).  The
 // single-pass formats use the same bytes as a ring of packed k-block stages (oz_stage_bytes).
 constexpr int OZ_UNITS = 14;
-constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster
+constexpr int OZ_GROUP_M = 8;  // row tiles per column sweep of the raster (default; the launch tuner may pick another)
 constexpr int OZ_KSEG = 16;    // floating-point formats: k-blocks (512 k-elements) per FP32 accumulation segment
 
 // Tile width and passes per slice count.  S = 5 runs its five groups g = 2..6 in one pass over
@@ -498,15 +499,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const int kseg = max(1, args.kseg);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // grouped raster: CTAs in launch order sweep the column tiles in groups of OZ_GROUP_M row tiles,
+    // grouped raster: CTAs in launch order sweep the column tiles in groups of args.group_m row tiles,
     // so that the A and B tiles the resident CTAs share fit in L2 together
     int m0, n0;
     {
         const int mt = gridDim.x, nt = gridDim.y;
         const int L = blockIdx.y * mt + blockIdx.x;
-        const int width = OZ_GROUP_M * nt;
-        const int first = (L / width) * OZ_GROUP_M;
-        const int gm = min(mt - first, OZ_GROUP_M);
+        const int G = args.group_m > 0 ? args.group_m : OZ_GROUP_M;
+        const int width = G * nt;
+        const int first = (L / width) * G;
+        const int gm = min(mt - first, G);
         m0 = (first + (L % width) % gm) * OZ_BM;
         n0 = ((L % width) / gm) * BN;
     }
@@ -1464,6 +1466,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.gamma_n = 0;
     a.g_row0 = 0;
     a.a_row0 = 0;
+    a.group_m = OZ_GROUP_M;
     a.S = S;
     a.ea = ea;
     a.eb = eb;
@@ -1495,6 +1498,13 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     PHF_CHECK_LAUNCH();
     return PHF_OK;
 }
+
+namespace {
+int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+                   const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
+                   double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
+                   int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m);
+}  // namespace
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n) {
@@ -1530,6 +1540,28 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
+    const TuneKey key{1, m, n, k, (long long)S * 4 + (gamma_n > 0) * 2 + trans, accumulate};
+    int group_m = tuned_choice(key);
+    if (t_tune_record) {
+        // the tuner repeats the launch; an accumulating launch then adds several times, which is harmless:
+        // the tuning evaluation's outputs are discarded and recomputed by the evaluation that follows
+        t_tune_record->push_back({key, {4, 8, 16}, [=](int g, cudaStream_t s) {
+                                      return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0,
+                                                            eb, D, ldd, accumulate, trans, err, s, gamma_n, g_row0,
+                                                            a_row0, kb_total, kb_pass, g);
+                                  }});
+    }
+    if (group_m < 0) group_m = OZ_GROUP_M;
+    return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0, eb, D, ldd, accumulate, trans,
+                          err, st, gamma_n, g_row0, a_row0, kb_total, kb_pass, group_m);
+}
+
+namespace {
+// the k passes of one oz_gemm_ex call with the given raster group
+int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+                   const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
+                   double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
+                   int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m) {
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;
@@ -1537,7 +1569,7 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
         a.kb0 = (int)kb0;
         a.kblocks = (int)std::min(kb_pass, kb_total - kb0);
         a.S = S;
-        a.ea = ea + a_row0;
+        a.ea = ea;
         a.eb = eb;
         a.D = D;
         a.ldd = ldd;
@@ -1549,6 +1581,7 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
         a.gamma_n = gamma_n;
         a.g_row0 = g_row0;
         a.a_row0 = a_row0;
+        a.group_m = group_m;
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
@@ -1559,6 +1592,7 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
     }
     return PHF_OK;
 }
+}  // namespace
 
 }  // namespace phf
 

@@ -305,6 +305,8 @@ int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_compl
                                        reinterpret_cast<cudaStream_t>(stream));
 }
 
+int phf_tuned_shapes(void) { return phf::tuned_entries(); }
+
 int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes) {
     if (!plan) return PHF_ERR_ARG;
     if (chunk) *chunk = plan->impl.b;

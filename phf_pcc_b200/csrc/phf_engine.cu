@@ -297,6 +297,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         p.streamed = (form == 3);
     }
     p.exact = d->gradient_mode == 1;
+    p.autotune = d->autotune != 0;
     p.library_gemm = (d->fp64_library_gemm != 0) && p.eri && p.prec == PHF_PREC_FP64;
     if (p.library_gemm) {
         cublasHandle_t h = nullptr;
@@ -1077,6 +1078,24 @@ bool hermitian_ok(const std::vector<cd> &H, const std::vector<cd> &S, int nci) {
 
 }  // namespace
 
+// Plans created with autotune: before the first capture, run `body` once directly while the GEMM
+// launchers record their launches, then let the launch tuner time the candidates of every shape not
+// yet tuned.  This evaluation's outputs are overwritten by the evaluation that follows.
+template <typename F>
+int maybe_tune(PlanImpl &p, cudaStream_t st, F &&body) {
+    if (!p.autotune || p.tuned || g_prof.on) return PHF_OK;
+    std::vector<TuneCall> calls;
+    t_tune_record = &calls;
+    const int rc = body(st);
+    t_tune_record = nullptr;
+    PHF_TRY(rc);
+    PHF_CUDA(cudaStreamSynchronize(st));
+    if (p.side) PHF_CUDA(cudaStreamSynchronize(p.side));
+    PHF_TRY(tune_recorded(calls, st));
+    p.tuned = true;
+    return PHF_OK;
+}
+
 // buildhsg semantics: newMO = [I; Z] (MO basis), outputs in Fortran layout on the host.
 // Run `body` (a fixed launch sequence of this plan) as a CUDA graph replayed on `st`: captured once
 // on a private stream at first use, so per call the host submits one graph instead of ~100
@@ -1153,6 +1172,10 @@ int plan_buildhsg(PlanImpl &p, const phf_complex *z, phf_complex *hmat, phf_comp
         else
             PHF_CUDA(cudaMemcpyAsync(p.bra, mb, MN * sizeof(zc), cudaMemcpyDeviceToDevice, st));
         PHF_TRY(zgemm_strided(M, N, M, 1, 1, Z1, vz(p.Refw, M, 1), vz(mk, N, 1), Z0, vo(p.kety, N, 1), nullptr, st));
+        if (v == 0 && p.autotune && !p.tuned) {
+            PHF_TRY(maybe_tune(p, st, [&](cudaStream_t s) -> int { return run_variant(p, 0, s); }));
+            PHF_TRY(zero_acc(p, st));
+        }
         PHF_TRY(launch_captured(p, v, st, [&](cudaStream_t s) -> int { return run_variant(p, v, s); }));
     }
     PHF_TRY(fold_acc(p, st));
@@ -1283,10 +1306,12 @@ int eval_enqueue(PlanImpl &p, const zc *d_c, zc *d_hs, zc *d_yg, zc *d_yr, cudaS
         }
         return PHF_OK;
     };
-    if (in_graph)
+    if (in_graph) {
         PHF_TRY(body(st));
-    else
+    } else {
+        PHF_TRY(maybe_tune(p, st, body));
         PHF_TRY(launch_captured(p, 4, st, body));
+    }
     PHF_CUDA(cudaMemcpyAsync(d_hs, p.accHS, 2 * ns * sizeof(zc), cudaMemcpyDeviceToDevice, st));
     if (p.chol) {
         // back to [alpha; beta] order: out[r] = acc[inv[r]]
@@ -1465,6 +1490,12 @@ int plan_eval_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc 
     }
     BatchGraph &bg = g_batch;
     if (!(bg.exec && bg.key == key && bg.epoch == g_plan_epoch && bg.device == dev)) {
+        // plans created with autotune are tuned (one direct evaluation each) before the batch is captured
+        for (int i = 0; i < count; ++i)
+            if (plans[i]->autotune && !plans[i]->tuned) {
+                PHF_TRY(eval_enqueue(*plans[i], d_c[i], d_hs[i], d_yg[i], d_yr[i], st, false));
+                PHF_TRY(read_flag(*plans[i], st));
+            }
         bg.release();
         PHF_TRY(batch_streams(dev));
         PHF_CUDA(cudaMalloc(&bg.d_flags, 2 * (size_t)count * sizeof(int)));

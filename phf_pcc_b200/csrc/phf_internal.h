@@ -2,6 +2,7 @@
 #pragma once
 #include <algorithm>
 #include <complex>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -54,6 +55,29 @@ struct Arena {
     }
 };
 
+
+// Per-shape launch choices found by timing (plans created with autotune): the FP64 GEMM's tile
+// shape and the int8 GEMM's raster group.  Every candidate of a shape computes bitwise the same
+// result (same per-element summation order), so a choice changes only the time.
+struct TuneKey {
+    int kind;                 // 0: FP64 GEMM tile shape, 1: int8 GEMM raster group
+    long long a, b, c, d, e;  // shape and layout parameters of the launch
+    bool operator==(const TuneKey &o) const {
+        return kind == o.kind && a == o.a && b == o.b && c == o.c && d == o.d && e == o.e;
+    }
+};
+struct TuneCall {
+    TuneKey key;
+    std::vector<int> candidates;
+    std::function<int(int, cudaStream_t)> launch;  // launch with a candidate on a stream
+};
+// the table: -1 when the shape has not been tuned
+int tuned_choice(const TuneKey &key);
+int tuned_entries();
+// while non-null, the GEMM launchers append every launch they make (thread-local)
+extern thread_local std::vector<TuneCall> *t_tune_record;
+// times every candidate of every recorded launch whose shape is not in the table yet, keeps the fastest
+int tune_recorded(std::vector<TuneCall> &calls, cudaStream_t st);
 
 // Largest N (occupied orbitals) whose N x N overlap fits the shared-memory inverse.
 constexpr int kMaxOverlapN = 112;
@@ -160,6 +184,7 @@ struct PlanImpl {
     cudaGraphExec_t gexec[5] = {};
     unsigned long long glaunch[5] = {};  // kernels in each graph (for the launch counter)
     bool graphs_ok = true;
+    bool autotune = false, tuned = false;    // time the launch choices of this plan's shapes once
     int nl = 0, ny = 0, npg = 0, nomega = 0;
     int wbeg = 0, wend = 0;          // grid points evaluated: [wbeg, wend)
     int nci = 0, ncisp = 0, ncipg = 0, cmplxconj = 1, qj = 0, sp = 1, nb = 0;

@@ -13,7 +13,7 @@
 // (re re, -im im, re im, im re), two for a real A.
 #include <type_traits>
 
-#include "phf_common.cuh"
+#include "phf_internal.h"
 
 namespace phf {
 
@@ -238,8 +238,19 @@ int launch_tile(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, 
     return PHF_OK;
 }
 
+// Tile shape 0 = 64 x 64, 1 = 128 x 32, 2 = 32 x 128.
+int launch_choice(int tile, int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
+                  const OutView &C, const long long *offs, cudaStream_t st) {
+    if (tile == 1) return launch_tile<128, 32>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    if (tile == 2) return launch_tile<32, 128>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    return launch_tile<64, 64>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+}
+
 }  // namespace
 
+// The tile comes from the launch tuner's table when the shape was tuned, else from rules set by
+// measurements of the per-point products: 128 x 32 for at most 32 output columns and at least 96
+// rows, 32 x 128 in the transposed case, 64 x 64 otherwise.
 int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
                   const OutView &C, const long long *offs, cudaStream_t st) {
     if (m <= 0 || n <= 0 || nb0 <= 0 || nb1 <= 0) return PHF_OK;
@@ -247,9 +258,15 @@ int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A
         set_error(PHF_ERR_ARG, "zgemm_strided: k <= 0");
         return PHF_ERR_ARG;
     }
-    if (n <= 32 && m >= 96) return launch_tile<128, 32>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
-    if (m <= 32 && n >= 96) return launch_tile<32, 128>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
-    return launch_tile<64, 64>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    const TuneKey key{0, (long long)m, (long long)n, (long long)k, (long long)nb0 * 65536 + nb1,
+                      (long long)(A.real * 4 + B.real * 2 + C.real) * 2 + (offs != nullptr)};
+    if (t_tune_record)
+        t_tune_record->push_back({key, {0, 1, 2}, [=](int tile, cudaStream_t s) {
+                                      return launch_choice(tile, m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, s);
+                                  }});
+    int tile = tuned_choice(key);
+    if (tile < 0) tile = (n <= 32 && m >= 96) ? 1 : ((m <= 32 && n >= 96) ? 2 : 0);
+    return launch_choice(tile, m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
 }
 
 }  // namespace phf

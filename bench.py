@@ -720,9 +720,9 @@ def run_batch(args):
     pts = sum(p.grid.npoints for p in probs)
     ws = 512 << 20
 
-    def make(prec):
+    def make(prec, tune=not args.no_autotune):
         return [api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, slices=args.slices, jk_form="eri",
-                         workspace_bytes=ws, **api_kwargs(p)) for p in probs]
+                         workspace_bytes=ws, autotune=tune, **api_kwargs(p)) for p in probs]
 
     def energies(outs):
         res = []
@@ -759,6 +759,12 @@ def run_batch(args):
 
     plans = make(args.precision)
     clk = clock_sampler(local)
+    t_tune = time.perf_counter()
+    tuned0 = int(_lib.load().phf_tuned_shapes())
+    api.eval_batch(plans, Cs)  # first call: tunes the plans' GEMM shapes (autotune) and captures the graph
+    torch.cuda.synchronize()
+    t_tune = time.perf_counter() - t_tune
+    tuned = int(_lib.load().phf_tuned_shapes()) - tuned0
     step_ms, outs, launches = time_batch(plans, args.steps, args.warmup, clk)
     # per-class device time, kernel by kernel
     _lib.profile_enable(True)
@@ -847,7 +853,9 @@ def run_batch(args):
                 "config": {"workload": f"{len(probs)} independent instances, n in {sizes}, N = n/2, L = 4n, "
                                        f"grids 112 / 800 points alternating, {pts} points in all",
                            "precision": args.precision, "jk_form": "eri", "points_per_step": pts,
-                           "batch_branches": branches, "l2": "flushed (256 MB write) between timed steps",
+                           "batch_branches": branches, "autotune": not args.no_autotune,
+                           "tuned_shapes": tuned, "tune_and_capture_s": t_tune,
+                           "l2": "flushed (256 MB write) between timed steps",
                            "parallelism": f"{world} independent batch(es), one per GPU"},
                 "max_abs_dE_vs_fp64": fp64["own_kernels"]["max_abs_dE_vs_fp64"] if fp64 else None,
                 "fp64_gpu": fp64, "roofline": roof, "cpu_baseline": cpu,
@@ -876,6 +884,7 @@ def main():
                          "(on by default for --config c3)")
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
+    ap.add_argument("--no-autotune", action="store_true", help="c4: plans without the launch tuner")
     ap.add_argument("--fp64-all", action="store_true",
                     help="also time the stored-exchange-matrix FP64 form above n = 128 and the factorized FP64 form")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")

@@ -499,7 +499,9 @@ def run_ours(args):
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
     slices = args.slices or 5
 
-    plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form, **kw)
+    tune = not args.no_autotune
+    plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
+                    autotune=tune, **kw)
     clk = clock_sampler(local)
     step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
@@ -527,7 +529,7 @@ def run_ours(args):
             forms.append(("factorized", False, "factorized"))
         for label, lib_gemm, jf in forms:
             plan64 = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="fp64", fp64_library_gemm=lib_gemm,
-                              jk_form=jf, **kw)
+                              jk_form=jf, autotune=tune, **kw)
             n64 = 1 if jf == "factorized" else max(1, min(args.steps, 3))
             ms64, E64, G64, _, prof64 = time_plan(torch, plan64, C, stream, n64, 1, flush, _lib)
             plan64.close()
@@ -582,7 +584,8 @@ def run_ours(args):
     e2e_steps = args.steps if args.e2e_steps is None else args.e2e_steps
     if e2e_steps > 0:
         z0 = np.zeros((p.M - p.N, p.N), dtype=np.complex128)
-        planh = api.Plan(ref=Ref, h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form, **kw)
+        planh = api.Plan(ref=Ref, h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
+                         autotune=tune, **kw)
         for i in range(1 + e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -673,7 +676,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded h, B_L, determinant)",
                 "config": {"workload": workload_name(p), "precision": args.precision, "jk_form": form,
-                           "points_per_step": p.grid.npoints, "chunk": chunk,
+                           "points_per_step": p.grid.npoints, "chunk": chunk, "autotune": tune,
                            "l2": "flushed (256 MB write) between timed steps",
                            "parallelism": f"{world} independent instance(s), one per GPU"},
                 "energy": float(E.item()), "fp64_gpu": fp64, "precision_study": study,
@@ -884,7 +887,7 @@ def main():
                          "(on by default for --config c3)")
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
-    ap.add_argument("--no-autotune", action="store_true", help="c4: plans without the launch tuner")
+    ap.add_argument("--no-autotune", action="store_true", help="plans without the launch tuner")
     ap.add_argument("--fp64-all", action="store_true",
                     help="also time the stored-exchange-matrix FP64 form above n = 128 and the factorized FP64 form")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")

@@ -84,8 +84,9 @@ def test_config2_adjoint_twenty_rotation_steps_against_fd_and_reference_gradient
     * against central finite differences (h = 1e-5) along a random direction, to 1e-6 relative;
     * against the reference's gradient: with Ref = I and the determinant in Thouless form
       [I; Z] = C C_occ^-1, LocalG's G[N:, :N] = dE/dZ* (PHF_fort/PHFTools.f90:203-247) from the
-      reference-mode plan on the full grid equals the autograd gradient's rows N: at [I; Z] (the
-      bra-side and exact gradients differ only by the grid's Hermiticity defect), to 1e-5 of max|G|;
+      reference-mode plan on the full grid equals the autograd gradient carried to Z by the chain
+      rule (the bra-side and exact gradients differ only by the grid's Hermiticity defect), to 1e-5
+      of max|G|;
     * and that reference gradient against the C oracle on a block of 4 grid points (the beta = 0
       Lebedev point): the block's LocalG gradient from the GPU plan and from the oracle within 1e-7,
       the block's energy within 1e-8 Eh."""
@@ -113,13 +114,11 @@ def test_config2_adjoint_twenty_rotation_steps_against_fd_and_reference_gradient
         C0 = p.C
         for step in range(20):
             C0 = synth.orbital_rotation(C0, 1e-2, rng)
-            Z = C0[N:] @ np.linalg.inv(C0[:N])
-            Ct = np.vstack([np.eye(N), Z])                 # the same determinant, Thouless form
-            C = torch.from_numpy(Ct).cuda().requires_grad_(True)
+            C = torch.from_numpy(C0).cuda().requires_grad_(True)
             E = projected_energy(C, pe)
             E.backward()
             grad = C.grad
-            d = rng.normal(size=Ct.shape) + 1j * rng.normal(size=Ct.shape)
+            d = rng.normal(size=C0.shape) + 1j * rng.normal(size=C0.shape)
             d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
             h = 1e-5
             with torch.no_grad():
@@ -128,10 +127,14 @@ def test_config2_adjoint_twenty_rotation_steps_against_fd_and_reference_gradient
             fd = (ep - em).item() / (2 * h)
             an = torch.real(torch.sum(torch.conj(grad) * d)).item()
             assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (step, fd, an)
-            # the reference's gradient on the full grid (bra side, LocalG), dE/dZ*
+            # the reference's gradient on the full grid (bra side, LocalG), dE/dZ* at the Thouless form
+            # [I; Z] = C0 A^-1 (A = C0[:N]) of the same determinant; E(C0) = E([I; Z] A), so
+            # dE/dZ* = (dE/dC0* A^H)[N:, :]
+            A = C0[:N]
+            Z = C0[N:] @ np.linalg.inv(A)
             H, S, Gm, Rm = pr.buildhsg(Z, check_hermitian=False)
             e_ref, G_ref = block_e_g(H, S, Gm, Rm)
-            gz = (grad.cpu().numpy() / 2.0)[N:, :]
+            gz = ((grad.cpu().numpy() / 2.0) @ A.conj().T)[N:, :]
             assert abs(e_ref - E.item()) <= 1e-9 * abs(E.item()), (step, e_ref, E.item())
             assert np.abs(gz - G_ref).max() <= 1e-5 * np.abs(G_ref).max(), (step, np.abs(gz - G_ref).max())
             # that gradient's machinery against the oracle on a block of grid points

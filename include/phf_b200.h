@@ -90,6 +90,22 @@ int phf_localg(const phf_complex *gradmat, const phf_complex *rdmmat, const phf_
                int nso, const phf_complex *fsp, const phf_complex *fpg, const phf_complex *fk, int nci, int ncisp,
                int ncipg, int cmplxconj, phf_complex *g);
 
+/* BuildSC (PHF_fort/PHFTools.f90:464-537, with BuildSC_Vec of PHF_fort/BuildSC_dr.f90): the
+ * grid-projected product of a coupled-cluster-shaped vector (c0, c1(M,M), c2(M,M,M,M), Fortran
+ * layouts c1(a,b) = c1[a + M*b], c2(a,b,c,d) = c2[a + M*(b + M*(c + M*d))]) with the projection of the
+ * reference determinant [I; 0], as LinDep.py:71-76 applies it: per grid point R = R1 R2 Rpg, the
+ * transition density of [I; 0], c1 and c2 transformed with R^H, BuildSC_Vec, weighted by
+ * weightsp det(R[:N,:N]) sum_pq weightpg conj(fpg_p) fpg_q (sum conj fsp)(sum fsp) and divided by the
+ * projected overlap.  As in the reference's loop, rk, fk and the Wigner angles (roota, rootb, rooty,
+ * qj) take no part (the Wigner factor is computed and then set to one, :516-518).  Host buffers in,
+ * t0, t1(M,M), t2(M,M,M,M) out.  FP64 on the GPU; M^4 complex per tensor per grid point of device
+ * memory, grid points run in chunks of a 4 GiB workspace. */
+int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
+                int npg, int qj, int ncisp, int ncipg, int ncik, const phf_complex *r1, const phf_complex *r2,
+                const phf_complex *rpg, const phf_complex *rk, const double *roota, const double *rootb,
+                const double *rooty, const double *weightsp, const double *weightpg, const phf_complex *fsp,
+                const phf_complex *fpg, const phf_complex *fk, phf_complex *t0, phf_complex *t1, phf_complex *t2);
+
 /* ---------------------------------------------------------------- plan API
  * A plan holds the Hamiltonian, the grid and the device workspace, so that repeated
  * energy/gradient evaluations (one per optimiser step, PHF.py:55-91) upload only Z or C. */

@@ -41,4 +41,14 @@ class _PHFToolsModule:
                           ncipg=ncipg)
 
 
+    def buildsc(self, c0, c1, c2, nocc, ngrid, qj, r1, r2, rpg, rk, roota, rootb, rooty, weightsp, weightpg, fsp,
+                fpg, fk, nso=None, npg=None, ncisp=None, ncipg=None, ncik=None):
+        """BuildSC (PHF_fort/PHFTools.f90:464-537) with the f2py argument order of its Fortran dummy
+        arguments (outputs t0, t1, t2 returned; dimensions optional).  The reference's LinDep.py:73
+        passes a different list (it inserts ``nci`` after ``J``), which does not match that Fortran
+        routine; this follows the Fortran."""
+        return api.buildsc(c0, c1, c2, nocc, ngrid, qj, r1, r2, rpg, rk, roota, rootb, rooty, weightsp, weightpg,
+                           fsp, fpg, fk, nso=nso, npg=npg, ncisp=ncisp, ncipg=ncipg, ncik=ncik)
+
+
 phftools = _PHFToolsModule()

@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import PREC, PHFError, check, phf_complex, phf_plan_desc
 
-__all__ = ["buildhsg", "buildhsg_chol", "localg", "Plan", "eval_batch", "check_status", "PHFError"]
+__all__ = ["buildhsg", "buildhsg_chol", "localg", "buildsc", "Plan", "eval_batch", "check_status", "PHFError"]
 
 
 def _fz(a):
@@ -160,6 +160,37 @@ def localg(gradmat, rdmmat, smat, e0, fsp, fpg, fk, cmplxconj, nso=None, nci=Non
                         _ptr(fpg), _ptr(fk), nci, ncisp, ncipg, int(cmplxconj), _ptr(G))
     check(st, "phf_localg")
     return G
+
+
+def buildsc(c0, c1, c2, nocc, ngrid, qj, r1, r2, rpg, rk, roota, rootb, rooty, weightsp, weightpg, fsp, fpg, fk,
+            nso=None, npg=None, ncisp=None, ncipg=None, ncik=None):
+    """BuildSC (PHF_fort/PHFTools.f90:464-537) on the GPU: (t0, t1 (M, M), t2 (M, M, M, M)) for the vector
+    (c0, c1, c2), Fortran-ordered complex128 outputs (see phf_buildsc in include/phf_b200.h)."""
+    c1, c2 = _fz(c1), _fz(c2)
+    M = int(nso) if nso is not None else c1.shape[0]
+    if c1.shape != (M, M) or c2.shape != (M, M, M, M):
+        raise ValueError("c1 must be (M, M) and c2 (M, M, M, M)")
+    r1, r2, rpg, rk = _fz(r1), _fz(r2), _fz(rpg), _fz(rk)
+    ng = np.ascontiguousarray(np.asarray(ngrid, dtype=np.int32).reshape(2))
+    npg = int(npg) if npg is not None else rpg.shape[0]
+    wsp, wpg = _fd(weightsp), _fd(weightpg)
+    fsp_, fpg_, fk_ = (np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.complex128))) for x in (fsp, fpg, fk))
+    ncisp = int(ncisp) if ncisp is not None else fsp_.size
+    ncipg = int(ncipg) if ncipg is not None else fpg_.size
+    ncik = int(ncik) if ncik is not None else fk_.size
+    if r1.shape != (int(ng[0]), M, M) or r2.shape != (int(ng[1]), M, M) or rpg.shape != (npg, M, M):
+        raise ValueError("rotation shapes do not match ngrid, npg and nso")
+    ra, rb, ry = (np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.float64))) for x in (roota, rootb, rooty))
+    c0c = complex(np.asarray(c0).item())
+    t0 = phf_complex()
+    t1 = np.zeros((M, M), dtype=np.complex128, order="F")
+    t2 = np.zeros((M, M, M, M), dtype=np.complex128, order="F")
+    st = _lib.load().phf_buildsc(phf_complex(c0c.real, c0c.imag), _ptr(c1), _ptr(c2), int(nocc), M, _ptr(ng), npg,
+                                 int(qj), ncisp, ncipg, ncik, _ptr(r1), _ptr(r2), _ptr(rpg), _ptr(rk), _ptr(ra),
+                                 _ptr(rb), _ptr(ry), _ptr(wsp), _ptr(wpg), _ptr(fsp_), _ptr(fpg_), _ptr(fk_),
+                                 ctypes.byref(t0), _ptr(t1), _ptr(t2))
+    check(st, "phf_buildsc")
+    return complex(t0.re, t0.im), t1, t2
 
 
 class Plan:

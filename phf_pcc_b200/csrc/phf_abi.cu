@@ -307,6 +307,33 @@ int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_compl
 
 int phf_tuned_shapes(void) { return phf::tuned_entries(); }
 
+int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
+                int npg, int qj, int ncisp, int ncipg, int ncik, const phf_complex *r1, const phf_complex *r2,
+                const phf_complex *rpg, const phf_complex *rk, const double *roota, const double *rootb,
+                const double *rooty, const double *weightsp, const double *weightpg, const phf_complex *fsp,
+                const phf_complex *fpg, const phf_complex *fk, phf_complex *t0, phf_complex *t1, phf_complex *t2) {
+    (void)qj, (void)ncik, (void)rk, (void)roota, (void)rootb, (void)rooty, (void)fk;
+    phf::set_error(PHF_OK, "");
+    if (!c1 || !c2 || !ngrid || !r1 || !r2 || !rpg || !weightsp || !weightpg || !fsp || !fpg || !t0 || !t1 || !t2 ||
+        nso <= 0 || nocc <= 0 || nocc > nso || ngrid[0] <= 0 || ngrid[1] <= 0 || npg <= 0 || ncisp <= 0 ||
+        ncipg <= 0) {
+        phf::set_error(PHF_ERR_ARG, "phf_buildsc: missing or non-positive argument");
+        return PHF_ERR_ARG;
+    }
+    if (nocc > phf::kMaxOverlapN) {
+        phf::set_error(PHF_ERR_UNSUPPORTED, "phf_buildsc: nocc above the overlap inverse's limit");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        phf::set_error(PHF_ERR_NO_DEVICE, "no CUDA device available");
+        return PHF_ERR_NO_DEVICE;
+    }
+    return phf::buildsc_run(c0, c1, c2, nocc, nso, ngrid, npg, r1, r2, rpg, weightsp, weightpg, ncisp, ncipg, fsp,
+                            fpg, 0, t0, t1, t2);
+}
+
 int phf_plan_info(const phf_plan *plan, int *chunk, size_t *workspace_bytes) {
     if (!plan) return PHF_ERR_ARG;
     if (chunk) *chunk = plan->impl.b;

@@ -237,6 +237,12 @@ struct PlanImpl {
 };
 
 
+// buildsc.cu: BuildSC (PHF_fort/PHFTools.f90:464-537) with host arrays in the reference's layouts
+int buildsc_run(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
+                int npg, const phf_complex *r1, const phf_complex *r2, const phf_complex *rpg, const double *weightsp,
+                const double *weightpg, int ncisp, int ncipg, const phf_complex *fsp, const phf_complex *fpg,
+                size_t workspace, phf_complex *t0, phf_complex *t1, phf_complex *t2);
+
 // phf_engine.cu
 int plan_eval_batch(PlanImpl *const *plans, int count, const zc *const *d_c, zc *const *d_hs, zc *const *d_yg,
                     zc *const *d_yr, cudaStream_t st);

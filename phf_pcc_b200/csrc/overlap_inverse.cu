@@ -1,6 +1,6 @@
 // Batched FP64 complex inverse, determinant and log-determinant of the rotated overlaps
-// S_w = bra^H R_w ket (N x N): one warp per grid point for N <= 32, else one CTA per grid point,
-// the matrix resident in shared memory.
+// S_w = bra^H R_w ket (N x N): one warp per grid point for N <= 32, else one CTA of 32 x 32 threads
+// per grid point, the matrix resident in shared memory.
 //
 // Replaces InvertC (ZGETRF + ZGETRI) and determinantC (ZGETRF) of PHF_fort/Wrappers.f90:195-336
 // as called from RDM (PHF_fort/PHFTools.f90:259-260).  Algorithm: in-place Gauss-Jordan
@@ -18,97 +18,107 @@ namespace phf {
 
 namespace {
 
-constexpr int NT = 256;
+// One CTA of 32 x 32 threads per grid point (N > 32): thread (ty, tx) updates the elements of rows
+// ty + 32 m and columns tx + 32 q, so a Gauss-Jordan step is four barriers -- the pivot search is one
+// warp's shuffle arg-max -- and no index division.  Element updates, pivot choice and the determinant
+// are those of the algorithm above, operation for operation.
+constexpr int GJ_T = 32;  // threads per row and per column of the CTA
 
-__global__ void __launch_bounds__(NT) gj_inverse_kernel(int N, const zc *__restrict__ S, long long s_rs,
-                                                        long long s_bs, zc *__restrict__ Sinv, long long i_rs,
-                                                        long long i_bs, zc *__restrict__ det, zc *__restrict__ logdet,
-                                                        int *__restrict__ flag) {
+__global__ void __launch_bounds__(GJ_T *GJ_T) gj_inverse_kernel(int N, const zc *__restrict__ S, long long s_rs,
+                                                                 long long s_bs, zc *__restrict__ Sinv, long long i_rs,
+                                                                 long long i_bs, zc *__restrict__ det,
+                                                                 zc *__restrict__ logdet, int *__restrict__ flag) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     zc *A = reinterpret_cast<zc *>(smem_raw);                 // N*N, row-major
     zc *rowk = A + (size_t)N * N;                             // N
     zc *colk = rowk + N;                                      // N
     int *perm = reinterpret_cast<int *>(colk + N);            // N
-    __shared__ double red_v[NT];
-    __shared__ int red_i[NT];
-    __shared__ int s_bad;
+    __shared__ int s_bad, s_piv;
+    __shared__ double s_pv;
 
-    const int tid = threadIdx.x;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * GJ_T + tx;
+    constexpr int NTH = GJ_T * GJ_T;
     const long long b = blockIdx.x;
     const zc *Sb = S + b * s_bs;
     if (tid == 0) s_bad = 0;
     __syncthreads();
-    for (int e = tid; e < N * N; e += NT) {
-        int i = e / N, j = e - i * N;
-        zc v = Sb[(long long)i * s_rs + j];
-        if (!isfinite(v.x) || !isfinite(v.y)) s_bad = 2;
-        A[e] = v;
-    }
+    for (int i = ty; i < N; i += GJ_T)
+        for (int j = tx; j < N; j += GJ_T) {
+            const zc v = Sb[(long long)i * s_rs + j];
+            if (!isfinite(v.x) || !isfinite(v.y)) s_bad = 2;
+            A[i * N + j] = v;
+        }
     __syncthreads();
 
-    double logabs = 0.0, phase = 0.0;
+    double logabs = 0.0, phase = 0.0;  // kept by thread 0
     zc d = mkz(1.0, 0.0);
     int nswap = 0;
     for (int k = 0; k < N && s_bad == 0; ++k) {
-        // pivot search: first index of the maximal |re| + |im| in rows k..N-1 of column k
-        double best = -1.0;
-        int bi = N;
-        for (int i = k + tid; i < N; i += NT) {
-            double a = abs1(A[i * N + k]);
-            if (a > best) { best = a; bi = i; }
-        }
-        red_v[tid] = best;
-        red_i[tid] = bi;
-        __syncthreads();
-        for (int s = NT / 2; s > 0; s >>= 1) {
-            if (tid < s) {
-                double ov = red_v[tid + s];
-                int oi = red_i[tid + s];
-                if (ov > red_v[tid] || (ov == red_v[tid] && oi < red_i[tid])) {
-                    red_v[tid] = ov;
-                    red_i[tid] = oi;
+        // pivot search (warp 0): first index of the maximal |re| + |im| in rows k..N-1 of column k
+        if (ty == 0) {
+            double best = -1.0;
+            int bi = N;
+            for (int i = k + tx; i < N; i += GJ_T) {
+                const double a = abs1(A[i * N + k]);
+                if (a > best) {
+                    best = a;
+                    bi = i;
                 }
             }
-            __syncthreads();
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                if (ov > best || (ov == best && oi < bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (tx == 0) {
+                s_piv = bi;
+                s_pv = best;
+            }
         }
-        const int p = red_i[0];
-        const double pv = red_v[0];
         __syncthreads();
+        const int p = s_piv;
+        const double pv = s_pv;
         if (!(pv > 0.0)) {  // exactly singular (or NaN pivot)
             if (tid == 0) s_bad = (pv == 0.0) ? 1 : 2;
             __syncthreads();
             break;
         }
-        if (p != k) {
-            for (int j = tid; j < N; j += NT) {
-                zc t = A[k * N + j];
-                A[k * N + j] = A[p * N + j];
-                A[p * N + j] = t;
-            }
+        if (p != k && tid < N) {
+            const zc t = A[k * N + tid];
+            A[k * N + tid] = A[p * N + tid];
+            A[p * N + tid] = t;
         }
         if (tid == 0) perm[k] = p;
         __syncthreads();
         const zc piv = A[k * N + k];
-        // running determinant and log-determinant (every thread keeps the same copy)
-        d = d * piv;
-        logabs += log(hypot(piv.x, piv.y));
-        phase += atan2(piv.y, piv.x);
-        if (p != k) {
-            d = mkz(-d.x, -d.y);
-            ++nswap;
+        if (tid == 0) {  // running determinant and log-determinant
+            d = d * piv;
+            logabs += log(hypot(piv.x, piv.y));
+            phase += atan2(piv.y, piv.x);
+            if (p != k) {
+                d = mkz(-d.x, -d.y);
+                ++nswap;
+            }
         }
         const zc inv = divz(mkz(1.0, 0.0), piv);
         // scaled pivot row (with 1/piv in column k) and the saved column k
-        for (int j = tid; j < N; j += NT) rowk[j] = (j == k) ? inv : A[k * N + j] * inv;
-        for (int i = tid; i < N; i += NT) colk[i] = A[i * N + k];
+        if (tid < N) rowk[tid] = (tid == k) ? inv : A[k * N + tid] * inv;
+        else if (tid < 2 * N && tid - N < NTH) colk[tid - N] = A[(tid - N) * N + k];
         __syncthreads();
-        for (int e = tid; e < N * N; e += NT) {
-            int i = e / N, j = e - i * N;
-            if (i == k) {
-                A[e] = rowk[j];
-            } else {
-                zc a = (j == k) ? mkz(0.0, 0.0) : A[e];
-                A[e] = a - colk[i] * rowk[j];
+        for (int i = ty; i < N; i += GJ_T) {
+            const zc ci = colk[i];
+            for (int j = tx; j < N; j += GJ_T) {
+                const int e = i * N + j;
+                if (i == k) {
+                    A[e] = rowk[j];
+                } else {
+                    const zc a = (j == k) ? mkz(0.0, 0.0) : A[e];
+                    A[e] = a - ci * rowk[j];
+                }
             }
         }
         __syncthreads();
@@ -118,21 +128,17 @@ __global__ void __launch_bounds__(NT) gj_inverse_kernel(int N, const zc *__restr
         // undo the row interchanges as column interchanges, in reverse order
         for (int k = N - 1; k >= 0; --k) {
             const int p = perm[k];
-            if (p != k) {
-                for (int i = tid; i < N; i += NT) {
-                    zc t = A[i * N + k];
-                    A[i * N + k] = A[i * N + p];
-                    A[i * N + p] = t;
-                }
+            if (p != k && tid < N) {
+                const zc t = A[tid * N + k];
+                A[tid * N + k] = A[tid * N + p];
+                A[tid * N + p] = t;
             }
             __syncthreads();
         }
     }
     zc *Ib = Sinv + b * i_bs;
-    for (int e = tid; e < N * N; e += NT) {
-        int i = e / N, j = e - i * N;
-        Ib[(long long)i * i_rs + j] = bad ? mkz(0.0, 0.0) : A[e];
-    }
+    for (int i = ty; i < N; i += GJ_T)
+        for (int j = tx; j < N; j += GJ_T) Ib[(long long)i * i_rs + j] = bad ? mkz(0.0, 0.0) : A[i * N + j];
     if (tid == 0) {
         if (bad) {
             det[b] = mkz(0.0, 0.0);
@@ -328,7 +334,7 @@ int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_b
     size_t smem = overlap_inverse_smem(N);
     PHF_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ProfScope prof(st, PROF_INVERSE);
-    gj_inverse_kernel<<<batch, NT, smem, st>>>(N, S, s_rs, s_bs, Sinv, i_rs, i_bs, det, logdet, flag);
+    gj_inverse_kernel<<<batch, dim3(GJ_T, GJ_T), smem, st>>>(N, S, s_rs, s_bs, Sinv, i_rs, i_bs, det, logdet, flag);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

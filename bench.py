@@ -493,7 +493,7 @@ def run_ours(args):
     p = problem_for(args.config, seed=1000 + rank)
     Ref, Z = p.ref_and_z()
     kw = api_kwargs(p)
-    form = jk_form_of(p)
+    form = jk_form_of(p) if args.jk_form == "auto" else args.jk_form
     C = torch.from_numpy(p.C).to(dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
@@ -888,6 +888,8 @@ def main():
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="plans without the launch tuner")
+    ap.add_argument("--jk-form", default="auto", choices=["auto", "eri", "streamed"],
+                    help="J/K form (auto: stored exchange matrix up to n = 128, streamed above)")
     ap.add_argument("--fp64-all", action="store_true",
                     help="also time the stored-exchange-matrix FP64 form above n = 128 and the factorized FP64 form")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")

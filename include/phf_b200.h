@@ -256,6 +256,10 @@ int phf_profile_enable(int on);
 int phf_profile_read(int kernel_class, double *total_ms, unsigned long long *launches);
 /* GEMM shapes the launch tuner has timed so far in this process (plans created with autotune). */
 int phf_tuned_shapes(void);
+/* Whether the int8 GEMM may run its 256-row tiles on CTA pairs (default 1; results are identical
+   either way).  Returns the previous setting.  Plans captured into CUDA graphs keep the form they
+   were captured with. */
+int phf_int8_cta_pairs(int on);
 /* Library version string. */
 const char *phf_version(void);
 

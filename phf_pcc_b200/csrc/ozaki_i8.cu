@@ -119,6 +119,34 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
+// CTA-pair form: the bytes land in this CTA's shared memory and complete on the mbarrier at the
+// shared::cluster address bar (the pair's leading CTA holds the full barriers of both halves).
+__device__ __forceinline__ void tma_load_2d_pair(const CUtensorMap *map, uint32_t bar, void *dst, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// shared::cluster address of the variable at shared::cta address a in cluster CTA `rank`
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t a, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// every thread of both CTAs of the cluster
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // Shared-memory matrix descriptor: K-major, SWIZZLE_128B (8 rows x 128 B atoms, SBO = 1024 B).
 __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     uint64_t d = 0;
@@ -152,18 +180,32 @@ __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = BN.
-template <int BN>
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = BM (128 for one CTA,
+// 256 for a CTA pair), N = BN.
+template <int BN, int BM = OZ_BM>
 __host__ __device__ constexpr uint32_t idesc_i8() {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
+// CG = 1: one CTA's 128 x N tile.  CG = 2: issued by the leading CTA of a pair for the pair's
+// 256 x N tile -- A rows 0..127 from this CTA's shared memory and 128..255 from the peer's at the
+// same offset, B columns 0..N/2-1 from this CTA and N/2..N-1 from the peer, each CTA's half of D
+// in its own TMEM at the same address.
+template <int CG>
 __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    if constexpr (CG == 2) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    }
 }
 
 // Instruction descriptors with FP32 accumulation, K-major A and B, M = 128, N = BN: kind::f16 with
@@ -196,6 +238,25 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+
+// CTA pair: one arrival, once the pair's MMAs issued so far complete, on the mbarrier at this
+// offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+    const unsigned short mask = 3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+template <int CG>
+__device__ __forceinline__ void mma_commit_cg(uint64_t *bar) {
+    if constexpr (CG == 2)
+        mma_commit_pair(bar);
+    else
+        mma_commit(bar);
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
@@ -352,24 +413,33 @@ constexpr uint32_t OZ_UNIT = 16384;
 // stage of the ring instead of whole 16 KB units: A (BM x 128 B) at 0, B (BN x 128 B) at BM 128 and,
 // for S = 5, the fifth slice's A (BM x 32 B) and B (BN x 32 B) behind them.  For S = 5 that is 35 KB
 // per k-block (6 stages in flight instead of 4.7 k-blocks of three units); the ring's depth, not its
-// bandwidth, is what keeps the MMAs fed.
+// bandwidth, is what keeps the MMAs fed.  In a CTA pair (CG = 2) each CTA's stage holds its own 128
+// rows of A and half of the tile's B rows (BN / 2): 28 KB for S = 5, eight stages.
 __host__ __device__ constexpr bool oz_staged(int S) { return oz_npass(S) == 1; }
-__host__ __device__ constexpr uint32_t oz_stage_bytes(int S) {
-    return (OZ_BM + (uint32_t)oz_bn(S)) * 128u + (oz_g1_width(S) == 1 ? (OZ_BM + (uint32_t)oz_bn(S)) * 32u : 0u);
+__host__ __device__ constexpr uint32_t oz_stage_b_rows(int S, int CG) { return (uint32_t)oz_bn(S) / (uint32_t)CG; }
+__host__ __device__ constexpr uint32_t oz_stage_bytes(int S, int CG = 1) {
+    return (OZ_BM + oz_stage_b_rows(S, CG)) * 128u +
+           (oz_g1_width(S) == 1 ? (OZ_BM + oz_stage_b_rows(S, CG)) * 32u : 0u);
 }
 // stage footprint in the ring, a multiple of 1024 bytes (the SWIZZLE_128B atom)
-__host__ __device__ constexpr uint32_t oz_stage_pitch(int S) { return (oz_stage_bytes(S) + 1023u) / 1024u * 1024u; }
-__host__ __device__ constexpr int oz_stages(int S) { return (int)((OZ_UNITS * OZ_UNIT) / oz_stage_pitch(S)); }
+__host__ __device__ constexpr uint32_t oz_stage_pitch(int S, int CG = 1) {
+    return (oz_stage_bytes(S, CG) + 1023u) / 1024u * 1024u;
+}
+__host__ __device__ constexpr int oz_stages(int S, int CG = 1) {
+    return (int)((OZ_UNITS * OZ_UNIT) / oz_stage_pitch(S, CG));
+}
+// the pair form: single-pass int8 slice counts
+__host__ __device__ constexpr bool oz_pair_ok(int S) { return S >= 1 && S <= 5; }
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
 // so that each descriptor is a tile's base descriptor plus a constant (+2 per 32 bytes): the
 // single issuing thread runs barely ahead of the tensor core, and any latency between two MMAs
 // is tensor-core idle time.  dA0/dB0: group-0 tiles, dA1/dB1: group-1 tiles.
-template <int S, int P>
+template <int S, int P, int CG = 1>
 __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64_t dB0, uint64_t dA1, uint64_t dB1,
                                              uint32_t acc_in) {
     constexpr int g0 = oz_g0(P), g1 = oz_g1(S, P), BN = oz_bn(S);
-    constexpr uint32_t idesc = idesc_i8<BN>();
+    constexpr uint32_t idesc = idesc_i8<BN, OZ_BM * CG>();
 #pragma unroll
     for (int g = g0; g <= g1; ++g) {
 #pragma unroll
@@ -377,7 +447,7 @@ __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64
             const int u = g - t;
             const uint64_t a = (t > OZ_GP ? dA1 : dA0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
             const uint64_t b = (u > OZ_GP ? dB1 : dB0) + (uint64_t)(2 * ((u - 1) % OZ_GP));
-            mma_i8(acc0 + (uint32_t)(g - g0) * BN, a, b, idesc, t > 1 ? 1u : acc_in);
+            mma_i8<CG>(acc0 + (uint32_t)(g - g0) * BN, a, b, idesc, t > 1 ? 1u : acc_in);
         }
     }
 }
@@ -406,12 +476,12 @@ __device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, u
 
 // The MMA issuer's k-block loop of pass P (u, ph: next ring unit -- or stage, for the single-pass
 // formats -- and its full-barrier parity).
-template <int S, int P>
+template <int S, int P, int CG = 1>
 __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
                                          uint64_t *full_bar, uint64_t *empty_bar, int *err) {
     if constexpr (oz_staged(S)) {
-        constexpr int NS = oz_stages(S), BN = oz_bn(S);
-        constexpr uint32_t PITCH = oz_stage_pitch(S);
+        constexpr int NS = oz_stages(S, CG);
+        constexpr uint32_t PITCH = oz_stage_pitch(S, CG), BR = oz_stage_b_rows(S, CG);
         for (int kb = 0; kb < KB; ++kb) {
             if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -423,12 +493,12 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
             } else {
                 uint64_t dA1 = 0, dB1 = 0;
                 if constexpr (oz_g1_width(S) == 1) {
-                    dA1 = sdesc_sw32(base + (OZ_BM + BN) * 128);
-                    dB1 = sdesc_sw32(base + (OZ_BM + BN) * 128 + OZ_BM * 32);
+                    dA1 = sdesc_sw32(base + (OZ_BM + BR) * 128);
+                    dB1 = sdesc_sw32(base + (OZ_BM + BR) * 128 + OZ_BM * 32);
                 }
-                issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
+                issue_kblock<S, P, CG>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
             }
-            mma_commit(&empty_bar[u]);  // the stage is reusable once these MMAs have read it
+            mma_commit_cg<CG>(&empty_bar[u]);  // the stage (in both CTAs of a pair) is reusable once read
             if (++u == NS) {
                 u = 0;
                 ph ^= 1u;
@@ -467,11 +537,16 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
     }
 }
 
-template <int S>
+template <int S, int CG = 1>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmB0,
                          const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
                          OzArgs args) {
+    // CG = 2: clusters of two CTAs share one 256 x BN tile (CTA rank r holds output rows 128 r ..
+    // 128 r + 127, and B rows r BN/2 .. r BN/2 + BN/2 - 1 in its ring); the leading CTA (rank 0)
+    // issues the pair's MMAs and holds the full barriers that both CTAs' loads complete on.
+    static_assert(CG == 1 || (CG == 2 && oz_pair_ok(S)), "the CTA-pair form takes single-pass int8 slices");
+    constexpr bool PAIR = CG == 2;
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = oz_smem_raw;
     if ((smem_u32(oz_smem_raw) & 1023u) != 0u) {  // the swizzled tiles need a 1024-byte aligned base
@@ -499,17 +574,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const int kseg = max(1, args.kseg);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // grouped raster: CTAs in launch order sweep the column tiles in groups of args.group_m row tiles,
-    // so that the A and B tiles the resident CTAs share fit in L2 together
+    const uint32_t rank = PAIR ? cluster_rank() : 0u;
+    // grouped raster: CTAs (CTA pairs) in launch order sweep the column tiles in groups of
+    // args.group_m row tiles (row-tile pairs), so that the A and B tiles the resident CTAs share fit
+    // in L2 together
     int m0, n0;
     {
-        const int mt = gridDim.x, nt = gridDim.y;
-        const int L = blockIdx.y * mt + blockIdx.x;
+        const int mt = gridDim.x / CG, nt = gridDim.y;
+        const int L = blockIdx.y * mt + blockIdx.x / CG;
         const int G = args.group_m > 0 ? args.group_m : OZ_GROUP_M;
         const int width = G * nt;
         const int first = (L / width) * G;
         const int gm = min(mt - first, G);
-        m0 = (first + (L % width) % gm) * OZ_BM;
+        m0 = ((first + (L % width) % gm) * CG + (int)rank) * OZ_BM;
         n0 = ((L % width) / gm) * BN;
     }
     const int am0 = m0 + args.a_row0;           // first row of the A tile in the A slice buffer
@@ -542,18 +619,29 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(kUnit, args.eb[n0 + c]) : 0.0;
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        if constexpr (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                smem_u32(tmem_slot)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                smem_u32(tmem_slot)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    // a pair's barriers are initialised in both CTAs before either CTA's loads or commits reach them
+    if constexpr (PAIR) cluster_sync_all();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
         if (lane == 0 && oz_staged(S)) {  // TMA producer, one stage per k-block
-            constexpr int NS = oz_stages(S);
-            constexpr uint32_t PITCH = oz_stage_pitch(S), BYTES = oz_stage_bytes(S);
+            constexpr int NS = oz_stages(S, CG);
+            constexpr uint32_t PITCH = oz_stage_pitch(S, CG), BYTES = oz_stage_bytes(S, CG);
+            constexpr int BR = (int)oz_stage_b_rows(S, CG);
+            const int nb0 = n0 + (int)rank * BR;  // this CTA's B rows
             int sg = 0;           // next stage
             uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
             bool wrapped = false;
@@ -564,12 +652,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     break;
                 }
                 unsigned char *dst = smem + (size_t)sg * PITCH;
-                mbar_arrive_expect_tx(&full_bar[sg], BYTES);
-                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
-                tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
-                if constexpr (W1 == 1) {
-                    tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
-                    tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
+                if constexpr (PAIR) {
+                    // both halves complete on the leading CTA's full barrier, which expects them both
+                    const uint32_t fb = cluster_addr(smem_u32(&full_bar[sg]), 0u);
+                    if (rank == 0) mbar_arrive_expect_tx(&full_bar[sg], 2 * BYTES);
+                    tma_load_2d_pair(&tmA0, fb, dst, kbg * 128, am0);
+                    tma_load_2d_pair(&tmB0, fb, dst + OZ_BM * 128, kbg * 128, nb0);
+                    if constexpr (W1 == 1) {
+                        tma_load_2d_pair(&tmA1, fb, dst + (OZ_BM + BR) * 128, kbg * 32, am0);
+                        tma_load_2d_pair(&tmB1, fb, dst + (OZ_BM + BR) * 128 + OZ_BM * 32, kbg * 32, nb0);
+                    }
+                } else {
+                    mbar_arrive_expect_tx(&full_bar[sg], BYTES);
+                    tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
+                    tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
+                    if constexpr (W1 == 1) {
+                        tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
+                        tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
+                    }
                 }
                 if (++sg == NS) {
                     sg = 0;
@@ -617,7 +717,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {  // MMA issuer
+        if (lane == 0 && rank == 0) {  // MMA issuer (a pair's leading CTA)
             int u = 0;         // next unit
             uint32_t ph = 0;   // parity of its full-barrier phase
             bool ok = true;
@@ -650,11 +750,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 }
                 const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
                 if (p == 0)
-                    ok = mma_pass<S, 0>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
+                    ok = mma_pass<S, 0, CG>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
                 else if constexpr (oz_npass(S) > 1)
                     ok = mma_pass<S, 1>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
                 if (!ok) *abort_flag = 1;
-                mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
+                // the pass's accumulators (in both CTAs of a pair) are final once its MMAs complete
+                mma_commit_cg<CG>(pass_bar);
             }
         }
     } else {
@@ -761,9 +862,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    // neither CTA of a pair leaves (freeing its shared memory and barriers) or frees TMEM while the
+    // other still uses them
+    if constexpr (PAIR) cluster_sync_all();
     if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
+        if constexpr (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
     }
 }
 
@@ -1409,6 +1516,17 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
 namespace {
 using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap, OzArgs);
 
+OzKernelFn oz_pair_kernel_for(int S) {
+    switch (S) {
+        case 1: return ozaki_i8_gemm_kernel<1, 2>;
+        case 2: return ozaki_i8_gemm_kernel<2, 2>;
+        case 3: return ozaki_i8_gemm_kernel<3, 2>;
+        case 4: return ozaki_i8_gemm_kernel<4, 2>;
+        case 5: return ozaki_i8_gemm_kernel<5, 2>;
+        default: return nullptr;
+    }
+}
+
 OzKernelFn oz_kernel_for(int S) {
     switch (S) {
         case 1: return ozaki_i8_gemm_kernel<1>;
@@ -1500,10 +1618,13 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
 }
 
 namespace {
-int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+int oz_gemm_launch(OzKernelFn kern, int cg, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
                    const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
                    double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
                    int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m);
+
+// Launch choices of the int8 GEMM: raster group g for single CTAs, 100 + g for CTA pairs.
+constexpr int kOzPairChoice = 100;
 }  // namespace
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
@@ -1526,39 +1647,53 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
-    CUtensorMap ta0, ta1, tb0, tb1;
+    CUtensorMap ta0, ta1, tb0, tb1, tp0, tp1;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
+    const long long mt = mpad / OZ_BM;
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, a_rows_pad, S, OZ_BM));
     PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
+    // CTA pairs (256 x BN tiles, each CTA loading half of the B rows) for single-pass int8 slices and
+    // more than one row tile
+    const bool pair_ok = oz_pair_ok(S) && mt >= 2 && !g_no_pair;
+    if (pair_ok) PHF_TRY(make_slice_maps(&tp0, &tp1, Bsl, kpad, npad, S, oz_bn(S) / 2));
     const long long kb_pass = oz_kb_pass(S);
     const long long kb_total = kpad / OZ_BK;
     const size_t smem = oz_smem_bytes();
-    const OzKernelFn kern = oz_kernel_for(S);
-    if (!kern) {
+    const OzKernelFn kern = oz_kernel_for(S), pkern = pair_ok ? oz_pair_kernel_for(S) : nullptr;
+    if (!kern || (pair_ok && !pkern)) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
+    if (pkern)
+        PHF_CUDA(cudaFuncSetAttribute((const void *)pkern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned ntiles = (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S));
+    const dim3 grid((unsigned)mt, ntiles, 1);                          // grouped raster
+    const dim3 pgrid((unsigned)(2 * ((mt + 1) / 2)), ntiles, 1);       // row tiles in pairs
+    const auto run = [=](int choice, cudaStream_t s) {
+        if (choice >= kOzPairChoice && pkern)
+            return oz_gemm_launch(pkern, 2, pgrid, smem, ta0, tp0, ta1, tp1, m, n, S, ea + a_row0, eb, D, ldd,
+                                  accumulate, trans, err, s, gamma_n, g_row0, a_row0, kb_total, kb_pass,
+                                  choice - kOzPairChoice);
+        return oz_gemm_launch(kern, 1, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0, eb, D, ldd, accumulate,
+                              trans, err, s, gamma_n, g_row0, a_row0, kb_total, kb_pass, choice % kOzPairChoice);
+    };
     const TuneKey key{1, m, n, k, (long long)S * 4 + (gamma_n > 0) * 2 + trans, accumulate};
-    int group_m = tuned_choice(key);
+    int choice = tuned_choice(key);
     if (t_tune_record) {
         // the tuner repeats the launch; an accumulating launch then adds several times, which is harmless:
         // the tuning evaluation's outputs are discarded and recomputed by the evaluation that follows
-        t_tune_record->push_back({key, {4, 8, 16}, [=](int g, cudaStream_t s) {
-                                      return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0,
-                                                            eb, D, ldd, accumulate, trans, err, s, gamma_n, g_row0,
-                                                            a_row0, kb_total, kb_pass, g);
-                                  }});
+        std::vector<int> cands{4, 8, 16};
+        if (pkern) cands.insert(cands.end(), {kOzPairChoice + 4, kOzPairChoice + 8, kOzPairChoice + 16});
+        t_tune_record->push_back({key, cands, run});
     }
-    if (group_m < 0) group_m = OZ_GROUP_M;
-    return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0, eb, D, ldd, accumulate, trans,
-                          err, st, gamma_n, g_row0, a_row0, kb_total, kb_pass, group_m);
+    if (choice < 0 || (choice >= kOzPairChoice && !pkern)) choice = (pkern ? kOzPairChoice : 0) + OZ_GROUP_M;
+    return run(choice, st);
 }
 
 namespace {
-// the k passes of one oz_gemm_ex call with the given raster group
-int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+// the k passes of one oz_gemm_ex call with the given raster group (cg = 2: clusters of two CTAs)
+int oz_gemm_launch(OzKernelFn kern, int cg, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
                    const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
                    double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
                    int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m) {
@@ -1585,7 +1720,23 @@ int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &t
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
-            kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
+            if (cg == 2) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = grid;
+                cfg.blockDim = dim3(OZ_THREADS, 1, 1);
+                cfg.dynamicSmemBytes = smem;
+                cfg.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = 2;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                PHF_CUDA(cudaLaunchKernelEx(&cfg, kern, ta0, tb0, ta1, tb1, a));
+            } else {
+                kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
+            }
         }
         ++g_launches;
         PHF_CHECK_LAUNCH();

@@ -307,6 +307,12 @@ int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_compl
 
 int phf_tuned_shapes(void) { return phf::tuned_entries(); }
 
+int phf_int8_cta_pairs(int on) {
+    const int was = !phf::g_no_pair;
+    phf::g_no_pair = on ? 0 : 1;
+    return was;
+}
+
 int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
                 int npg, int qj, int ncisp, int ncipg, int ncik, const phf_complex *r1, const phf_complex *r2,
                 const phf_complex *rpg, const phf_complex *rk, const double *roota, const double *rootb,

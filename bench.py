@@ -888,8 +888,8 @@ def main():
     ap.add_argument("--slices", type=int, default=0, help="int8 slices per operand (0 = library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="plans without the launch tuner")
-    ap.add_argument("--no-int8-pairs", action="store_true",
-                    help="int8 GEMMs on single CTAs only (no CTA pairs; same results)")
+    ap.add_argument("--narrow-mma", action="store_true",
+                    help="int8 GEMMs with one MMA per slice pair instead of the wide issue (same results)")
     ap.add_argument("--jk-form", default="auto", choices=["auto", "eri", "streamed"],
                     help="J/K form (auto: stored exchange matrix up to n = 128, streamed above)")
     ap.add_argument("--fp64-all", action="store_true",
@@ -900,10 +900,10 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.no_int8_pairs:
+    if args.narrow_mma:
         from phf_pcc_b200 import _lib
 
-        _lib.load().phf_int8_cta_pairs(0)
+        _lib.load().phf_int8_wide_mma(0)
     if args.config == "c4":
         return run_batch(args)
     return run_ours(args)

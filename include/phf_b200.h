@@ -256,10 +256,11 @@ int phf_profile_enable(int on);
 int phf_profile_read(int kernel_class, double *total_ms, unsigned long long *launches);
 /* GEMM shapes the launch tuner has timed so far in this process (plans created with autotune). */
 int phf_tuned_shapes(void);
-/* Whether the int8 GEMM may run its 256-row tiles on CTA pairs (default 1; results are identical
-   either way).  Returns the previous setting.  Plans captured into CUDA graphs keep the form they
-   were captured with. */
-int phf_int8_cta_pairs(int on);
+/* Whether the int8 GEMM (1 to 5 slices) issues one tensor-core MMA per A slice against the B slices
+   it multiplies, laid side by side (default 1), or one MMA per slice pair (0).  The int32 sums are the
+   same, so results are identical either way; the setting exists for comparisons.  Returns the previous
+   setting.  Plans captured into CUDA graphs keep the form they were captured with. */
+int phf_int8_wide_mma(int on);
 /* Library version string. */
 const char *phf_version(void);
 

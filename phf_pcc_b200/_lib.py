@@ -73,7 +73,7 @@ SIGNATURES = {
     "phf_kernel_launches": (ctypes.c_ulonglong, []),
     "phf_version": (ctypes.c_char_p, []),
     "phf_tuned_shapes": (_I, []),
-    "phf_int8_cta_pairs": (_I, [_I]),
+    "phf_int8_wide_mma": (_I, [_I]),
     "phf_buildsc": (_I, [phf_complex, _P, _P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                          _P, _P, _P, _P, _P]),
     "phf_profile_enable": (_I, [_I]),

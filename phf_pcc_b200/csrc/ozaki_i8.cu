@@ -119,34 +119,6 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
-// CTA-pair form: the bytes land in this CTA's shared memory and complete on the mbarrier at the
-// shared::cluster address bar (the pair's leading CTA holds the full barriers of both halves).
-__device__ __forceinline__ void tma_load_2d_pair(const CUtensorMap *map, uint32_t bar, void *dst, int c0, int c1) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
-        "%4}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1)
-        : "memory");
-}
-
-// shared::cluster address of the variable at shared::cta address a in cluster CTA `rank`
-__device__ __forceinline__ uint32_t cluster_addr(uint32_t a, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-    return r;
-}
-
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-// every thread of both CTAs of the cluster
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
 // Shared-memory matrix descriptor: K-major, SWIZZLE_128B (8 rows x 128 B atoms, SBO = 1024 B).
 __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     uint64_t d = 0;
@@ -180,32 +152,23 @@ __device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = BM (128 for one CTA,
-// 256 for a CTA pair), N = BN.
-template <int BN, int BM = OZ_BM>
+// Instruction descriptor: kind::i8, D = s32, A = B = s8, both K-major, M = 128, N = BN.
+template <int BN>
 __host__ __device__ constexpr uint32_t idesc_i8() {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
 }
 
-// CG = 1: one CTA's 128 x N tile.  CG = 2: issued by the leading CTA of a pair for the pair's
-// 256 x N tile -- A rows 0..127 from this CTA's shared memory and 128..255 from the peer's at the
-// same offset, B columns 0..N/2-1 from this CTA and N/2..N-1 from the peer, each CTA's half of D
-// in its own TMEM at the same address.
-template <int CG>
+// the same for an N known only as a value (a multiple of 16, at most 256)
+__host__ __device__ constexpr uint32_t idesc_i8_n(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
+
 __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    if constexpr (CG == 2) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-    } else {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-            "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-    }
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 // Instruction descriptors with FP32 accumulation, K-major A and B, M = 128, N = BN: kind::f16 with
@@ -238,25 +201,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
-}
-
-// CTA pair: one arrival, once the pair's MMAs issued so far complete, on the mbarrier at this
-// offset in both CTAs of the pair
-__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
-    const unsigned short mask = 3;
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-            smem_u32(bar)),
-        "h"(mask)
-        : "memory");
-}
-
-template <int CG>
-__device__ __forceinline__ void mma_commit_cg(uint64_t *bar) {
-    if constexpr (CG == 2)
-        mma_commit_pair(bar);
-    else
-        mma_commit(bar);
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
@@ -413,33 +357,44 @@ constexpr uint32_t OZ_UNIT = 16384;
 // stage of the ring instead of whole 16 KB units: A (BM x 128 B) at 0, B (BN x 128 B) at BM 128 and,
 // for S = 5, the fifth slice's A (BM x 32 B) and B (BN x 32 B) behind them.  For S = 5 that is 35 KB
 // per k-block (6 stages in flight instead of 4.7 k-blocks of three units); the ring's depth, not its
-// bandwidth, is what keeps the MMAs fed.  In a CTA pair (CG = 2) each CTA's stage holds its own 128
-// rows of A and half of the tile's B rows (BN / 2): 28 KB for S = 5, eight stages.
+// bandwidth, is what keeps the MMAs fed.
 __host__ __device__ constexpr bool oz_staged(int S) { return oz_npass(S) == 1; }
-__host__ __device__ constexpr uint32_t oz_stage_b_rows(int S, int CG) { return (uint32_t)oz_bn(S) / (uint32_t)CG; }
-__host__ __device__ constexpr uint32_t oz_stage_bytes(int S, int CG = 1) {
-    return (OZ_BM + oz_stage_b_rows(S, CG)) * 128u +
-           (oz_g1_width(S) == 1 ? (OZ_BM + oz_stage_b_rows(S, CG)) * 32u : 0u);
+__host__ __device__ constexpr uint32_t oz_stage_bytes(int S) {
+    return (OZ_BM + (uint32_t)oz_bn(S)) * 128u + (oz_g1_width(S) == 1 ? (OZ_BM + (uint32_t)oz_bn(S)) * 32u : 0u);
 }
 // stage footprint in the ring, a multiple of 1024 bytes (the SWIZZLE_128B atom)
-__host__ __device__ constexpr uint32_t oz_stage_pitch(int S, int CG = 1) {
-    return (oz_stage_bytes(S, CG) + 1023u) / 1024u * 1024u;
+__host__ __device__ constexpr uint32_t oz_stage_pitch(int S) { return (oz_stage_bytes(S) + 1023u) / 1024u * 1024u; }
+__host__ __device__ constexpr int oz_stages(int S) { return (int)((OZ_UNITS * OZ_UNIT) / oz_stage_pitch(S)); }
+
+// Wide issue (single-pass int8, S <= 5).  The products A_t B_u of one A slice t go to the groups
+// g = t + u = t + 1 .. S + 1, whose accumulators sit side by side in TMEM (group g at columns
+// (g - 2) BN); so when the stage holds the B slices one after another -- slice u at rows
+// (u - 1) BN .. u BN - 1 of one 32-byte-row (SWIZZLE_32B) operand -- the products of A_t with
+// B_1 .. B_{S+1-t} are ONE matrix product with an (S + 1 - t) BN-row B operand, written to TMEM
+// columns (t - 1) BN onwards.  Per 32-element k-block that is S such products (split into MMAs of
+// at most 256 columns: 8 MMAs for S = 5 instead of 15), and each A slice is read from shared
+// memory once per MMA instead of once per slice pair: 77 KB of operand reads per k-block instead
+// of 105 KB for S = 5.  The int32 sums are the same, so results are bitwise those of the narrow
+// issue.  Stage: A's group-0 box (BM x 128 B, SWIZZLE_128B) at 0, the S B slices (S x BN x 32 B)
+// at BM 128, the fifth A slice (BM x 32 B) behind them.
+__host__ __device__ constexpr bool oz_wide_ok(int S) { return S >= 1 && S <= 5; }
+__host__ __device__ constexpr uint32_t oz_wide_b_off() { return OZ_BM * 128u; }
+__host__ __device__ constexpr uint32_t oz_wide_a1_off(int S) { return OZ_BM * 128u + (uint32_t)S * oz_bn(S) * 32u; }
+__host__ __device__ constexpr uint32_t oz_wide_stage_bytes(int S) {
+    return oz_wide_a1_off(S) + (oz_g1_width(S) == 1 ? OZ_BM * 32u : 0u);
 }
-__host__ __device__ constexpr int oz_stages(int S, int CG = 1) {
-    return (int)((OZ_UNITS * OZ_UNIT) / oz_stage_pitch(S, CG));
-}
-// the pair form: single-pass int8 slice counts
-__host__ __device__ constexpr bool oz_pair_ok(int S) { return S >= 1 && S <= 5; }
+__host__ __device__ constexpr uint32_t oz_wide_stage_pitch(int S) { return (oz_wide_stage_bytes(S) + 1023u) / 1024u * 1024u; }
+__host__ __device__ constexpr int oz_wide_stages(int S) { return (int)((OZ_UNITS * OZ_UNIT) / oz_wide_stage_pitch(S)); }
 
 // One k-block of pass P: every slice pair (t, g - t) of the pass's groups g is one MMA.  Unrolled,
 // so that each descriptor is a tile's base descriptor plus a constant (+2 per 32 bytes): the
 // single issuing thread runs barely ahead of the tensor core, and any latency between two MMAs
 // is tensor-core idle time.  dA0/dB0: group-0 tiles, dA1/dB1: group-1 tiles.
-template <int S, int P, int CG = 1>
+template <int S, int P>
 __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64_t dB0, uint64_t dA1, uint64_t dB1,
                                              uint32_t acc_in) {
     constexpr int g0 = oz_g0(P), g1 = oz_g1(S, P), BN = oz_bn(S);
-    constexpr uint32_t idesc = idesc_i8<BN, OZ_BM * CG>();
+    constexpr uint32_t idesc = idesc_i8<BN>();
 #pragma unroll
     for (int g = g0; g <= g1; ++g) {
 #pragma unroll
@@ -447,7 +402,30 @@ __device__ __forceinline__ void issue_kblock(uint32_t acc0, uint64_t dA0, uint64
             const int u = g - t;
             const uint64_t a = (t > OZ_GP ? dA1 : dA0) + (uint64_t)(2 * ((t - 1) % OZ_GP));
             const uint64_t b = (u > OZ_GP ? dB1 : dB0) + (uint64_t)(2 * ((u - 1) % OZ_GP));
-            mma_i8<CG>(acc0 + (uint32_t)(g - g0) * BN, a, b, idesc, t > 1 ? 1u : acc_in);
+            mma_i8(acc0 + (uint32_t)(g - g0) * BN, a, b, idesc, t > 1 ? 1u : acc_in);
+        }
+    }
+}
+
+// One k-block of the wide issue: for each A slice t, its product with B slices 1 .. S + 1 - t
+// as MMAs of at most 256 columns whose TMEM column offsets are multiples of 32 (480 = 256 + 224,
+// 384 = 192 + 192, 288 = 160 + 128 for S = 5).  A_1's MMAs cover every group's columns, so with
+// acc_in = 0 they start the accumulators of the tile's first k-block.
+template <int S>
+__device__ __forceinline__ void issue_kblock_wide(uint32_t acc0, uint64_t dA0, uint64_t dA1, uint32_t bbase,
+                                                  uint32_t acc_in) {
+    constexpr int BN = oz_bn(S);
+#pragma unroll
+    for (int t = 1; t <= S; ++t) {
+        const uint64_t a = t > OZ_GP ? dA1 : dA0 + (uint64_t)(2 * (t - 1));
+        const int nt = (S + 1 - t) * BN;
+        const int parts = (nt + 255) / 256;
+        const int w = ((nt + parts - 1) / parts + 31) / 32 * 32;
+#pragma unroll
+        for (int q = 0; q < parts; ++q) {
+            const int r0 = q * w, np = min(w, nt - r0);
+            mma_i8(acc0 + (uint32_t)((t - 1) * BN + r0), a, sdesc_sw32(bbase + (uint32_t)r0 * 32u), idesc_i8_n(np),
+                   t > 1 ? 1u : acc_in);
         }
     }
 }
@@ -476,12 +454,28 @@ __device__ __forceinline__ void issue_kblock_float(uint32_t acc0, uint64_t dA, u
 
 // The MMA issuer's k-block loop of pass P (u, ph: next ring unit -- or stage, for the single-pass
 // formats -- and its full-barrier parity).
-template <int S, int P, int CG = 1>
+template <int S, int P, bool WIDE = false>
 __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t &ph, uint32_t smem_base,
                                          uint64_t *full_bar, uint64_t *empty_bar, int *err) {
-    if constexpr (oz_staged(S)) {
-        constexpr int NS = oz_stages(S, CG);
-        constexpr uint32_t PITCH = oz_stage_pitch(S, CG), BR = oz_stage_b_rows(S, CG);
+    if constexpr (WIDE) {
+        constexpr int NS = oz_wide_stages(S);
+        constexpr uint32_t PITCH = oz_wide_stage_pitch(S);
+        for (int kb = 0; kb < KB; ++kb) {
+            if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = smem_base + (uint32_t)u * PITCH;
+            const uint64_t dA1 = oz_g1_width(S) == 1 ? sdesc_sw32(base + oz_wide_a1_off(S)) : 0;
+            issue_kblock_wide<S>(acc0, sdesc_sw128(base), dA1, base + oz_wide_b_off(), kb > 0 ? 1u : 0u);
+            mma_commit(&empty_bar[u]);  // the stage is reusable once these MMAs have read it
+            if (++u == NS) {
+                u = 0;
+                ph ^= 1u;
+            }
+        }
+        return true;
+    } else if constexpr (oz_staged(S)) {
+        constexpr int NS = oz_stages(S), BN = oz_bn(S);
+        constexpr uint32_t PITCH = oz_stage_pitch(S);
         for (int kb = 0; kb < KB; ++kb) {
             if (!mbar_wait(&full_bar[u], ph, err, 2)) return false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -493,12 +487,12 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
             } else {
                 uint64_t dA1 = 0, dB1 = 0;
                 if constexpr (oz_g1_width(S) == 1) {
-                    dA1 = sdesc_sw32(base + (OZ_BM + BR) * 128);
-                    dB1 = sdesc_sw32(base + (OZ_BM + BR) * 128 + OZ_BM * 32);
+                    dA1 = sdesc_sw32(base + (OZ_BM + BN) * 128);
+                    dB1 = sdesc_sw32(base + (OZ_BM + BN) * 128 + OZ_BM * 32);
                 }
-                issue_kblock<S, P, CG>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
+                issue_kblock<S, P>(acc0, dA0, dB0, dA1, dB1, kb > 0 ? 1u : 0u);
             }
-            mma_commit_cg<CG>(&empty_bar[u]);  // the stage (in both CTAs of a pair) is reusable once read
+            mma_commit(&empty_bar[u]);  // the stage is reusable once these MMAs have read it
             if (++u == NS) {
                 u = 0;
                 ph ^= 1u;
@@ -537,16 +531,13 @@ __device__ __forceinline__ bool mma_pass(uint32_t acc0, int KB, int &u, uint32_t
     }
 }
 
-template <int S, int CG = 1>
+// tmBw: the B operand's group-0 slices as 32-byte boxes (the wide issue's per-slice B loads)
+template <int S, bool WIDE = false>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmB0,
                          const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
-                         OzArgs args) {
-    // CG = 2: clusters of two CTAs share one 256 x BN tile (CTA rank r holds output rows 128 r ..
-    // 128 r + 127, and B rows r BN/2 .. r BN/2 + BN/2 - 1 in its ring); the leading CTA (rank 0)
-    // issues the pair's MMAs and holds the full barriers that both CTAs' loads complete on.
-    static_assert(CG == 1 || (CG == 2 && oz_pair_ok(S)), "the CTA-pair form takes single-pass int8 slices");
-    constexpr bool PAIR = CG == 2;
+                         const __grid_constant__ CUtensorMap tmBw, OzArgs args) {
+    static_assert(!WIDE || oz_wide_ok(S), "the wide issue takes single-pass int8 slices");
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     unsigned char *smem = oz_smem_raw;
     if ((smem_u32(oz_smem_raw) & 1023u) != 0u) {  // the swizzled tiles need a 1024-byte aligned base
@@ -574,19 +565,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const int kseg = max(1, args.kseg);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t rank = PAIR ? cluster_rank() : 0u;
-    // grouped raster: CTAs (CTA pairs) in launch order sweep the column tiles in groups of
-    // args.group_m row tiles (row-tile pairs), so that the A and B tiles the resident CTAs share fit
-    // in L2 together
+    // grouped raster: CTAs in launch order sweep the column tiles in groups of args.group_m row tiles,
+    // so that the A and B tiles the resident CTAs share fit in L2 together
     int m0, n0;
     {
-        const int mt = gridDim.x / CG, nt = gridDim.y;
-        const int L = blockIdx.y * mt + blockIdx.x / CG;
+        const int mt = gridDim.x, nt = gridDim.y;
+        const int L = blockIdx.y * mt + blockIdx.x;
         const int G = args.group_m > 0 ? args.group_m : OZ_GROUP_M;
         const int width = G * nt;
         const int first = (L / width) * G;
         const int gm = min(mt - first, G);
-        m0 = ((first + (L % width) % gm) * CG + (int)rank) * OZ_BM;
+        m0 = (first + (L % width) % gm) * OZ_BM;
         n0 = ((L % width) / gm) * BN;
     }
     const int am0 = m0 + args.a_row0;           // first row of the A tile in the A slice buffer
@@ -608,7 +597,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA0)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB0)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(WIDE ? &tmBw : &tmB0)) : "memory");
         if (W1 > 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA1)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB1)) : "memory");
@@ -619,29 +608,48 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(kUnit, args.eb[n0 + c]) : 0.0;
     }
     if (warp == 1) {
-        if constexpr (PAIR) {
-            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
-                smem_u32(tmem_slot)));
-            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
-        } else {
-            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
-                smem_u32(tmem_slot)));
-            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-        }
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    // a pair's barriers are initialised in both CTAs before either CTA's loads or commits reach them
-    if constexpr (PAIR) cluster_sync_all();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0 && oz_staged(S)) {  // TMA producer, one stage per k-block
-            constexpr int NS = oz_stages(S, CG);
-            constexpr uint32_t PITCH = oz_stage_pitch(S, CG), BYTES = oz_stage_bytes(S, CG);
-            constexpr int BR = (int)oz_stage_b_rows(S, CG);
-            const int nb0 = n0 + (int)rank * BR;  // this CTA's B rows
+        if (lane == 0 && WIDE) {  // TMA producer, one wide stage per k-block
+            constexpr int NS = oz_wide_stages(S);
+            constexpr uint32_t PITCH = oz_wide_stage_pitch(S), BYTES = oz_wide_stage_bytes(S);
+            constexpr int U0 = S < OZ_GP ? S : OZ_GP;  // B slices in the group-0 buffer
+            int sg = 0;
+            uint32_t eph = 0;
+            bool wrapped = false;
+            for (int kb = 0; kb < KB && !*abort_flag; ++kb) {
+                const int kbg = args.kb0 + kz0 + kb;
+                if (wrapped && !mbar_wait(&empty_bar[sg], eph, args.err, 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                unsigned char *dst = smem + (size_t)sg * PITCH;
+                unsigned char *bdst = dst + oz_wide_b_off();
+                mbar_arrive_expect_tx(&full_bar[sg], BYTES);
+                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
+#pragma unroll
+                for (int u = 0; u < U0; ++u)  // slice u + 1 of B: 32 bytes of each 128-byte k-block row
+                    tma_load_2d(&tmBw, &full_bar[sg], bdst + u * BN * 32, kbg * 128 + u * 32, n0);
+                if constexpr (W1 == 1) {
+                    tma_load_2d(&tmB1, &full_bar[sg], bdst + OZ_GP * BN * 32, kbg * 32, n0);
+                    tma_load_2d(&tmA1, &full_bar[sg], dst + oz_wide_a1_off(S), kbg * 32, am0);
+                }
+                if (++sg == NS) {
+                    sg = 0;
+                    if (wrapped) eph ^= 1u;
+                    wrapped = true;
+                }
+            }
+        } else if (lane == 0 && oz_staged(S)) {  // TMA producer, one stage per k-block
+            constexpr int NS = oz_stages(S);
+            constexpr uint32_t PITCH = oz_stage_pitch(S), BYTES = oz_stage_bytes(S);
             int sg = 0;           // next stage
             uint32_t eph = 0;     // parity of the empty-barrier phase that frees it (after the first lap)
             bool wrapped = false;
@@ -652,24 +660,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     break;
                 }
                 unsigned char *dst = smem + (size_t)sg * PITCH;
-                if constexpr (PAIR) {
-                    // both halves complete on the leading CTA's full barrier, which expects them both
-                    const uint32_t fb = cluster_addr(smem_u32(&full_bar[sg]), 0u);
-                    if (rank == 0) mbar_arrive_expect_tx(&full_bar[sg], 2 * BYTES);
-                    tma_load_2d_pair(&tmA0, fb, dst, kbg * 128, am0);
-                    tma_load_2d_pair(&tmB0, fb, dst + OZ_BM * 128, kbg * 128, nb0);
-                    if constexpr (W1 == 1) {
-                        tma_load_2d_pair(&tmA1, fb, dst + (OZ_BM + BR) * 128, kbg * 32, am0);
-                        tma_load_2d_pair(&tmB1, fb, dst + (OZ_BM + BR) * 128 + OZ_BM * 32, kbg * 32, nb0);
-                    }
-                } else {
-                    mbar_arrive_expect_tx(&full_bar[sg], BYTES);
-                    tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
-                    tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
-                    if constexpr (W1 == 1) {
-                        tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
-                        tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
-                    }
+                mbar_arrive_expect_tx(&full_bar[sg], BYTES);
+                tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
+                tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
+                if constexpr (W1 == 1) {
+                    tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
+                    tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
                 }
                 if (++sg == NS) {
                     sg = 0;
@@ -717,7 +713,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             }
         }
     } else if (warp == 1) {
-        if (lane == 0 && rank == 0) {  // MMA issuer (a pair's leading CTA)
+        if (lane == 0) {  // MMA issuer
             int u = 0;         // next unit
             uint32_t ph = 0;   // parity of its full-barrier phase
             bool ok = true;
@@ -750,12 +746,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 }
                 const uint32_t acc0 = tmem_base + ((p > 0 && keep) ? 256u : 0u);
                 if (p == 0)
-                    ok = mma_pass<S, 0, CG>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
+                    ok = mma_pass<S, 0, WIDE>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
                 else if constexpr (oz_npass(S) > 1)
                     ok = mma_pass<S, 1>(acc0, KB, u, ph, smem_base, full_bar, empty_bar, args.err);
                 if (!ok) *abort_flag = 1;
-                // the pass's accumulators (in both CTAs of a pair) are final once its MMAs complete
-                mma_commit_cg<CG>(pass_bar);
+                mma_commit(pass_bar);  // the pass's accumulators are final once its MMAs complete
             }
         }
     } else {
@@ -862,15 +857,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    // neither CTA of a pair leaves (freeing its shared memory and barriers) or frees TMEM while the
-    // other still uses them
-    if constexpr (PAIR) cluster_sync_all();
     if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if constexpr (PAIR)
-            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
-        else
-            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
     }
 }
 
@@ -1356,9 +1345,11 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // 2-D map over one slice group of an operand: dimension 0 = bytes of a row (KB k-block segments of
-// seg_bytes), dimension 1 = rows; a box is one k-block segment of box_rows rows.
+// seg_bytes), dimension 1 = rows; a box is box_bytes (default: one k-block segment) of box_rows rows,
+// swizzled at its own width.
 int make_group_map(CUtensorMap *map, const signed char *base, long long KB, int seg_bytes, long long rows_pad,
-                   int box_rows) {
+                   int box_rows, int box_bytes = 0) {
+    if (box_bytes <= 0) box_bytes = seg_bytes;
     auto enc = get_encode();
     if (!enc) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
@@ -1367,12 +1358,12 @@ int make_group_map(CUtensorMap *map, const signed char *base, long long KB, int 
     const long long rowb = KB * seg_bytes;
     cuuint64_t dims[2] = {(cuuint64_t)rowb, (cuuint64_t)rows_pad};
     cuuint64_t strides[1] = {(cuuint64_t)rowb};
-    cuuint32_t box[2] = {(cuuint32_t)seg_bytes, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_bytes, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<signed char *>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     seg_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
-                                      : (seg_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B),
+                     box_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                      : (box_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B),
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error(PHF_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -1392,6 +1383,12 @@ int make_slice_maps(CUtensorMap *g0, CUtensorMap *g1, const signed char *base, l
         return PHF_OK;
     }
     return make_group_map(g1, base + rows_pad * KB * 128, KB, 32 * w, rows_pad, box_rows);
+}
+
+// The wide issue's map of an operand's group-0 slices: one slice (32 bytes of a 128-byte k-block row)
+// of box_rows rows per box, SWIZZLE_32B.
+int make_wide_map(CUtensorMap *map, const signed char *base, long long kpad, long long rows_pad, int box_rows) {
+    return make_group_map(map, base, kpad / OZ_BK, 128, rows_pad, box_rows, 32);
 }
 
 }  // namespace
@@ -1514,15 +1511,16 @@ int oz_gemm(int m, int n, int k, int S, const signed char *Asl, const int *ea, c
 }
 
 namespace {
-using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap, OzArgs);
+using OzKernelFn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap,
+                            const CUtensorMap, OzArgs);
 
-OzKernelFn oz_pair_kernel_for(int S) {
+OzKernelFn oz_wide_kernel_for(int S) {
     switch (S) {
-        case 1: return ozaki_i8_gemm_kernel<1, 2>;
-        case 2: return ozaki_i8_gemm_kernel<2, 2>;
-        case 3: return ozaki_i8_gemm_kernel<3, 2>;
-        case 4: return ozaki_i8_gemm_kernel<4, 2>;
-        case 5: return ozaki_i8_gemm_kernel<5, 2>;
+        case 1: return ozaki_i8_gemm_kernel<1, true>;
+        case 2: return ozaki_i8_gemm_kernel<2, true>;
+        case 3: return ozaki_i8_gemm_kernel<3, true>;
+        case 4: return ozaki_i8_gemm_kernel<4, true>;
+        case 5: return ozaki_i8_gemm_kernel<5, true>;
         default: return nullptr;
     }
 }
@@ -1568,10 +1566,13 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     const long long kpad = oz_pad_k(k), kb_total = kpad / OZ_BK;
     if (nsplit <= 1 || kb_total > oz_kb_pass(S) || kb_total < 2 * nsplit)
         return oz_gemm_t(m, n, k, S, Asl, ea, Bsl, eb, D, ldd, 0, trans, err, st);
-    CUtensorMap ta0, ta1, tb0, tb1;
+    CUtensorMap ta0, ta1, tb0, tb1, tbw;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n);
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, mpad, S, OZ_BM));
     PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
+    const bool wide = oz_wide_ok(S) && !g_narrow_mma;
+    if (wide) PHF_TRY(make_wide_map(&tbw, Bsl, kpad, npad, oz_bn(S)));
+    else tbw = tb0;
     const long long rows = trans ? n : m;
     const long long dz = rows * ldd;
     OzArgs a;
@@ -1595,7 +1596,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.dz = dz;
     a.err = err;
     const size_t smem = oz_smem_bytes();
-    const OzKernelFn kern = oz_kernel_for(S);
+    const OzKernelFn kern = wide ? oz_wide_kernel_for(S) : oz_kernel_for(S);
     if (!kern) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
@@ -1604,7 +1605,7 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), (unsigned)nsplit);
     {
         ProfScope prof(st, PROF_JK);
-        kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
+        kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, tbw, a);
     }
     ++g_launches;
     PHF_CHECK_LAUNCH();
@@ -1618,13 +1619,11 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
 }
 
 namespace {
-int oz_gemm_launch(OzKernelFn kern, int cg, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
-                   const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
-                   double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
-                   int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m);
-
-// Launch choices of the int8 GEMM: raster group g for single CTAs, 100 + g for CTA pairs.
-constexpr int kOzPairChoice = 100;
+int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+                   const CUtensorMap &ta1, const CUtensorMap &tb1, const CUtensorMap &tbw, int m, int n, int S,
+                   const int *ea, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
+                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, long long kb_total, long long kb_pass,
+                   int group_m);
 }  // namespace
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
@@ -1647,56 +1646,46 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
-    CUtensorMap ta0, ta1, tb0, tb1, tp0, tp1;
+    CUtensorMap ta0, ta1, tb0, tb1, tbw;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
-    const long long mt = mpad / OZ_BM;
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, a_rows_pad, S, OZ_BM));
     PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
-    // CTA pairs (256 x BN tiles, each CTA loading half of the B rows) for single-pass int8 slices and
-    // more than one row tile
-    const bool pair_ok = oz_pair_ok(S) && mt >= 2 && !g_no_pair;
-    if (pair_ok) PHF_TRY(make_slice_maps(&tp0, &tp1, Bsl, kpad, npad, S, oz_bn(S) / 2));
+    const bool wide = oz_wide_ok(S) && !g_narrow_mma;  // single-pass int8: the wide issue
+    if (wide) PHF_TRY(make_wide_map(&tbw, Bsl, kpad, npad, oz_bn(S)));
+    else tbw = tb0;
     const long long kb_pass = oz_kb_pass(S);
     const long long kb_total = kpad / OZ_BK;
     const size_t smem = oz_smem_bytes();
-    const OzKernelFn kern = oz_kernel_for(S), pkern = pair_ok ? oz_pair_kernel_for(S) : nullptr;
-    if (!kern || (pair_ok && !pkern)) {
+    const OzKernelFn kern = wide ? oz_wide_kernel_for(S) : oz_kernel_for(S);
+    if (!kern) {
         set_error(PHF_ERR_ARG, "oz_gemm: slices out of range");
         return PHF_ERR_ARG;
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (pkern)
-        PHF_CUDA(cudaFuncSetAttribute((const void *)pkern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const unsigned ntiles = (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S));
-    const dim3 grid((unsigned)mt, ntiles, 1);                          // grouped raster
-    const dim3 pgrid((unsigned)(2 * ((mt + 1) / 2)), ntiles, 1);       // row tiles in pairs
-    const auto run = [=](int choice, cudaStream_t s) {
-        if (choice >= kOzPairChoice && pkern)
-            return oz_gemm_launch(pkern, 2, pgrid, smem, ta0, tp0, ta1, tp1, m, n, S, ea + a_row0, eb, D, ldd,
-                                  accumulate, trans, err, s, gamma_n, g_row0, a_row0, kb_total, kb_pass,
-                                  choice - kOzPairChoice);
-        return oz_gemm_launch(kern, 1, grid, smem, ta0, tb0, ta1, tb1, m, n, S, ea + a_row0, eb, D, ldd, accumulate,
-                              trans, err, s, gamma_n, g_row0, a_row0, kb_total, kb_pass, choice % kOzPairChoice);
-    };
+    dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
     const TuneKey key{1, m, n, k, (long long)S * 4 + (gamma_n > 0) * 2 + trans, accumulate};
-    int choice = tuned_choice(key);
+    int group_m = tuned_choice(key);
     if (t_tune_record) {
         // the tuner repeats the launch; an accumulating launch then adds several times, which is harmless:
         // the tuning evaluation's outputs are discarded and recomputed by the evaluation that follows
-        std::vector<int> cands{4, 8, 16};
-        if (pkern) cands.insert(cands.end(), {kOzPairChoice + 4, kOzPairChoice + 8, kOzPairChoice + 16});
-        t_tune_record->push_back({key, cands, run});
+        t_tune_record->push_back({key, {4, 8, 16}, [=](int g, cudaStream_t s) {
+                                      return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, tbw, m, n, S,
+                                                            ea + a_row0, eb, D, ldd, accumulate, trans, err, s,
+                                                            gamma_n, g_row0, a_row0, kb_total, kb_pass, g);
+                                  }});
     }
-    if (choice < 0 || (choice >= kOzPairChoice && !pkern)) choice = (pkern ? kOzPairChoice : 0) + OZ_GROUP_M;
-    return run(choice, st);
+    if (group_m < 0) group_m = OZ_GROUP_M;
+    return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, tbw, m, n, S, ea + a_row0, eb, D, ldd, accumulate,
+                          trans, err, st, gamma_n, g_row0, a_row0, kb_total, kb_pass, group_m);
 }
 
 namespace {
-// the k passes of one oz_gemm_ex call with the given raster group (cg = 2: clusters of two CTAs)
-int oz_gemm_launch(OzKernelFn kern, int cg, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
-                   const CUtensorMap &ta1, const CUtensorMap &tb1, int m, int n, int S, const int *ea, const int *eb,
-                   double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n,
-                   int g_row0, int a_row0, long long kb_total, long long kb_pass, int group_m) {
+// the k passes of one oz_gemm_ex call with the given raster group
+int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
+                   const CUtensorMap &ta1, const CUtensorMap &tb1, const CUtensorMap &tbw, int m, int n, int S,
+                   const int *ea, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
+                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, long long kb_total, long long kb_pass,
+                   int group_m) {
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;
@@ -1720,23 +1709,7 @@ int oz_gemm_launch(OzKernelFn kern, int cg, dim3 grid, size_t smem, const CUtens
         a.err = err;
         {
             ProfScope prof(st, PROF_JK);
-            if (cg == 2) {
-                cudaLaunchConfig_t cfg = {};
-                cfg.gridDim = grid;
-                cfg.blockDim = dim3(OZ_THREADS, 1, 1);
-                cfg.dynamicSmemBytes = smem;
-                cfg.stream = st;
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = 2;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.attrs = attr;
-                cfg.numAttrs = 1;
-                PHF_CUDA(cudaLaunchKernelEx(&cfg, kern, ta0, tb0, ta1, tb1, a));
-            } else {
-                kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, a);
-            }
+            kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, tbw, a);
         }
         ++g_launches;
         PHF_CHECK_LAUNCH();

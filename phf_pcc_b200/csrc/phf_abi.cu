@@ -307,9 +307,9 @@ int phf_plan_eval_device_async(phf_plan *plan, const phf_complex *d_c, phf_compl
 
 int phf_tuned_shapes(void) { return phf::tuned_entries(); }
 
-int phf_int8_cta_pairs(int on) {
-    const int was = !phf::g_no_pair;
-    phf::g_no_pair = on ? 0 : 1;
+int phf_int8_wide_mma(int on) {
+    const int was = !phf::g_narrow_mma;
+    phf::g_narrow_mma = on ? 0 : 1;
     return was;
 }
 

@@ -41,7 +41,7 @@
 namespace phf {
 
 unsigned long long g_launches = 0;
-int g_no_pair = 0;
+int g_narrow_mma = 0;
 
 // ---------------------------------------------------------------- per-class event timing
 namespace {
@@ -255,16 +255,14 @@ int build_exchange_matrix(PlanImpl &p);
 constexpr int kDSplit = 4;  // split-k of the Coulomb GEMM d = B vec P (small output, k = n^2)
 
 // Spatial indices i per exchange panel of the streamed form: panels of at most 8192 exchange rows
-// (i, k), with the fewest padded rows over all panels (the int8 GEMM's CTA pairs take 256-row
-// tiles), ties to the larger panel (fewer launches).  n = 200: 32 (6 panels of 6400 rows, 25 pair
-// tiles each, and one of 1600).
+// (i, k), with the fewest padded rows over all panels (GEMM tiles are 128 rows), ties to the larger
+// panel (fewer launches).  n = 200: 32 (6 panels of 6400 rows and one of 1600).
 int choose_ipanel(int n) {
-    const auto pad256 = [](long long r) { return (r + 255) / 256 * 256; };
     int best = 1;
     long long best_rows = -1;
     for (int I = 1; I <= n && (long long)I * n <= std::max<long long>(8192, n); ++I) {
         const long long full = n / I, rest = n % I;
-        const long long rows = full * pad256((long long)I * n) + (rest ? pad256(rest * n) : 0);
+        const long long rows = full * oz_pad_rows((long long)I * n) + (rest ? oz_pad_rows(rest * n) : 0);
         if (best_rows < 0 || rows <= best_rows) {
             best_rows = rows;
             best = I;

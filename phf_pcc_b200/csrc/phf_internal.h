@@ -74,8 +74,9 @@ struct TuneCall {
 // the table: -1 when the shape has not been tuned
 int tuned_choice(const TuneKey &key);
 int tuned_entries();
-// non-zero: the int8 GEMM runs single CTAs only (no CTA pairs), for comparisons
-extern int g_no_pair;
+// non-zero: the int8 GEMM issues one MMA per slice pair instead of the wide issue (same results),
+// for comparisons
+extern int g_narrow_mma;
 // while non-null, the GEMM launchers append every launch they make (thread-local)
 extern thread_local std::vector<TuneCall> *t_tune_record;
 // times every candidate of every recorded launch whose shape is not in the table yet, keeps the fastest

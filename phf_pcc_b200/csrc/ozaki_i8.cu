@@ -30,8 +30,14 @@
 //   warp 1      TMEM allocation (512 columns) and the single-thread tcgen05.mma issuer.  S = 5
 //               runs all five groups g = 2..6 in one pass over 128 x 96 tiles (five int32
 //               accumulators, 480 columns); otherwise the tile is 128 x 128 and the groups run in
-//               passes of four over the whole k range.  Per k-block every slice pair of the
-//               pass's groups is one 128 x BN x 32 MMA
+//               passes of four over the whole k range.  S <= 5 (the wide issue, the default):
+//               per k-block one product per A slice t with the B slices 1 .. S + 1 - t laid side
+//               by side, as MMAs of up to 256 columns (8 for S = 5); the narrow issue, kept for
+//               comparison and used for S = 6, 7, makes every slice pair of the pass's groups one
+//               128 x BN x 32 MMA (15 for S = 5).  At S = 5 the narrow issue ran at ~68 cycles per
+//               128 x 96 x 32 MMA against 48 for the int8 rate, with the producer waiting on a
+//               full ring (the operand reads of the narrow MMAs, not the loads, set the pace);
+//               the wide issue reads 77 instead of 105 KB of shared memory per k-block
 //   warps 2-5   epilogue after each pass: tcgen05.ld 32x32b.x32 of the pass's groups, int32 ->
 //               FP64 with 254^{2-g} scaling.  For S = 6 the first pass's FP64 sums are parked in
 //               TMEM (columns 0..255, where groups 2 and 3 were) and the second pass, accumulating
@@ -807,7 +813,55 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 mbar_arrive(&acc_empty[b]);  // accumulator b may take segment sg + 2
             }
         }
-        for (int p = 0; p < npass && !oz_float(S); ++p) {
+        // Single-pass int8 tiles with a plain row-major D: the scaled tile goes through shared memory (the
+        // ring, idle once the last MMA has completed) and out as whole rows, so that a warp's stores are
+        // 32 consecutive doubles instead of one double in each of 32 rows.  Same values, same order of
+        // operations as store_row_chunk; for short k (a few k-blocks) the store is most of the tile's time.
+        constexpr bool kStageable = oz_npass(S) == 1 && !oz_float(S);
+        const bool staged = kStageable && args.gamma_n == 0 && !args.trans;
+        if (staged) {
+            const bool ok = mbar_wait(pass_bar, 0, args.err, 4);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const bool go = ok && !*abort_flag;
+            constexpr int TP = BN + 1;  // row pitch in doubles: a warp's column-j writes hit distinct banks
+            double *T = reinterpret_cast<double *>(smem);
+            const int rl = quarter * 32 + lane;
+            if (go) {
+#pragma unroll 1
+                for (int c = 0; c < BN / 32; ++c) {
+                    double acc[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+#pragma unroll 1
+                    for (int g = oz_g1(S, 0); g >= oz_g0(0) && KB > 0; --g) {
+                        uint32_t v[32];
+                        tmem_ld32(lane_base + (uint32_t)(g - oz_g0(0)) * BN + c * 32, v);
+                        const double sc = kPow254[g - 2];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], sc, acc[j]);
+                    }
+                    const double *cs = colscale + c * 32;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) T[rl * TP + c * 32 + j] = acc[j] * rowscale * cs[j];
+                }
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
+            if (go) {
+                const bool add = args.accumulate != 0;
+#pragma unroll 1
+                for (int r = quarter * 32; r < quarter * 32 + 32; ++r) {
+                    const int grow = m0 + r;
+                    if (grow >= args.m) break;
+                    double *drow = Dz + (long long)grow * args.ldd + n0;
+                    const double *trow = T + r * TP;
+#pragma unroll
+                    for (int c = lane; c < BN; c += 32) {
+                        if (n0 + c < args.n) drow[c] = add ? drow[c] + trow[c] : trow[c];
+                    }
+                }
+            }
+        }
+        for (int p = 0; p < npass && !oz_float(S) && !staged; ++p) {
             const bool ok = mbar_wait(pass_bar, p & 1, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!ok || *abort_flag) break;
@@ -981,69 +1035,101 @@ __global__ void __launch_bounds__(SL_NT) slice_rows_kernel(int m, int k, const d
     }
 }
 
-// Columns of the spin-summed density P_w = rho_aa + rho_bb for the Coulomb term: column
-// c = 2 w + part holds part(rho_w[2p][2q] + rho_w[2p+1][2q+1]) at k = p n + q.
-__global__ void __launch_bounds__(SL_NT) slice_p_cols_kernel(int n, const zc *rho, int S, long long npad,
-                                                             long long kpad, signed char *out, int *eb) {
-    __shared__ double sh[SL_NT];
-    const long long c = blockIdx.x;
-    const int part = (int)(c & 1);
-    const long long w = c >> 1;
-    const int M = 2 * n;
-    const zc *R = rho + w * (long long)M * M;
-    const int k = n * n;
+// The same for short rows (kpad <= 1024): one warp per row, eight rows per CTA, the row maximum by
+// warp shuffles (one CTA per row leaves most of a 256-thread block idle when k is a few hundred).
+constexpr int SLW_ROWS = 8;
+__global__ void __launch_bounds__(32 * SLW_ROWS) slice_rows_warp_kernel(int m, int k, const double *A, long long lda,
+                                                                        long long cs, int S, long long mpad,
+                                                                        long long kpad, signed char *out, int *ea) {
+    const long long row = (long long)blockIdx.x * SLW_ROWS + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= m) return;
+    const double *a = A + row * lda;
     double mx = 0.0;
-    for (int e = threadIdx.x; e < k; e += SL_NT) {
-        int p = e / n, q = e - p * n;
-        zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
-        mx = fmax(mx, fabs(part ? v.y : v.x));
-    }
-    mx = block_max(mx, sh);
-    const int ex = exp_of_max(mx);
-    if (threadIdx.x == 0) eb[c] = ex;
-    const SliceScale sc = slice_scale(ex, S);
-    for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
-        double x = 0.0;
-        if (e < k) {
-            int p = (int)(e / n), q = (int)(e - (long long)p * n);
-            zc v = R[(long long)(2 * p) * M + 2 * q] + R[(long long)(2 * p + 1) * M + 2 * q + 1];
-            x = part ? v.y : v.x;
-        }
-        slice_value(x, sc, S, out, c, npad, kpad >> 5, e);
+    for (int j = lane; j < k; j += 32) mx = fmax(mx, fabs(a[(long long)j * cs]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = exp_of_max(mx);
+    if (lane == 0) ea[row] = e;
+    const SliceScale sc = slice_scale(e, S);
+    for (long long j = lane; j < kpad; j += 32) {
+        double x = (j < k) ? a[j * cs] : 0.0;
+        slice_value(x, sc, S, out, row, mpad, kpad >> 5, j);
     }
 }
 
-// Columns of the exchange operand: for grid point w and spin block (sigma, tau) of rho_w
-// (M x M complex, interleaved spin order, row-major, rows at rho + w * M * M), column
-// c = (w * 4 + sigma * 2 + tau) * 2 + part holds part(rho_w[2l + sigma][2j + tau]) at k = l n + j.
-__global__ void __launch_bounds__(SL_NT) slice_rho_cols_kernel(int n, const zc *rho, int S, long long npad,
-                                                               long long kpad, signed char *out, int *eb) {
-    __shared__ double sh[SL_NT];
-    const long long c = blockIdx.x;
-    const int part = (int)(c & 1), st = (int)((c >> 1) & 3);
-    const long long w = c >> 3;
-    const int sg = st >> 1, tu = st & 1;
-    const int M = 2 * n;
-    const zc *R = rho + w * (long long)M * M;
+// Both density operands of one grid point w, from rho_w (M x M complex, interleaved spin order;
+// element [r][q] at rho[w ws + r rs + q]) in two passes over it (column maxima, then digits):
+//   exchange columns c = (4 w + 2 sigma + tau) 2 + part: part(rho_w[2l + sigma][2j + tau]) at k = l n + j;
+//   Coulomb columns c = 2 w + part: part(P_w[l][j]), P_w = rho_aa + rho_bb (the spin-summed density).
+// Thread-iteration (l, j) reads the 2 x 2 spin block of rho_w at rows 2l, 2l + 1, columns 2j, 2j + 1 as
+// two 32-byte pieces, so consecutive j are consecutive 32-byte segments of the two rows; the ten
+// values it yields (8 exchange, 2 Coulomb) keep ten running maxima.  rs and ws are even.
+constexpr int SD_NT = 256;
+__global__ void __launch_bounds__(SD_NT, 3) slice_density_kernel(int n, const zc *__restrict__ rho, long long rs,
+                                                              long long ws, int S, long long npadK, long long npadP,
+                                                              long long kpad, signed char *Ksl, int *eK,
+                                                              signed char *Psl, int *eP) {
+    __shared__ double sh[10][SD_NT / 32];
+    const long long w = blockIdx.x;
+    const zc *R = rho + w * ws;
     const int k = n * n;
-    double mx = 0.0;
-    for (int e = threadIdx.x; e < k; e += SL_NT) {
-        int l = e / n, j = e - l * n;
-        zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
-        mx = fmax(mx, fabs(part ? v.y : v.x));
-    }
-    mx = block_max(mx, sh);
-    const int ex = exp_of_max(mx);
-    if (threadIdx.x == 0) eb[c] = ex;
-    const SliceScale sc = slice_scale(ex, S);
-    for (long long e = threadIdx.x; e < kpad; e += SL_NT) {
-        double x = 0.0;
-        if (e < k) {
-            int l = (int)(e / n), j = (int)(e - (long long)l * n);
-            zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
-            x = part ? v.y : v.x;
+    const long long KB = kpad >> 5;
+    // the 2 x 2 block (l, j): v[2 sigma + tau] = rho_w[2l + sigma][2j + tau]
+    auto block = [&](int e, zc (&v)[4]) {
+        const int l = e / n, j = e - l * n;
+        const double2 *r0 = reinterpret_cast<const double2 *>(R + (long long)(2 * l) * rs + 2 * j), *r1 = r0 + rs;
+        const double2 a0 = __ldg(r0), a1 = __ldg(r0 + 1), b0 = __ldg(r1), b1 = __ldg(r1 + 1);
+        v[0] = mkz(a0.x, a0.y);
+        v[1] = mkz(a1.x, a1.y);
+        v[2] = mkz(b0.x, b0.y);
+        v[3] = mkz(b1.x, b1.y);
+    };
+    double mx[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) mx[q] = 0.0;
+    for (int e = threadIdx.x; e < k; e += SD_NT) {
+        zc v[4];
+        block(e, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            mx[2 * q] = fmax(mx[2 * q], fabs(v[q].x));
+            mx[2 * q + 1] = fmax(mx[2 * q + 1], fabs(v[q].y));
         }
-        slice_value(x, sc, S, out, c, npad, kpad >> 5, e);
+        mx[8] = fmax(mx[8], fabs(v[0].x + v[3].x));
+        mx[9] = fmax(mx[9], fabs(v[0].y + v[3].y));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 10; ++q) {
+        double m = mx[q];
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) sh[q][wid] = m;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 10; ++q) {
+        double m = 0.0;
+        for (int i = 0; i < SD_NT / 32; ++i) m = fmax(m, sh[q][i]);
+        mx[q] = m;
+    }
+    SliceScale sc[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) sc[q] = slice_scale(exp_of_max(mx[q]), S);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (threadIdx.x == q) eK[8 * w + q] = sc[q].e;
+    if (threadIdx.x == 8) eP[2 * w] = sc[8].e;
+    if (threadIdx.x == 9) eP[2 * w + 1] = sc[9].e;
+    for (long long e = threadIdx.x; e < kpad; e += SD_NT) {
+        zc v[4] = {mkz(0.0), mkz(0.0), mkz(0.0), mkz(0.0)};
+        if (e < k) block((int)e, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            slice_value(v[q].x, sc[2 * q], S, Ksl, 8 * w + 2 * q, npadK, KB, e);
+            slice_value(v[q].y, sc[2 * q + 1], S, Ksl, 8 * w + 2 * q + 1, npadK, KB, e);
+        }
+        slice_value(v[0].x + v[3].x, sc[8], S, Psl, 2 * w, npadP, KB, e);
+        slice_value(v[0].y + v[3].y, sc[9], S, Psl, 2 * w + 1, npadP, KB, e);
     }
 }
 
@@ -1405,17 +1491,25 @@ int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long
 int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long long cs, int S, long long rows_pad,
                           signed char *out, int *ea, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
-    slice_rows_kernel<<<m, SL_NT, 0, st>>>(m, k, A, lda, cs, S, rows_pad, oz_pad_k(k), out, ea);
+    if (oz_pad_k(k) <= 1024)
+        slice_rows_warp_kernel<<<(unsigned)((m + SLW_ROWS - 1) / SLW_ROWS), 32 * SLW_ROWS, 0, st>>>(
+            m, k, A, lda, cs, S, rows_pad, oz_pad_k(k), out, ea);
+    else
+        slice_rows_kernel<<<m, SL_NT, 0, st>>>(m, k, A, lda, cs, S, rows_pad, oz_pad_k(k), out, ea);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
 }
 
-int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st) {
-    const long long ncols = 8LL * b;
+int oz_slice_density(int n, int bc, const zc *rho, long long rs, long long ws, int S, signed char *Ksl, int *eK,
+                     long long npadK, signed char *Psl, int *eP, long long npadP, cudaStream_t st) {
+    if (n < 1 || bc < 1 || 8LL * bc > npadK || 2LL * bc > npadP || !oz_format_ok(S) || (rs & 1) || (ws & 1)) {
+        set_error(PHF_ERR_ARG, "oz_slice_density: columns outside the slice buffers or odd strides");
+        return PHF_ERR_ARG;
+    }
     ProfScope prof(st, PROF_MEMORY);
-    slice_rho_cols_kernel<<<(unsigned)ncols, SL_NT, 0, st>>>(n, rho, S, oz_pad_cols(ncols), oz_pad_k((long long)n * n),
-                                                             out, eb);
+    slice_density_kernel<<<(unsigned)bc, SD_NT, 0, st>>>(n, rho, rs, ws, S, npadK, npadP, oz_pad_k((long long)n * n),
+                                                          Ksl, eK, Psl, eP);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
@@ -1476,16 +1570,6 @@ int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra
     const long long npadK = oz_pad_cols(8LL * bc), npadP = oz_pad_cols(2LL * bc), kpad = oz_pad_k((long long)n * n);
     ProfScope prof(st, PROF_MEMORY);
     PHF_CUDA(cudaLaunchKernelEx(&cfg, fn, n, N, Xs, ld, bra, npadK, npadP, kpad, Ksl, eK, Psl, eP));
-    ++g_launches;
-    PHF_CHECK_LAUNCH();
-    return PHF_OK;
-}
-
-int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st) {
-    const long long ncols = 2LL * b;
-    ProfScope prof(st, PROF_MEMORY);
-    slice_p_cols_kernel<<<(unsigned)ncols, SL_NT, 0, st>>>(n, rho, S, oz_pad_cols(ncols), oz_pad_k((long long)n * n),
-                                                           out, eb);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

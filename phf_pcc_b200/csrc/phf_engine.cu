@@ -560,6 +560,9 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             else per += (8 * n2 * oz_slots(p.slices)) / sizeof(zc) + 1  // exchange slices
                         + (2 * n2 + 2 * (size_t)p.L) * oz_slots(p.slices) / sizeof(zc) + 1    // Coulomb slices
                         + p.L + n2;                                                // d^T, J pairs
+            // int8 density GEMM: the X rows' slices and exponents
+            if (p.prec != PHF_PREC_FP64 && !oz_rho_slice_ok(n) && p.slices <= 7)
+                per += ((size_t)M * oz_pad_k(2LL * N) * oz_slots(p.slices) + 4 * (size_t)M) / sizeof(zc) + 1;
         } else if (p.chol) {
             per += (size_t)p.L * N * N + (size_t)p.L * MN + p.L;
         } else {
@@ -627,6 +630,18 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.dT, 2 * b * (size_t)p.L));
             PHF_TRY(p.arena.alloc(&p.dpart, (size_t)kDSplit * 2 * b * (size_t)p.L));
             PHF_TRY(p.arena.alloc(&p.Jr, 2 * b * n2));
+            // n > 64 with int8 slices: rho_w = X_w bra^H for the whole chunk as one int8 GEMM
+            p.rho_i8 = !oz_rho_slice_ok(n) && p.slices <= 7;
+            if (p.rho_i8) {
+                const long long xrows = oz_pad_rows((long long)M * p.b), brows = oz_pad_cols(2LL * M);
+                PHF_TRY(p.arena.alloc(&p.Xsl, oz_slice_bytes(xrows, 2LL * N, p.slices)));
+                PHF_TRY(p.arena.alloc(&p.eX, (size_t)xrows));
+                PHF_TRY(p.arena.alloc(&p.BRop, (size_t)2 * M * 2 * N));
+                PHF_TRY(p.arena.alloc(&p.BRsl, oz_slice_bytes(brows, 2LL * N, p.slices)));
+                PHF_TRY(p.arena.alloc(&p.eBR, (size_t)brows));
+                PHF_CUDA(cudaMemset(p.Xsl, 0, oz_slice_bytes(xrows, 2LL * N, p.slices)));
+                PHF_CUDA(cudaMemset(p.BRsl, 0, oz_slice_bytes(brows, 2LL * N, p.slices)));
+            }
         }
     } else if (p.chol) {
         PHF_TRY(p.arena.alloc(&p.T, (size_t)p.L * bNN));
@@ -776,9 +791,26 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     const long long ld = (long long)b * N, MM = (long long)M * M, n2 = (long long)n * n;
     // tensor-core path with n <= 64: the operand columns are formed and sliced in one kernel, no density in HBM
     const bool fused = p.prec != PHF_PREC_FP64 && oz_rho_slice_ok(n);
-    if (!fused)
+    // n > 64 with int8 slices: the densities of the whole chunk as ONE int8 GEMM.  Row (i, w) of X,
+    // X_w[i][:] at Xs + (i b + w) N (the points' X blocks side by side), is a row of 2N reals
+    // (re, im interleaved), and rho_w[i][j] = sum_k X_w[i][k] conj(bra[j][k]) is its product with
+    // rows 2j (real part) and 2j + 1 (imaginary part) of the bra's 2M x 2N operand.  The result,
+    // (M b) x 2M reals, is rho_w[i][j] at Rho + (i b + w) M + j: row stride b M, point stride M.
+    long long rrs = M, rws = MM;
+    if (p.rho_i8) {
+        const long long xrows = oz_pad_rows((long long)M * b);
+        PHF_TRY(oz_slice_rows((int)((long long)M * b), 2 * N, reinterpret_cast<const double *>(p.Xs), 2LL * N,
+                              p.slices, xrows, p.Xsl, p.eX, st));
+        PHF_TRY(launch_bra_rho_operand(M, N, p.bra, p.BRop, st));
+        PHF_TRY(oz_slice_rows(2 * M, 2 * N, p.BRop, 2LL * N, p.slices, oz_pad_cols(2LL * M), p.BRsl, p.eBR, st));
+        PHF_TRY(oz_gemm_t((int)((long long)M * b), 2 * M, 2 * N, p.slices, p.Xsl, p.eX, p.BRsl, p.eBR,
+                          reinterpret_cast<double *>(p.Rho), 2LL * M, 0, 0, p.ozerr, st));
+        rrs = (long long)b * M;
+        rws = M;
+    } else if (!fused) {
         PHF_TRY(zgemm_strided(M, M, N, bc, 1, Z1, vz(p.Xs, ld, 1, N), vz(p.bra, 1, N, 0, 0, 1), Z0,
                               vo(p.Rho, M, 1, MM), nullptr, st));
+    }
     if (p.prec == PHF_PREC_FP64) {
         PHF_TRY(launch_gather_p(n, bc, p.Rho, p.Pvec, b, st));
         PHF_TRY(zgemm_strided(L, bc, (int)n2, 1, 1, Z1, vd(p.Bst, n2, 1), vz(p.Pvec, b, 1), Z0, vo(p.dvec, b, 1),
@@ -789,7 +821,8 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         if (fused)
             PHF_TRY(oz_rho_slice(n, N, bc, p.Xs, ld, p.bra, p.slices, p.Bsl, p.eb, p.Psl, p.ePc, st));
         else
-            PHF_TRY(oz_slice_p_cols(n, bc, p.Rho, p.slices, p.Psl, p.ePc, st));
+            PHF_TRY(oz_slice_density(n, bc, p.Rho, rrs, rws, p.slices, p.Bsl, p.eb, oz_pad_cols(8LL * bc), p.Psl,
+                                     p.ePc, oz_pad_cols(2LL * bc), st));
     }
     // tensor-core path: the Coulomb chain runs on a second stream beside the exchange GEMM (independent
     // operands and outputs; its small, latency-bound launches fill the SMs the exchange GEMM's last
@@ -848,7 +881,6 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st));
     } else {
-        if (!fused) PHF_TRY(oz_slice_rho_cols(n, bc, p.Rho, p.slices, p.Bsl, p.eb, st));
         // K (as K^T, 8 bc x n^2) written by the GEMM epilogue as -K into Gamma's complex M x M blocks
         if (p.streamed)
             PHF_TRY(exchange_streamed(p, bc, st));

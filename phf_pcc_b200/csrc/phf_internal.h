@@ -123,6 +123,9 @@ int launch_gather_p(int n, int b, const zc *rho, zc *P, long long ldp, cudaStrea
 int launch_gather_kin(int n, int b, const zc *rho, zc *Kin, long long ldk, cudaStream_t st);
 // streamed FP64 form: EKp[(i - i0) n + k][l n + j] = G[(i - i0) n + l][k n + j] for one panel of ipanel i's
 int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *EKp, long long lde, cudaStream_t st);
+// The bra's real operand for rho = X bra^H as a real GEMM on interleaved (re, im) rows of X: row 2j =
+// (Re b_j0, Im b_j0, Re b_j1, ...), row 2j + 1 = (-Im b_j0, Re b_j0, ...) (bra M x N row-major).
+int launch_bra_rho_operand(int M, int N, const zc *bra, double *out, cudaStream_t st);
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
                           cudaStream_t st);
@@ -145,8 +148,10 @@ int oz_slice_rows(int m, int k, const double *A, long long lda, int S, long long
                   cudaStream_t st);
 int oz_slice_rows_strided(int m, int k, const double *A, long long lda, long long cs, int S, long long rows_pad,
                           signed char *out, int *ea, cudaStream_t st);
-int oz_slice_rho_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
-int oz_slice_p_cols(int n, int b, const zc *rho, int S, signed char *out, int *eb, cudaStream_t st);
+// Exchange columns (8 per point) and Coulomb columns (2 per point) of points 0 .. bc-1 of the densities
+// rho_w (element [r][q] of point w at rho[w ws + r rs + q]; rs, ws even), sliced with their exponents.
+int oz_slice_density(int n, int bc, const zc *rho, long long rs, long long ws, int S, signed char *Ksl, int *eK,
+                     long long npadK, signed char *Psl, int *eP, long long npadP, cudaStream_t st);
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st,
               int gamma_n = 0);  // gamma_n > 0: -K^T written into Gamma (exchange GEMM, m = n^2)
@@ -235,6 +240,12 @@ struct PlanImpl {
     // Coulomb term on the tensor cores: d = B vec P, J = B^T d (B = Cholesky vectors as L x n^2)
     signed char *B1sl = nullptr, *B2sl = nullptr, *Psl = nullptr, *dsl = nullptr;
     int *eB1 = nullptr, *eB2 = nullptr, *ePc = nullptr, *edc = nullptr;
+    // int8 density GEMM (n > 64): rows (i, w) of X as an (M b) x 2N real matrix and the bra's
+    // 2M x 2N real operand, sliced; rho_i8 when the plan forms rho this way
+    bool rho_i8 = false;
+    signed char *Xsl = nullptr, *BRsl = nullptr;
+    int *eX = nullptr, *eBR = nullptr;
+    double *BRop = nullptr;
     double *dT = nullptr, *Jr = nullptr, *dpart = nullptr;  // dpart: split-k partials of d^T
     ~PlanImpl();
 };

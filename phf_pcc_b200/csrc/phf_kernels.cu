@@ -554,6 +554,28 @@ int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long 
     return PHF_OK;
 }
 
+// out (2M x 2N): rows 2j and 2j + 1 of the real operand of rho = X bra^H (see launch_bra_rho_operand)
+__global__ void bra_rho_operand_kernel(int M, int N, const zc *bra, double *out) {
+    const long long total = (long long)M * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(e / N), k = (int)(e - (long long)j * N);
+        const zc b = bra[e];
+        double *r0 = out + (long long)(2 * j) * (2 * N) + 2 * k, *r1 = r0 + 2 * N;
+        r0[0] = b.x;
+        r0[1] = b.y;
+        r1[0] = -b.y;
+        r1[1] = b.x;
+    }
+}
+
+int launch_bra_rho_operand(int M, int N, const zc *bra, double *out, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    bra_rho_operand_kernel<<<grid_for((long long)M * N), NT, 0, st>>>(M, N, bra, out);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *EKp, long long lde, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     ek_panel_kernel<<<(unsigned)((long long)ipanel * n), NT, 0, st>>>(n, G, ldg, EKp, lde);

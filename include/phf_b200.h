@@ -106,6 +106,36 @@ int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, in
                 const double *rooty, const double *weightsp, const double *weightpg, const phf_complex *fsp,
                 const phf_complex *fpg, const phf_complex *fk, phf_complex *t0, phf_complex *t1, phf_complex *t2);
 
+/* PbarHbarOlap (SUCCSD_Boson_cmplx/FPUCC.f90:14-48 declaration, body :49-272): the grid kernel of
+ * projected CCSD, which the reference's PCC solver (Main.f90 PGCC -> BroydenIter, Broyden.f90) calls once
+ * per iteration.  For every grid point (il, iy, ipg) with R = R1(il) R2(iy) Rpg(ipg), EvalKernel
+ * (FPUCC.f90:529-602): the amplitudes (t1, t2) transformed by R (DSTT2: the Thouless form of R [1; T1]
+ * and the double similarity transform of T2, FPUCC_Tools.f90:697-722, PCCCI.f90:14-276), the CCSD energy
+ * and residuals of the transformed amplitudes with the Fock matrix of (hone, htwo) (CCRes.f90), and the
+ * lambda / eps tensors of BuildKernSD (FPUCC_Tools.f90:291-436), summed with the weight
+ * weightsp weightpg(ipg,p,q) Wigner(qj,m,n) conj(fsp(m)) fsp(n) conj(fpg(p)) fpg(q) over m, n, p, q; with
+ * ncik == 2 a second pass with conjugated hone, htwo, t1, t2, R Rk(2) and weight times fk(2); with
+ * sp == 2 the spin-flip components are projected out (ProjSz, MO order [occ alpha, occ beta, vir alpha,
+ * vir beta]).  Layouts (Fortran, M = nso, v = nso - nocc):
+ *   hone(i,j) = hone[i + M*j];  htwo(i,j,k,l) = htwo[i + M*(j + M*(k + M*l))]  antisymmetrised <ij||kl>
+ *   t1(a,i) = t1[a + v*i];  t2(a,b,i,j) = t2[a + v*(b + v*(i + nocc*j))]      (a, b virtual from 0)
+ *   r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty as phf_buildhsg (npoints = ngrid);
+ *   rk(t,i,j) = rk[t + ncik*(i + M*j)];  fsp: ncisp = 2*qj+1 entries, fpg: ncipg, fk: ncik
+ *   outputs olap0, eolap0 (scalars), olapex1, eolapex1 (v x nocc), olapex2, eolapex2 (v,v,nocc,nocc).
+ * ref and nao are accepted as in the reference (nao = nso/2 or 0) and not used.  trunode 1 or 2 (the SD
+ * kernel); 3 (adding the (T) energy) returns PHF_ERR_UNSUPPORTED, other values PHF_ERR_ARG (the
+ * reference STOPs).  FP64 on the GPU, nso <= 112; M^4 complex per grid point of device memory (grid
+ * points run in chunks of `workspace` bytes, 0 = 16 GiB).  comm is not taken: the reference's rank
+ * split over iy is a partial sum over grid points that callers add. */
+int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_complex *olapex2, phf_complex *eolap0,
+                     phf_complex *eolapex1, phf_complex *eolapex2, const phf_complex *hone, const phf_complex *htwo,
+                     const phf_complex *ref, const phf_complex *t1, const phf_complex *t2, int nocc, int nao, int nso,
+                     double enuc, int qj, int sp, const int *npoints, int npg, int ncisp, int ncipg, int ncik,
+                     const phf_complex *r1, const phf_complex *r2, const phf_complex *rpg, const phf_complex *rk,
+                     const double *roota, const double *rootb, const double *rooty, const double *weightsp,
+                     const double *weightpg, const phf_complex *fsp, const phf_complex *fpg, const phf_complex *fk,
+                     int trunode, size_t workspace);
+
 /* ---------------------------------------------------------------- plan API
  * A plan holds the Hamiltonian, the grid and the device workspace, so that repeated
  * energy/gradient evaluations (one per optimiser step, PHF.py:55-91) upload only Z or C. */

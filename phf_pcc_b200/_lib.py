@@ -76,6 +76,8 @@ SIGNATURES = {
     "phf_int8_wide_mma": (_I, [_I]),
     "phf_buildsc": (_I, [phf_complex, _P, _P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                          _P, _P, _P, _P, _P]),
+    "phf_pbarhbarolap": (_I, [_P] * 11 + [_I, _I, _I, ctypes.c_double, _I, _I, _P, _I, _I, _I, _I] + [_P] * 12
+                         + [_I, ctypes.c_size_t]),
     "phf_profile_enable": (_I, [_I]),
     "phf_ozaki_dgemm": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P]),
     "phf_tc_dgemm": (_I, [_I, _I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong,

@@ -13,7 +13,8 @@ import numpy as np
 from . import _lib
 from ._lib import PREC, PHFError, check, phf_complex, phf_plan_desc
 
-__all__ = ["buildhsg", "buildhsg_chol", "localg", "buildsc", "Plan", "eval_batch", "check_status", "PHFError"]
+__all__ = ["buildhsg", "buildhsg_chol", "localg", "buildsc", "pbarhbarolap", "Plan", "eval_batch", "check_status",
+           "PHFError"]
 
 
 def _fz(a):
@@ -191,6 +192,43 @@ def buildsc(c0, c1, c2, nocc, ngrid, qj, r1, r2, rpg, rk, roota, rootb, rooty, w
                                  ctypes.byref(t0), _ptr(t1), _ptr(t2))
     check(st, "phf_buildsc")
     return complex(t0.re, t0.im), t1, t2
+
+
+def pbarhbarolap(hone, htwo, ref, t1, t2, nocc, nao, nso, enuc, qj, sp, npoints, npg, ncisp, ncipg, ncik, r1, r2,
+                 rpg, rk, roota, rootb, rooty, weightsp, weightpg, fsp, fpg, fk, trunode, comm=None, workspace=0):
+    """PbarHbarOlap (SUCCSD_Boson_cmplx/FPUCC.f90:14-272), the projected-CCSD grid kernel, on the GPU.
+
+    Arguments in the order of the Fortran dummy arguments after the outputs; returns
+    (Olap0, OlapEx1 (v, nocc), OlapEx2 (v, v, nocc, nocc), EOlap0, EOlapEx1, EOlapEx2) as complex scalars
+    and Fortran-ordered complex128 arrays (v = nso - nocc).  ``ref`` and ``nao`` are accepted and not used,
+    as in the reference; ``comm`` is not used (the grid is not split over ranks here).  ``workspace``:
+    device bytes per chunk of grid points (0 = 16 GiB).  See phf_pbarhbarolap in include/phf_b200.h."""
+    del comm
+    M, o = int(nso), int(nocc)
+    v = M - o
+    hone_, htwo_, t1_, t2_ = _fz(hone), _fz(htwo), _fz(t1), _fz(t2)
+    if hone_.shape != (M, M) or htwo_.shape != (M, M, M, M) or t1_.shape != (v, o) or t2_.shape != (v, v, o, o):
+        raise ValueError("hone (M, M), htwo (M, M, M, M), t1 (v, o) and t2 (v, v, o, o) expected")
+    ng = np.ascontiguousarray(np.asarray(npoints, dtype=np.int32).reshape(2))
+    r1_, r2_, rpg_, rk_ = _fz(r1), _fz(r2), _fz(rpg), _fz(rk)
+    if r1_.shape != (int(ng[0]), M, M) or r2_.shape != (int(ng[1]), M, M) or rpg_.shape != (int(npg), M, M):
+        raise ValueError("rotation shapes do not match npoints, npg and nso")
+    if rk_.ndim != 3 or rk_.shape[0] < int(ncik) or rk_.shape[1:] != (M, M):
+        raise ValueError("rk must be (ncik, nso, nso)")
+    ra, rb, ry = (np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.float64))) for x in (roota, rootb, rooty))
+    wsp, wpg = _fd(weightsp), _fd(weightpg)
+    fsp_, fpg_, fk_ = (np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.complex128))) for x in (fsp, fpg, fk))
+    ref_ = _fz(ref) if ref is not None else None
+    out0, oute0 = phf_complex(), phf_complex()
+    ex1, eex1 = (np.zeros((v, o), dtype=np.complex128, order="F") for _ in range(2))
+    ex2, eex2 = (np.zeros((v, v, o, o), dtype=np.complex128, order="F") for _ in range(2))
+    st = _lib.load().phf_pbarhbarolap(
+        ctypes.byref(out0), _ptr(ex1), _ptr(ex2), ctypes.byref(oute0), _ptr(eex1), _ptr(eex2), _ptr(hone_),
+        _ptr(htwo_), _ptr(ref_), _ptr(t1_), _ptr(t2_), o, int(nao), M, float(enuc), int(qj), int(sp), _ptr(ng),
+        int(npg), int(ncisp), int(ncipg), int(ncik), _ptr(r1_), _ptr(r2_), _ptr(rpg_), _ptr(rk_), _ptr(ra), _ptr(rb),
+        _ptr(ry), _ptr(wsp), _ptr(wpg), _ptr(fsp_), _ptr(fpg_), _ptr(fk_), int(trunode), int(workspace))
+    check(st, "phf_pbarhbarolap")
+    return complex(out0.re, out0.im), ex1, ex2, complex(oute0.re, oute0.im), eex1, eex2
 
 
 class Plan:

@@ -252,6 +252,22 @@ struct PlanImpl {
 
 
 // buildsc.cu: BuildSC (PHF_fort/PHFTools.f90:464-537) with host arrays in the reference's layouts
+// pcc.cu: PbarHbarOlap (SUCCSD_Boson_cmplx/FPUCC.f90:14-272) with host arrays in the reference's layouts
+struct PccArgs {
+    const phf_complex *hone, *htwo, *t1, *t2;
+    int nocc, nso;
+    double enuc;
+    int qj, sp;
+    const int *npoints;
+    int npg, ncisp, ncipg, ncik;
+    const phf_complex *r1, *r2, *rpg, *rk;
+    const double *roota, *rootb, *rooty, *weightsp, *weightpg;
+    const phf_complex *fsp, *fpg, *fk;
+    size_t workspace;
+};
+int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1, phf_complex *olapex2,
+                     phf_complex *eolap0, phf_complex *eolapex1, phf_complex *eolapex2);
+
 int buildsc_run(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
                 int npg, const phf_complex *r1, const phf_complex *r2, const phf_complex *rpg, const double *weightsp,
                 const double *weightpg, int ncisp, int ncipg, const phf_complex *fsp, const phf_complex *fpg,

@@ -81,3 +81,26 @@ def test_tensor_core_gemm_entries_validate_arguments_before_any_device_call():
     assert lib.phf_tc_dgemm(8, 8, 8, 2, 0, p, 4, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
     assert lib.phf_tc_dgemm(0, 8, 8, 3, 0, p, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
     assert lib.phf_tc_dgemm(8, 8, 8, 2, 0, null, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
+
+
+def test_pbarhbarolap_rejects_options_before_any_device_call():
+    """TrunODE 3 (the (T) correction) is not built, TrunODE outside 1..3 is an error (the reference
+    STOPs), and nso above the inverse's limit is refused -- all before device memory is touched."""
+    import ctypes
+
+    lib = _lib.load()
+    p = ctypes.c_void_p(8)
+    ng = (ctypes.c_int * 2)(1, 1)
+
+    def call(nocc=2, nso=8, trunode=1, ncisp=1, qj=0, ncik=1):
+        return lib.phf_pbarhbarolap(p, p, p, p, p, p, p, p, p, p, p, nocc, nso // 2, nso, 0.0, qj, 1, ng, 1, ncisp, 1,
+                                    ncik, p, p, p, p, p, p, p, p, p, p, p, p, trunode, 0)
+
+    assert call(trunode=3) == _lib.PHF_ERR_UNSUPPORTED
+    assert call(trunode=-3) == _lib.PHF_ERR_UNSUPPORTED
+    assert call(trunode=0) == _lib.PHF_ERR_ARG
+    assert call(trunode=4) == _lib.PHF_ERR_ARG
+    assert call(nso=114, nocc=4) == _lib.PHF_ERR_UNSUPPORTED
+    assert call(ncisp=2) == _lib.PHF_ERR_ARG      # ncisp must be 2 qj + 1
+    assert call(ncik=3) == _lib.PHF_ERR_ARG
+    assert call(nocc=8) == _lib.PHF_ERR_ARG        # no virtual orbitals

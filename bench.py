@@ -28,6 +28,7 @@ Multi-GPU (torchrun, one process per GPU): every rank evaluates its own independ
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -873,13 +874,181 @@ def run_batch(args):
     return 0
 
 
+PCC_METRIC = "projected-CCSD grid kernel (PbarHbarOlap) grid-pts/s, FP64 on the GPU; vs host CPU"
+
+
+def pcc_call_args(p):
+    """PbarHbarOlap's inputs after its outputs, in the Fortran order (SUCCSD_Boson_cmplx/FPUCC.f90:14-17)."""
+    M, o = p["HOne"].shape[0], p["NOcc"]
+    return (p["HOne"], p["HTwo"], None, p["T1"], p["T2"], o, M // 2, M, p["ENuc"], p["QJ"], p["SP"], p["NPoints"],
+            p["Npg"], len(p["fsp"]), len(p["fpg"]), p["ncik"], p["R1"], p["R2"], p["Rpg"], p["Rk"], p["Roota"],
+            p["Rootb"], p["Rooty"], p["Weightsp"], p["Weightpg"], p["fsp"], p["fpg"], p["fk"], p["TrunODE"])
+
+
+def pcc_workload():
+    from phf_pcc_b200 import synth
+
+    c = synth.PCC_CONFIG
+    p = synth.make_pcc_problem(c["n"], c["N"], c["L"], ngrid=c["ngrid"], seed=0)
+    p.pop("MO")
+    M, o = p["HOne"].shape[0], p["NOcc"]
+    npts = p["NPoints"][0] * p["NPoints"][1] * p["Npg"]
+    name = (f"projected CCSD grid kernel: n={c['n']} M={M} NOcc={o}, dense <pq||rs>, grid "
+            f"{p['NPoints'][0]}x{p['NPoints'][1]}x{p['Npg']} = {npts} points, TrunODE 1")
+    return p, npts, name
+
+
+def pcc_cpu_sample(p, seconds_target):
+    """Time the numpy oracle of PbarHbarOlap (all host threads through BLAS) on a bounded block of grid
+    points; returns (points/s, threads, description, (w0, w1), oracle sums of the block)."""
+    from oracle import phf_pcc as pcc
+
+    nth = os.cpu_count() or 1
+    npts = p["NPoints"][0] * p["NPoints"][1] * p["Npg"]
+    t0 = time.perf_counter()
+    out = pcc.pbarhbarolap(**p, points=[0])
+    t1 = time.perf_counter() - t0
+    k = int(max(1, min(npts, seconds_target / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    out = pcc.pbarhbarolap(**p, points=list(range(k)))
+    t2 = time.perf_counter() - t0
+    return k / t2, nth, f"{k} of {npts} grid points (numpy oracle, BLAS threads = host cores), {t2:.1f} s", \
+        (0, k), out
+
+
+def run_pcc_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    p, npts, name = pcc_workload()
+    _, _, _, (w0, w1), _ = pcc_cpu_sample(p, args.cpu_seconds)
+    from oracle import phf_pcc as pcc
+
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        pcc.pbarhbarolap(**p, points=list(range(w0, w1)))
+        if i >= args.warmup:
+            vals.append((w1 - w0) / (time.perf_counter() - t0))
+    v = statistics.median(vals)
+    nth = os.cpu_count() or 1
+    line = {"metric": PCC_METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * npts / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": name, "points_per_step": npts},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nth, "cpu_model": cpu_model(), "kind": "port",
+                             "sample": f"{w1 - w0} of {npts} grid points per step (numpy oracle); rate scaled to "
+                                       "the full grid"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line, default=_json_default), flush=True)
+    return 0
+
+
+def run_pcc(args):
+    import torch
+
+    from phf_pcc_b200 import _lib, api
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    p, npts, name = pcc_workload()
+    cargs = pcc_call_args(p)
+    lib = _lib.load()
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+    ms, fl = ctypes.c_double(), ctypes.c_double()
+    for _ in range(args.warmup):
+        out = api.pbarhbarolap(*cargs)
+    torch.cuda.synchronize()
+    dev_ms, wall, flops = [], [], 0.0
+    launches0 = lib.phf_kernel_launches()
+    clk = clock_sampler(local)
+    clk.__enter__()
+    try:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = api.pbarhbarolap(*cargs)       # host arrays in, host sums out (synchronous)
+            wall.append(time.perf_counter() - t0)
+            lib.phf_pbarhbarolap_stats(ctypes.byref(ms), ctypes.byref(fl))
+            dev_ms.append(ms.value)
+            flops = fl.value
+    finally:
+        clk.__exit__(None, None, None)
+    launches = (lib.phf_kernel_launches() - launches0) // max(1, args.steps)
+    t = torch.tensor([sum(dev_ms) / len(dev_ms), sum(wall) / len(wall)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, wall_s = float(t[0]), float(t[1])
+    value = world * npts / (step_ms * 1e-3)
+    if rank == 0:
+        fp64_peak = measure_fp64_peak(torch, dev)
+        achieved = flops / (step_ms * 1e-3) / 1e12
+        h2d = sum(np.asarray(x).nbytes for x in cargs if isinstance(x, np.ndarray))
+        d2h = 2 * 16 + sum(np.asarray(x).nbytes for x in (out[1], out[2], out[4], out[5]))
+        roof = {"bound": "fp64 tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "kernel": "zgemm_kernel (all contractions of the pipeline, FP64 mma.sync m8n8k4)",
+                "note": "achieved = FP64 flops the pipeline's GEMMs executed (8 m n k per complex product) / "
+                        "device time of the whole pipeline (elementwise kernels and inverses included)",
+                "gemm_flops_per_step": flops}
+        cpu, parity = None, None
+        if not args.no_cpu:
+            v, nth, desc, (w0, w1), ora = pcc_cpu_sample(p, args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": nth, "cpu_model": cpu_model(), "kind": "port",
+                   "sample": desc + "; rate scaled to the full grid (per-point work is independent)"}
+            # the same block on the GPU: the first w1 gamma points of the first Lebedev point
+            k = min(w1, p["NPoints"][1])
+            if k < w1:
+                from oracle import phf_pcc as pcc
+                ora = pcc.pbarhbarolap(**p, points=list(range(k)))
+            q = dict(p)
+            q.update(R1=p["R1"][:1], R2=p["R2"][:k], NPoints=(1, k), Roota=p["Roota"][:1], Rootb=p["Rootb"][:1],
+                     Rooty=p["Rooty"][:k], Weightsp=p["Weightsp"][:1, :k])
+            got = api.pbarhbarolap(*pcc_call_args(q))
+            rel = max(float(np.abs(np.asarray(g) - np.asarray(r)).max() / max(np.abs(np.asarray(r)).max(), 1e-300))
+                      for g, r in zip(got, ora))
+            e_g, e_o = got[3] / got[0], ora[3] / ora[0]
+            parity = {"points": [0, k], "max_rel_diff_of_sums": rel, "energy_of_block": e_o.real,
+                      "abs_dE_vs_oracle": abs(e_g - e_o), "oracle": "numpy restatement of PbarHbarOlap"}
+        line = {"metric": PCC_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded h, B_L, amplitudes)",
+                "config": {"workload": name, "points_per_step": npts,
+                           "l2": "flushed (256 MB write) between timed steps",
+                           "timing": "device time of the grid pipeline inside each call (CUDA events on its "
+                                     "stream, inputs uploaded before the first event)",
+                           "parallelism": f"{world} independent instance(s), one per GPU"},
+                "energy_ratio": (out[3] / out[0]).real, "oracle_parity": parity, "roofline": roof,
+                "cpu_baseline": cpu,
+                "e2e": {"value": world * npts / wall_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h,
+                        "path": "phf_pbarhbarolap through PUCC_X2-style api.pbarhbarolap: host arrays in (device "
+                                "buffers allocated and filled inside the call), host sums out"},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line, default=_json_default), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c3", "c4", "c5", "pcc"])
     ap.add_argument("--batch", type=int, default=256, help="instances for --config c4")
     ap.add_argument("--precision", default="ozaki_i8", choices=["fp64", "ozaki_i8", "bf16x3", "tf32"])
     ap.add_argument("--study", action="store_true",
@@ -899,7 +1068,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
-        return run_reference(args)
+        return run_pcc_reference(args) if args.config == "pcc" else run_reference(args)
+    if args.config == "pcc":
+        return run_pcc(args)
     if args.narrow_mma:
         from phf_pcc_b200 import _lib
 

@@ -136,6 +136,11 @@ int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_complex *olap
                      const double *weightpg, const phf_complex *fsp, const phf_complex *fpg, const phf_complex *fk,
                      int trunode, size_t workspace);
 
+/* Device time in ms of the last phf_pbarhbarolap call's grid pipeline (from the first launch after the
+ * inputs are uploaded to the end of the last sum, CUDA events on its stream) and the FP64 flops its
+ * GEMMs executed (8 m n k per complex product).  No counterpart in the reference. */
+int phf_pbarhbarolap_stats(double *device_ms, double *gemm_flops);
+
 /* ---------------------------------------------------------------- plan API
  * A plan holds the Hamiltonian, the grid and the device workspace, so that repeated
  * energy/gradient evaluations (one per optimiser step, PHF.py:55-91) upload only Z or C. */

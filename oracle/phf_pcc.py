@@ -389,41 +389,9 @@ def pbarhbar_res_from_olap(Olap0, OlapEx1, OlapEx2, EOlap0, EOlapEx1, EOlapEx2, 
 
 
 def make_pcc_problem(n, N, L, ngrid=(14, 8), seed=0, amp=0.05, spin_blocked=False, pg="None", SP=1, J=0):
-    """Seeded projected-CC input in an orthonormal MO basis: H1, antisymmetrised H2, the grid
-    rotations transformed to the MOs (ao2mo(R, MO, 2) = MO^H R MO, as Main_PCC.py:35-40), and
-    amplitudes T1 (v, o), T2 (v, v, o, o) antisymmetric, entries N(0, amp).
-
-    ``spin_blocked``: MOs of definite spin in the order [occ alpha, occ beta, vir alpha, vir beta]
-    (what ProjSz assumes for SP = 2)."""
+    """The seeded projected-CC input of ``phf_pcc_b200.synth.make_pcc_problem`` (test data, not oracle
+    arithmetic)."""
     from phf_pcc_b200 import synth
-    from oracle import phf_oracle as orc
 
-    p = synth.make_problem(n, N, L, ngrid=ngrid, seed=seed, pg=pg, SP=SP, J=J)
-    M = p.M
-    rng = np.random.default_rng(seed + 7919)
-    if spin_blocked:
-        Qa = synth.random_unitary(n, rng)
-        Qb = synth.random_unitary(n, rng)
-        na = N // 2
-        cols = [np.concatenate([Qa[:, :na], np.zeros((n, na))]),
-                np.concatenate([np.zeros((n, N - na)), Qb[:, :N - na]]),
-                np.concatenate([Qa[:, na:], np.zeros((n, n - na))]),
-                np.concatenate([np.zeros((n, n - N + na)), Qb[:, N - na:]])]
-        MO = np.concatenate(cols, axis=1)
-    else:
-        MO = p.Qfull
-    H1 = orc.mo_transform_1(p.hone_ao(), MO)
-    H2 = orc.mo_transform_2(orc.dense_htwo_from_chol(p.B), MO)
-    g = p.grid
-    R1 = np.array([MO.conj().T @ r @ MO for r in g.R1])
-    R2 = np.array([MO.conj().T @ r @ MO for r in g.R2])
-    Rpg = np.array([MO.conj().T @ r @ MO for r in g.Rpg])
-    v, o = M - N, N
-    T1 = amp * (rng.normal(size=(v, o)) + 1j * rng.normal(size=(v, o)))
-    T2 = amp * (rng.normal(size=(v, v, o, o)) + 1j * rng.normal(size=(v, v, o, o)))
-    T2 = asymm2(T2) / 4
-    return dict(HOne=H1, HTwo=H2, T1=T1, T2=T2, NOcc=N, ENuc=0.0, QJ=g.J, SP=g.SP, NPoints=(g.R1.shape[0], g.R2.shape[0]),
-                Npg=g.npg, ncik=1, R1=R1, R2=R2, Rpg=Rpg, Rk=np.array([np.eye(M, dtype=complex)] * 2),
-                Roota=g.roota, Rootb=g.rootb, Rooty=g.rooty, Weightsp=g.weightsp, Weightpg=g.weightpg,
-                fsp=np.ones(g.ncisp, complex), fpg=np.ones(g.ncipg, complex), fk=np.ones(2, complex), TrunODE=1,
-                MO=MO)
+    return synth.make_pcc_problem(n, N, L, ngrid=ngrid, seed=seed, amp=amp, spin_blocked=spin_blocked, pg=pg,
+                                  SP=SP, J=J)

@@ -78,6 +78,7 @@ SIGNATURES = {
                          _P, _P, _P, _P, _P]),
     "phf_pbarhbarolap": (_I, [_P] * 11 + [_I, _I, _I, ctypes.c_double, _I, _I, _P, _I, _I, _I, _I] + [_P] * 12
                          + [_I, ctypes.c_size_t]),
+    "phf_pbarhbarolap_stats": (_I, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "phf_profile_enable": (_I, [_I]),
     "phf_ozaki_dgemm": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P]),
     "phf_tc_dgemm": (_I, [_I, _I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P, ctypes.c_longlong,

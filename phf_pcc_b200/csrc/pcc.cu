@@ -33,6 +33,9 @@ namespace {
 
 constexpr int NT = 256;
 constexpr int MAXD = 6;
+
+// device time of the grid pipeline of the last call (uploads excluded) and the FP64 flops its GEMMs ran
+double g_pcc_ms = 0.0, g_pcc_flops = 0.0;
 const zc ONE{1.0, 0.0}, ZERO{0.0, 0.0};
 
 // ---------------------------------------------------------------- strided tensor views
@@ -130,6 +133,48 @@ __global__ void ew_kernel(EwArgs g) {
         if (use_beta) v = v + g.beta * g.C[oc];
         g.C[oc] = v;
     }
+}
+
+// C(i, j)_w = beta C + alpha sum_s T(i, j, s)_w   (the partial products of a split-k GEMM, T contiguous)
+__global__ void splitk_reduce_kernel(int m, int n, int S, long long total, const zc *T, OutView C, zc alpha,
+                                     zc beta) {
+    const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
+        const long long w = e / ((long long)m * n);
+        const long long r = e - w * (long long)m * n;
+        const int i = (int)(r % m), j = (int)(r / m);
+        const zc *t = T + (w * S) * (long long)m * n + r;
+        zc acc{0.0, 0.0};
+        for (int q = 0; q < S; ++q) acc = acc + t[(long long)q * m * n];
+        zc v = alpha * acc;
+        zc *c = C.p + w * C.bs0 + i * C.rs + j * C.cs;
+        if (use_beta) v = v + beta * *c;
+        *c = v;
+    }
+}
+
+// T[w S + s] = sum over the k-slice s of op(A)[k] op(B)[k]  (scalar contractions: one CTA per point and slice)
+__global__ void dot_kernel(long long k, int S, View A, View B, zc *T) {
+    __shared__ zc sh[NT];
+    const long long w = blockIdx.x / S;
+    const int s = (int)(blockIdx.x - w * S);
+    const long long ks = (k + S - 1) / S, k0 = s * ks, k1 = (k0 + ks < k) ? k0 + ks : k;
+    const zc *a = static_cast<const zc *>(A.p) + w * A.bs0;
+    const zc *b = static_cast<const zc *>(B.p) + w * B.bs0;
+    zc acc{0.0, 0.0};
+    for (long long q = k0 + threadIdx.x; q < k1; q += NT) {
+        zc x = a[q * A.cs], y = b[q * B.rs];
+        if (A.conj) x.y = -x.y;
+        if (B.conj) y.y = -y.y;
+        acc = acc + x * y;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = NT / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) T[blockIdx.x] = sh[0];
 }
 
 // r_w = 1 / x_w
@@ -545,8 +590,53 @@ int ein(Ctx &x, const char *spec, zc alpha, const TV &A, const TV &B, zc beta, c
     PHF_TRY(check_view(x, va.p, m, k, va.rs, va.cs, pts, va.bs0, nb, va.bs1, spec));
     PHF_TRY(check_view(x, vb.p, k, n, vb.rs, vb.cs, pts, vb.bs0, nb, vb.bs1, spec));
     PHF_TRY(check_view(x, vc.p, m, n, vc.rs, vc.cs, pts, vc.bs0, nb, vc.bs1, spec));
-    PHF_TRY(zgemm_strided((int)m, (int)n, (int)k, pts, (int)nb, alpha, va, vb, best.tempC ? ZERO : beta, vc, nullptr,
-                          x.st));
+    const zc cbeta = best.tempC ? ZERO : beta;
+    const long long tiles = (long long)pts * nb * ((m + 63) / 64) * ((n + 63) / 64);
+    if (m == 1 && n == 1 && nb == 1 && k >= 256) {
+        // a scalar per point: a blocked dot product, k split over S CTAs per point, then the sum of the parts
+        const int S = (int)std::max<long long>(1, std::min<long long>(k / 2048 + 1, (8 * 148 + pts - 1) / pts));
+        zc *T = x.take((size_t)S * pts);
+        if (!T) return pool_error();
+        PHF_TRY(check_view(x, T, 1, 1, 0, 0, pts, S, S, 1, spec));
+        dot_kernel<<<(unsigned)(pts * S), NT, 0, x.st>>>(k, S, va, vb, T);
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+        splitk_reduce_kernel<<<blocks_for(pts), NT, 0, x.st>>>(1, 1, S, pts, T, vc, alpha, cbeta);
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+    } else if (nb == 1 && tiles < 2 * 148 && k >= 1024) {
+        // few output tiles and a long k: split k over S batches of partial products, then sum them
+        const int S = (int)std::max<long long>(2, std::min<long long>(k / 256, (4 * 148 + tiles - 1) / tiles));
+        const long long ks = k / S, rem = k - S * ks;
+        zc *T = x.take((size_t)(m * n * S) * pts);
+        if (!T) return pool_error();
+        View a2 = va, b2 = vb;
+        a2.bs1 = ks * va.cs;
+        b2.bs1 = ks * vb.rs;
+        OutView t2;
+        t2.p = T;
+        t2.rs = 1;
+        t2.cs = m;
+        t2.bs0 = m * n * S;
+        t2.bs1 = m * n;
+        PHF_TRY(check_view(x, T, m, n, 1, m, pts, m * n * S, S, m * n, spec));
+        PHF_TRY(zgemm_strided((int)m, (int)n, (int)ks, pts, S, ONE, a2, b2, ZERO, t2, nullptr, x.st));
+        if (rem) {
+            View a3 = va, b3 = vb;
+            a3.p = static_cast<const zc *>(va.p) + S * ks * va.cs;
+            b3.p = static_cast<const zc *>(vb.p) + S * ks * vb.rs;
+            OutView t3 = t2;
+            t3.bs1 = 0;
+            PHF_TRY(zgemm_strided((int)m, (int)n, (int)rem, pts, 1, ONE, a3, b3, ONE, t3, nullptr, x.st));
+        }
+        const long long total = m * n * pts;
+        splitk_reduce_kernel<<<blocks_for(total), NT, 0, x.st>>>((int)m, (int)n, S, total, T, vc, alpha, cbeta);
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+    } else {
+        PHF_TRY(zgemm_strided((int)m, (int)n, (int)k, pts, (int)nb, alpha, va, vb, cbeta, vc, nullptr, x.st));
+    }
+    g_pcc_flops += 8.0 * (double)m * (double)n * (double)k * (double)nb * pts;
     if (best.tempC) {
         const std::string back = lc + "->" + sp.c;
         PHF_TRY(ew(x, back.c_str(), ONE, c, nullptr, beta, C, pts));
@@ -774,6 +864,18 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
         return t;
     };
 
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    PHF_CUDA(cudaEventCreate(&ev0));
+    PHF_CUDA(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evg{ev0, ev1};
+    g_pcc_flops = 0.0;
+    PHF_CUDA(cudaEventRecord(ev0, st));
     for (int pass = 0; pass < (g.ncik == 2 ? 2 : 1); ++pass) {
         const zc *h1 = pass ? H1c : H1;
         zc *h2 = pass ? H2c : H2;
@@ -1089,11 +1191,15 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
         PHF_TRY(mask_sz(x, tens(aE2, {v, v, o, o}, false), o, v, nao));
         PHF_TRY(mask_sz(x, tens(aL2, {v, v, o, o}, false), o, v, nao));
     }
+    PHF_CUDA(cudaEventRecord(ev1, st));
     std::vector<cd> h((size_t)nacc);
     int hflag = 0;
     PHF_CUDA(cudaMemcpyAsync(h.data(), acc, nacc * sizeof(zc), cudaMemcpyDeviceToHost, st));
     PHF_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     PHF_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    PHF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    g_pcc_ms = ms;
     if (hflag & 1) {
         set_error(PHF_ERR_SINGULAR, "pbarhbarolap: a rotated occupied block or the transform V is exactly singular");
         return PHF_ERR_SINGULAR;
@@ -1157,4 +1263,10 @@ extern "C" int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_co
     phf::PccArgs g{hone, htwo, t1, t2, nocc, nso, enuc, qj, sp, npoints, npg, ncisp, ncipg, ncik, r1, r2, rpg, rk,
                    roota, rootb, rooty, weightsp, weightpg, fsp, fpg, fk, workspace};
     return phf::pbarhbarolap_run(g, olap0, olapex1, olapex2, eolap0, eolapex1, eolapex2);
+}
+
+extern "C" int phf_pbarhbarolap_stats(double *device_ms, double *gemm_flops) {
+    if (device_ms) *device_ms = phf::g_pcc_ms;
+    if (gemm_flops) *gemm_flops = phf::g_pcc_flops;
+    return PHF_OK;
 }

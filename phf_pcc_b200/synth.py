@@ -19,7 +19,8 @@ import numpy as np
 
 from .grid import ProjectionGrid, make_grid
 
-__all__ = ["Problem", "make_problem", "random_unitary", "orbital_rotation", "CONFIGS", "config_problem"]
+__all__ = ["Problem", "make_problem", "random_unitary", "orbital_rotation", "CONFIGS", "config_problem",
+           "make_pcc_problem", "PCC_CONFIG"]
 
 
 def random_unitary(M: int, rng: np.random.Generator) -> np.ndarray:
@@ -116,3 +117,64 @@ def batch_problems(count: int = 256, seed: int = 0):
         grid = (14, 8) if i % 2 == 0 else (50, 16)
         out.append(make_problem(n, n // 2, 4 * n, ngrid=grid, seed=seed * 100003 + i))
     return out
+
+
+def _antisym_htwo(B):
+    """Spin-orbital <ij||kl> from spatial Cholesky vectors (L, n, n): (pq|rs) = sum_L B_L[pq] B_L[rs] in the
+    spin blocks of Main_PHF.py:22-29, then Mulliken -> Dirac with antisymmetrisation (makeH.py:63-67)."""
+    n = B.shape[1]
+    M = 2 * n
+    eri = np.einsum("Lpq,Lrs->pqrs", B, B, optimize=True)
+    Hm = np.zeros((M, M, M, M))
+    a, b = slice(0, n), slice(n, M)
+    for s1 in (a, b):
+        for s2 in (a, b):
+            Hm[s1, s1, s2, s2] = eri
+    d = np.einsum("ijkl->ikjl", Hm)
+    return d - np.einsum("ijkl->ijlk", d)
+
+
+def make_pcc_problem(n, N, L, ngrid=(14, 8), seed=0, amp=0.05, spin_blocked=False, pg="None", SP=1, J=0):
+    """Seeded projected-CC input (the arguments of PbarHbarOlap, SUCCSD_Boson_cmplx/FPUCC.f90:14-48) in an
+    orthonormal MO basis: HOne, antisymmetrised HTwo, the grid rotations transformed to the MOs
+    (MO^H R MO, as Main_PCC.py:35-40 does with ao2mo), and amplitudes T1 (v, o), T2 (v, v, o, o)
+    antisymmetric with entries N(0, amp).  The Hamiltonian generator is ``make_problem``'s.
+
+    ``spin_blocked``: MOs of definite spin in the order [occ alpha, occ beta, vir alpha, vir beta]
+    (what the SP = 2 projection ProjSz assumes)."""
+    p = make_problem(n, N, L, ngrid=ngrid, seed=seed, pg=pg, SP=SP, J=J)
+    M = p.M
+    rng = np.random.default_rng(seed + 7919)
+    if spin_blocked:
+        Qa = random_unitary(n, rng)
+        Qb = random_unitary(n, rng)
+        na = N // 2
+        cols = [np.concatenate([Qa[:, :na], np.zeros((n, na))]),
+                np.concatenate([np.zeros((n, N - na)), Qb[:, :N - na]]),
+                np.concatenate([Qa[:, na:], np.zeros((n, n - na))]),
+                np.concatenate([np.zeros((n, n - N + na)), Qb[:, N - na:]])]
+        MO = np.concatenate(cols, axis=1)
+    else:
+        MO = p.Qfull
+    Mc = MO.conj()
+    H1 = Mc.T @ p.hone_ao() @ MO
+    H2 = np.einsum("abcd,ai,bj,ck,dl->ijkl", _antisym_htwo(p.B), Mc, Mc, MO, MO, optimize=True)
+    g = p.grid
+    R1 = np.array([Mc.T @ r @ MO for r in g.R1])
+    R2 = np.array([Mc.T @ r @ MO for r in g.R2])
+    Rpg = np.array([Mc.T @ r @ MO for r in g.Rpg])
+    v, o = M - N, N
+    T1 = amp * (rng.normal(size=(v, o)) + 1j * rng.normal(size=(v, o)))
+    T2 = amp * (rng.normal(size=(v, v, o, o)) + 1j * rng.normal(size=(v, v, o, o)))
+    T2 = T2 - np.einsum("abij->abji", T2)
+    T2 = (T2 - np.einsum("abij->baij", T2)) / 4
+    return dict(HOne=H1, HTwo=H2, T1=T1, T2=T2, NOcc=N, ENuc=0.0, QJ=g.J, SP=g.SP,
+                NPoints=(g.R1.shape[0], g.R2.shape[0]), Npg=g.npg, ncik=1, R1=R1, R2=R2, Rpg=Rpg,
+                Rk=np.array([np.eye(M, dtype=complex)] * 2), Roota=g.roota, Rootb=g.rootb, Rooty=g.rooty,
+                Weightsp=g.weightsp, Weightpg=g.weightpg, fsp=np.ones(g.ncisp, complex),
+                fpg=np.ones(g.ncipg, complex), fk=np.ones(2, complex), TrunODE=1, MO=MO)
+
+
+# The projected-CC grid workload: configuration 1's Hamiltonian generator and grid (n = 20, M = 40,
+# N = 10, Lebedev 14 x 8 gamma = 112 points), CCSD-shaped amplitudes
+PCC_CONFIG = dict(n=20, N=10, L=120, ngrid=(14, 8))

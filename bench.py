@@ -189,9 +189,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def problem_for(name: str, seed: int):
+def problem_for(name: str, seed: int, ngrid=None):
+    """The configuration's problem; ``ngrid`` (Lebedev points, gamma points) replaces its grid, for
+    profiling a configuration's kernels on a smaller grid."""
     from phf_pcc_b200 import synth
-    return synth.config_problem(name, seed=seed)
+    if not ngrid:
+        return synth.config_problem(name, seed=seed)
+    c = synth.CONFIGS[name]
+    return synth.make_problem(c["n"], c["N"], c["L"], ngrid=tuple(ngrid), seed=seed, pg=c["pg"])
 
 
 def api_kwargs(p):
@@ -256,10 +261,15 @@ def quoted_flops_per_point(p):
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant exchange launch, from
 # ncu captures of these workloads, with the note that says what was captured.
 TRAFFIC = {
-    ("c2", "ozaki_i8"): (0.840e9 + 0.251e9,
-                         "DRAM read + write of one K launch (4096 x 8192 x 4096, 1024-point chunk) from an ncu "
-                         "capture; algorithmic bytes of that launch: A slices 84 MB + B slices 168 MB + FP64 "
-                         "output 268 MB = 5.2e8"),
+    ("c2", "ozaki_i8"): (2.412e9 + 0.820e9,
+                         "DRAM read + write of the K launch (4096 x 25600 x 4096, the whole 3200-point chunk, wide "
+                         "MMA issue) from an ncu capture (profiles/ozaki_i8_gemm_c2.md); algorithmic bytes of that "
+                         "launch: A slices 84 MB + B slices 524 MB + FP64 output 839 MB = 1.45e9"),
+    ("c5", "ozaki_i8"): (36.2e9,
+                         "DRAM read + write of one exchange-panel GEMM (3200 x 25600 x 40000 in two k passes), "
+                         "scaled by the columns (points) from an ncu capture of the same panel shape on a 384-point "
+                         "grid (4.34 GB for 3200 x 3072 x 40000; profiles/ozaki_i8_gemm_c5_panel.md); algorithmic "
+                         "bytes of the full launch: A slices 0.64 GB + B slices 5.12 GB + FP64 output 0.66 GB = 6.4e9"),
 }
 
 
@@ -380,7 +390,7 @@ def run_reference(args):
         from phf_pcc_b200 import synth
         p = synth.batch_problems(args.batch, seed=1000)[0]
     else:
-        p = problem_for(args.config, seed=0)
+        p = problem_for(args.config, seed=0, ngrid=args.ngrid)
     nth = os.cpu_count() or 1
     setup = oracle_setup(p)
     # size the per-step sample once (about --cpu-seconds of CPU work), then time every step on it
@@ -491,7 +501,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
-    p = problem_for(args.config, seed=1000 + rank)
+    p = problem_for(args.config, seed=1000 + rank, ngrid=args.ngrid)
     Ref, Z = p.ref_and_z()
     kw = api_kwargs(p)
     form = jk_form_of(p) if args.jk_form == "auto" else args.jk_form
@@ -502,7 +512,7 @@ def run_ours(args):
 
     tune = not args.no_autotune
     plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
-                    autotune=tune, **kw)
+                    autotune=tune, exchange_panel=args.exchange_panel, **kw)
     clk = clock_sampler(local)
     step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
@@ -1064,6 +1074,10 @@ def main():
     ap.add_argument("--fp64-all", action="store_true",
                     help="also time the stored-exchange-matrix FP64 form above n = 128 and the factorized FP64 form")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
+    ap.add_argument("--ngrid", type=lambda t: [int(v) for v in t.split(",")], default=None,
+                    help="Lebedev,gamma points replacing the configuration's grid (profiling on a smaller grid)")
+    ap.add_argument("--exchange-panel", type=int, default=0,
+                    help="streamed form: spatial indices per exchange panel (0 = the plan's choice)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

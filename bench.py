@@ -896,16 +896,17 @@ def pcc_call_args(p):
             p["Rootb"], p["Rooty"], p["Weightsp"], p["Weightpg"], p["fsp"], p["fpg"], p["fk"], p["TrunODE"])
 
 
-def pcc_workload():
+def pcc_workload(trunode=1):
     from phf_pcc_b200 import synth
 
     c = synth.PCC_CONFIG
     p = synth.make_pcc_problem(c["n"], c["N"], c["L"], ngrid=c["ngrid"], seed=0)
     p.pop("MO")
+    p["TrunODE"] = trunode
     M, o = p["HOne"].shape[0], p["NOcc"]
     npts = p["NPoints"][0] * p["NPoints"][1] * p["Npg"]
     name = (f"projected CCSD grid kernel: n={c['n']} M={M} NOcc={o}, dense <pq||rs>, grid "
-            f"{p['NPoints'][0]}x{p['NPoints'][1]}x{p['Npg']} = {npts} points, TrunODE 1")
+            f"{p['NPoints'][0]}x{p['NPoints'][1]}x{p['Npg']} = {npts} points, TrunODE {trunode}")
     return p, npts, name
 
 
@@ -930,7 +931,7 @@ def pcc_cpu_sample(p, seconds_target):
 def run_pcc_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    p, npts, name = pcc_workload()
+    p, npts, name = pcc_workload(args.trunode)
     _, _, _, (w0, w1), _ = pcc_cpu_sample(p, args.cpu_seconds)
     from oracle import phf_pcc as pcc
 
@@ -970,7 +971,7 @@ def run_pcc(args):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-    p, npts, name = pcc_workload()
+    p, npts, name = pcc_workload(args.trunode)
     cargs = pcc_call_args(p)
     lib = _lib.load()
     flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
@@ -1079,6 +1080,8 @@ def main():
                     help="Lebedev,gamma points replacing the configuration's grid (profiling on a smaller grid)")
     ap.add_argument("--exchange-panel", type=int, default=0,
                     help="streamed form: spatial indices per exchange panel (0 = the plan's choice)")
+    ap.add_argument("--trunode", type=int, default=1, choices=[1, 2, 3],
+                    help="--config pcc: TrunODE of the grid kernel (3 adds the (T) energy at every point)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -122,9 +122,11 @@ int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, in
  *   r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty as phf_buildhsg (npoints = ngrid);
  *   rk(t,i,j) = rk[t + ncik*(i + M*j)];  fsp: ncisp = 2*qj+1 entries, fpg: ncipg, fk: ncik
  *   outputs olap0, eolap0 (scalars), olapex1, eolapex1 (v x nocc), olapex2, eolapex2 (v,v,nocc,nocc).
- * ref and nao are accepted as in the reference (nao = nso/2 or 0) and not used.  trunode 1 or 2 (the SD
- * kernel); 3 (adding the (T) energy) returns PHF_ERR_UNSUPPORTED, other values PHF_ERR_ARG (the
- * reference STOPs).  FP64 on the GPU, nso <= 112; M^4 complex per grid point of device memory (grid
+ * ref and nao are accepted as in the reference (nao = nso/2 or 0) and not used.  trunode 1, 2 or -3 run
+ * the SD kernel (BuildKernSD takes |trunode|); 3 also adds the (T) energy of the transformed amplitudes
+ * to eps0 at every point (CCSD_T_Ene, SUCCSD_Boson_cmplx/CCSD_T.f90:10-108, FPUCC.f90:577-581; o^3 v^3
+ * complex per point of extra device memory, a few points at a time); other values return PHF_ERR_ARG
+ * (the reference STOPs).  FP64 on the GPU, nso <= 112; M^4 complex per grid point of device memory (grid
  * points run in chunks of `workspace` bytes, 0 = 16 GiB).  comm is not taken: the reference's rank
  * split over iy is a partial sum over grid points that callers add. */
 int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_complex *olapex2, phf_complex *eolap0,

@@ -19,6 +19,7 @@ It restates, in numpy, the reference's FP64 grid kernel of projected CCSD
 * ``build_kern_sd`` -- FPUCC_Tools.f90:291-436 (BuildKernSD)
 * ``cc_energy``     -- CCRes.f90:9-29; ``cc_itms`` -- CCRes.f90:355-537; ``cc_res12`` --
                        CCRes.f90:164-353; ``asymm2`` -- CCRes.f90:31-70; ``aperm`` -- :120-162
+* ``ccsd_t_energy`` -- CCSD_T.f90:10-108 (CCSD_T_Ene, get_wv, Perm3, DirectSum3)
 * ``proj_sz1`` / ``proj_sz2_vo`` -- FPUCC_Tools.f90:150-234
 * ``wigner``        -- Wrappers.f90:769-797 (argument order J, N, M as declared there)
 
@@ -43,7 +44,7 @@ import numpy as np
 
 __all__ = [
     "wigner", "build_thouless_z", "proj_t1", "int_tran4_sim", "mkfock_mo", "trans_t2", "ci2cc", "build_w", "dstt2",
-    "asymm2", "aperm", "cc_energy", "cc_itms", "cc_res12", "build_kern_sd", "proj_sz1", "proj_sz2_vo",
+    "asymm2", "aperm", "cc_energy", "cc_itms", "cc_res12", "ccsd_t_energy", "build_kern_sd", "proj_sz1", "proj_sz2_vo",
     "eval_kernel", "point_weights", "pbarhbarolap", "pbarhbar_res_from_olap", "make_pcc_problem",
 ]
 
@@ -295,12 +296,43 @@ def build_kern_sd(Fock, ERI, ESCF, U1t, U2t, o, SP):
     return Ovl1, Ovl2, EOvl0, EOvl1, EOvl2
 
 
+def ccsd_t_energy(F, H2, T1, T2, o):
+    """CCSD_T_Ene (CCSD_T.f90:10-52) with get_wv (:54-70) and Perm3 (:72-88): the (T) energy of the
+    amplitudes, a triangular loop a >= b >= c over virtual triples."""
+    M = F.shape[0]
+    v = M - o
+    fvo = F[o:, :o]
+    vvvo, ovoo, vvoo = H2[o:, o:, o:, :o], H2[:o, o:, :o, :o], H2[o:, o:, :o, :o]
+    fd = np.diag(F)
+    eijk = fd[:o, None, None] + fd[None, :o, None] + fd[None, None, :o]           # DirectSum3
+    eabc = fd[o:, None, None] + fd[None, o:, None] + fd[None, None, o:]
+
+    def get_wv(a, b, c):
+        w = np.einsum("dk,dij->kij", vvvo[b, c], T2[a], **ES)                     # At_dot_B (:62)
+        w = w - np.einsum("xl,lyz->xyz", T2[b, c], ovoo[:, a], **ES)             # A_dot_B (:63)
+        vv = np.einsum("x,yz->xyz", T1[a], vvoo[b, c]) + np.einsum("x,yz->xyz", fvo[a], T2[b, c])  # A_outer_B
+        vv = vv + w
+        w = w + np.einsum("kij->ijk", w) + np.einsum("jki->ijk", w)              # Perm3: w + w(k,i,j) + w(j,k,i)
+        return w, vv
+
+    ene = 0j
+    for a in range(v):
+        for b in range(a + 1):
+            for c in range(b + 1):
+                wabc, vabc = get_wv(a, b, c)
+                wcab, vcab = get_wv(c, a, b)
+                wbac, vbac = get_wv(b, a, c)
+                w = (wabc + wcab - wbac) / (eijk - eabc[a, b, c])
+                ene += np.sum(w * np.conj(vabc + vcab - vbac))
+    return ene / 2
+
+
 def eval_kernel(HOne, HTwo, T1, T2, ENuc, RotMat, o, SP, TrunODE, fock=None):
-    """EvalKernel (FPUCC.f90:529-602) for TrunODE 1 and 2 (the SD kernel; TrunODE 3 adds the
-    (T) energy, which this restatement does not cover).  Returns
-    (eps0, lambda0, eps1, eps2, lambda1, lambda2)."""
-    if abs(TrunODE) not in (1, 2):
-        raise ValueError("TrunODE 1 or 2")
+    """EvalKernel (FPUCC.f90:529-602): the SD kernel for |TrunODE| 1 to 3, plus the (T) energy of the
+    transformed amplitudes when TrunODE == 3 (:577-581).  Returns (eps0, lambda0, eps1, eps2, lambda1,
+    lambda2)."""
+    if abs(TrunODE) not in (1, 2, 3):
+        raise ValueError("TrunODE 1, 2 or 3")
     M = HOne.shape[0]
     U0t, U1t, U2t = dstt2(RotMat, T1, T2, o)                                    # :561
     STot = U0t                                                                  # :565
@@ -309,6 +341,8 @@ def eval_kernel(HOne, HTwo, T1, T2, ENuc, RotMat, o, SP, TrunODE, fock=None):
     Fock, ESCF = fock                                                           # :566
     ESCF = ESCF + ENuc                                                          # :567
     Ovl1, Ovl2, eps0, EOvl1, EOvl2 = build_kern_sd(Fock, HTwo, ESCF, U1t, U2t, o, SP)   # :568-572
+    if TrunODE == 3:                                                            # :577-581
+        eps0 = eps0 + ccsd_t_energy(Fock, HTwo, U1t, U2t, o)
     lam1t, lam2t, eps1t, eps2t = Ovl1, Ovl2, EOvl1, EOvl2
     if SP == 2:                                                                 # :584-589
         lam1t, eps1t = proj_sz1(lam1t, o, M), proj_sz1(eps1t, o, M)

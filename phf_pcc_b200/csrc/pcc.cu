@@ -177,6 +177,72 @@ __global__ void dot_kernel(long long k, int S, View A, View B, zc *T) {
     if (threadIdx.x == 0) T[blockIdx.x] = sh[0];
 }
 
+// The (T) energy's triangular sum (CCSD_T_Ene, SUCCSD_Boson_cmplx/CCSD_T.f90:10-108) for one virtual
+// triple a >= b >= c (blockIdx.x) of one grid point (blockIdx.y):
+//   w = Perm3(W[abc] + W[cab] - W[bac]),  v = V[abc] + V[cab] - V[bac],
+//   V[pqr](x,y,z) = W[pqr](x,y,z) + T1(p,x) <qr||yz> + f(p,x) T2(q,r,y,z)          (get_wv, :54-70)
+//   part = sum_xyz w / (f_x + f_y + f_z - f_a - f_b - f_c) conj(v)
+// with W[pqr](x,y,z) = sum_d <qr||dx> T2(p,d,y,z) - sum_l T2(q,r,x,l) <la||yz> at W[x + o(y + o(z + o(p + v(q + v r))))]
+// and Perm3 w(x,y,z) = w(x,y,z) + w(z,x,y) + w(y,z,x).
+struct TriplesArgs {
+    int o, v;
+    const int *tri;     // 3 per triple: a, b, c
+    const zc *W;        // per point stride wps
+    long long wps;
+    const zc *T1;       // per point (v x o), stride t1ps
+    long long t1ps;
+    const zc *T2;       // per point (v, v, o, o), stride t2ps
+    long long t2ps;
+    const zc *vvoo;     // <ab||ij> view: strides 1, M, M^2, M^3
+    const zc *fvo;      // F(o + a, i): strides 1, M
+    const zc *fd;       // the Fock matrix F (M x M, column-major): its diagonal is read
+    int M;
+    zc *part;           // [point][triple]
+    long long ntri;
+};
+
+__global__ void triples_kernel(TriplesArgs g) {
+    __shared__ zc sh[NT];
+    const long long t = blockIdx.x;
+    const int w = blockIdx.y;
+    const int o = g.o, v = g.v, M = g.M;
+    const int a = g.tri[3 * t], b = g.tri[3 * t + 1], c = g.tri[3 * t + 2];
+    const long long o3 = (long long)o * o * o, M2 = (long long)M * M;
+    const zc *Wp = g.W + w * g.wps;
+    const zc *t1 = g.T1 + w * g.t1ps, *t2 = g.T2 + w * g.t2ps;
+    const int trip[3][3] = {{a, b, c}, {c, a, b}, {b, a, c}};
+    const double sgn[3] = {1.0, 1.0, -1.0};
+    long long base[3];
+    for (int q = 0; q < 3; ++q) base[q] = o3 * (trip[q][0] + (long long)v * (trip[q][1] + (long long)v * trip[q][2]));
+    const long long dg = M + 1;  // F(i, i) at fd[i (M + 1)]
+    const zc eabc = g.fd[(o + a) * dg] + g.fd[(o + b) * dg] + g.fd[(o + c) * dg];
+    zc acc{0.0, 0.0};
+    for (int e = threadIdx.x; e < o3; e += NT) {
+        const int x = e % o, y = (e / o) % o, z = e / (o * o);
+        const long long e1 = e, e2 = z + o * (x + (long long)o * y), e3 = y + o * (z + (long long)o * x);
+        zc wv{0.0, 0.0}, vv{0.0, 0.0};
+        for (int q = 0; q < 3; ++q) {
+            const int p = trip[q][0], r1 = trip[q][1], r2 = trip[q][2];
+            const zc *Wq = Wp + base[q];
+            const zc w0 = Wq[e1];
+            wv = wv + sgn[q] * (w0 + Wq[e2] + Wq[e3]);
+            const zc extra = t1[p + (long long)v * x] * g.vvoo[r1 + M * (r2 + (long long)M * (y + (long long)M * z))] +
+                             g.fvo[p + (long long)M * x] * t2[r1 + (long long)v * (r2 + (long long)v * (y + (long long)o * z))];
+            vv = vv + sgn[q] * (w0 + extra);
+        }
+        const zc d = (g.fd[x * dg] + g.fd[y * dg] + g.fd[z * dg]) - eabc;
+        acc = acc + divz(wv, d) * conjz(vv);
+    }
+    (void)M2;
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = NT / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) g.part[w * g.ntri + t] = sh[0];
+}
+
 // r_w = 1 / x_w
 __global__ void recip_kernel(int n, const zc *x, zc *r) {
     const int w = blockIdx.x * NT + threadIdx.x;
@@ -835,8 +901,32 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
     Ctx x;
     x.ar = &ar;
     x.one = one;
-    x.cap = (size_t)b * (size_t)(2 * M4 + 64);
+    // (T) energy (TrunODE 3): the W tensor of a few points at a time, the triples a >= b >= c
+    const long long o3v3 = (long long)o * o * o * v * v * v;
+    x.cap = std::max<size_t>((size_t)b * (size_t)(2 * M4 + 64), g.trunode == 3 ? 2 * (size_t)o3v3 + 64 : 0);
     PHF_TRY(ar.alloc(&x.pool, x.cap));
+    const long long ntri = (long long)v * (v + 1) * (v + 2) / 6;
+    int nsubT = 0;
+    zc *Wtrip = nullptr, *tpart = nullptr;
+    int *trid = nullptr;
+    if (g.trunode == 3) {
+        const long long by_budget = (long long)(budget / 2) / (o3v3 * (long long)sizeof(zc));
+        const long long by_pool = (long long)(x.cap / 2) / o3v3;
+        nsubT = (int)std::max<long long>(1, std::min<long long>({(long long)b, by_budget, by_pool}));
+        if (by_pool < 1) {
+            set_error(PHF_ERR_UNSUPPORTED, "pbarhbarolap: the (T) tensor of one point exceeds the workspace");
+            return PHF_ERR_UNSUPPORTED;
+        }
+        PHF_TRY(ar.alloc(&Wtrip, (size_t)nsubT * (size_t)o3v3));
+        PHF_TRY(ar.alloc(&tpart, (size_t)nsubT * (size_t)ntri));
+        PHF_TRY(ar.alloc(&trid, 3 * (size_t)ntri));
+        std::vector<int> tr;
+        tr.reserve(3 * (size_t)ntri);
+        for (int a = 0; a < v; ++a)      // the order of the reference's loops (CCSD_T.f90:38-40)
+            for (int bb = 0; bb <= a; ++bb)
+                for (int c = 0; c <= bb; ++c) tr.insert(tr.end(), {a, bb, c});
+        PHF_CUDA(cudaMemcpy(trid, tr.data(), tr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // accumulators: eps0, lambda0, eps1, lambda1, eps2, lambda2
     zc *acc = nullptr;
     const long long nacc = 2 + 2 * vo + 2 * vvoo;
@@ -1149,6 +1239,39 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
             PHF_TRY(ew(x, "bi,aj->abij", mkz(-1), W1v, &r1v, ONE, EO2v));
             PHF_TRY(ew(x, "bj,ai->abij", ONE, W1v, &r1v, ONE, EO2v));
             PHF_TRY(ew(x, "aj,bi->abij", mkz(-1), W1v, &r1v, ONE, EO2v));
+            if (g.trunode == 3) {  // EvalKernel :577-581: eps0 += the (T) energy of (W1, W2) after BuildKernSD
+                const TV Hvvvo_ = blk(H2v, {o, o, o, 0}, {v, v, v, o});
+                for (int s0 = 0; s0 < bc; s0 += nsubT) {
+                    const int ns = std::min(nsubT, bc - s0);
+                    x.npts = ns;
+                    const size_t mark = x.used;
+                    TV Wt = tens(Wtrip, {o, o, o, v, v, v});
+                    TV W2s = W2v, W1s = W1v;
+                    W2s.p += s0 * W2v.ps;
+                    W1s.p += s0 * W1v.ps;
+                    // W(x,y,z,a,b,c) = sum_d <bc||dx> T2(a,d,y,z) - sum_l T2(b,c,x,l) <la||yz>   (get_wv :62-63)
+                    PHF_TRY(ein(x, "bcdx,adyz->xyzabc", ONE, Hvvvo_, W2s, ZERO, Wt));
+                    PHF_TRY(ein(x, "bcxl,layz->xyzabc", mkz(-1), W2s, Hovoo, ONE, Wt));
+                    PHF_TRY(check_view(x, Wtrip, o3v3, 1, 1, 0, ns, o3v3, 1, 0, "(T) W"));
+                    PHF_TRY(check_view(x, tpart, ntri, 1, 1, 0, ns, ntri, 1, 0, "(T) parts"));
+                    PHF_TRY(check_view(x, W2s.p, vvoo, 1, 1, 0, ns, W2v.ps, 1, 0, "(T) T2"));
+                    PHF_TRY(check_view(x, W1s.p, vo, 1, 1, 0, ns, W1v.ps, 1, 0, "(T) T1"));
+                    TriplesArgs ta{o, v, trid, Wtrip, o3v3, W1s.p, W1v.ps, W2s.p, W2v.ps, Hvvoo.p, Fvo_s.p, F, M, tpart,
+                                   ntri};
+                    triples_kernel<<<dim3((unsigned)ntri, (unsigned)ns), NT, 0, st>>>(ta);
+                    ++g_launches;
+                    PHF_CHECK_LAUNCH();
+                    TV pv;
+                    pv.p = tpart;
+                    pv.nd = 1;
+                    pv.dim[0] = (int)ntri;
+                    pv.st[0] = 1;
+                    pv.ps = ntri;
+                    PHF_TRY(ein(x, "t,t->", mkz(0.5), pv, ones_v((int)ntri), ONE, scal(EO0 + s0)));
+                    x.used = mark;
+                }
+                x.npts = bc;
+            }
             if (sz) {  // BuildKernSD :329-332, :398-400, :426-428 and EvalKernel :584-589
                 PHF_TRY(mask_sz(x, W1v, o, v, nao));
                 PHF_TRY(mask_sz(x, EO1v, o, v, nao));
@@ -1242,11 +1365,7 @@ extern "C" int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_co
         return PHF_ERR_ARG;
     }
     const int t = trunode < 0 ? -trunode : trunode;
-    if (t == 3) {
-        phf::set_error(PHF_ERR_UNSUPPORTED, "phf_pbarhbarolap: TrunODE 3 (the (T) energy correction) is not built");
-        return PHF_ERR_UNSUPPORTED;
-    }
-    if (t != 1 && t != 2) {  // BuildKernSD STOPs 'ODE truncation type not recognized' (FPUCC_Tools.f90:314)
+    if (t < 1 || t > 3) {  // BuildKernSD STOPs 'ODE truncation type not recognized' (FPUCC_Tools.f90:314)
         phf::set_error(PHF_ERR_ARG, "phf_pbarhbarolap: ODE truncation type not recognized");
         return PHF_ERR_ARG;
     }
@@ -1261,7 +1380,7 @@ extern "C" int phf_pbarhbarolap(phf_complex *olap0, phf_complex *olapex1, phf_co
         return PHF_ERR_NO_DEVICE;
     }
     phf::PccArgs g{hone, htwo, t1, t2, nocc, nso, enuc, qj, sp, npoints, npg, ncisp, ncipg, ncik, r1, r2, rpg, rk,
-                   roota, rootb, rooty, weightsp, weightpg, fsp, fpg, fk, workspace};
+                   roota, rootb, rooty, weightsp, weightpg, fsp, fpg, fk, trunode, workspace};
     return phf::pbarhbarolap_run(g, olap0, olapex1, olapex2, eolap0, eolapex1, eolapex2);
 }
 

@@ -263,6 +263,7 @@ struct PccArgs {
     const phf_complex *r1, *r2, *rpg, *rk;
     const double *roota, *rootb, *rooty, *weightsp, *weightpg;
     const phf_complex *fsp, *fpg, *fk;
+    int trunode;
     size_t workspace;
 };
 int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1, phf_complex *olapex2,

@@ -84,8 +84,8 @@ def test_tensor_core_gemm_entries_validate_arguments_before_any_device_call():
 
 
 def test_pbarhbarolap_rejects_options_before_any_device_call():
-    """TrunODE 3 (the (T) correction) is not built, TrunODE outside 1..3 is an error (the reference
-    STOPs), and nso above the inverse's limit is refused -- all before device memory is touched."""
+    """TrunODE outside 1..3 is an error (the reference STOPs) and nso above the inverse's limit is
+    refused -- both before device memory is touched."""
     import ctypes
 
     lib = _lib.load()
@@ -96,9 +96,8 @@ def test_pbarhbarolap_rejects_options_before_any_device_call():
         return lib.phf_pbarhbarolap(p, p, p, p, p, p, p, p, p, p, p, nocc, nso // 2, nso, 0.0, qj, 1, ng, 1, ncisp, 1,
                                     ncik, p, p, p, p, p, p, p, p, p, p, p, p, trunode, 0)
 
-    assert call(trunode=3) == _lib.PHF_ERR_UNSUPPORTED
-    assert call(trunode=-3) == _lib.PHF_ERR_UNSUPPORTED
     assert call(trunode=0) == _lib.PHF_ERR_ARG
+    assert call(trunode=-4) == _lib.PHF_ERR_ARG
     assert call(trunode=4) == _lib.PHF_ERR_ARG
     assert call(nso=114, nocc=4) == _lib.PHF_ERR_UNSUPPORTED
     assert call(ncisp=2) == _lib.PHF_ERR_ARG      # ncisp must be 2 qj + 1

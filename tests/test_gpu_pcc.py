@@ -69,6 +69,33 @@ def test_pbarhbarolap_matches_oracle(case):
     _compare(got, ref)
 
 
+@pytest.mark.parametrize("case", [
+    dict(n=4, N=4, ngrid=(6, 2), seed=8),
+    dict(n=5, N=4, ngrid=(6, 2), seed=9, pg="C2v", SP=1),
+    dict(n=4, N=4, ngrid=(1, 3), seed=10, SP=2, spin_blocked=True),
+])
+def test_pbarhbarolap_with_triples_matches_oracle(case):
+    """TrunODE 3: the (T) energy of the transformed amplitudes added to eps0 at every point (CCSD_T.f90);
+    TrunODE -3 is the SD kernel (the reference adds (T) only for +3)."""
+    p = _problem(**case)
+    p["TrunODE"] = 3
+    _compare(_gpu(p), pcc.pbarhbarolap(**p))
+    p["TrunODE"] = -3
+    _compare(_gpu(p), pcc.pbarhbarolap(**p))
+
+
+def test_triples_split_over_sub_batches():
+    """The (T) tensor (o^3 v^3 per point) is formed a few points at a time: at M = 12, o = 4 it is larger
+    than the per-point scratch, so the 24 points of a chunk run in two sub-batches; a one-point workspace
+    runs one point per chunk."""
+    p = _problem(6, 4, (6, 4), seed=12)
+    p["TrunODE"] = 3
+    whole = _gpu(p)
+    _compare(whole, pcc.pbarhbarolap(**p))
+    small = _gpu(p, workspace=1 << 16)
+    _compare(small, whole, tol=1e-12)
+
+
 def test_chunked_grid_equals_one_chunk():
     p = _problem(4, 4, (6, 4), seed=6)
     whole = _gpu(p)

@@ -182,7 +182,8 @@ __global__ void dot_kernel(long long k, int S, View A, View B, zc *T) {
 //   w = Perm3(W[abc] + W[cab] - W[bac]),  v = V[abc] + V[cab] - V[bac],
 //   V[pqr](x,y,z) = W[pqr](x,y,z) + T1(p,x) <qr||yz> + f(p,x) T2(q,r,y,z)          (get_wv, :54-70)
 //   part = sum_xyz w / (f_x + f_y + f_z - f_a - f_b - f_c) conj(v)
-// with W[pqr](x,y,z) = sum_d <qr||dx> T2(p,d,y,z) - sum_l T2(q,r,x,l) <la||yz> at W[x + o(y + o(z + o(p + v(q + v r))))]
+// with W[pqr](x,y,z) = sum_d <qr||dx> T2(p,d,y,z) - sum_l T2(q,r,x,l) <lp||yz> at W[x + o(q + v(r + v(p + v(y + o z))))]
+// (the rows (x, q, r) of the GEMM that forms it, then its columns (p, y, z))
 // and Perm3 w(x,y,z) = w(x,y,z) + w(z,x,y) + w(y,z,x).
 struct TriplesArgs {
     int o, v;
@@ -213,13 +214,15 @@ __global__ void triples_kernel(TriplesArgs g) {
     const int trip[3][3] = {{a, b, c}, {c, a, b}, {b, a, c}};
     const double sgn[3] = {1.0, 1.0, -1.0};
     long long base[3];
-    for (int q = 0; q < 3; ++q) base[q] = o3 * (trip[q][0] + (long long)v * (trip[q][1] + (long long)v * trip[q][2]));
+    for (int q = 0; q < 3; ++q) base[q] = (long long)o * (trip[q][1] + (long long)v * (trip[q][2] + (long long)v * trip[q][0]));
+    const long long ov3 = (long long)o * v * v * v;
     const long long dg = M + 1;  // F(i, i) at fd[i (M + 1)]
     const zc eabc = g.fd[(o + a) * dg] + g.fd[(o + b) * dg] + g.fd[(o + c) * dg];
     zc acc{0.0, 0.0};
     for (int e = threadIdx.x; e < o3; e += NT) {
         const int x = e % o, y = (e / o) % o, z = e / (o * o);
-        const long long e1 = e, e2 = z + o * (x + (long long)o * y), e3 = y + o * (z + (long long)o * x);
+        const long long e1 = x + ov3 * (y + (long long)o * z), e2 = z + ov3 * (x + (long long)o * y),
+                        e3 = y + ov3 * (z + (long long)o * x);
         zc wv{0.0, 0.0}, vv{0.0, 0.0};
         for (int q = 0; q < 3; ++q) {
             const int p = trip[q][0], r1 = trip[q][1], r2 = trip[q][2];
@@ -241,6 +244,69 @@ __global__ void triples_kernel(TriplesArgs g) {
         __syncthreads();
     }
     if (threadIdx.x == 0) g.part[w * g.ntri + t] = sh[0];
+}
+
+// The same sum without the W tensor (o <= kTriplesFusedMaxO): for its triple the CTA forms
+//   S(x,y,z) = sum_q sgn_q W[pqr_q](x,y,z)   over the orders (abc), (cab), (bac), signs +, +, -,
+// from <qr||dx>, T2 and <la||yz> directly into shared memory, then
+//   w = S(x,y,z) + S(z,x,y) + S(y,z,x)  (Perm3 is linear),  v = S(x,y,z) + sum_q sgn_q (T1 <||> + f T2)_q.
+constexpr int kTriplesFusedMaxO = 18;
+
+__global__ void triples_fused_kernel(TriplesArgs g, const zc *vvvo, const zc *ovoo) {
+    extern __shared__ zc Ssh[];
+    __shared__ zc red[NT];
+    const long long t = blockIdx.x;
+    const int w = blockIdx.y;
+    const int o = g.o, v = g.v, M = g.M;
+    const int a = g.tri[3 * t], b = g.tri[3 * t + 1], c = g.tri[3 * t + 2];
+    const int o3 = o * o * o;
+    const long long M2 = (long long)M * M, M3 = M2 * M;
+    const zc *t1 = g.T1 + w * g.t1ps, *t2 = g.T2 + w * g.t2ps;
+    const int trip[3][3] = {{a, b, c}, {c, a, b}, {b, a, c}};
+    const double sgn[3] = {1.0, 1.0, -1.0};
+    const long long dg = M + 1;
+    for (int e = threadIdx.x; e < o3; e += NT) {
+        const int x = e % o, y = (e / o) % o, z = e / (o * o);
+        zc acc{0.0, 0.0};
+        for (int q = 0; q < 3; ++q) {
+            const int p = trip[q][0], r1 = trip[q][1], r2 = trip[q][2];
+            zc wq{0.0, 0.0};
+            // sum_d <r1 r2||d x> T2(p, d, y, z)      (vvvo(r1, r2, d, x) at r1 + M r2 + M^2 d + M^3 x)
+            const zc *vp = vvvo + r1 + (long long)M * r2 + M3 * x;
+            const zc *tp = t2 + p + (long long)v * v * (y + (long long)o * z);
+            for (int d = 0; d < v; ++d) wq = wq + vp[M2 * d] * tp[(long long)v * d];
+            // - sum_l T2(r1, r2, x, l) <l p||y z>    (ovoo(l, p, y, z) at l + M p + M^2 y + M^3 z)
+            const zc *sp = t2 + r1 + (long long)v * (r2 + (long long)v * x);
+            const zc *op = ovoo + (long long)M * p + M2 * y + M3 * z;
+            for (int l = 0; l < o; ++l) wq = wq - sp[(long long)v * v * o * l] * op[l];
+            acc = acc + sgn[q] * wq;
+        }
+        Ssh[e] = acc;
+    }
+    __syncthreads();
+    const zc eabc = g.fd[(o + a) * dg] + g.fd[(o + b) * dg] + g.fd[(o + c) * dg];
+    zc sum{0.0, 0.0};
+    for (int e = threadIdx.x; e < o3; e += NT) {
+        const int x = e % o, y = (e / o) % o, z = e / (o * o);
+        const zc s1 = Ssh[e];
+        const zc wv = s1 + Ssh[z + o * (x + o * y)] + Ssh[y + o * (z + o * x)];
+        zc vv = s1;
+        for (int q = 0; q < 3; ++q) {
+            const int p = trip[q][0], r1 = trip[q][1], r2 = trip[q][2];
+            const zc extra = t1[p + (long long)v * x] * g.vvoo[r1 + M * (r2 + (long long)M * (y + (long long)M * z))] +
+                             g.fvo[p + (long long)M * x] * t2[r1 + (long long)v * (r2 + (long long)v * (y + (long long)o * z))];
+            vv = vv + sgn[q] * extra;
+        }
+        const zc d = (g.fd[x * dg] + g.fd[y * dg] + g.fd[z * dg]) - eabc;
+        sum = sum + divz(wv, d) * conjz(vv);
+    }
+    red[threadIdx.x] = sum;
+    __syncthreads();
+    for (int h = NT / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) g.part[w * g.ntri + t] = red[0];
 }
 
 // r_w = 1 / x_w
@@ -903,21 +969,30 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
     x.one = one;
     // (T) energy (TrunODE 3): the W tensor of a few points at a time, the triples a >= b >= c
     const long long o3v3 = (long long)o * o * o * v * v * v;
-    x.cap = std::max<size_t>((size_t)b * (size_t)(2 * M4 + 64), g.trunode == 3 ? 2 * (size_t)o3v3 + 64 : 0);
+    x.cap = (size_t)b * (size_t)(2 * M4 + 64);
     PHF_TRY(ar.alloc(&x.pool, x.cap));
     const long long ntri = (long long)v * (v + 1) * (v + 2) / 6;
     int nsubT = 0;
     zc *Wtrip = nullptr, *tpart = nullptr;
     int *trid = nullptr;
+    // the W tensor of a point with its GEMM operands (rows (x,b,c) x k = v + o, k x columns (a,y,z))
+    const long long tens_per = o3v3 + ((long long)o * v * v + (long long)v * o * o) * (v + o);
+    const long long by_budget = (long long)(budget / 2) / (tens_per * (long long)sizeof(zc));
+    // W per point in half the workspace: the GEMM path; else, for o <= 18, one o^3 sum per triple in
+    // shared memory
+    const bool fusedT = by_budget < 1 && o <= kTriplesFusedMaxO;
+    zc *Aop = nullptr, *Bop = nullptr;
     if (g.trunode == 3) {
-        const long long by_budget = (long long)(budget / 2) / (o3v3 * (long long)sizeof(zc));
-        const long long by_pool = (long long)(x.cap / 2) / o3v3;
-        nsubT = (int)std::max<long long>(1, std::min<long long>({(long long)b, by_budget, by_pool}));
-        if (by_pool < 1) {
+        if (by_budget < 1 && !fusedT) {
             set_error(PHF_ERR_UNSUPPORTED, "pbarhbarolap: the (T) tensor of one point exceeds the workspace");
             return PHF_ERR_UNSUPPORTED;
         }
-        PHF_TRY(ar.alloc(&Wtrip, (size_t)nsubT * (size_t)o3v3));
+        nsubT = fusedT ? b : (int)std::min<long long>((long long)b, by_budget);
+        if (!fusedT) {
+            PHF_TRY(ar.alloc(&Wtrip, (size_t)nsubT * (size_t)o3v3));
+            PHF_TRY(ar.alloc(&Aop, (size_t)nsubT * (size_t)((long long)o * v * v * (v + o))));
+            PHF_TRY(ar.alloc(&Bop, (size_t)nsubT * (size_t)((long long)v * o * o * (v + o))));
+        }
         PHF_TRY(ar.alloc(&tpart, (size_t)nsubT * (size_t)ntri));
         PHF_TRY(ar.alloc(&trid, 3 * (size_t)ntri));
         std::vector<int> tr;
@@ -1245,20 +1320,51 @@ int pbarhbarolap_run(const PccArgs &g, phf_complex *olap0, phf_complex *olapex1,
                     const int ns = std::min(nsubT, bc - s0);
                     x.npts = ns;
                     const size_t mark = x.used;
-                    TV Wt = tens(Wtrip, {o, o, o, v, v, v});
                     TV W2s = W2v, W1s = W1v;
                     W2s.p += s0 * W2v.ps;
                     W1s.p += s0 * W1v.ps;
-                    // W(x,y,z,a,b,c) = sum_d <bc||dx> T2(a,d,y,z) - sum_l T2(b,c,x,l) <la||yz>   (get_wv :62-63)
-                    PHF_TRY(ein(x, "bcdx,adyz->xyzabc", ONE, Hvvvo_, W2s, ZERO, Wt));
-                    PHF_TRY(ein(x, "bcxl,layz->xyzabc", mkz(-1), W2s, Hovoo, ONE, Wt));
-                    PHF_TRY(check_view(x, Wtrip, o3v3, 1, 1, 0, ns, o3v3, 1, 0, "(T) W"));
                     PHF_TRY(check_view(x, tpart, ntri, 1, 1, 0, ns, ntri, 1, 0, "(T) parts"));
                     PHF_TRY(check_view(x, W2s.p, vvoo, 1, 1, 0, ns, W2v.ps, 1, 0, "(T) T2"));
                     PHF_TRY(check_view(x, W1s.p, vo, 1, 1, 0, ns, W1v.ps, 1, 0, "(T) T1"));
+                    PHF_TRY(check_tv(x, Hvvvo_, 1, "(T) <vv||vo>"));
+                    PHF_TRY(check_tv(x, Hovoo, 1, "(T) <ov||oo>"));
+                    PHF_TRY(check_tv(x, Hvvoo, 1, "(T) <vv||oo>"));
+                    PHF_TRY(check_tv(x, Fvo_s, 1, "(T) F_vo"));
                     TriplesArgs ta{o, v, trid, Wtrip, o3v3, W1s.p, W1v.ps, W2s.p, W2v.ps, Hvvoo.p, Fvo_s.p, F, M, tpart,
                                    ntri};
-                    triples_kernel<<<dim3((unsigned)ntri, (unsigned)ns), NT, 0, st>>>(ta);
+                    if (fusedT) {
+                        const size_t sm = (size_t)o * o * o * sizeof(zc);
+                        PHF_CUDA(cudaFuncSetAttribute(triples_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)sm));
+                        triples_fused_kernel<<<dim3((unsigned)ntri, (unsigned)ns), NT, sm, st>>>(ta, Hvvvo_.p, Hovoo.p);
+                    } else {
+                        // W(x,b,c,a,y,z) = sum_d <bc||dx> T2(a,d,y,z) - sum_l T2(b,c,x,l) <la||yz>  (get_wv :62-63) as
+                        // one GEMM with k = v + o: rows (x,b,c) of A = [<bc||dx> | -T2(b,c,x,l)], columns (a,y,z) of
+                        // B = [T2(a,d,y,z); <la||yz>]
+                        const long long mT = (long long)o * v * v, nT = (long long)v * o * o, kT = (long long)v + o;
+                        TV Ad = tens(Aop, {o, v, v, v}), Al = tens(Aop, {o, v, v, o}), Bd = tens(Bop, {v, v, o, o}),
+                           Bl = tens(Bop, {o, v, o, o});
+                        Ad.ps = Al.ps = mT * kT;
+                        Bd.ps = Bl.ps = kT * nT;
+                        Al.p += mT * v;  // A: column-major m x k, d columns then l columns
+                        Ad.st[3] = Al.st[3] = mT;
+                        Bl.p += v;       // B: column-major k x n, d rows then l rows
+                        Bd.st[0] = Bl.st[0] = 1;
+                        Bd.st[1] = Bl.st[1] = kT;
+                        Bd.st[2] = Bl.st[2] = kT * v;
+                        Bd.st[3] = Bl.st[3] = kT * v * o;
+                        PHF_TRY(ew(x, "bcdx->xbcd", ONE, Hvvvo_, nullptr, ZERO, Ad));
+                        PHF_TRY(ew(x, "bcxl->xbcl", mkz(-1), W2s, nullptr, ZERO, Al));
+                        PHF_TRY(ew(x, "adyz->dayz", ONE, W2s, nullptr, ZERO, Bd));
+                        PHF_TRY(ew(x, "layz->layz", ONE, Hovoo, nullptr, ZERO, Bl));
+                        PHF_TRY(check_view(x, Aop, mT, kT, 1, mT, ns, mT * kT, 1, 0, "(T) A"));
+                        PHF_TRY(check_view(x, Bop, kT, nT, 1, kT, ns, kT * nT, 1, 0, "(T) B"));
+                        PHF_TRY(check_view(x, Wtrip, mT, nT, 1, mT, ns, o3v3, 1, 0, "(T) W"));
+                        PHF_TRY(zgemm_strided((int)mT, (int)nT, (int)kT, ns, 1, ONE, View{Aop, 1, mT, mT * kT},
+                                              View{Bop, 1, kT, kT * nT}, ZERO, OutView{Wtrip, 1, mT, o3v3}, nullptr, st));
+                        g_pcc_flops += 8.0 * (double)mT * (double)nT * (double)kT * ns;
+                        triples_kernel<<<dim3((unsigned)ntri, (unsigned)ns), NT, 0, st>>>(ta);
+                    }
                     ++g_launches;
                     PHF_CHECK_LAUNCH();
                     TV pv;

@@ -85,15 +85,21 @@ def test_pbarhbarolap_with_triples_matches_oracle(case):
 
 
 def test_triples_split_over_sub_batches():
-    """The (T) tensor (o^3 v^3 per point) is formed a few points at a time: at M = 12, o = 4 it is larger
-    than the per-point scratch, so the 24 points of a chunk run in two sub-batches; a one-point workspace
-    runs one point per chunk."""
+    """With (T): the default workspace runs the W-tensor GEMM path; a 64 KiB workspace (one grid point per
+    chunk, no room for W) runs the fused shared-memory kernel.  Both give the oracle's sums."""
     p = _problem(6, 4, (6, 4), seed=12)
     p["TrunODE"] = 3
     whole = _gpu(p)
     _compare(whole, pcc.pbarhbarolap(**p))
     small = _gpu(p, workspace=1 << 16)
     _compare(small, whole, tol=1e-12)
+
+
+def test_triples_tensor_path_large_occupied_space():
+    """o = 20, above the fused (T) kernel's o <= 18: the W-tensor GEMM path at the configuration-1 size."""
+    p = _problem(20, 20, (6, 1), seed=13)
+    p["TrunODE"] = 3
+    _compare(_gpu(p), pcc.pbarhbarolap(**p))
 
 
 def test_chunked_grid_equals_one_chunk():

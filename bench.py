@@ -526,6 +526,44 @@ def run_ours(args):
     plan.close()
     torch.cuda.empty_cache()
 
+    # (measured right after the device timing, so that both run under the same thermal and power state;
+    # the FP64 comparison runs below heat the GPU, which then clocks lower under the power cap)
+    # end to end with host buffers: (1) the plan API an optimiser loop uses (Hamiltonian set up once;
+    # per call: Z host -> device, the grid pass, Hmat/Smat/Gradmat/Rdmmat device -> host, and the
+    # energy and LocalG gradient); (2) the one-shot drop-in call, which also rebuilds the
+    # Hamiltonian-side plan every call.  Ref is the unitary whose first N columns are the benchmark's
+    # determinant, so Z = 0 is the same state as `value`'s (the energies are reported side by side).
+    e2e_vals, e2e_once = [], []
+    h2d = d2h = h2d_once = 0
+    e2e_energy = None
+    e2e_steps = args.steps if args.e2e_steps is None else args.e2e_steps
+    if e2e_steps > 0:
+        z0 = np.zeros((p.M - p.N, p.N), dtype=np.complex128)
+        planh = api.Plan(ref=Ref, h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
+                         autotune=tune, **kw)
+        for i in range(1 + e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = planh.buildhsg(z0, check_hermitian=False)
+            e2e_energy, _ = block_energy_gradient(p, *out, api.localg)
+            t1 = time.perf_counter()
+            if i > 0:
+                e2e_vals.append(p.grid.npoints / (t1 - t0))
+        planh.close()
+        torch.cuda.empty_cache()
+        # per call the plan uploads newMO and its conjugate (the AO vectors are formed on the device)
+        h2d = 2 * p.M * p.N * 16
+        d2h = sum(x.nbytes for x in out)
+        for i in range(1 + min(e2e_steps, 2)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = api.buildhsg_chol(p.h, p.B, Ref, z0, precision=args.precision, check_hermitian=False, **kw)
+            t1 = time.perf_counter()
+            if i > 0:
+                e2e_once.append(p.grid.npoints / (t1 - t0))
+        torch.cuda.empty_cache()
+        h2d_once = (p.h.nbytes + p.B.nbytes + Ref.nbytes + z0.nbytes + kw["r1"].nbytes + kw["r2"].nbytes +
+                    kw["rpg"].nbytes + kw["weightsp"].nbytes + kw["weightpg"].nbytes)
     # the plain FP64 forms on the same problem (comparison and error reference): the exchange-matrix
     # form of the benchmark workload (stored for n <= 128, streamed above) with this library's FP64
     # GEMM kernels and with cuBLAS DGEMM for the exchange products; the speed-up is judged against the
@@ -585,42 +623,6 @@ def run_ours(args):
             r["meets_1e-7_grad"] = r["max_abs_dgrad_vs_fp64"] <= 1e-7
             r["tc_tops"] = tc_ops_per_step(p, prec, slices, form, chunks) / (r["jk_ms_per_step"] * 1e-3) / 1e12
 
-    # end to end with host buffers: (1) the plan API an optimiser loop uses (Hamiltonian set up once;
-    # per call: Z host -> device, the grid pass, Hmat/Smat/Gradmat/Rdmmat device -> host, and the
-    # energy and LocalG gradient); (2) the one-shot drop-in call, which also rebuilds the
-    # Hamiltonian-side plan every call.  Ref is the unitary whose first N columns are the benchmark's
-    # determinant, so Z = 0 is the same state as `value`'s (the energies are reported side by side).
-    e2e_vals, e2e_once = [], []
-    h2d = d2h = h2d_once = 0
-    e2e_energy = None
-    e2e_steps = args.steps if args.e2e_steps is None else args.e2e_steps
-    if e2e_steps > 0:
-        z0 = np.zeros((p.M - p.N, p.N), dtype=np.complex128)
-        planh = api.Plan(ref=Ref, h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
-                         autotune=tune, **kw)
-        for i in range(1 + e2e_steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            out = planh.buildhsg(z0, check_hermitian=False)
-            e2e_energy, _ = block_energy_gradient(p, *out, api.localg)
-            t1 = time.perf_counter()
-            if i > 0:
-                e2e_vals.append(p.grid.npoints / (t1 - t0))
-        planh.close()
-        torch.cuda.empty_cache()
-        # per call the plan uploads newMO and its conjugate (the AO vectors are formed on the device)
-        h2d = 2 * p.M * p.N * 16
-        d2h = sum(x.nbytes for x in out)
-        for i in range(1 + min(e2e_steps, 2)):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            out = api.buildhsg_chol(p.h, p.B, Ref, z0, precision=args.precision, check_hermitian=False, **kw)
-            t1 = time.perf_counter()
-            if i > 0:
-                e2e_once.append(p.grid.npoints / (t1 - t0))
-        torch.cuda.empty_cache()
-        h2d_once = (p.h.nbytes + p.B.nbytes + Ref.nbytes + z0.nbytes + kw["r1"].nbytes + kw["r2"].nbytes +
-                    kw["rpg"].nbytes + kw["weightsp"].nbytes + kw["weightpg"].nbytes)
     e2e_val = statistics.median(e2e_vals) * world if e2e_vals else None
     e2e_once_val = statistics.median(e2e_once) * world if e2e_once else None
 

@@ -263,14 +263,14 @@ def quoted_flops_per_point(p):
 TRAFFIC = {
     ("c2", "ozaki_i8"): (2.412e9 + 0.820e9,
                          "DRAM read + write of the K launch (4096 x 25600 x 4096, the whole 3200-point chunk, wide "
-                         "MMA issue) from an ncu capture (profiles/ozaki_i8_gemm_c2.md); algorithmic bytes of that "
+                         "MMA issue) from an ncu capture of this workload; algorithmic bytes of that "
                          "launch: A slices 84 MB + B slices 524 MB + FP64 output 839 MB = 1.45e9"),
     ("c5", "ozaki_i8"): (81.5e9,
                          "DRAM read + write of one exchange-panel GEMM of the benchmark's panels (7800 x 25600 x "
                          "40000, 39 index rows i, two k passes), scaled by the columns (points) from an ncu capture "
-                         "of the same panel on a 384-point grid (9.78 GB for 7800 x 3072 x 40000; "
-                         "profiles/ozaki_i8_gemm_c5_panel.md); algorithmic bytes of the full launch: A slices 1.56 GB "
-                         "+ B slices 5.12 GB + FP64 output 1.60 GB = 8.3e9"),
+                         "of the same panel on a 384-point grid (9.78 GB for 7800 x 3072 x 40000); algorithmic "
+                         "bytes of the full launch: A slices 1.56 GB + B slices 5.12 GB + FP64 output 1.60 GB "
+                         "= 8.3e9"),
 }
 
 

@@ -213,23 +213,68 @@ def jk_form_of(p):
     return "eri" if p.n <= 128 else "streamed"
 
 
-def jk_flops_per_point(p, form):
+def sym_active(p, form, precision, sym="auto"):
+    """Whether the library runs the streamed form with the exchange symmetry (pairs i <= k against the
+    symmetric half of each density, i < k against the antisymmetric half): on by default in FP64 and,
+    for n > 64, in the tensor-core precisions."""
+    return form == "streamed" and sym != "off" and (precision == "fp64" or p.n > 64)
+
+
+def choose_ipanel(n):
+    """Spatial indices per exchange panel of the streamed form, as the library chooses them: at most
+    8192 exchange rows, fewest 128-row padded rows over all panels, ties to the larger panel."""
+    best, best_rows = 1, -1
+    for I in range(1, n + 1):
+        if I * n > max(8192, n):
+            break
+        rows = (n // I) * (-(-I * n // 128) * 128) + ((-(-(n % I) * n // 128) * 128) if n % I else 0)
+        if best_rows < 0 or rows <= best_rows:
+            best, best_rows = I, rows
+    return best
+
+
+def sym_panels(n, ipanel=0):
+    """Panels (i0, indices) of the symmetric form: a panel starting at i0 takes max(1, ipanel n / (n - i0))
+    indices, so that its Gram block (indices x n rows, (n - i0) n columns) stays within ipanel n x n^2."""
+    budget = (ipanel or choose_ipanel(n)) * n
+    out, i0 = [], 0
+    while i0 < n:
+        ip = max(1, min(n - i0, budget // (n - i0)))
+        out.append((i0, ip))
+        i0 += ip
+    return out
+
+
+def jk_flops_per_point(p, form, sym=False, precision="ozaki_i8"):
     """Algorithmic real flops of the exchange/Coulomb contraction per grid point.
 
     eri / streamed:  K = EK (n^2 x n^2, real) times 4 complex density columns: 16 n^4, and the
                      Coulomb term d = B vec P, J = B^T d: 8 L n^2 (the streamed form also
                      regenerates EK once per chunk: jk_regen_flops, counted as executed work)
+    streamed with the exchange symmetry: the pair rows times 8 real columns, 16 (p_le^2 + p_lt^2) with
+                     p_le = n(n+1)/2 and p_lt = n(n-1)/2 (about 8 n^4); in the tensor-core forms the
+                     Coulomb d runs over the pairs too: 4 L (p_le + n^2)
     factorized form: T = V^H X (8 L N^2 M), Q = X T' (8 L N^2 M), GX = sum_L B_L Q_L (8 L n^2 N)"""
     n, N, M, L = p.n, p.N, p.M, p.L
+    if form == "streamed" and sym:
+        ple, plt = n * (n + 1) / 2, n * (n - 1) / 2
+        coul = 8.0 * L * n * n if precision == "fp64" else 4.0 * L * (ple + n * n)
+        return 16.0 * (ple * ple + plt * plt) + coul
     if form in ("eri", "streamed"):
         return 16.0 * n ** 4 + 8.0 * L * n * n
     return 8.0 * L * N * N * M * 2 + 8.0 * L * n * n * N
 
 
-def jk_regen_flops(p, form, chunks):
+def jk_regen_flops(p, form, chunks, sym=False, ipanel=0):
     """Flops of the streamed form's exchange-row regeneration per evaluation: the Gram products
-    B^T B (n^2 x n^2, k = L) once per chunk."""
-    return 2.0 * p.n ** 4 * p.L * chunks if form == "streamed" else 0.0
+    B^T B (n^2 x n^2, k = L) once per chunk; with the exchange symmetry each panel's Gram block keeps
+    only the columns k >= i0 (panel indices x n rows, (n - i0) n columns)."""
+    if form != "streamed":
+        return 0.0
+    if sym:
+        n = p.n
+        return 2.0 * p.L * chunks * sum(ip * n * (n - i0) * n for i0, ip in sym_panels(n, ipanel))
+    return 2.0 * p.n ** 4 * p.L * chunks
 
 
 def tc_reps(precision, slices):
@@ -240,10 +285,10 @@ def tc_reps(precision, slices):
     return 3.0 if precision == "bf16x3" else 1.0
 
 
-def tc_ops_per_step(p, precision, slices, form, chunks):
+def tc_ops_per_step(p, precision, slices, form, chunks, sym=False, ipanel=0):
     """Executed tensor-core operations of the J/K contraction per evaluation (2 per multiply-add)."""
-    return tc_reps(precision, slices) * (jk_flops_per_point(p, form) * p.grid.npoints +
-                                         jk_regen_flops(p, form, chunks))
+    return tc_reps(precision, slices) * (jk_flops_per_point(p, form, sym, precision) * p.grid.npoints +
+                                         jk_regen_flops(p, form, chunks, sym, ipanel))
 
 
 def tc_ops_per_point(p, precision, slices):
@@ -512,8 +557,10 @@ def run_ours(args):
     slices = args.slices or 5
 
     tune = not args.no_autotune
+    xs = {"auto": "auto", "on": True, "off": False}[args.exchange_symmetry]
+    sym = sym_active(p, form, args.precision, args.exchange_symmetry)
     plan = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
-                    autotune=tune, exchange_panel=args.exchange_panel, **kw)
+                    autotune=tune, exchange_panel=args.exchange_panel, exchange_symmetry=xs, **kw)
     clk = clock_sampler(local)
     step_ms, E, G, launches, prof = time_plan(torch, plan, C, stream, args.steps, args.warmup, flush, _lib, clk)
     t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
@@ -540,7 +587,7 @@ def run_ours(args):
     if e2e_steps > 0:
         z0 = np.zeros((p.M - p.N, p.N), dtype=np.complex128)
         planh = api.Plan(ref=Ref, h=p.h, B=p.B, precision=args.precision, slices=args.slices, jk_form=form,
-                         autotune=tune, **kw)
+                         autotune=tune, exchange_panel=args.exchange_panel, exchange_symmetry=xs, **kw)
         for i in range(1 + e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -579,7 +626,8 @@ def run_ours(args):
             forms.append(("factorized", False, "factorized"))
         for label, lib_gemm, jf in forms:
             plan64 = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="fp64", fp64_library_gemm=lib_gemm,
-                              jk_form=jf, autotune=tune, **kw)
+                              jk_form=jf, autotune=tune, exchange_panel=args.exchange_panel, exchange_symmetry=xs,
+                              **kw)
             n64 = 1 if jf == "factorized" else max(1, min(args.steps, 3))
             ms64, E64, G64, _, prof64 = time_plan(torch, plan64, C, stream, n64, 1, flush, _lib)
             plan64.close()
@@ -609,7 +657,8 @@ def run_ours(args):
         for prec in ("ozaki_i8", "bf16x3", "tf32"):
             if prec == args.precision:
                 continue
-            plan_s = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, slices=args.slices, jk_form=form, **kw)
+            plan_s = api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, slices=args.slices, jk_form=form,
+                              exchange_panel=args.exchange_panel, exchange_symmetry=xs, **kw)
             ms_s, E_s, G_s, _, prof_s = time_plan(torch, plan_s, C, stream, max(1, min(args.steps, 3)), 2, flush,
                                                   _lib)
             plan_s.close()
@@ -621,7 +670,8 @@ def run_ours(args):
         for prec, r in study.items():
             r["meets_1e-8_Eh"] = r["abs_dE_vs_fp64"] <= 1e-8
             r["meets_1e-7_grad"] = r["max_abs_dgrad_vs_fp64"] <= 1e-7
-            r["tc_tops"] = tc_ops_per_step(p, prec, slices, form, chunks) / (r["jk_ms_per_step"] * 1e-3) / 1e12
+            r["tc_tops"] = tc_ops_per_step(p, prec, slices, form, chunks, sym_active(p, form, prec, args.exchange_symmetry),
+                                           args.exchange_panel) / (r["jk_ms_per_step"] * 1e-3) / 1e12
 
     e2e_val = statistics.median(e2e_vals) * world if e2e_vals else None
     e2e_once_val = statistics.median(e2e_once) * world if e2e_once else None
@@ -630,10 +680,11 @@ def run_ours(args):
         peaks = _peaks()
         jk_ms, jk_n = prof[0]
         all_ms = sum(v[0] for v in prof.values())
-        alg = jk_flops_per_point(p, form)
+        alg = jk_flops_per_point(p, form, sym, args.precision)
+        regen = jk_regen_flops(p, form, chunks, sym, args.exchange_panel)
         fp64_peak = measure_fp64_peak(torch, dev)
         if args.precision == "fp64":
-            achieved = (alg * p.grid.npoints + jk_regen_flops(p, form, chunks)) * args.steps / (jk_ms * 1e-3) / 1e12
+            achieved = (alg * p.grid.npoints + regen) * args.steps / (jk_ms * 1e-3) / 1e12
             roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                     "frac": achieved / fp64_peak, "traffic": None,
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
@@ -644,7 +695,8 @@ def run_ours(args):
             peak = 2.0 * bf16 if bf16 else i8
             if args.precision != "ozaki_i8":  # dense bf16 rate; TF32 runs at half of it
                 peak = bf16 * (0.5 if args.precision == "tf32" else 1.0) if bf16 else None
-            achieved = tc_ops_per_step(p, args.precision, slices, form, chunks) * args.steps / (jk_ms * 1e-3) / 1e12
+            achieved = (tc_ops_per_step(p, args.precision, slices, form, chunks, sym, args.exchange_panel) * args.steps
+                        / (jk_ms * 1e-3) / 1e12)
             unit = {"ozaki_i8": "TOP/s (int8)", "bf16x3": "TFLOP/s (bf16)", "tf32": "TFLOP/s (tf32)"}[args.precision]
             traffic = TRAFFIC.get((args.config, args.precision))
             roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
@@ -660,14 +712,15 @@ def run_ours(args):
                     "bf16_tflops_measured": bf16,
                     "kernel": "ozaki_i8_gemm_kernel (tcgen05 kind::%s, exchange, exchange-row regeneration and "
                               "Coulomb GEMMs)" % {"ozaki_i8": "i8", "bf16x3": "f16 (bf16)", "tf32": "tf32"}[args.precision],
-                    "fp64_equivalent_tflops": (alg * p.grid.npoints + jk_regen_flops(p, form, chunks)) * args.steps
+                    "fp64_equivalent_tflops": (alg * p.grid.npoints + regen) * args.steps
                                               / (jk_ms * 1e-3) / 1e12,
                     "fp64_dgemm_peak_tflops": fp64_peak}
         roof.update({"jk_form": form, "jk_launches": jk_n, "jk_ms_per_step": jk_ms / args.steps,
                      "jk_share_of_device_time": jk_ms / all_ms if all_ms else None,
                      "device_ms_by_class": {k: v[0] / args.steps for k, v in
                                             zip(("jk", "other_gemm", "overlap_inverse", "memory"), prof.values())},
-                     "alg_flops_per_point": alg, "regen_flops_per_step": jk_regen_flops(p, form, chunks),
+                     "exchange_symmetry": sym,
+                     "alg_flops_per_point": alg, "regen_flops_per_step": regen,
                      "quoted_flops_per_point": quoted_flops_per_point(p)})
         cpu = None
         parity = None
@@ -677,9 +730,11 @@ def run_ours(args):
             cpu = {"value": v, "unit": UNIT, "cores": nth, "cpu_model": cpu_model(), "kind": "port",
                    "sample": desc + "; rate scaled to the full grid (per-point work is independent)"}
             pk = dict(h=p.h, B=p.B, **kw)
-            plist = [(args.precision, dict(pk, precision=args.precision, slices=args.slices, jk_form=form))]
+            xk = dict(exchange_panel=args.exchange_panel, exchange_symmetry=xs)
+            plist = [(args.precision, dict(pk, precision=args.precision, slices=args.slices, jk_form=form, **xk))]
             if args.precision != "fp64":
-                plist.append(("fp64_cublas_exchange", dict(pk, precision="fp64", jk_form=form, fp64_library_gemm=True)))
+                plist.append(("fp64_cublas_exchange", dict(pk, precision="fp64", jk_form=form, fp64_library_gemm=True,
+                                                           **xk)))
             parity = oracle_parity(p, setup[0], block, ora, plist)
             parity["oracle"] = setup[1]
             del setup
@@ -690,6 +745,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded h, B_L, determinant)",
                 "config": {"workload": workload_name(p), "precision": args.precision, "jk_form": form,
+                           "exchange_symmetry": sym,
                            "points_per_step": p.grid.npoints, "chunk": chunk, "autotune": tune,
                            "l2": "flushed (256 MB write) between timed steps",
                            "parallelism": f"{world} independent instance(s), one per GPU"},
@@ -1080,6 +1136,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--ngrid", type=lambda t: [int(v) for v in t.split(",")], default=None,
                     help="Lebedev,gamma points replacing the configuration's grid (profiling on a smaller grid)")
+    ap.add_argument("--exchange-symmetry", choices=("auto", "on", "off"), default="auto",
+                    help="streamed form: run the exchange over index pairs with the symmetric and antisymmetric "
+                         "density halves (auto: wherever the library offers it), or over the full rows (off)")
     ap.add_argument("--exchange-panel", type=int, default=0,
                     help="streamed form: spatial indices per exchange panel (0 = the plan's choice)")
     ap.add_argument("--trunode", type=int, default=1, choices=[1, 2, 3],

@@ -182,12 +182,22 @@ typedef struct {
                                                  (the rank split of PHFTools.f90:53-57) */
     int exchange_panel;                       /* jk_form 3: spatial indices i per exchange panel (rows (i, k)
                                                  of the exchange matrix formed at once); 0 = automatic
-                                                 (at most 4096 rows, fewest padded rows) */
+                                                 (at most 8192 rows, fewest padded rows).  With the
+                                                 exchange symmetry, a panel starting at i0 takes
+                                                 max(1, exchange_panel n / (n - i0)) indices, so that each
+                                                 panel's Gram block stays within exchange_panel n x n^2 */
     int autotune;                             /* 1: at the plan's first evaluation, time the candidate launch
                                                  choices of every GEMM shape the plan uses (FP64 GEMM tile
                                                  shape, int8 GEMM raster group) and keep the fastest; the table
                                                  is shared by all plans of the process.  Results are bitwise
                                                  those of the untuned plan */
+    int exchange_symmetry;                    /* jk_form 3: 0 = automatic (on where available), 1 = on, 2 = off.
+                                                 On: the exchange uses K(rho^T) = K(rho)^T of real integrals --
+                                                 rows (i <= k) against the symmetric half of each density and
+                                                 rows (i < k) against the antisymmetric half, half the exchange
+                                                 GEMM's work and of its rows' regeneration; the FP64 form and the
+                                                 tensor-core forms with n > 64 (n <= 64 tensor-core plans slice
+                                                 the densities in the fused kernel and run the full rows) */
 } phf_plan_desc;
 
 int phf_plan_create(const phf_plan_desc *desc, phf_plan **plan);

@@ -48,6 +48,7 @@ class phf_plan_desc(ctypes.Structure):
         ("point_end", ctypes.c_int),
         ("exchange_panel", ctypes.c_int),
         ("autotune", ctypes.c_int),
+        ("exchange_symmetry", ctypes.c_int),
     ]
 
 

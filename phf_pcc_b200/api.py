@@ -245,12 +245,17 @@ class Plan:
     J/K, FP64 only); "auto" takes "eri" up to n = 128 and "streamed" above.  ``gradient``:
     "reference" (the reference's bra-side gradient, LocalG) or "exact" (dE/dC* including the
     ket-side term; used by autograd).  ``autotune``: time the launch choices of the plan's GEMM shapes
-    at its first evaluation (bitwise the same results)."""
+    at its first evaluation (bitwise the same results).  ``exchange_symmetry`` (streamed form):
+    "auto" (on where available), True or False -- with it the exchange runs over index pairs i <= k
+    against the symmetric half of each density and i < k against the antisymmetric half (K(rho^T) =
+    K(rho)^T for real integrals): half the exchange GEMM's work.  Available in FP64 and, for n > 64,
+    in the tensor-core precisions."""
 
     def __init__(self, *, ref, ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb,
                  rooty, qj, sp, h=None, B=None, hone=None, htwo=None, precision="fp64", slices=0,
                  workspace_bytes=0, jk_form="auto", gradient="reference", fp64_library_gemm=False,
-                 point_range=None, npg=None, ncipg=None, nso=None, exchange_panel=0, autotune=False):
+                 point_range=None, npg=None, ncipg=None, nso=None, exchange_panel=0, autotune=False,
+                 exchange_symmetry="auto"):
         self._g = _Grid(ngrid, nci, cmplxconj, ncisp, nocc, r1, r2, rpg, weightsp, weightpg, roota, rootb, rooty, qj,
                         sp, npg, ncipg, nso)
         g = self._g
@@ -275,6 +280,10 @@ class Plan:
         d.jk_form = {"auto": 0, "eri": 1, "factorized": 2, "streamed": 3}[jk_form]
         d.exchange_panel = int(exchange_panel)
         d.autotune = 1 if autotune else 0
+        if exchange_symmetry == "auto" or exchange_symmetry is None:
+            d.exchange_symmetry = 0
+        else:
+            d.exchange_symmetry = 1 if exchange_symmetry else 2
         self.jk_form = jk_form
         d.gradient_mode = {"reference": 0, "exact": 1}[gradient]
         d.fp64_library_gemm = 1 if fp64_library_gemm else 0

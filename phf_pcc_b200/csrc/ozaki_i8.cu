@@ -244,7 +244,10 @@ struct OzArgs {
     int kseg;            // floating-point formats: k-blocks per FP32 accumulation segment (>= 1)
     int gamma_n;         // > 0: exchange-to-Gamma output (see store_row_chunk), n spatial orbitals
     int g_row0;          // exchange-to-Gamma output: global row of output row 0 (a panel of the exchange rows)
+    int gamma_mode;      // exchange-to-Gamma rows: 0 full (i n + k), 1 symmetric pairs, 2 antisymmetric pairs
+    const int *g_pairs;  // modes 1, 2: pair (i, k) of global row g packed as i << 16 | k
     int a_row0;          // A tiles are read from row a_row0 + m0 of the A slice buffer (a row range of it)
+    int b_row0;          // B tiles are read from row b_row0 + n0 of the B slice buffer
     int group_m;         // row tiles per column sweep of the raster
     int *err;
 };
@@ -252,27 +255,54 @@ struct OzArgs {
 // Stores one epilogue thread's 32 consecutive columns col0 .. col0 + 31 of output row `row` (values
 // acc * rowscale * cs): element (row, col) at D[row ldd + col], or D[col ldd + row] when args.trans,
 // added to what is there when `add`.  Exchange-to-Gamma mode (args.gamma_n = n > 0): the product is
-// K^T of the exchange GEMM, row = i n + k, col = (4 w + 2 sigma + tau) 2 + part, and -K goes
-// straight into the complex M x M matrix Gamma_w (D = Gamma as doubles) at [2i + sigma][2k + tau];
-// the Coulomb term is added to the diagonal spin blocks afterwards.
+// K^T of the exchange GEMM, col = (4 w + 2 sigma + tau) 2 + part, and -K goes straight into the
+// complex M x M matrix Gamma_w (D = Gamma as doubles); the Coulomb term is added to the diagonal spin
+// blocks afterwards.  Rows by args.gamma_mode (g = args.g_row0 + row):
+//   0: g = i n + k, -K_{sigma tau}[i][k] at [2i + sigma][2k + tau];
+//   1: pair (i, k), i <= k, of g_pairs[g]: the symmetric-density part KS of K[i][k] and K[k][i]
+//      (equal), -KS stored at [2i + sigma][2k + tau] and at [2k + sigma][2i + tau];
+//   2: pair (i, k), i < k: the antisymmetric-density part KA (K[i][k] = KS + KA, K[k][i] = KS - KA),
+//      -KA added at [2i + sigma][2k + tau] and +KA at [2k + sigma][2i + tau] (after mode 1's stores).
 __device__ __forceinline__ void store_row_chunk(const OzArgs &args, double *Dz, int row, int col0,
                                                 const double (&acc)[32], double rowscale, const double *cs,
                                                 bool add) {
     if (args.gamma_n > 0) {
-        const int gn = args.gamma_n, M = 2 * gn, grow = args.g_row0 + row, i = grow / gn, k = grow - i * gn;
+        const int gn = args.gamma_n, M = 2 * gn, grow = args.g_row0 + row;
+        int i, k;
+        if (args.gamma_mode == 0) {
+            i = grow / gn;
+            k = grow - i * gn;
+        } else {
+            const int pr = __ldg(args.g_pairs + grow);
+            i = pr >> 16;
+            k = pr & 0xffff;
+        }
+        const bool mirror = args.gamma_mode != 0 && i != k;
+        const bool acc_both = add || args.gamma_mode == 2;
 #pragma unroll
         for (int j = 0; j < 32; j += 2) {
             const int col = col0 + j;
             if (col < args.n) {
                 const int w = col >> 3, sg = (col >> 2) & 1, tu = (col >> 1) & 1;
                 double2 *g = reinterpret_cast<double2 *>(Dz) + ((long long)w * M + 2 * i + sg) * M + 2 * k + tu;
-                double2 v = make_double2(-(acc[j] * rowscale * cs[j]), -(acc[j + 1] * rowscale * cs[j + 1]));
-                if (add) {
+                const double2 u = make_double2(acc[j] * rowscale * cs[j], acc[j + 1] * rowscale * cs[j + 1]);
+                double2 v = make_double2(-u.x, -u.y);
+                if (acc_both) {
                     const double2 o = *g;
                     v.x = o.x + v.x;
                     v.y = o.y + v.y;
                 }
                 *g = v;
+                if (mirror) {
+                    double2 *h = reinterpret_cast<double2 *>(Dz) + ((long long)w * M + 2 * k + sg) * M + 2 * i + tu;
+                    double2 t = args.gamma_mode == 2 ? u : make_double2(-u.x, -u.y);
+                    if (acc_both) {
+                        const double2 o = *h;
+                        t.x = o.x + t.x;
+                        t.y = o.y + t.y;
+                    }
+                    *h = t;
+                }
             }
         }
         return;
@@ -585,6 +615,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         n0 = ((L % width) / gm) * BN;
     }
     const int am0 = m0 + args.a_row0;           // first row of the A tile in the A slice buffer
+    const int bn0 = n0 + args.b_row0;           // first row of the B tile in the B slice buffer
     const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
     const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
     double *const Dz = args.D + (long long)blockIdx.z * args.dz;
@@ -642,9 +673,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
 #pragma unroll
                 for (int u = 0; u < U0; ++u)  // slice u + 1 of B: 32 bytes of each 128-byte k-block row
-                    tma_load_2d(&tmBw, &full_bar[sg], bdst + u * BN * 32, kbg * 128 + u * 32, n0);
+                    tma_load_2d(&tmBw, &full_bar[sg], bdst + u * BN * 32, kbg * 128 + u * 32, bn0);
                 if constexpr (W1 == 1) {
-                    tma_load_2d(&tmB1, &full_bar[sg], bdst + OZ_GP * BN * 32, kbg * 32, n0);
+                    tma_load_2d(&tmB1, &full_bar[sg], bdst + OZ_GP * BN * 32, kbg * 32, bn0);
                     tma_load_2d(&tmA1, &full_bar[sg], dst + oz_wide_a1_off(S), kbg * 32, am0);
                 }
                 if (++sg == NS) {
@@ -668,10 +699,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 unsigned char *dst = smem + (size_t)sg * PITCH;
                 mbar_arrive_expect_tx(&full_bar[sg], BYTES);
                 tma_load_2d(&tmA0, &full_bar[sg], dst, kbg * 128, am0);
-                tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, n0);
+                tma_load_2d(&tmB0, &full_bar[sg], dst + OZ_BM * 128, kbg * 128, bn0);
                 if constexpr (W1 == 1) {
                     tma_load_2d(&tmA1, &full_bar[sg], dst + (OZ_BM + BN) * 128, kbg * 32, am0);
-                    tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, n0);
+                    tma_load_2d(&tmB1, &full_bar[sg], dst + (OZ_BM + BN) * 128 + OZ_BM * 32, kbg * 32, bn0);
                 }
                 if (++sg == NS) {
                     sg = 0;
@@ -700,14 +731,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         if (j == 0) {
                             tma_load_2d(&tmA0, &full_bar[u], dst, kbg * 128, am0);
                         } else if (j == 1) {
-                            tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, n0);
+                            tma_load_2d(&tmB0, &full_bar[u], dst, kbg * 128, bn0);
                         } else if (W1 <= 2) {  // j == 2: A and B of group 1 at 32- or 64-byte rows
                             tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 32 * W1, am0);
-                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 32 * W1, kbg * 32 * W1, n0);
+                            tma_load_2d(&tmB1, &full_bar[u], dst + OZ_BM * 32 * W1, kbg * 32 * W1, bn0);
                         } else if (j == 2) {
                             tma_load_2d(&tmA1, &full_bar[u], dst, kbg * 128, am0);
                         } else {
-                            tma_load_2d(&tmB1, &full_bar[u], dst, kbg * 128, n0);
+                            tma_load_2d(&tmB1, &full_bar[u], dst, kbg * 128, bn0);
                         }
                         if (++u == OZ_UNITS) {
                             u = 0;
@@ -1164,6 +1195,230 @@ __global__ void __launch_bounds__(SL_NT) slice_ek_panel_kernel(int n, const doub
     }
 }
 
+// Symmetric exchange form.  For real integrals K(rho^T) = K(rho)^T, so with rho = rho_s + rho_a (its
+// symmetric and antisymmetric halves) and the pairs (i <= k), resp. (i < k), of the index pairs:
+//   K[i][k] = KS(i, k) + KA(i, k),  K[k][i] = KS(i, k) - KA(i, k),
+//   KS(i, k) = sum_{l <= j} EKS[(i, k)][(l, j)] rho_s[l][j],  EKS = (il|kj) + (ij|kl) (l < j), (il|kl) (l = j),
+//   KA(i, k) = sum_{l < j}  EKA[(i, k)][(l, j)] rho_a[l][j],  EKA = (il|kj) - (ij|kl),
+// half the rows and half the contraction length of the full exchange matrix (KA(i, i) = 0).  Pairs are
+// numbered in row order: pair_le(l, j) = l n - l (l - 1) / 2 + (j - l), pair_lt(l, j) = l (n - 1) - l (l - 1) / 2
+// + (j - l - 1); the same numbering indexes the exchange rows and the contraction (k) elements.
+__host__ __device__ __forceinline__ long long pair_le(long long n, long long l, long long j) {
+    return l * n - l * (l - 1) / 2 + (j - l);
+}
+__host__ __device__ __forceinline__ long long pair_lt(long long n, long long l, long long j) {
+    return l * (n - 1) - l * (l - 1) / 2 + (j - l - 1);
+}
+
+// Symmetric and antisymmetric exchange rows of one panel from its Gram block: pair (i, k), i <= k, of
+// symmetric panel row r = pairs[t0 + r] (t0 = pair_le(i0, i0)) reads the n x n block
+// B[l][j] = G[(i - i0) n + l][(k - k0) n + j] = (il|kj) (row stride ldg) and writes symmetric row r
+// (EKS at k-index pair_le(l, j)) and, when i < k, antisymmetric row ra = r - (i - i0) - 1 (EKA at
+// pair_lt(l, j); the panel's diagonal pairs precede it).  The block goes through shared memory as the
+// 32 x 32 tile pairs B[lt][jt], B[jt][lt] (lt <= jt), so that B[l][j] and B[j][l] are both read in
+// coalesced rows, twice: row maxima, then slices.  Exponents e_s[r], e_a[ra].
+constexpr int EKS_TP = 33;  // tile pitch (doubles): row and column reads of a warp hit distinct banks
+__global__ void __launch_bounds__(SL_NT) slice_ek_sym_panel_kernel(int n, int i0, int k0, const int *__restrict__ pairs,
+                                                                   long long t0, const double *__restrict__ G,
+                                                                   long long ldg, int S, long long rows_pad_s,
+                                                                   long long kpad_s, signed char *out_s, int *e_s,
+                                                                   long long rows_pad_a, long long kpad_a,
+                                                                   signed char *out_a, int *e_a) {
+    __shared__ double T1[32 * EKS_TP], T2[32 * EKS_TP];
+    __shared__ double sh[SL_NT];
+    const long long r = blockIdx.x;
+    const int pr = __ldg(pairs + t0 + r), i = pr >> 16, k = pr & 0xffff;
+    const bool anti = i < k;
+    const long long ra = r - (i - i0) - 1;
+    const double *g = G + (long long)(i - i0) * n * ldg + (long long)(k - k0) * n;
+    const int nt = (n + 31) / 32, lane = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const long long kks = (long long)n * (n + 1) / 2, kka = (long long)n * (n - 1) / 2;
+    double mxs = 0.0, mxa = 0.0;
+    SliceScale scs = slice_scale(0, S), sca = slice_scale(0, S);
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int lt = 0; lt < nt; ++lt) {
+            for (int jt = lt; jt < nt; ++jt) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int a = ty + 8 * q;
+                    const int l1 = lt * 32 + a, j1 = jt * 32 + lane;
+                    T1[a * EKS_TP + lane] = (l1 < n && j1 < n) ? g[(long long)l1 * ldg + j1] : 0.0;
+                    if (jt != lt) {
+                        const int l2 = jt * 32 + a, j2 = lt * 32 + lane;
+                        T2[a * EKS_TP + lane] = (l2 < n && j2 < n) ? g[(long long)l2 * ldg + j2] : 0.0;
+                    }
+                }
+                __syncthreads();
+                const double *U = (jt == lt) ? T1 : T2;  // U[b][a] = B[jt 32 + b][lt 32 + a]
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int a = ty + 8 * q, l = lt * 32 + a, j = jt * 32 + lane;
+                    if (l <= j && j < n) {
+                        const double x = T1[a * EKS_TP + lane], y = U[lane * EKS_TP + a];
+                        const double sv = (l == j) ? x : x + y, av = x - y;
+                        if (pass == 0) {
+                            mxs = fmax(mxs, fabs(sv));
+                            if (l < j) mxa = fmax(mxa, fabs(av));
+                        } else {
+                            slice_value(sv, scs, S, out_s, r, rows_pad_s, kpad_s >> 5, pair_le(n, l, j));
+                            if (anti && l < j) slice_value(av, sca, S, out_a, ra, rows_pad_a, kpad_a >> 5, pair_lt(n, l, j));
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (pass == 0) {
+            mxs = block_max(mxs, sh);
+            mxa = block_max(mxa, sh);
+            const int es = exp_of_max(mxs), ea = exp_of_max(mxa);
+            if (threadIdx.x == 0) {
+                e_s[r] = es;
+                if (anti) e_a[ra] = ea;
+            }
+            scs = slice_scale(es, S);
+            sca = slice_scale(ea, S);
+        }
+    }
+    for (long long e = kks + threadIdx.x; e < kpad_s; e += SL_NT) slice_value(0.0, scs, S, out_s, r, rows_pad_s, kpad_s >> 5, e);
+    if (anti)
+        for (long long e = kka + threadIdx.x; e < kpad_a; e += SL_NT)
+            slice_value(0.0, sca, S, out_a, ra, rows_pad_a, kpad_a >> 5, e);
+}
+
+// Density operands of one grid point w in the symmetric exchange form, from rho_w (element [r][q] at
+// rho[w ws + r rs + q], as slice_density_kernel), rho^{st}[l][j] = rho_w[2l + s][2j + t], over the pairs
+// l <= j (pairs[t] = l << 16 | j, t = pair_le(l, j)):
+//   symmetric exchange columns c = (4w + 2s + t) 2 + part at k-index t: part of rho_s^{st}[l][j] =
+//     (rho^{st}[l][j] + rho^{st}[j][l]) / 2;
+//   antisymmetric exchange columns (same c) at k-index pair_lt(l, j), l < j: part of rho_a^{st}[l][j] =
+//     (rho^{st}[l][j] - rho^{st}[j][l]) / 2;
+//   Coulomb columns c = 2w + part at k-index t: part of the symmetric half of P = rho^{aa} + rho^{bb} (the
+//     Cholesky operand holds B_L[l][j] (2 - delta_lj) there: sum_lj B_L[l][j] P[l][j] with B_L symmetric).
+// Each pair reads the 2 x 2 spin blocks (l, j) and (j, l) as two 32-byte pieces each; 18 running
+// maxima, then the slices.
+constexpr int SDS_NT = 256;
+__global__ void __launch_bounds__(SDS_NT, 2) slice_density_sym_kernel(int n, const int *__restrict__ pairs,
+                                                                     const zc *__restrict__ rho, long long rs,
+                                                                     long long ws, int S, long long npadK,
+                                                                     long long kpad_s, long long kpad_a,
+                                                                     signed char *Ks, int *eKs, signed char *Ka,
+                                                                     int *eKa, long long npadP, signed char *Psl,
+                                                                     int *eP) {
+    __shared__ double sh[18][SDS_NT / 32];
+    __shared__ int exs[18];
+    const long long w = blockIdx.x;
+    const zc *R = rho + w * ws;
+    const long long kks = (long long)n * (n + 1) / 2, kka = (long long)n * (n - 1) / 2;
+    auto block = [&](int l, int j, zc (&v)[4]) {
+        const double2 *r0 = reinterpret_cast<const double2 *>(R + (long long)(2 * l) * rs + 2 * j), *r1 = r0 + rs;
+        const double2 a0 = __ldg(r0), a1 = __ldg(r0 + 1), b0 = __ldg(r1), b1 = __ldg(r1 + 1);
+        v[0] = mkz(a0.x, a0.y);
+        v[1] = mkz(a1.x, a1.y);
+        v[2] = mkz(b0.x, b0.y);
+        v[3] = mkz(b1.x, b1.y);
+    };
+    // halves of pair t: sv (symmetric), av (antisymmetric, zero for l = j)
+    auto halves = [&](long long t, zc (&sv)[4], zc (&av)[4], int &l, int &j) {
+        const int pr = __ldg(pairs + t);
+        l = pr >> 16;
+        j = pr & 0xffff;
+        zc v[4];
+        block(l, j, v);
+        if (l == j) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                sv[q] = v[q];
+                av[q] = mkz(0.0);
+            }
+        } else {
+            zc u[4];
+            block(j, l, u);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                sv[q] = mkz(0.5 * (v[q].x + u[q].x), 0.5 * (v[q].y + u[q].y));
+                av[q] = mkz(0.5 * (v[q].x - u[q].x), 0.5 * (v[q].y - u[q].y));
+            }
+        }
+    };
+    {
+        double mx[18];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) mx[q] = 0.0;
+        for (long long t = threadIdx.x; t < kks; t += SDS_NT) {
+            zc sv[4], av[4];
+            int l, j;
+            halves(t, sv, av, l, j);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                mx[2 * q] = fmax(mx[2 * q], fabs(sv[q].x));
+                mx[2 * q + 1] = fmax(mx[2 * q + 1], fabs(sv[q].y));
+                mx[8 + 2 * q] = fmax(mx[8 + 2 * q], fabs(av[q].x));
+                mx[9 + 2 * q] = fmax(mx[9 + 2 * q], fabs(av[q].y));
+            }
+            mx[16] = fmax(mx[16], fabs(sv[0].x + sv[3].x));
+            mx[17] = fmax(mx[17], fabs(sv[0].y + sv[3].y));
+        }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+            double m = mx[q];
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) sh[q][wid] = m;
+        }
+        __syncthreads();
+        if (threadIdx.x < 18) {
+            double m = 0.0;
+            for (int i = 0; i < SDS_NT / 32; ++i) m = fmax(m, sh[threadIdx.x][i]);
+            const int e = exp_of_max(m);
+            exs[threadIdx.x] = e;
+            if (threadIdx.x < 8) eKs[8 * w + threadIdx.x] = e;
+            else if (threadIdx.x < 16) eKa[8 * w + threadIdx.x - 8] = e;
+            else eP[2 * w + threadIdx.x - 16] = e;
+        }
+        __syncthreads();
+    }
+    const long long KBs = kpad_s >> 5, KBa = kpad_a >> 5;
+    for (long long t = threadIdx.x; t < kpad_s; t += SDS_NT) {
+        zc sv[4] = {mkz(0.0), mkz(0.0), mkz(0.0), mkz(0.0)}, av[4] = {mkz(0.0), mkz(0.0), mkz(0.0), mkz(0.0)};
+        int l = 0, j = 0;
+        if (t < kks) halves(t, sv, av, l, j);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            slice_value(sv[q].x, slice_scale(exs[2 * q], S), S, Ks, 8 * w + 2 * q, npadK, KBs, t);
+            slice_value(sv[q].y, slice_scale(exs[2 * q + 1], S), S, Ks, 8 * w + 2 * q + 1, npadK, KBs, t);
+        }
+        slice_value(sv[0].x + sv[3].x, slice_scale(exs[16], S), S, Psl, 2 * w, npadP, KBs, t);
+        slice_value(sv[0].y + sv[3].y, slice_scale(exs[17], S), S, Psl, 2 * w + 1, npadP, KBs, t);
+        if (t < kks && l < j) {
+            const long long u = pair_lt(n, l, j);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                slice_value(av[q].x, slice_scale(exs[8 + 2 * q], S), S, Ka, 8 * w + 2 * q, npadK, KBa, u);
+                slice_value(av[q].y, slice_scale(exs[9 + 2 * q], S), S, Ka, 8 * w + 2 * q + 1, npadK, KBa, u);
+            }
+        }
+    }
+    for (long long u = kka + threadIdx.x; u < kpad_a; u += SDS_NT) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) slice_value(0.0, slice_scale(exs[8 + q], S), S, Ka, 8 * w + q, npadK, KBa, u);
+    }
+}
+
+// Rows of the Cholesky operand of the symmetric Coulomb contraction: row L holds B_L[l][j] (2 - delta_lj)
+// at k-index pair_le(l, j) (B_L[l][j] = Bst[L n^2 + l n + j]), as FP64 rows of length n (n + 1) / 2.
+__global__ void cholesky_pairs_kernel(int n, int L, const double *__restrict__ Bst, const int *__restrict__ pairs,
+                                      double *out) {
+    const long long kks = (long long)n * (n + 1) / 2, tot = kks * L, n2 = (long long)n * n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long row = e / kks, t = e - row * kks;
+        const int pr = pairs[t], l = pr >> 16, j = pr & 0xffff;
+        const double b = Bst[row * n2 + (long long)l * n + j];
+        out[e] = l == j ? b : 2.0 * b;
+    }
+}
+
 // ------------------------------------------------------------------ fused density + operand slicing
 // D (8 x 8) += A (8 x 4, row-major) B (4 x 8, column-major), FP64 tensor cores.
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -1530,6 +1785,53 @@ int oz_slice_ek_panel(int n, int ipanel, const double *G, long long ldg, int S, 
     return PHF_OK;
 }
 
+int oz_slice_ek_sym_panel(int n, int i0, int ipanel, int k0, const int *pairs, const double *G, long long ldg, int S,
+                          long long rows_pad_s, signed char *out_s, int *e_s, long long rows_pad_a, signed char *out_a,
+                          int *e_a, cudaStream_t st) {
+    const long long nn = n;
+    // sum_{i = i0}^{i0 + ipanel - 1} (n - i) pairs (i, k >= i), of which ipanel are diagonal
+    const long long rows_s = ipanel * (nn - i0) - (long long)ipanel * (ipanel - 1) / 2;
+    const long long rows_a = rows_s - ipanel;
+    if (n < 1 || n > 65535 || i0 < 0 || ipanel < 1 || i0 + ipanel > n || k0 < 0 || k0 > i0 || rows_s > rows_pad_s ||
+        rows_a > rows_pad_a || ldg < (nn - k0) * nn) {
+        set_error(PHF_ERR_ARG, "oz_slice_ek_sym_panel: panel rows outside the slice buffers or a short Gram block");
+        return PHF_ERR_ARG;
+    }
+    ProfScope prof(st, PROF_MEMORY);
+    slice_ek_sym_panel_kernel<<<(unsigned)rows_s, SL_NT, 0, st>>>(
+        n, i0, k0, pairs, pair_le(nn, i0, i0), G, ldg, S, rows_pad_s, oz_pad_k(nn * (nn + 1) / 2), out_s, e_s,
+        rows_pad_a, oz_pad_k(nn * (nn - 1) / 2), out_a, e_a);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int oz_slice_density_sym(int n, int bc, const int *pairs, const zc *rho, long long rs, long long ws, int S,
+                         signed char *Ks, int *eKs, signed char *Ka, int *eKa, long long npadK, signed char *Psl,
+                         int *eP, long long npadP, cudaStream_t st) {
+    if (n < 2 || n > 65535 || bc < 1 || 8LL * bc > npadK || 2LL * bc > npadP || !oz_format_ok(S) || (rs & 1) ||
+        (ws & 1)) {
+        set_error(PHF_ERR_ARG, "oz_slice_density_sym: columns outside the slice buffers or odd strides");
+        return PHF_ERR_ARG;
+    }
+    const long long nn = n;
+    ProfScope prof(st, PROF_MEMORY);
+    slice_density_sym_kernel<<<(unsigned)bc, SDS_NT, 0, st>>>(n, pairs, rho, rs, ws, S, npadK,
+                                                             oz_pad_k(nn * (nn + 1) / 2), oz_pad_k(nn * (nn - 1) / 2),
+                                                             Ks, eKs, Ka, eKa, npadP, Psl, eP);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int oz_cholesky_pairs(int n, int L, const double *Bst, const int *pairs, double *out, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    cholesky_pairs_kernel<<<148 * 8, 256, 0, st>>>(n, L, Bst, pairs, out);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 bool oz_rho_slice_ok(int n) { return n >= 1 && n <= 64; }
 
 int oz_rho_slice(int n, int N, int bc, const zc *Xs, long long ld, const zc *bra, int S, signed char *Ksl, int *eK,
@@ -1668,7 +1970,10 @@ int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int
     a.kseg = OZ_KSEG;
     a.gamma_n = 0;
     a.g_row0 = 0;
+    a.gamma_mode = 0;
+    a.g_pairs = nullptr;
     a.a_row0 = 0;
+    a.b_row0 = 0;
     a.group_m = OZ_GROUP_M;
     a.S = S;
     a.ea = ea;
@@ -1706,8 +2011,8 @@ namespace {
 int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
                    const CUtensorMap &ta1, const CUtensorMap &tb1, const CUtensorMap &tbw, int m, int n, int S,
                    const int *ea, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
-                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, long long kb_total, long long kb_pass,
-                   int group_m);
+                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, const OzEx &ex, long long kb_total,
+                   long long kb_pass, int group_m);
 }  // namespace
 
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
@@ -1717,13 +2022,26 @@ int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea,
 
 int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,
                const signed char *Bsl, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
-               cudaStream_t st, int gamma_n, int g_row0) {
-    if (gamma_n > 0 && (g_row0 < 0 || (long long)g_row0 + m > (long long)gamma_n * gamma_n || n % 8 != 0)) {
-        set_error(PHF_ERR_ARG, "oz_gemm: the Gamma output needs rows within [0, n^2) and 8 columns per point");
-        return PHF_ERR_ARG;
+               cudaStream_t st, int gamma_n, int g_row0, const OzEx &ex) {
+    if (gamma_n > 0) {
+        const long long gn = gamma_n;
+        const long long grows = ex.gamma_mode == 0 ? gn * gn : (ex.gamma_mode == 1 ? gn * (gn + 1) / 2 : gn * (gn - 1) / 2);
+        if (ex.gamma_mode < 0 || ex.gamma_mode > 2 || (ex.gamma_mode != 0 && (!ex.g_pairs || gamma_n > 65535)) ||
+            g_row0 < 0 || (long long)g_row0 + m > grows || n % 8 != 0 || trans) {
+            set_error(PHF_ERR_ARG, "oz_gemm: the Gamma output needs rows within its exchange rows (n^2, or the "
+                                   "n(n+1)/2 or n(n-1)/2 pairs with their table) and 8 columns per point");
+            return PHF_ERR_ARG;
+        }
     }
     if (a_row0 < 0 || (long long)a_row0 + m > a_rows_pad) {
         set_error(PHF_ERR_ARG, "oz_gemm: A row range outside its slice buffer");
+        return PHF_ERR_ARG;
+    }
+    const long long b_rows_pad = ex.b_rows_pad > 0 ? ex.b_rows_pad : oz_pad_cols(n);
+    // (the last column tile may reach past the buffer: TMA fills rows beyond the map's extent with zeros,
+    // and the epilogue stores only columns < n)
+    if (ex.b_row0 < 0 || (long long)ex.b_row0 + n > b_rows_pad || b_rows_pad % OZ_BN != 0) {
+        set_error(PHF_ERR_ARG, "oz_gemm: B row range outside its slice buffer");
         return PHF_ERR_ARG;
     }
     if (!oz_format_ok(S)) {
@@ -1733,9 +2051,9 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
     CUtensorMap ta0, ta1, tb0, tb1, tbw;
     const long long mpad = oz_pad_rows(m), npad = oz_pad_cols(n), kpad = oz_pad_k(k);
     PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, a_rows_pad, S, OZ_BM));
-    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, npad, S, oz_bn(S)));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, b_rows_pad, S, oz_bn(S)));
     const bool wide = oz_wide_ok(S) && !g_narrow_mma;  // single-pass int8: the wide issue
-    if (wide) PHF_TRY(make_wide_map(&tbw, Bsl, kpad, npad, oz_bn(S)));
+    if (wide) PHF_TRY(make_wide_map(&tbw, Bsl, kpad, b_rows_pad, oz_bn(S)));
     else tbw = tb0;
     const long long kb_pass = oz_kb_pass(S);
     const long long kb_total = kpad / OZ_BK;
@@ -1747,20 +2065,20 @@ int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_r
     }
     PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)(mpad / OZ_BM), (unsigned)((npad + oz_bn(S) - 1) / oz_bn(S)), 1);  // grouped raster
-    const TuneKey key{1, m, n, k, (long long)S * 4 + (gamma_n > 0) * 2 + trans, accumulate};
+    const TuneKey key{1, m, n, k, (long long)S * 16 + ex.gamma_mode * 4 + (gamma_n > 0) * 2 + trans, accumulate};
     int group_m = tuned_choice(key);
     if (t_tune_record) {
         // the tuner repeats the launch; an accumulating launch then adds several times, which is harmless:
         // the tuning evaluation's outputs are discarded and recomputed by the evaluation that follows
         t_tune_record->push_back({key, {4, 8, 16}, [=](int g, cudaStream_t s) {
                                       return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, tbw, m, n, S,
-                                                            ea + a_row0, eb, D, ldd, accumulate, trans, err, s,
-                                                            gamma_n, g_row0, a_row0, kb_total, kb_pass, g);
+                                                            ea + a_row0, eb + ex.b_row0, D, ldd, accumulate, trans,
+                                                            err, s, gamma_n, g_row0, a_row0, ex, kb_total, kb_pass, g);
                                   }});
     }
     if (group_m < 0) group_m = OZ_GROUP_M;
-    return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, tbw, m, n, S, ea + a_row0, eb, D, ldd, accumulate,
-                          trans, err, st, gamma_n, g_row0, a_row0, kb_total, kb_pass, group_m);
+    return oz_gemm_launch(kern, grid, smem, ta0, tb0, ta1, tb1, tbw, m, n, S, ea + a_row0, eb + ex.b_row0, D, ldd,
+                          accumulate, trans, err, st, gamma_n, g_row0, a_row0, ex, kb_total, kb_pass, group_m);
 }
 
 namespace {
@@ -1768,8 +2086,8 @@ namespace {
 int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &ta0, const CUtensorMap &tb0,
                    const CUtensorMap &ta1, const CUtensorMap &tb1, const CUtensorMap &tbw, int m, int n, int S,
                    const int *ea, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
-                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, long long kb_total, long long kb_pass,
-                   int group_m) {
+                   cudaStream_t st, int gamma_n, int g_row0, int a_row0, const OzEx &ex, long long kb_total,
+                   long long kb_pass, int group_m) {
     for (long long kb0 = 0; kb0 < kb_total; kb0 += kb_pass) {
         OzArgs a;
         a.m = m;
@@ -1788,7 +2106,10 @@ int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &t
         a.kseg = OZ_KSEG;
         a.gamma_n = gamma_n;
         a.g_row0 = g_row0;
+        a.gamma_mode = ex.gamma_mode;
+        a.g_pairs = ex.g_pairs;
         a.a_row0 = a_row0;
+        a.b_row0 = ex.b_row0;
         a.group_m = group_m;
         a.err = err;
         {

@@ -245,6 +245,10 @@ int validate(const phf_plan_desc *d) {
         set_error(PHF_ERR_ARG, "exchange_panel must be >= 0");
         return PHF_ERR_ARG;
     }
+    if (d->exchange_symmetry < 0 || d->exchange_symmetry > 2) {
+        set_error(PHF_ERR_ARG, "exchange_symmetry must be 0, 1 or 2");
+        return PHF_ERR_ARG;
+    }
     return PHF_OK;
 }
 
@@ -320,6 +324,25 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         const int n = d->nso / 2;
         p.ek_ipanel = d->exchange_panel > 0 ? std::min(d->exchange_panel, n) : choose_ipanel(n);
         p.ek_npanel = (n + p.ek_ipanel - 1) / p.ek_ipanel;
+        // the exchange symmetry: FP64, and the tensor-core forms whose densities are sliced apart from
+        // the density GEMM (n > 64)
+        const bool sym_ok = n >= 2 && n <= 65535 && (p.prec == PHF_PREC_FP64 || !oz_rho_slice_ok(n));
+        if (d->exchange_symmetry == 1 && !sym_ok) {
+            set_error(PHF_ERR_UNSUPPORTED, "exchange_symmetry needs the FP64 form or n > 64 (tensor-core forms)");
+            return PHF_ERR_UNSUPPORTED;
+        }
+        p.ek_sym = sym_ok && d->exchange_symmetry != 2;
+        if (p.ek_sym) {
+            // panels of indices i with Gram blocks (i n + l) x ((k >= i0) n + j) of at most ek_ipanel n x n^2
+            const long long budget = (long long)p.ek_ipanel * n;
+            p.ek_i0.clear();
+            for (int i0 = 0; i0 < n;) {
+                p.ek_i0.push_back(i0);
+                i0 += (int)std::max<long long>(1, std::min<long long>(n - i0, budget / (n - i0)));
+            }
+            p.ek_i0.push_back(n);
+            p.ek_npanel = (int)p.ek_i0.size() - 1;
+        }
     }
     p.nl = d->ngrid[0];
     p.ny = d->ngrid[1];
@@ -557,7 +580,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         if (p.chol && p.eri) {
             per += 2 * MM + 2 * n2 + p.L;                       // Rho, Gam, Pvec, Jvec, dvec
             if (p.prec == PHF_PREC_FP64) per += 8 * n2;         // Kin, Kvec
-            else per += (8 * n2 * oz_slots(p.slices)) / sizeof(zc) + 1  // exchange slices
+            else per += (8 * (n2 + 64) * oz_slots(p.slices)) / sizeof(zc) + 1  // exchange slices
                         + (2 * n2 + 2 * (size_t)p.L) * oz_slots(p.slices) / sizeof(zc) + 1    // Coulomb slices
                         + p.L + n2;                                                // d^T, J pairs
             // int8 density GEMM: the X rows' slices and exponents
@@ -614,10 +637,16 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
             PHF_TRY(p.arena.alloc(&p.Kin, 4 * b * n2));
             PHF_TRY(p.arena.alloc(&p.Kvec, 4 * b * n2));
         } else {
-            const size_t bsl = oz_slice_bytes(oz_pad_cols(8 * (long long)b), (long long)n2, p.slices);
+            const long long npadK = oz_pad_cols(8 * (long long)b);
+            size_t bsl = oz_slice_bytes(npadK, (long long)n2, p.slices);
+            if (p.ek_sym) {  // symmetric-half columns (k = n(n+1)/2), then the antisymmetric halves
+                p.bsl_a_off = oz_slice_bytes(npadK, (long long)n * (n + 1) / 2, p.slices);
+                bsl = std::max(bsl, p.bsl_a_off + oz_slice_bytes(npadK, (long long)n * (n - 1) / 2, p.slices));
+                PHF_TRY(p.arena.alloc(&p.eb_a, (size_t)npadK));
+            }
             PHF_TRY(p.arena.alloc(&p.Bsl, bsl));
             PHF_CUDA(cudaMemset(p.Bsl, 0, bsl));
-            PHF_TRY(p.arena.alloc(&p.eb, (size_t)oz_pad_cols(8 * (long long)b)));
+            PHF_TRY(p.arena.alloc(&p.eb, (size_t)npadK));
             const long long c2 = oz_pad_cols(2 * (long long)b);
             const size_t psl = oz_slice_bytes(c2, (long long)n2, p.slices);
             const size_t dsl = oz_slice_bytes(c2, p.L, p.slices);
@@ -662,12 +691,15 @@ namespace {
 // batched n x n x L products); sliced (int8 digits, BF16 pairs or TF32) for the tensor-core back-end.
 // Coulomb operands of the tensor-core path: B (L x n^2, rows of Bst) and B^T (n^2 x L, strided rows of
 // Bst).  B^T's slices are also both operands of the streamed form's Gram blocks.
+// With the exchange symmetry the Coulomb contraction d_L = sum_lj B_L[l][j] P[l][j] runs over the pairs
+// l <= j (B_L symmetric): B's rows hold B_L[l][j] (2 - delta_lj) in pair order and the density operand
+// the symmetric half of P.
 int build_coulomb_slices(PlanImpl &p) {
     const int n = p.n, L = p.L;
-    const long long n2 = (long long)n * n;
+    const long long n2 = (long long)n * n, kc = p.ek_sym ? (long long)n * (n + 1) / 2 : n2;
     PHF_TRY(p.arena.alloc(&p.ozerr, 1));
     PHF_CUDA(cudaMemset(p.ozerr, 0, sizeof(int)));
-    const size_t b1 = oz_slice_bytes(oz_pad_rows(L), n2, p.slices);
+    const size_t b1 = oz_slice_bytes(oz_pad_rows(L), kc, p.slices);
     const size_t b2 = oz_slice_bytes(oz_pad_rows(n2), L, p.slices);
     PHF_TRY(p.arena.alloc(&p.B1sl, b1));
     PHF_TRY(p.arena.alloc(&p.B2sl, b2));
@@ -675,8 +707,42 @@ int build_coulomb_slices(PlanImpl &p) {
     PHF_CUDA(cudaMemset(p.B2sl, 0, b2));
     PHF_TRY(p.arena.alloc(&p.eB1, (size_t)oz_pad_rows(L)));
     PHF_TRY(p.arena.alloc(&p.eB2, (size_t)oz_pad_rows(n2)));
-    PHF_TRY(oz_slice_rows_strided(L, (int)n2, p.Bst, n2, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
+    if (p.ek_sym) {
+        double *Bp = nullptr;
+        PHF_TRY(p.arena.alloc(&Bp, (size_t)(L * kc)));
+        PHF_TRY(oz_cholesky_pairs(n, L, p.Bst, p.pairs_le, Bp, 0));
+        PHF_TRY(oz_slice_rows_strided(L, (int)kc, Bp, kc, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
+        PHF_CUDA(cudaDeviceSynchronize());
+        p.arena.free_one(Bp);
+    } else {
+        PHF_TRY(oz_slice_rows_strided(L, (int)n2, p.Bst, n2, 1, p.slices, oz_pad_rows(L), p.B1sl, p.eB1, 0));
+    }
     PHF_TRY(oz_slice_rows_strided((int)n2, L, p.Bst, 1, n2, p.slices, oz_pad_rows(n2), p.B2sl, p.eB2, 0));
+    return PHF_OK;
+}
+
+// Rows of panel [i0, i0 + ip) in the symmetric exchange form: pairs (i, k >= i) and (i, k > i).
+inline long long sym_rows(int n, int i0, int ip) { return (long long)ip * (n - i0) - (long long)ip * (ip - 1) / 2; }
+inline long long pair_index_le(long long n, long long l, long long j) { return l * n - l * (l - 1) / 2 + (j - l); }
+inline long long pair_index_lt(long long n, long long l, long long j) {
+    return l * (n - 1) - l * (l - 1) / 2 + (j - l - 1);
+}
+
+// The pair tables of the symmetric form (i << 16 | k in row order, i <= k and i < k), on the device.
+int upload_pair_tables(PlanImpl &p) {
+    const int n = p.n;
+    std::vector<int> le, lt;
+    le.reserve((size_t)n * (n + 1) / 2);
+    lt.reserve((size_t)n * (n - 1) / 2);
+    for (int i = 0; i < n; ++i)
+        for (int k = i; k < n; ++k) {
+            le.push_back(i << 16 | k);
+            if (k > i) lt.push_back(i << 16 | k);
+        }
+    PHF_TRY(p.arena.alloc(&p.pairs_le, le.size()));
+    PHF_TRY(p.arena.alloc(&p.pairs_lt, std::max<size_t>(lt.size(), 1)));
+    PHF_CUDA(cudaMemcpy(p.pairs_le, le.data(), le.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!lt.empty()) PHF_CUDA(cudaMemcpy(p.pairs_lt, lt.data(), lt.size() * sizeof(int), cudaMemcpyHostToDevice));
     return PHF_OK;
 }
 
@@ -684,16 +750,32 @@ int build_exchange_matrix(PlanImpl &p) {
     const int n = p.n, L = p.L;
     const long long n2 = (long long)n * n;
     if (p.streamed) {  // buffers of one exchange panel; the rows themselves are formed per chunk
+        // (symmetric form: a panel's Gram block, ip n x (n - i0) n, and its rows, rows_s x n(n+1)/2 plus
+        // rows_a x n(n-1)/2 with rows_a < rows_s <= ip (n - i0), fit in the full form's ek_ipanel n x n^2)
         const long long rows = (long long)p.ek_ipanel * n;
         PHF_TRY(p.arena.alloc(&p.Gp, (size_t)(rows * n2)));
+        if (p.ek_sym) PHF_TRY(upload_pair_tables(p));
         if (p.prec == PHF_PREC_FP64) {
             PHF_TRY(p.arena.alloc(&p.EKp, (size_t)(rows * n2)));
         } else {
-            const size_t bytes = oz_slice_bytes(oz_pad_rows(rows), n2, p.slices);
+            size_t bytes = oz_slice_bytes(oz_pad_rows(rows), n2, p.slices);
+            long long erows = oz_pad_rows(rows);
+            if (p.ek_sym) {
+                const long long kks = (long long)n * (n + 1) / 2, kka = (long long)n * (n - 1) / 2;
+                bytes = 0;
+                erows = 0;
+                for (int pi = 0; pi < p.ek_npanel; ++pi) {
+                    const int i0 = p.ek_i0[pi], ip = p.ek_i0[pi + 1] - i0;
+                    const long long rs = oz_pad_rows(sym_rows(n, i0, ip)),
+                                    ra = oz_pad_rows(std::max<long long>(sym_rows(n, i0, ip) - ip, 1));
+                    bytes = std::max(bytes, oz_slice_bytes(rs, kks, p.slices) + oz_slice_bytes(ra, kka, p.slices));
+                    erows = std::max(erows, rs + ra);
+                }
+            }
             PHF_TRY(p.arena.alloc(&p.EKpsl, bytes));
             PHF_CUDA(cudaMemset(p.EKpsl, 0, bytes));
-            PHF_TRY(p.arena.alloc(&p.eEKp, (size_t)oz_pad_rows(rows)));
-            PHF_CUDA(cudaMemset(p.eEKp, 0, (size_t)oz_pad_rows(rows) * sizeof(int)));
+            PHF_TRY(p.arena.alloc(&p.eEKp, (size_t)erows));
+            PHF_CUDA(cudaMemset(p.eEKp, 0, (size_t)erows * sizeof(int)));
             PHF_TRY(build_coulomb_slices(p));
         }
         PHF_CUDA(cudaDeviceSynchronize());
@@ -730,7 +812,92 @@ int build_exchange_matrix(PlanImpl &p) {
 // Kin into the matching rows of Kvec.  Tensor-core forms: the panel is sliced, and the product's
 // epilogue writes -K of the panel's rows straight into Gamma.  The Gram block costs 2 n^2 ipanel L
 // flops per panel (2 n^4 L per chunk against 16 n^4 per grid point).
+// Symmetric form (p.ek_sym): panel p covers i in [ek_i0[p], ek_i0[p + 1]); its Gram block keeps only
+// the columns (k >= i0, j), G[(i - i0) n + l][(k - i0) n + j] (row stride (n - i0) n), and yields the
+// panel's symmetric rows (pairs i <= k) and antisymmetric rows (i < k), each multiplied by the matching
+// half of the chunk's densities: half the exchange GEMM's and the Gram blocks' work of the full form.
+int exchange_streamed_sym(PlanImpl &p, int bc, cudaStream_t st) {
+    const int n = p.n, L = p.L, b = p.b;
+    const long long nn = n, n2 = nn * nn, kks = nn * (nn + 1) / 2, kka = nn * (nn - 1) / 2;
+    for (int pi = 0; pi < p.ek_npanel; ++pi) {
+        const int i0 = p.ek_i0[pi], ip = p.ek_i0[pi + 1] - i0;
+        const long long gcols = (nn - i0) * nn, rows_s = sym_rows(n, i0, ip), rows_a = rows_s - ip;
+        const int grows = ip * n;
+        const long long ts0 = pair_index_le(nn, i0, i0), ta0 = rows_a > 0 ? pair_index_lt(nn, i0, i0 + 1) : 0;
+        if (p.prec == PHF_PREC_FP64) {
+            double *EKs = p.EKp, *EKa = p.EKp + rows_s * kks;
+            double *Kv = reinterpret_cast<double *>(p.Kvec);
+            const double *Ki = reinterpret_cast<const double *>(p.Kin);
+            if (p.library_gemm) {
+                cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
+                const double one = 1.0, zero = 0.0;
+                ProfScope prof(st, PROF_JK);
+                // column-major: G^T (gcols x grows) = (columns k >= i0 of B^T) * (rows of B^T)^T
+                if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS ||
+                    cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)gcols, grows, L, &one, p.Bst + (size_t)i0 * n,
+                                (int)n2, p.Bst + (size_t)i0 * n, (int)n2, &zero, p.Gp, (int)gcols) !=
+                        CUBLAS_STATUS_SUCCESS) {
+                    set_error(PHF_ERR_CUDA, "cublasDgemm (exchange panel) failed");
+                    return PHF_ERR_CUDA;
+                }
+            } else {
+                OutView o = vo(reinterpret_cast<zc *>(p.Gp), gcols, 1);
+                o.real = 1;
+                PHF_TRY(zgemm_strided(grows, (int)gcols, L, 1, 1, Z1, vd(p.Bst + (size_t)i0 * n, 1, n2),
+                                      vd(p.Bst + (size_t)i0 * n, n2, 1), Z0, o, nullptr, st));
+            }
+            PHF_TRY(launch_ek_sym_panel(n, i0, ip, i0, p.pairs_le, p.Gp, gcols, EKs, EKa, st));
+            if (p.library_gemm) {
+                cublasHandle_t h = reinterpret_cast<cublasHandle_t>(p.cublas);
+                const double one = 1.0, zero = 0.0;
+                ProfScope prof(st, PROF_JK);
+                if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, 8 * bc, (int)rows_s, (int)kks, &one, Ki, 8 * b, EKs,
+                                (int)kks, &zero, Kv + (size_t)ts0 * 8 * b, 8 * b) != CUBLAS_STATUS_SUCCESS ||
+                    (rows_a > 0 &&
+                     cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, 8 * bc, (int)rows_a, (int)kka, &one,
+                                 Ki + (size_t)kks * 8 * b, 8 * b, EKa, (int)kka, &zero,
+                                 Kv + (size_t)(kks + ta0) * 8 * b, 8 * b) != CUBLAS_STATUS_SUCCESS)) {
+                    set_error(PHF_ERR_CUDA, "cublasDgemm (exchange rows) failed");
+                    return PHF_ERR_CUDA;
+                }
+            } else {
+                PHF_TRY(zgemm_strided((int)rows_s, 4 * bc, (int)kks, 1, 1, Z1, vd(EKs, kks, 1), vz(p.Kin, 4LL * b, 1),
+                                      Z0, vo(p.Kvec + (size_t)ts0 * 4 * b, 4LL * b, 1), nullptr, st));
+                if (rows_a > 0)
+                    PHF_TRY(zgemm_strided((int)rows_a, 4 * bc, (int)kka, 1, 1, Z1, vd(EKa, kka, 1),
+                                          vz(p.Kin + (size_t)kks * 4 * b, 4LL * b, 1), Z0,
+                                          vo(p.Kvec + (size_t)(kks + ta0) * 4 * b, 4LL * b, 1), nullptr, st));
+            }
+        } else {
+            OzEx gx;
+            gx.b_rows_pad = oz_pad_rows(n2);
+            gx.b_row0 = i0 * n;
+            PHF_TRY(oz_gemm_ex(grows, (int)gcols, L, p.slices, p.B2sl, oz_pad_rows(n2), i0 * n, p.eB2, p.B2sl, p.eB2,
+                               p.Gp, gcols, 0, 0, p.ozerr, st, 0, 0, gx));
+            const long long rps = oz_pad_rows(rows_s), rpa = oz_pad_rows(std::max<long long>(rows_a, 1));
+            signed char *As = p.EKpsl, *Aa = p.EKpsl + oz_slice_bytes(rps, kks, p.slices);
+            int *es = p.eEKp, *ea = p.eEKp + rps;
+            PHF_TRY(oz_slice_ek_sym_panel(n, i0, ip, i0, p.pairs_le, p.Gp, gcols, p.slices, rps, As, es, rpa, Aa, ea,
+                                          st));
+            OzEx sx;
+            sx.gamma_mode = 1;
+            sx.g_pairs = p.pairs_le;
+            PHF_TRY(oz_gemm_ex((int)rows_s, 8 * bc, (int)kks, p.slices, As, rps, 0, es, p.Bsl, p.eb,
+                               reinterpret_cast<double *>(p.Gam), 0, 0, 0, p.ozerr, st, n, (int)ts0, sx));
+            if (rows_a > 0) {
+                OzEx ax;
+                ax.gamma_mode = 2;
+                ax.g_pairs = p.pairs_lt;
+                PHF_TRY(oz_gemm_ex((int)rows_a, 8 * bc, (int)kka, p.slices, Aa, rpa, 0, ea, p.Bsl + p.bsl_a_off,
+                                   p.eb_a, reinterpret_cast<double *>(p.Gam), 0, 0, 0, p.ozerr, st, n, (int)ta0, ax));
+            }
+        }
+    }
+    return PHF_OK;
+}
+
 int exchange_streamed(PlanImpl &p, int bc, cudaStream_t st) {
+    if (p.ek_sym) return exchange_streamed_sym(p, bc, st);
     const int n = p.n, L = p.L, b = p.b;
     const long long n2 = (long long)n * n, prow = (long long)p.ek_ipanel * n;
     for (int pi = 0; pi < p.ek_npanel; ++pi) {
@@ -820,6 +987,10 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     } else {
         if (fused)
             PHF_TRY(oz_rho_slice(n, N, bc, p.Xs, ld, p.bra, p.slices, p.Bsl, p.eb, p.Psl, p.ePc, st));
+        else if (p.ek_sym)
+            PHF_TRY(oz_slice_density_sym(n, bc, p.pairs_le, p.Rho, rrs, rws, p.slices, p.Bsl, p.eb,
+                                         p.Bsl + p.bsl_a_off, p.eb_a, oz_pad_cols(8LL * bc), p.Psl, p.ePc,
+                                         oz_pad_cols(2LL * bc), st));
         else
             PHF_TRY(oz_slice_density(n, bc, p.Rho, rrs, rws, p.slices, p.Bsl, p.eb, oz_pad_cols(8LL * bc), p.Psl,
                                      p.ePc, oz_pad_cols(2LL * bc), st));
@@ -830,8 +1001,9 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     // event times of overlapping kernels would count the shared time twice.
     cudaStream_t js = st;
     const bool fork = p.prec != PHF_PREC_FP64 && !g_prof.on;
+    const int kcoul = p.ek_sym ? n * (n + 1) / 2 : (int)n2;  // Coulomb contraction over pairs l <= j, or all (l, j)
     if (p.prec != PHF_PREC_FP64 && !fork) {
-        PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
+        PHF_TRY(oz_gemm_splitk(L, 2 * bc, kcoul, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
                                p.ozerr, st));
         PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, st));
         PHF_TRY(oz_gemm_t((int)n2, 2 * bc, L, p.slices, p.B2sl, p.eB2, p.dsl, p.edc, p.Jr, n2, 0, 1, p.ozerr, st));
@@ -849,7 +1021,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         PHF_CUDA(cudaStreamWaitEvent(p.side, p.ev_fork, 0));
         js = p.side;
         // d^T (2 bc x L) = (B vec P)^T, then J (n^2 x 2 bc, real/imag pairs) = B^T d
-        PHF_TRY(oz_gemm_splitk(L, 2 * bc, (int)n2, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
+        PHF_TRY(oz_gemm_splitk(L, 2 * bc, kcoul, p.slices, p.B1sl, p.eB1, p.Psl, p.ePc, p.dT, L, 1, kDSplit, p.dpart,
                                p.ozerr, js));
         PHF_TRY(oz_slice_rows_strided(2 * bc, L, p.dT, L, 1, p.slices, oz_pad_cols(2LL * bc), p.dsl, p.edc, js));
         // J^T (2 bc x n^2): transposed output keeps the epilogue's FP64 stores coalesced
@@ -858,7 +1030,10 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
     }
     prof_set_class(PROF_JK);
     if (p.prec == PHF_PREC_FP64) {
-        PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
+        if (p.ek_sym)
+            PHF_TRY(launch_gather_kin_sym(n, bc, p.pairs_le, p.Rho, p.Kin, 4LL * b, st));
+        else
+            PHF_TRY(launch_gather_kin(n, bc, p.Rho, p.Kin, 4LL * b, st));
         if (p.streamed) {
             PHF_TRY(exchange_streamed(p, bc, st));
         } else if (p.library_gemm) {
@@ -879,7 +1054,8 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
                                   vo(p.Kvec, 4LL * b, 1), nullptr, st));
         }
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st));
+        PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st,
+                                      p.ek_sym));
     } else {
         // K (as K^T, 8 bc x n^2) written by the GEMM epilogue as -K into Gamma's complex M x M blocks
         if (p.streamed)

@@ -128,7 +128,13 @@ int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *E
 int launch_bra_rho_operand(int M, int N, const zc *bra, double *out, cudaStream_t st);
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
-                          cudaStream_t st);
+                          cudaStream_t st, int ksym = 0);
+// symmetric exchange form, FP64: the panel's symmetric rows EKs (rows_s x n(n+1)/2) and antisymmetric
+// rows EKa (x n(n-1)/2) from its Gram block (as oz_slice_ek_sym_panel), and Kin's symmetric rows (pair_le
+// order) followed by its antisymmetric rows (pair_lt order) from the dense densities
+int launch_ek_sym_panel(int n, int i0, int ipanel, int k0, const int *pairs, const double *G, long long ldg,
+                        double *EKs, double *EKa, cudaStream_t st);
+int launch_gather_kin_sym(int n, int b, const int *pairs, const zc *rho, zc *Kin, long long ldk, cudaStream_t st);
 
 // ozaki_i8.cu: FP64-accurate GEMM from int8 slices on tcgen05.  The slice-count argument S is 1..7
 // int8 slices, or one of two floating-point operand formats contracted by the same kernel:
@@ -155,15 +161,41 @@ int oz_slice_density(int n, int bc, const zc *rho, long long rs, long long ws, i
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st,
               int gamma_n = 0);  // gamma_n > 0: -K^T written into Gamma (exchange GEMM, m = n^2)
+// Optional operand ranges and exchange-to-Gamma row modes of oz_gemm_ex:
+//   b_rows_pad, b_row0: B rows (the output's columns) [b_row0, b_row0 + n) of a slice buffer of
+//     b_rows_pad rows (0: a buffer of oz_pad_cols(n) rows), eb indexed by that buffer's rows;
+//   gamma_mode: Gamma output rows 0 = exchange rows i n + k; 1 = symmetric pairs (i <= k), 2 =
+//     antisymmetric pairs (i < k), pair of global row g = g_pairs[g] (i << 16 | k).
+struct OzEx {
+    long long b_rows_pad = 0;
+    int b_row0 = 0;
+    int gamma_mode = 0;
+    const int *g_pairs = nullptr;
+};
 // oz_gemm_t with A rows [a_row0, a_row0 + m) of a slice buffer of a_rows_pad rows (ea indexed by that
 // buffer's rows) and, in the Gamma mode, output row 0 at exchange row g_row0 (a panel of the exchange rows)
 int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,
                const signed char *Bsl, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
-               cudaStream_t st, int gamma_n, int g_row0);
+               cudaStream_t st, int gamma_n, int g_row0, const OzEx &ex = OzEx());
 // slices of the exchange rows (i, k), i in [i0, i0 + ipanel), from the panel's Gram block G
 // (G[(i - i0) n + l][k n + j] = sum_L B_L[i][l] B_L[k][j], row stride ldg); k-index l n + j
 int oz_slice_ek_panel(int n, int ipanel, const double *G, long long ldg, int S, long long rows_pad, signed char *out,
                       int *ea, cudaStream_t st);
+// Symmetric exchange form (n <= 65535; pairs tables: pair t -> i << 16 | k in row order, i <= k):
+// the symmetric rows (pairs (i, k), i in [i0, i0 + ipanel), k >= i; rows_s = sum (n - i)) and the
+// antisymmetric rows (k > i; rows_s - ipanel) of one panel, sliced from its Gram block
+// G[(i - i0) n + l][(k - k0) n + j] (row stride ldg >= (n - k0) n, k0 <= i0)
+int oz_slice_ek_sym_panel(int n, int i0, int ipanel, int k0, const int *pairs, const double *G, long long ldg, int S,
+                          long long rows_pad_s, signed char *out_s, int *e_s, long long rows_pad_a, signed char *out_a,
+                          int *e_a, cudaStream_t st);
+// the symmetric and antisymmetric exchange columns (8 each per point) and the symmetric Coulomb columns
+// (2 per point) of the densities, k-indices in pair order (see ozaki_i8.cu)
+int oz_slice_density_sym(int n, int bc, const int *pairs, const zc *rho, long long rs, long long ws, int S,
+                         signed char *Ks, int *eKs, signed char *Ka, int *eKa, long long npadK, signed char *Psl,
+                         int *eP, long long npadP, cudaStream_t st);
+// out (L x n(n+1)/2, FP64): B_L[l][j] (2 - delta_lj) at k-index pair_le(l, j), the Cholesky operand of the
+// symmetric Coulomb contraction
+int oz_cholesky_pairs(int n, int L, const double *Bst, const int *pairs, double *out, cudaStream_t st);
 int oz_gemm_splitk(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl,
                    const int *eb, double *D, long long ldd, int trans, int nsplit, double *part, int *err,
                    cudaStream_t st);
@@ -181,6 +213,11 @@ struct PlanImpl {
                                      // from the Cholesky vectors in panels of ek_ipanel spatial indices i,
                                      // each used against the whole chunk and then overwritten
     int ek_ipanel = 0, ek_npanel = 0;
+    int ek_sym = 0;                  // streamed form with the exchange symmetry (pairs i <= k, i < k)
+    std::vector<int> ek_i0;          // symmetric form: panel p covers indices [ek_i0[p], ek_i0[p + 1])
+    int *pairs_le = nullptr, *pairs_lt = nullptr;  // pair t -> i << 16 | k, i <= k, resp. i < k, row order
+    int *eb_a = nullptr;             // exponents of the antisymmetric density columns (tensor-core form)
+    size_t bsl_a_off = 0;            // byte offset of their slices in Bsl
     int exact = 0;                   // also accumulate the ket-side gradient (gradient_mode 1)
     int library_gemm = 0;            // FP64 exchange GEMM through cuBLAS (comparison form)
     void *cublas = nullptr;          // cublasHandle_t when library_gemm

@@ -271,10 +271,12 @@ __global__ void gather_kin_kernel(int n, int b, const zc *rho, zc *Kin, long lon
 // J: complex J[(i n + k) ldj + w], or real/imaginary pairs with element (ik, c) of Jr at
 //    Jr[ik jrs + c jcs], c = 2 w + part;
 // K: complex Kc[(i n + k) ldk + 4 w + st], or pairs with element (ik, c) of Kr at Kr[ik krs + c kcs],
-//    c = 2 (4 w + st) + part.
+//    c = 2 (4 w + st) + part.  ksym (complex Kc only): K from its symmetric-form parts, KS of the pair
+//    (min(i, k), max(i, k)) at row pair_le and KA at row n(n + 1)/2 + pair_lt (row order of the pairs),
+//    K[i][k] = KS + KA for i < k, KS - KA for i > k, KS for i = k.
 __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs,
                                       long long jcs, const zc *Kc, long long ldk, const double *Kr, long long krs,
-                                      long long kcs, zc *Gam) {
+                                      long long kcs, zc *Gam, int ksym) {
     const int M = 2 * n;
     const long long tot = (long long)M * M * b;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
@@ -284,7 +286,16 @@ __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, 
         long long ik = (long long)i * n + k;
         int st = sg * 2 + tu;
         zc kv;
-        if (Kc) {
+        if (Kc && ksym) {
+            const long long lo = i < k ? i : k, hi = i < k ? k : i, nn = n;
+            const long long ts = lo * nn - lo * (lo - 1) / 2 + (hi - lo);
+            kv = Kc[ts * ldk + 4 * w + st];
+            if (lo != hi) {
+                const long long ta = nn * (nn + 1) / 2 + lo * (nn - 1) - lo * (lo - 1) / 2 + (hi - lo - 1);
+                const zc ka = Kc[ta * ldk + 4 * w + st];
+                kv = i < k ? kv + ka : kv - ka;
+            }
+        } else if (Kc) {
             kv = Kc[ik * ldk + 4 * w + st];
         } else {
             const long long cc = 2 * (4 * w + st);
@@ -361,6 +372,75 @@ __global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long lon
         zc *g = Gam + (w * M + 2 * i + sg) * M + 2 * k + sg;
         const zc jv = mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
         *g = *g + jv;
+    }
+}
+
+// Symmetric and antisymmetric FP64 exchange rows of one panel from its Gram block (the symmetric
+// exchange form; the tensor-core slicer slice_ek_sym_panel_kernel does the same with slices):
+// pair (i, k) = pairs[t0 + r] of symmetric row r, B[l][j] = G[(i - i0) n + l][(k - k0) n + j];
+// EKs[r][pair_le(l, j)] = B[l][j] + B[j][l] (l < j), B[l][l] (l = j); for i < k
+// EKa[r - (i - i0) - 1][pair_lt(l, j)] = B[l][j] - B[j][l] (l < j).  Row lengths n(n+1)/2, n(n-1)/2.
+// 32 x 32 tile pairs through shared memory, so that both B[l][j] and B[j][l] are read in rows.
+__global__ void __launch_bounds__(256) ek_sym_panel_kernel(int n, int i0, int k0, const int *__restrict__ pairs,
+                                                           long long t0, const double *__restrict__ G, long long ldg,
+                                                           double *__restrict__ EKs, double *__restrict__ EKa) {
+    __shared__ double T1[32 * 33], T2[32 * 33];
+    const long long r = blockIdx.x, nn = n;
+    const int pr = __ldg(pairs + t0 + r), i = pr >> 16, k = pr & 0xffff;
+    const bool anti = i < k;
+    const long long ra = r - (i - i0) - 1;
+    const double *g = G + (long long)(i - i0) * n * ldg + (long long)(k - k0) * n;
+    double *es = EKs + r * (nn * (nn + 1) / 2), *ea = anti ? EKa + ra * (nn * (nn - 1) / 2) : nullptr;
+    const int nt = (n + 31) / 32, lane = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int lt = 0; lt < nt; ++lt) {
+        for (int jt = lt; jt < nt; ++jt) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int a = ty + 8 * q;
+                const int l1 = lt * 32 + a, j1 = jt * 32 + lane;
+                T1[a * 33 + lane] = (l1 < n && j1 < n) ? g[(long long)l1 * ldg + j1] : 0.0;
+                if (jt != lt) {
+                    const int l2 = jt * 32 + a, j2 = lt * 32 + lane;
+                    T2[a * 33 + lane] = (l2 < n && j2 < n) ? g[(long long)l2 * ldg + j2] : 0.0;
+                }
+            }
+            __syncthreads();
+            const double *U = (jt == lt) ? T1 : T2;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int a = ty + 8 * q, l = lt * 32 + a, j = jt * 32 + lane;
+                if (l <= j && j < n) {
+                    const double x = T1[a * 33 + lane], y = U[lane * 33 + a];
+                    es[(long long)l * nn - (long long)l * (l - 1) / 2 + (j - l)] = (l == j) ? x : x + y;
+                    if (anti && l < j) ea[(long long)l * (nn - 1) - (long long)l * (l - 1) / 2 + (j - l - 1)] = x - y;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Kin in the symmetric exchange form: rows t = pair_le(l, j) (pairs[t] = l << 16 | j) hold
+// rho_s^{st}[l][j] = (rho_w[2l + s][2j + t] + rho_w[2j + s][2l + t]) / 2 at column 4w + st (row stride ldk);
+// rows n(n+1)/2 + pair_lt(l, j), l < j, the antisymmetric halves (difference / 2).  rho_w dense M x M.
+__global__ void gather_kin_sym_kernel(int n, int b, const int *__restrict__ pairs, const zc *rho, zc *Kin,
+                                      long long ldk) {
+    const int M = 2 * n;
+    const long long nn = n, kks = nn * (nn + 1) / 2, tot = kks * b * 4;
+    for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
+        const long long t = e / (4LL * b), c = e - t * 4LL * b, w = c >> 2;
+        const int sg = (int)((c >> 1) & 1), tu = (int)(c & 1);
+        const int pr = pairs[t], l = pr >> 16, j = pr & 0xffff;
+        const zc *R = rho + w * (long long)M * M;
+        const zc v = R[(long long)(2 * l + sg) * M + 2 * j + tu];
+        if (l == j) {
+            Kin[t * ldk + c] = v;
+        } else {
+            const zc u = R[(long long)(2 * j + sg) * M + 2 * l + tu];
+            Kin[t * ldk + c] = mkz(0.5 * (v.x + u.x), 0.5 * (v.y + u.y));
+            const long long ta = kks + (long long)l * (nn - 1) - (long long)l * (l - 1) / 2 + (j - l - 1);
+            Kin[ta * ldk + c] = mkz(0.5 * (v.x - u.x), 0.5 * (v.y - u.y));
+        }
     }
 }
 
@@ -576,6 +656,30 @@ int launch_bra_rho_operand(int M, int N, const zc *bra, double *out, cudaStream_
     return PHF_OK;
 }
 
+int launch_ek_sym_panel(int n, int i0, int ipanel, int k0, const int *pairs, const double *G, long long ldg,
+                        double *EKs, double *EKa, cudaStream_t st) {
+    const long long rows_s = (long long)ipanel * (n - i0) - (long long)ipanel * (ipanel - 1) / 2;
+    if (n < 1 || n > 65535 || i0 < 0 || ipanel < 1 || i0 + ipanel > n || k0 < 0 || k0 > i0 ||
+        ldg < ((long long)n - k0) * n) {
+        set_error(PHF_ERR_ARG, "launch_ek_sym_panel: panel outside the index range or a short Gram block");
+        return PHF_ERR_ARG;
+    }
+    const long long nn = n, t0 = (long long)i0 * nn - (long long)i0 * (i0 - 1) / 2;
+    ProfScope prof(st, PROF_MEMORY);
+    ek_sym_panel_kernel<<<(unsigned)rows_s, 256, 0, st>>>(n, i0, k0, pairs, t0, G, ldg, EKs, EKa);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int launch_gather_kin_sym(int n, int b, const int *pairs, const zc *rho, zc *Kin, long long ldk, cudaStream_t st) {
+    ProfScope prof(st, PROF_MEMORY);
+    gather_kin_sym_kernel<<<grid_for((long long)n * (n + 1) / 2 * b * 4), NT, 0, st>>>(n, b, pairs, rho, Kin, ldk);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *EKp, long long lde, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     ek_panel_kernel<<<(unsigned)((long long)ipanel * n), NT, 0, st>>>(n, G, ldg, EKp, lde);
@@ -586,10 +690,10 @@ int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *E
 
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
-                          cudaStream_t st) {
+                          cudaStream_t st, int ksym) {
     ProfScope prof(st, PROF_MEMORY);
     assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, ldj, Jr, jrs, jcs, Kc, ldk, Kr, krs, kcs,
-                                                                    Gam);
+                                                                    Gam, ksym);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -103,3 +103,29 @@ def test_pbarhbarolap_rejects_options_before_any_device_call():
     assert call(ncisp=2) == _lib.PHF_ERR_ARG      # ncisp must be 2 qj + 1
     assert call(ncik=3) == _lib.PHF_ERR_ARG
     assert call(nocc=8) == _lib.PHF_ERR_ARG        # no virtual orbitals
+
+
+def test_plan_rejects_exchange_options_before_any_device_call():
+    """exchange_symmetry outside 0..2 and a negative exchange_panel are argument errors of
+    phf_plan_create, found before the device is touched (the pointers are never dereferenced)."""
+    import ctypes
+
+    lib = _lib.load()
+    ng = (ctypes.c_int * 2)(1, 1)
+
+    def create(**kw):
+        d = _lib.phf_plan_desc()
+        d.nso, d.nocc, d.nchol, d.npg, d.nci, d.ncisp, d.ncipg, d.cmplxconj, d.sp = 8, 2, 3, 1, 1, 1, 1, 1, 1
+        d.ngrid = ctypes.cast(ng, ctypes.c_void_p)
+        for f in ("h", "bvec", "ref", "r1", "r2", "rpg", "weightsp", "weightpg", "roota", "rootb", "rooty"):
+            setattr(d, f, 8)
+        d.jk_form = 3
+        for k, v in kw.items():
+            setattr(d, k, v)
+        h = ctypes.c_void_p()
+        return lib.phf_plan_create(ctypes.byref(d), ctypes.byref(h))
+
+    assert create(exchange_symmetry=3) == _lib.PHF_ERR_ARG
+    assert b"exchange_symmetry" in lib.phf_last_error()
+    assert create(exchange_symmetry=-1) == _lib.PHF_ERR_ARG
+    assert create(exchange_panel=-1) == _lib.PHF_ERR_ARG

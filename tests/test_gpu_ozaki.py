@@ -115,9 +115,11 @@ def test_int8_pipeline_matches_fp64_on_ragged_sizes(n, N, L):
 def test_automatic_form_above_n128_streamed_matches_fp64_factorized(n):
     """Above n = 128 the automatic J/K form is the streamed one (no n^4 matrix; n = 130: panels of
     the 16900 x 16900 exchange matrix regenerated from the Cholesky vectors) in every precision; it
-    must agree with the rank-N factorized FP64 form, which shares none of its exchange arithmetic.  At
-    n = 170 (k = n^2 = 28900) each panel's exchange GEMM needs two launches for exact int32 group
-    sums, the second adding into Gamma."""
+    must agree with the rank-N factorized FP64 form, which shares none of its exchange arithmetic.  The
+    automatic streamed form uses the exchange symmetry (pairs i <= k and i < k, k = n(n+1)/2 and
+    n(n-1)/2); the full exchange rows (exchange_symmetry off) are checked too: at n = 170 (k = n^2 =
+    28900) each of their panels' exchange GEMMs needs two launches for exact int32 group sums, the
+    second adding into Gamma."""
     import torch
 
     from phf_pcc_b200 import synth
@@ -129,10 +131,13 @@ def test_automatic_form_above_n128_streamed_matches_fp64_factorized(n):
                roota=kw["roota"], rootb=kw["rootb"], rooty=kw["rooty"], qj=kw["QJ"], sp=kw["SP"])
     C = torch.from_numpy(p.C).cuda()
     res = {}
-    for label, prec, form in (("fact", "fp64", "factorized"), ("fp64", "fp64", "auto"), ("i8", "ozaki_i8", "auto")):
-        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, jk_form=form, **akw) as plan:
+    for label, prec, form, sym in (("fact", "fp64", "factorized", "auto"), ("fp64", "fp64", "auto", "auto"),
+                                   ("i8", "ozaki_i8", "auto", "auto"), ("fp64 full", "fp64", "auto", False),
+                                   ("i8 full", "ozaki_i8", "auto", False)):
+        with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision=prec, jk_form=form, exchange_symmetry=sym,
+                      **akw) as plan:
             res[label] = [t.cpu().numpy() for t in plan.eval_device(C)]
         torch.cuda.empty_cache()
-    for label, rel in (("fp64", 1e-11), ("i8", 1e-9)):
+    for label, rel in (("fp64", 1e-11), ("i8", 1e-9), ("fp64 full", 1e-11), ("i8 full", 1e-9)):
         for a, b, what in zip(res[label], res["fact"], ("HS", "Yg", "Yr")):
             assert _close(a, b, rel), (label, what, float(np.abs(a - b).max()))

@@ -310,12 +310,13 @@ TRAFFIC = {
                          "DRAM read + write of the K launch (4096 x 25600 x 4096, the whole 3200-point chunk, wide "
                          "MMA issue) from an ncu capture of this workload; algorithmic bytes of that "
                          "launch: A slices 84 MB + B slices 524 MB + FP64 output 839 MB = 1.45e9"),
-    ("c5", "ozaki_i8"): (81.5e9,
-                         "DRAM read + write of one exchange-panel GEMM of the benchmark's panels (7800 x 25600 x "
-                         "40000, 39 index rows i, two k passes), scaled by the columns (points) from an ncu capture "
-                         "of the same panel on a 384-point grid (9.78 GB for 7800 x 3072 x 40000); algorithmic "
-                         "bytes of the full launch: A slices 1.56 GB + B slices 5.12 GB + FP64 output 1.60 GB "
-                         "= 8.3e9"),
+    ("c5", "ozaki_i8"): (39.0e9,
+                         "DRAM read + write of the first panel's symmetric exchange GEMM (7059 pair rows x 25600 x "
+                         "20100, the exchange symmetry's largest launch), scaled by the columns (points) from an ncu "
+                         "capture of the same panel on a 384-point grid (4.68 GB for 7059 x 3072 x 20100; an upper "
+                         "estimate, the A-slice reads do not grow with the columns); algorithmic bytes of the full "
+                         "launch: A slices 0.71 GB + B slices 2.58 GB + FP64 output at both mirror positions "
+                         "2.89 GB = 6.2e9"),
 }
 
 

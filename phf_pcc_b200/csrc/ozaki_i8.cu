@@ -279,29 +279,37 @@ __device__ __forceinline__ void store_row_chunk(const OzArgs &args, double *Dz, 
         }
         const bool mirror = args.gamma_mode != 0 && i != k;
         const bool acc_both = add || args.gamma_mode == 2;
+        double2 *const G2 = reinterpret_cast<double2 *>(Dz);
+        // element (column pair q) of the chunk: Gamma_w[2i + sg][2k + tu] and its mirror [2k + sg][2i + tu]
+        auto at = [&](int col, bool mir) {
+            const int w = col >> 3, sg = (col >> 2) & 1, tu = (col >> 1) & 1;
+            return mir ? G2 + ((long long)w * M + 2 * k + sg) * M + 2 * i + tu
+                       : G2 + ((long long)w * M + 2 * i + sg) * M + 2 * k + tu;
+        };
+        // Accumulating stores read Gamma first: each batch of eight column pairs issues all its loads
+        // before its stores (the addresses of distinct columns, and of an element and its mirror, never
+        // coincide), so that the loads' latencies overlap instead of following one another.
 #pragma unroll
-        for (int j = 0; j < 32; j += 2) {
-            const int col = col0 + j;
-            if (col < args.n) {
-                const int w = col >> 3, sg = (col >> 2) & 1, tu = (col >> 1) & 1;
-                double2 *g = reinterpret_cast<double2 *>(Dz) + ((long long)w * M + 2 * i + sg) * M + 2 * k + tu;
-                const double2 u = make_double2(acc[j] * rowscale * cs[j], acc[j + 1] * rowscale * cs[j + 1]);
-                double2 v = make_double2(-u.x, -u.y);
-                if (acc_both) {
-                    const double2 o = *g;
-                    v.x = o.x + v.x;
-                    v.y = o.y + v.y;
+        for (int jb = 0; jb < 32; jb += 16) {
+            double2 og[8], oh[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int col = col0 + jb + 2 * q;
+                og[q] = oh[q] = make_double2(0.0, 0.0);
+                if (acc_both && col < args.n) {
+                    og[q] = *at(col, false);
+                    if (mirror) oh[q] = *at(col, true);
                 }
-                *g = v;
-                if (mirror) {
-                    double2 *h = reinterpret_cast<double2 *>(Dz) + ((long long)w * M + 2 * k + sg) * M + 2 * i + tu;
-                    double2 t = args.gamma_mode == 2 ? u : make_double2(-u.x, -u.y);
-                    if (acc_both) {
-                        const double2 o = *h;
-                        t.x = o.x + t.x;
-                        t.y = o.y + t.y;
-                    }
-                    *h = t;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int j = jb + 2 * q, col = col0 + j;
+                if (col < args.n) {
+                    const double2 u = make_double2(acc[j] * rowscale * cs[j], acc[j + 1] * rowscale * cs[j + 1]);
+                    *at(col, false) = make_double2(og[q].x - u.x, og[q].y - u.y);
+                    if (mirror)
+                        *at(col, true) = args.gamma_mode == 2 ? make_double2(oh[q].x + u.x, oh[q].y + u.y)
+                                                              : make_double2(oh[q].x - u.x, oh[q].y - u.y);
                 }
             }
         }

@@ -270,6 +270,18 @@ int phf_ozaki_dgemm(int m, int n, int k, int slices, const double *dA, long long
 int phf_tc_dgemm(int m, int n, int k, int precision, int slices, const double *dA, long long lda, const double *dBt,
                  long long ldb, double *dD, long long ldd, void *stream);
 
+/* Inverse, determinant and log-determinant of `batch` complex n x n matrices (interleaved re/im
+ * doubles, row-major, matrix b at dS + 2 n^2 b), the step inside every grid point of BuildHSG: it
+ * replaces InvertC (ZGETRF + ZGETRI) and determinantC (ZGETRF), PHF_fort/Wrappers.f90:195-336, as
+ * RDM calls them (PHF_fort/PHFTools.f90:259-260).  FP64 Gauss-Jordan elimination with partial
+ * pivoting on |re| + |im| (the pivots of LU with partial pivoting), n <= 112.  dSinv as dS; ddet and
+ * dlogdet hold one complex each per matrix (log det = log|det| + i arg, arg in (-pi, pi]); dflag is
+ * one device int the call overwrites.  A singular matrix returns PHF_ERR_SINGULAR and a non-finite
+ * entry PHF_ERR_NONFINITE, with that matrix's outputs zeroed (det 0, log det -inf).  Device
+ * pointers; synchronous on `stream`. */
+int phf_overlap_inverse(int n, int batch, const double *dS, double *dSinv, double *ddet, double *dlogdet, int *dflag,
+                        void *stream);
+
 /* The same product as phf_ozaki_dgemm for callers that cannot allocate device memory at the
  * point of the call: programs whose device memory belongs to another allocator (a framework's
  * caching pool, or a fixed arena reserved at start-up, where a cudaMalloc of this library's own

@@ -87,6 +87,7 @@ SIGNATURES = {
     "phf_ozaki_dgemm_noalloc": (_I, [_I, _I, _I, _I, _P, ctypes.c_longlong, _P, ctypes.c_longlong, _P,
                                      ctypes.c_longlong, _P]),
     "phf_ozaki_dgemm_noalloc_scratch_bytes": (ctypes.c_size_t, [_I, _I, _I, _I]),
+    "phf_overlap_inverse": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "phf_profile_read": (_I, [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 

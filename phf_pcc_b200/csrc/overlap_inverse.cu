@@ -155,6 +155,207 @@ __global__ void __launch_bounds__(GJ_T *GJ_T) gj_inverse_kernel(int N, const zc 
     }
 }
 
+// 32 < N <= 100: the matrix held in registers.  A CTA of R x C threads (R = ceil(N / MR),
+// C = ceil(N / MC)) per grid point; thread (r, c) keeps the MR x MC elements of rows r + R m and
+// columns c + C q for the whole elimination, so a step reads and writes no matrix element through
+// shared memory: only the pivot column (N values), the scaled pivot row (N values) and one
+// candidate per thread row pass through it, with two barriers per step.
+//
+// Rows are not interchanged.  Step k takes as pivot the eligible row p (not pivoted before) of
+// maximal |re| + |im| in column k; ties go to the row that the interchanging form would hold at the
+// lowest position, so the pivot sequence, the interchange count and every element update are those of
+// gj_inverse_kernel (the positions are tracked in shared memory: pos[row], row_at[position]).  With
+// p_k the pivot row of step k, the stored result E satisfies E[p_j][k] = inv(S)[j][p_k], which the
+// write-out undoes: element (row, col) goes to inv(S)[step_of_row[row]][piv_row[col]].
+constexpr int GR_NMAX = 128;  // bound of the shared pivot arrays
+
+template <int MR, int MC, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
+    gj_inverse_reg_kernel(int N, int R, int C, const zc *__restrict__ S, long long s_rs, long long s_bs,
+                          zc *__restrict__ Sinv, long long i_rs, long long i_bs, zc *__restrict__ det,
+                          zc *__restrict__ logdet, int *__restrict__ flag) {
+    // The thread grid covers rows 0 .. R MR - 1 and columns 0 .. C MC - 1; the entries outside the
+    // N x N matrix are zero and stay zero (their column entries and pivot-row entries are zero in
+    // every step before step N), are never taken as pivots before step N (value 0, and positions
+    // above every row of the matrix), and are not written out.  So no update needs a bounds test.
+    // colk alternates between two buffers by step parity: step k's column is still read in the update
+    // phase after the second barrier, while the owners of column k + 1 may already publish theirs
+    __shared__ zc rowk[GR_NMAX], colk2[2][GR_NMAX], pivs[GR_NMAX];
+    __shared__ int pos[GR_NMAX], row_at[GR_NMAX], step_of_row[GR_NMAX], piv_row[GR_NMAX];
+    __shared__ double cand_v[32];
+    __shared__ int cand_pos[32], cand_row[32];
+    __shared__ int s_bad;
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    const bool own = tid < R * C;
+    const int r = own ? tid / C : 0, c = own ? tid - (tid / C) * C : 0;
+    const int nrow = R * MR;
+    const long long b = blockIdx.x;
+    const zc *Sb = S + b * s_bs;
+    if (tid == 0) s_bad = 0;
+    for (int i = tid; i < nrow; i += blockDim.x) {
+        pos[i] = i;
+        row_at[i] = i;
+    }
+    __syncthreads();
+    zc a[MR][MC];
+#pragma unroll
+    for (int m = 0; m < MR; ++m)
+#pragma unroll
+        for (int q = 0; q < MC; ++q) {
+            const int row = r + R * m, col = c + C * q;
+            zc v = mkz(0.0, 0.0);
+            if (own && row < N && col < N) {
+                v = Sb[(long long)row * s_rs + col];
+                if (!isfinite(v.x) || !isfinite(v.y)) s_bad = 2;
+            }
+            a[m][q] = v;
+        }
+    __syncthreads();
+
+    int nswap = 0;  // kept by thread 0
+    for (int k = 0; k < N && s_bad == 0; ++k) {
+        zc *colk = colk2[k & 1];
+        // (A) the owners of column k (slot q with c + C q == k: one q at most) publish it, then pick
+        // their best eligible row from the published values
+        bool owner = false;
+#pragma unroll
+        for (int q = 0; q < MC; ++q) {
+            if (own && c + C * q == k) {
+                owner = true;
+#pragma unroll
+                for (int m = 0; m < MR; ++m) colk[r + R * m] = a[m][q];
+            }
+        }
+        if (owner) {
+            double best = -1.0;
+            int bpos = GR_NMAX, brow = -1;
+            for (int row = r; row < nrow; row += R) {
+                const int ps = pos[row];
+                if (ps >= k) {
+                    const double av = abs1(colk[row]);
+                    if (av > best || (av == best && ps < bpos)) {
+                        best = av;
+                        bpos = ps;
+                        brow = row;
+                    }
+                }
+            }
+            cand_v[r] = best;
+            cand_pos[r] = bpos;
+            cand_row[r] = brow;
+        }
+        __syncthreads();
+        // (B) every warp reduces the R candidates: maximal value, then lowest position
+        double pv = lane < R ? cand_v[lane] : -1.0;
+        int pp = lane < R ? cand_pos[lane] : GR_NMAX;
+        int p = lane < R ? cand_row[lane] : -1;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, pv, off);
+            const int op = __shfl_xor_sync(0xffffffffu, pp, off);
+            const int orow = __shfl_xor_sync(0xffffffffu, p, off);
+            if (ov > pv || (ov == pv && op < pp)) {
+                pv = ov;
+                pp = op;
+                p = orow;
+            }
+        }
+        if (!(pv > 0.0)) {  // exactly singular (or NaN pivot): every thread leaves at the same step
+            if (tid == 0) s_bad = (pv == 0.0) ? 1 : 2;
+            break;
+        }
+        const zc piv = colk[p];
+        if (own && r == p % R) {  // the owners of row p write the scaled pivot row
+            const zc inv = divz(mkz(1.0, 0.0), piv);
+            const int mp = p / R;
+#pragma unroll
+            for (int m = 0; m < MR; ++m)
+                if (m == mp) {
+#pragma unroll
+                    for (int q = 0; q < MC; ++q) {
+                        const int col = c + C * q;
+                        rowk[col] = (col == k) ? inv : a[m][q] * inv;
+                    }
+                }
+        }
+        if (tid == 0) {  // pivots (det and log det are formed from them at the end) and the positions
+            pivs[k] = piv;
+            if (pp != k) {
+                ++nswap;
+                const int q = row_at[k];
+                row_at[pp] = q;
+                pos[q] = pp;
+                row_at[k] = p;
+                pos[p] = k;
+            }
+            step_of_row[p] = k;
+            piv_row[k] = p;
+        }
+        __syncthreads();
+        // (C) rank-1 update of the register-resident elements
+        if (own) {
+            zc rk[MC];
+#pragma unroll
+            for (int q = 0; q < MC; ++q) rk[q] = rowk[c + C * q];
+#pragma unroll
+            for (int m = 0; m < MR; ++m) {
+                if (r + R * m == p) {
+#pragma unroll
+                    for (int q = 0; q < MC; ++q) a[m][q] = rk[q];
+                } else {
+                    const zc ci = colk[r + R * m];
+#pragma unroll
+                    for (int q = 0; q < MC; ++q) {
+                        const zc x = (c + C * q == k) ? mkz(0.0, 0.0) : a[m][q];
+                        a[m][q] = x - ci * rk[q];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int bad = s_bad;
+    zc *Ib = Sinv + b * i_bs;
+    if (own) {
+#pragma unroll
+        for (int m = 0; m < MR; ++m)
+#pragma unroll
+            for (int q = 0; q < MC; ++q) {
+                const int row = r + R * m, col = c + C * q;
+                if (row < N && col < N) {
+                    if (bad)
+                        Ib[(long long)row * i_rs + col] = mkz(0.0, 0.0);
+                    else
+                        Ib[(long long)step_of_row[row] * i_rs + piv_row[col]] = a[m][q];
+                }
+            }
+    }
+    if (tid == 0) {
+        if (bad) {
+            det[b] = mkz(0.0, 0.0);
+            logdet[b] = mkz(-INFINITY, 0.0);
+            atomicOr(flag, bad);
+        } else {
+            // det = (-1)^{#interchanges} prod(pivots), the product and sums taken in pivot order
+            zc d = mkz(1.0, 0.0);
+            double logabs = 0.0, phase = 0.0;
+            for (int k = 0; k < N; ++k) {
+                const zc piv = pivs[k];
+                d = d * piv;
+                logabs += log(hypot(piv.x, piv.y));
+                phase += atan2(piv.y, piv.x);
+            }
+            if (nswap & 1) d = mkz(-d.x, -d.y);
+            det[b] = d;
+            const double pi = 3.14159265358979323846;
+            double ph = fmod(phase + pi * (nswap & 1), 2.0 * pi);
+            if (ph > pi) ph -= 2.0 * pi;
+            if (ph <= -pi) ph += 2.0 * pi;
+            logdet[b] = mkz(logabs, ph);
+        }
+    }
+}
 
 // N <= 32: one warp per matrix (lane j owns column j), four matrices per CTA.  The same
 // Gauss-Jordan steps as gj_inverse_kernel -- pivot = first index of the largest |re| + |im| in rows
@@ -331,6 +532,23 @@ int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_b
         PHF_CHECK_LAUNCH();
         return PHF_OK;
     }
+    if (N <= 100) {
+        // register-resident elimination: MR x MC elements per thread, R x C <= 512 threads, R <= 32
+        const bool small = N <= 64;
+        const int MR = small ? 4 : 5, MC = 4;
+        const int R = (N + MR - 1) / MR, C = (N + MC - 1) / MC;
+        const unsigned threads = (unsigned)((R * C + 31) / 32 * 32);
+        ProfScope prof(st, PROF_INVERSE);
+        if (small)
+            gj_inverse_reg_kernel<4, 4, 256, 2><<<batch, threads, 0, st>>>(N, R, C, S, s_rs, s_bs, Sinv, i_rs, i_bs,
+                                                                            det, logdet, flag);
+        else
+            gj_inverse_reg_kernel<5, 4, 512, 1><<<batch, threads, 0, st>>>(N, R, C, S, s_rs, s_bs, Sinv, i_rs, i_bs,
+                                                                            det, logdet, flag);
+        ++g_launches;
+        PHF_CHECK_LAUNCH();
+        return PHF_OK;
+    }
     size_t smem = overlap_inverse_smem(N);
     PHF_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ProfScope prof(st, PROF_INVERSE);
@@ -341,3 +559,37 @@ int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_b
 }
 
 }  // namespace phf
+
+extern "C" int phf_overlap_inverse(int n, int batch, const double *dS, double *dSinv, double *ddet, double *dlogdet,
+                                   int *dflag, void *stream) {
+    using namespace phf;
+    set_error(PHF_OK, "");
+    if (n <= 0 || batch <= 0 || !dS || !dSinv || !ddet || !dlogdet || !dflag) {
+        set_error(PHF_ERR_ARG, "phf_overlap_inverse: bad sizes or null pointer");
+        return PHF_ERR_ARG;
+    }
+    if (n > 112) {  // the shared-memory form holds n^2 complex per CTA
+        set_error(PHF_ERR_UNSUPPORTED, "phf_overlap_inverse: n above the inverse's limit of 112");
+        return PHF_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const long long nn = (long long)n * n;
+    PHF_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), st));
+    PHF_TRY(overlap_inverse(n, batch, reinterpret_cast<const zc *>(dS), n, nn, reinterpret_cast<zc *>(dSinv), n, nn,
+                            reinterpret_cast<zc *>(ddet), reinterpret_cast<zc *>(dlogdet), dflag, st));
+    int flag = 0;
+    PHF_CUDA(cudaMemcpyAsync(&flag, dflag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        set_error(PHF_ERR_CUDA, "stream synchronize failed");
+        return PHF_ERR_CUDA;
+    }
+    if (flag & 1) {
+        set_error(PHF_ERR_SINGULAR, "phf_overlap_inverse: an exactly singular matrix");
+        return PHF_ERR_SINGULAR;
+    }
+    if (flag & 2) {
+        set_error(PHF_ERR_NONFINITE, "phf_overlap_inverse: a non-finite entry");
+        return PHF_ERR_NONFINITE;
+    }
+    return PHF_OK;
+}

@@ -517,6 +517,15 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         PHF_CUDA(cudaMemcpy(p.h, hh.data(), hh.size() * sizeof(double), cudaMemcpyHostToDevice));
         PHF_CUDA(cudaMemcpy(p.Bst, Bst.data(), Bst.size() * sizeof(double), cudaMemcpyHostToDevice));
         if (p.eri) PHF_TRY(build_exchange_matrix(p));
+        // exchange-matrix forms: with h exactly symmetric (H1 = H1^H), H1 is added to Gamma where J is,
+        // so one product gives F X = (H1 + J - K) X and e1 = tr(bra^H H1 X) = sum conj(H1 bra) X
+        p.fold_h = p.eri;
+        for (int i = 0; i < n && p.fold_h; ++i)
+            for (int j = 0; j < i; ++j)
+                if (hh[(size_t)i * n + j] != hh[(size_t)j * n + i]) {
+                    p.fold_h = false;
+                    break;
+                }
     } else {
         std::vector<cd> h1(MM);
         for (int i = 0; i < M; ++i)
@@ -556,8 +565,8 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
     PHF_TRY(p.arena.alloc(&p.compHS, 2 * nslot));
     PHF_TRY(p.arena.alloc(&p.tmpG, MN));
     PHF_TRY(p.arena.alloc(&p.outMM, 2 * nslot * MM));  // every slot's Gradmat and Rdmmat block
+    if (p.exact || p.fold_h) PHF_TRY(p.arena.alloc(&p.Hb, MN));
     if (p.exact) {
-        PHF_TRY(p.arena.alloc(&p.Hb, MN));
         PHF_TRY(p.arena.alloc(&p.accKG, nslot * MN));
         PHF_TRY(p.arena.alloc(&p.compKG, nslot * MN));
         PHF_TRY(p.arena.alloc(&p.accKR, nslot * MN));
@@ -614,7 +623,7 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
         PHF_TRY(p.arena.alloc(&p.Prk, bMN));
         PHF_TRY(p.arena.alloc(&p.Prk2, bMN));
     }
-    PHF_TRY(p.arena.alloc(&p.HX, bMN));
+    if (!p.fold_h) PHF_TRY(p.arena.alloc(&p.HX, bMN));
     PHF_TRY(p.arena.alloc(&p.GX, bMN));
     {
         unsigned char *sc = nullptr;
@@ -1055,7 +1064,7 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         }
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_assemble_gamma(n, bc, p.Jvec, b, nullptr, 0, 0, p.Kvec, 4LL * b, nullptr, 0, 0, p.Gam, st,
-                                      p.ek_sym));
+                                      p.ek_sym, p.fold_h ? p.h : nullptr));
     } else {
         // K (as K^T, 8 bc x n^2) written by the GEMM epilogue as -K into Gamma's complex M x M blocks
         if (p.streamed)
@@ -1065,11 +1074,14 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
                               reinterpret_cast<double *>(p.Gam), 0, 0, 0, p.ozerr, st, n));
         if (fork) PHF_CUDA(cudaStreamWaitEvent(st, p.ev_join, 0));  // the Coulomb chain is done
         prof_set_class(PROF_GEMM);
-        PHF_TRY(launch_add_coulomb_diag(n, bc, p.Jr, 1, n2, p.Gam, st));
+        PHF_TRY(launch_add_coulomb_diag(n, bc, p.Jr, 1, n2, p.Gam, st, p.fold_h ? p.h : nullptr));
     }
     PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
                           st));
-    PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, p.HX));  // then GX <- HX + Gamma X
+    if (p.fold_h)  // GX = F X: e2 = tr(bra^H F X) / 2 - e1 / 2
+        PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, nullptr, p.e1, 0.5));
+    else
+        PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, p.HX));  // then GX <- HX + Gamma X
     return PHF_OK;
 }
 
@@ -1083,7 +1095,7 @@ int ket_side(PlanImpl &p, int v, int bc, int w0, cudaStream_t st) {
                           nullptr, st));
     PHF_TRY(zgemm_strided(M, N, N, bc, 1, ZM1, vz(p.bra, N, 1), vz(p.W, 1, ld, N, 0, 1), Z1, vo(p.Vk, ld, 1, N),
                           nullptr, st));
-    PHF_TRY(launch_ket_prep(M, N, bc, p.Hb, p.bra, p.e1, p.e2, p.Vk, ld, st));
+    PHF_TRY(launch_ket_prep(M, N, bc, p.fold_h ? nullptr : p.Hb, p.bra, p.e1, p.e2, p.Vk, ld, st));
     PHF_TRY(zgemm_strided(M, N, N, bc, 1, Z1, vz(p.Vk, ld, 1, N), vz(p.Sinv, 1, ld, N, 0, 1), Z0, vo(p.Pk, ld, 1, N),
                           nullptr, st));
     PHF_TRY(zgemm_strided(M, N, N, bc, 1, Z1, vz(p.bra, N, 1), vz(p.Sinv, 1, ld, N, 0, 1), Z0, vo(p.Prk, ld, 1, N),
@@ -1119,7 +1131,7 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
     const long long ld2 = (long long)p.ny * p.npg * N;  // T2 column-blocked: T2[r][(iy npg + ig) N + j]
     PHF_TRY(zgemm_strided(M, N, M, p.npg, p.ny, Z1, vz(p.R2, M, 1, 0, MM), vz(p.T1, N, 1, MN, 0), Z0,
                           vo(p.T2, ld2, 1, N, (long long)p.npg * N), nullptr, st));
-    if (p.exact)  // H1 bra (Cholesky forms: h applied to both spin rows of the interleaved order)
+    if (p.exact || p.fold_h)  // H1 bra (Cholesky forms: h applied to both spin rows of the interleaved order)
         PHF_TRY(zgemm_strided(n, 2 * N, n, 1, 1, Z1, vd(p.h, n, 1), vz(p.bra, 2 * N, 1), Z0, vo(p.Hb, 2 * N, 1), nullptr,
                               st));
     if (p.chol && !p.eri) {
@@ -1155,12 +1167,14 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
                               st));
         // HX and e1 = tr(bra^H H1 X)
         // (Cholesky form: X viewed as n x (2 ld) with spin sigma at column offset sigma*ld, batched over sigma)
-        if (p.chol)
+        if (p.fold_h)  // H1 is part of Gamma: no HX; e1 = sum conj(H1 bra) X (H1 symmetric)
+            PHF_TRY(launch_trace_conj(M, N, bc, p.Hb, p.Xs, ld, p.e1, 1.0, st));
+        else if (p.chol)
             PHF_TRY(zgemm_strided(n, bc * N, n, 2, 1, Z1, vd(p.h, n, 1), vz(p.Xs, 2 * ld, 1, ld), Z0,
                                   vo(p.HX, 2 * ld, 1, ld), nullptr, st));
         else
             PHF_TRY(zgemm_strided(M, bc * N, M, 1, 1, Z1, vz(p.H1, M, 1), vz(p.Xs, ld, 1), Z0, vo(p.HX, ld, 1), nullptr, st));
-        PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.HX, ld, p.e1, 1.0, st));
+        if (!p.fold_h) PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.HX, ld, p.e1, 1.0, st));
         // Gamma(rho_w) X_w and e2
         if (p.chol && p.eri) {
             PHF_TRY(gamma_x_eri(p, bc, st));

@@ -94,11 +94,14 @@ int overlap_inverse(int N, int batch, const zc *S, long long s_rs, long long s_b
 // phf_kernels.cu
 int launch_tprime(int Ltot, int N, int b, zc *T, long long ldT, zc *e2part, cudaStream_t st);
 int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cudaStream_t st);
-// out[w] = scale tr(C^H X_w); with `add`, X_w <- X_w + add_w afterwards (same layout as X)
+// out[w] = scale tr(C^H X_w) (minus sub_scale sub[w] with `sub`); with `add`, X_w <- X_w + add_w
+// afterwards (same layout as X)
 int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale,
-                      cudaStream_t st, const zc *add = nullptr);
+                      cudaStream_t st, const zc *add = nullptr, const zc *sub = nullptr, double sub_scale = 0.0);
 int launch_add_inplace(int M, int N, int b, const zc *A, zc *G, long long ldX, cudaStream_t st);
-int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st);
+// Gamma's diagonal spin blocks += J (+ h, the one-electron matrix, when given)
+int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st,
+                            const double *h = nullptr);
 int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, const zc *T2, long long ld2, zc *Ys,
                         long long ld, cudaStream_t st);
 int launch_epilogue(int M, int N, int b, zc *G, zc *X, long long ldX, const zc *det, const zc *e1,
@@ -128,7 +131,7 @@ int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *E
 int launch_bra_rho_operand(int M, int N, const zc *bra, double *out, cudaStream_t st);
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
-                          cudaStream_t st, int ksym = 0);
+                          cudaStream_t st, int ksym = 0, const double *h = nullptr);
 // symmetric exchange form, FP64: the panel's symmetric rows EKs (rows_s x n(n+1)/2) and antisymmetric
 // rows EKa (x n(n-1)/2) from its Gram block (as oz_slice_ek_sym_panel), and Kin's symmetric rows (pair_le
 // order) followed by its antisymmetric rows (pair_lt order) from the dense densities
@@ -246,6 +249,7 @@ struct PlanImpl {
     int *slotmap = nullptr;                            // 4 x nb^2
     int *permdev = nullptr;                            // 2M: [0,M) working->reference, [M,2M) reference->working
     double *h = nullptr, *Bst = nullptr;               // Cholesky form
+    bool fold_h = false;  // exchange-matrix forms with an exactly symmetric h: Gamma holds H1 + J - K
     zc *H1 = nullptr, *H2r = nullptr;                  // dense form
     // per evaluation
     zc *bra = nullptr, *ket = nullptr, *kety = nullptr, *newmo = nullptr, *newmoc = nullptr;

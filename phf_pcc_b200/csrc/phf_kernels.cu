@@ -58,9 +58,10 @@ __global__ void __launch_bounds__(NT) rowsum_kernel(int ncols, const zc *in, zc 
     if (threadIdx.x == 0) out[r] = scale * s;
 }
 
-// out[w] = scale * sum_{r,j} conj(C[r*N + j]) * X[r*ldX + w*N + j]   (tr(C^H X_w))
+// out[w] = scale * sum_{r,j} conj(C[r*N + j]) * X[r*ldX + w*N + j]   (tr(C^H X_w)), minus
+// sub_scale * sub[w] when `sub` is given
 __global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *C, zc *X, long long ldX, zc *out,
-                                                        double scale, const zc *add) {
+                                                        double scale, const zc *add, const zc *sub, double sub_scale) {
     __shared__ zc sh[NT];
     const long long w = blockIdx.x;
     zc s = mkz(0, 0);
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(NT) trace_conj_kernel(int M, int N, const zc *
         if (add) X[o] = x + add[o];  // X <- X + add once the trace has read X
     }
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) out[w] = scale * s;
+    if (threadIdx.x == 0) out[w] = sub ? scale * s - sub_scale * sub[w] : scale * s;
 }
 
 // Energy/gradient epilogue over a chunk of b grid points (Gradient, PHFTools.f90:291-308, in
@@ -276,7 +277,7 @@ __global__ void gather_kin_kernel(int n, int b, const zc *rho, zc *Kin, long lon
 //    K[i][k] = KS + KA for i < k, KS - KA for i > k, KS for i = k.
 __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs,
                                       long long jcs, const zc *Kc, long long ldk, const double *Kr, long long krs,
-                                      long long kcs, zc *Gam, int ksym) {
+                                      long long kcs, zc *Gam, int ksym, const double *h) {
     const int M = 2 * n;
     const long long tot = (long long)M * M * b;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
@@ -305,12 +306,14 @@ __global__ void assemble_gamma_kernel(int n, int b, const zc *J, long long ldj, 
         if (sg == tu) {
             if (J) g = g + J[ik * ldj + w];
             else g = g + mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
+            if (h) g.x += h[ik];
         }
         Gam[e] = g;
     }
 }
 
-// ket-side gradient: V_w += H1 C + conj(h_w) C   (V already holds Gamma_w^H C - C W_w^H)
+// ket-side gradient: V_w += H1 C + conj(h_w) C   (V already holds Gamma_w^H C - C W_w^H; Hb = H1 C is
+// null when Gamma holds H1 + J - K, whose adjoint already brought H1 C in)
 __global__ void ket_prep_kernel(int M, int N, int b, const zc *Hb, const zc *bra, const zc *e1, const zc *e2, zc *V,
                                 long long ld) {
     const long long total = (long long)M * b * N;
@@ -318,7 +321,8 @@ __global__ void ket_prep_kernel(int M, int N, int b, const zc *Hb, const zc *bra
         long long r = e / ((long long)b * N), c = e - r * ((long long)b * N);
         int w = (int)(c / N), j = (int)(c - (long long)w * N);
         zc h = conjz(e1[w] + e2[w]);
-        V[r * ld + c] = V[r * ld + c] + Hb[r * N + j] + h * bra[r * N + j];
+        const zc hb = Hb ? Hb[r * N + j] : mkz(0.0, 0.0);
+        V[r * ld + c] = V[r * ld + c] + hb + h * bra[r * N + j];
     }
 }
 
@@ -358,10 +362,12 @@ __global__ void spin_block_y_kernel(int n, int N, int bc, int w0, int blk, const
     }
 }
 
-// Coulomb term of the tensor-core path: Gamma_w[2i + s][2k + s] += J_w(i, k) for both spins s, with
+// Coulomb term of the tensor-core path: Gamma_w[2i + s][2k + s] += J_w(i, k) (+ h[i][k] with `h`: the
+// one-electron matrix folded in, Gamma becoming the Fock matrix H1 + J - K) for both spins s, with
 // J_w's real and imaginary parts at Jr[ik jrs + (2w) jcs] and Jr[ik jrs + (2w + 1) jcs] (Gamma already
 // holds -K from the exchange GEMM).
-__global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam) {
+__global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam,
+                                        const double *h) {
     const int M = 2 * n;
     const long long nn = (long long)n * n, tot = 2LL * nn * b;
     for (long long e = blockIdx.x * (long long)NT + threadIdx.x; e < tot; e += (long long)gridDim.x * NT) {
@@ -370,7 +376,8 @@ __global__ void add_coulomb_diag_kernel(int n, int b, const double *Jr, long lon
         const long long ik = rem - (long long)sg * nn;
         const int i = (int)(ik / n), k = (int)(ik - (long long)i * n);
         zc *g = Gam + (w * M + 2 * i + sg) * M + 2 * k + sg;
-        const zc jv = mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
+        zc jv = mkz(Jr[ik * jrs + 2 * w * jcs], Jr[ik * jrs + (2 * w + 1) * jcs]);
+        if (h) jv.x += h[ik];
         *g = *g + jv;
     }
 }
@@ -486,9 +493,9 @@ int launch_rowsum(int nrows, int ncols, const zc *in, zc *out, double scale, cud
 }
 
 int launch_trace_conj(int M, int N, int b, const zc *C, zc *X, long long ldX, zc *out, double scale, cudaStream_t st,
-                      const zc *add) {
+                      const zc *add, const zc *sub, double sub_scale) {
     ProfScope prof(st, PROF_MEMORY);
-    trace_conj_kernel<<<b, NT, 0, st>>>(M, N, C, X, ldX, out, scale, add);
+    trace_conj_kernel<<<b, NT, 0, st>>>(M, N, C, X, ldX, out, scale, add, sub, sub_scale);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
@@ -626,9 +633,10 @@ int launch_spin_block_y(int n, int N, int bc, int w0, int blk, const zc *R1b, co
     return PHF_OK;
 }
 
-int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st) {
+int launch_add_coulomb_diag(int n, int b, const double *Jr, long long jrs, long long jcs, zc *Gam, cudaStream_t st,
+                            const double *h) {
     ProfScope prof(st, PROF_MEMORY);
-    add_coulomb_diag_kernel<<<grid_for(2LL * n * n * b), NT, 0, st>>>(n, b, Jr, jrs, jcs, Gam);
+    add_coulomb_diag_kernel<<<grid_for(2LL * n * n * b), NT, 0, st>>>(n, b, Jr, jrs, jcs, Gam, h);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
@@ -690,10 +698,10 @@ int launch_ek_panel(int n, int ipanel, const double *G, long long ldg, double *E
 
 int launch_assemble_gamma(int n, int b, const zc *J, long long ldj, const double *Jr, long long jrs, long long jcs,
                           const zc *Kc, long long ldk, const double *Kr, long long krs, long long kcs, zc *Gam,
-                          cudaStream_t st, int ksym) {
+                          cudaStream_t st, int ksym, const double *h) {
     ProfScope prof(st, PROF_MEMORY);
     assemble_gamma_kernel<<<grid_for(4LL * n * n * b), NT, 0, st>>>(n, b, J, ldj, Jr, jrs, jcs, Kc, ldk, Kr, krs, kcs,
-                                                                    Gam, ksym);
+                                                                    Gam, ksym, h);
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;

@@ -83,6 +83,20 @@ def test_tensor_core_gemm_entries_validate_arguments_before_any_device_call():
     assert lib.phf_tc_dgemm(8, 8, 8, 2, 0, null, 8, p, 8, p, 8, null) == _lib.PHF_ERR_ARG
 
 
+def test_overlap_inverse_validates_arguments_before_any_device_call():
+    """phf_overlap_inverse rejects empty sizes and null pointers (PHF_ERR_ARG) and n above the
+    inverse's limit of 112 (PHF_ERR_UNSUPPORTED) before touching device memory."""
+    import ctypes
+
+    lib = _lib.load()
+    p = ctypes.c_void_p(8)
+    null = ctypes.c_void_p(0)
+    assert lib.phf_overlap_inverse(0, 4, p, p, p, p, p, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_overlap_inverse(8, 0, p, p, p, p, p, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_overlap_inverse(8, 4, p, p, p, p, null, null) == _lib.PHF_ERR_ARG
+    assert lib.phf_overlap_inverse(113, 4, p, p, p, p, p, null) == _lib.PHF_ERR_UNSUPPORTED
+
+
 def test_pbarhbarolap_rejects_options_before_any_device_call():
     """TrunODE outside 1..3 is an error (the reference STOPs) and nso above the inverse's limit is
     refused -- both before device memory is touched."""

@@ -1158,8 +1158,9 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
                                   nullptr, st));
             Y = p.Ys2;
         }
-        // S_w = bra^H Y_w
-        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(Y, ld, 1), Z0, vo(p.S, ld, 1), nullptr,
+        // S_w = bra^H Y_w, formed as its transpose Y^T conj(bra) (bc N rows, N columns: for N <= 112 one
+        // column tile of the FP64 GEMM instead of N rows padded to the row tile)
+        PHF_TRY(zgemm_strided(bc * N, N, M, 1, 1, Z1, vz(Y, 1, ld), vz(p.bra, N, 1, 0, 0, 1), Z0, vo(p.S, 1, ld), nullptr,
                               st));
         PHF_TRY(overlap_inverse(N, bc, p.S, ld, N, p.Sinv, ld, N, p.det, p.logdet, p.flag, st));
         // X_w = Y_w S_w^-1
@@ -1207,8 +1208,8 @@ int run_variant(PlanImpl &p, int v, cudaStream_t st) {
             prof_set_class(PROF_GEMM);
             PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, p.HX));  // then GX <- HX + Gamma X
         }
-        // GX now holds F X = HX + Gamma X:  W = bra^H F X;  GX <- F X - X W
-        PHF_TRY(zgemm_strided(N, bc * N, M, 1, 1, Z1, vz(p.bra, 1, N, 0, 0, 1), vz(p.GX, ld, 1), Z0, vo(p.W, ld, 1),
+        // GX now holds F X = HX + Gamma X:  W = bra^H F X (as its transpose, like S);  GX <- F X - X W
+        PHF_TRY(zgemm_strided(bc * N, N, M, 1, 1, Z1, vz(p.GX, 1, ld), vz(p.bra, N, 1, 0, 0, 1), Z0, vo(p.W, 1, ld),
                               nullptr, st));
         PHF_TRY(zgemm_strided(M, N, N, bc, 1, ZM1, vz(p.Xs, ld, 1, N), vz(p.W, ld, 1, N), Z1, vo(p.GX, ld, 1, N), nullptr,
                               st));

@@ -6,8 +6,9 @@
 // batches need no copies.  A may be real (real x complex products: Cholesky vectors and
 // the one-electron matrix applied to complex orbitals).
 //
-// Tiling: BM x BN output tile per 256-thread CTA (64 x 64, 128 x 32 or 32 x 128), k-step 16; the
-// next k-tile is prefetched into registers while the current one is consumed from shared memory.
+// Tiling: BM x BN output tile per CTA of (BM / 32) (BN / 16) warps (64 x 64, 128 x 32 and 32 x 128 on
+// 8 warps; 32 x 112 on 7 and 64 x 112 on 14 for products with 97..112 output columns, such as the
+// per-point products with N = 100 orbitals), k-step 16, the k-tiles staged by cp.async.
 // The products run on the FP64 tensor cores (mma.sync m8n8k4 .f64): each of the 8 warps owns a
 // 32 x 16 block of the tile as 4 x 2 blocks of 8 x 8, and a complex product is four real MMAs
 // (re re, -im im, re im, im re), two for a real A.
@@ -19,7 +20,12 @@ namespace phf {
 
 namespace {
 
-constexpr int BK = 16, NT = 256;
+constexpr int BK = 16;
+
+template <int BM, int BN>
+__host__ __device__ constexpr int zg_threads() { return (BM / 32) * (BN / 16) * 32; }
+template <int BM, int BN>
+__host__ __device__ constexpr int zg_min_blocks() { return zg_threads<BM, BN>() <= 256 ? 2 : 1; }
 
 template <bool AREAL>
 struct ATile {
@@ -52,10 +58,11 @@ __device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int byte
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes_valid) : "memory");
 }
 
-// Shared-memory stages of the k loop (cp.async pipeline): three for the 64 x 64 tile, two for the
-// narrow tiles (their products are mostly k = 32, two k-tiles; two stages let two CTAs share an SM).
+// Shared-memory stages of the k loop (cp.async pipeline): three for the 64 x 64 and the 112-column
+// tiles, two for the narrow tiles (their products are mostly k = 32, two k-tiles; two stages let two
+// CTAs share an SM).
 template <int BM, int BN>
-__host__ __device__ constexpr int zg_stages() { return BM == BN ? 3 : 2; }
+__host__ __device__ constexpr int zg_stages() { return (BM == BN || BN == 112) ? 3 : 2; }
 
 template <bool AREAL, int BM, int BN>
 constexpr size_t zg_smem_bytes() {
@@ -71,12 +78,15 @@ constexpr size_t zg_smem_bytes() {
 // conjugation is applied when fragments are read.  A real B (only the exchange-matrix build) is
 // loaded with plain loads into the same stages.
 template <bool AREAL, int BM, int BN>
-__global__ void __launch_bounds__(NT, 2) zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B,
-                                                   zc beta, OutView C, const long long *__restrict__ offs) {
+__global__ void __launch_bounds__(zg_threads<BM, BN>(), zg_min_blocks<BM, BN>())
+    zgemm_kernel(int m, int n, int k, int nb0, int ntn, zc alpha, View A, View B, zc beta, OutView C,
+                 const long long *__restrict__ offs) {
     using TA = typename ATile<AREAL>::T;
     constexpr int WARPS_N = BN / 16;
-    static_assert((BM / 32) * WARPS_N * 32 == NT, "tile/warp mismatch");
-    constexpr int LA = (BM * BK) / NT, LB = (BN * BK) / NT;  // elements loaded per thread
+    constexpr int NT = zg_threads<BM, BN>();
+    static_assert(BM % 32 == 0 && BN % 16 == 0, "tile/warp mismatch");
+    // elements loaded per thread and k-tile (the last round partial when NT does not divide the tile)
+    constexpr int LA = (BM * BK + NT - 1) / NT, LB = (BN * BK + NT - 1) / NT;
     constexpr int PA = BM + 1, PB = BN + 1;                    // row pitches (elements)
     constexpr int ZG_STAGES = zg_stages<BM, BN>();
     extern __shared__ __align__(16) unsigned char zg_smem[];
@@ -109,6 +119,7 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(int m, int n, int k, int n
 #pragma unroll
         for (int r = 0; r < LA; ++r) {
             const int e = tid + NT * r;
+            if ((BM * BK) % NT != 0 && e >= BM * BK) break;
             int i, kk;
             if (a_mfast) { i = e % BM; kk = e / BM; }
             else { kk = e % BK; i = e / BK; }
@@ -122,6 +133,7 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(int m, int n, int k, int n
 #pragma unroll
         for (int r = 0; r < LB; ++r) {
             const int e = tid + NT * r;
+            if ((BN * BK) % NT != 0 && e >= BN * BK) break;
             int j, kk;
             if (b_nfast) { j = e % BN; kk = e / BN; }
             else { kk = e % BK; j = e / BK; }
@@ -225,24 +237,28 @@ int launch_tile(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, 
         PHF_CUDA(cudaFuncSetAttribute(zgemm_kernel<true, BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         ProfScope prof(st, -1);
-        zgemm_kernel<true, BM, BN><<<grid, NT, smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+        zgemm_kernel<true, BM, BN><<<grid, zg_threads<BM, BN>(), smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C,
+                                                                             offs);
     } else {
         constexpr size_t smem = zg_smem_bytes<false, BM, BN>();
         PHF_CUDA(cudaFuncSetAttribute(zgemm_kernel<false, BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         ProfScope prof(st, -1);
-        zgemm_kernel<false, BM, BN><<<grid, NT, smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta, C, offs);
+        zgemm_kernel<false, BM, BN><<<grid, zg_threads<BM, BN>(), smem, st>>>(m, n, k, nb0, ntn, alpha, A, B, beta,
+                                                                              C, offs);
     }
     ++g_launches;
     PHF_CHECK_LAUNCH();
     return PHF_OK;
 }
 
-// Tile shape 0 = 64 x 64, 1 = 128 x 32, 2 = 32 x 128.
+// Tile shape 0 = 64 x 64, 1 = 128 x 32, 2 = 32 x 128, 3 = 32 x 112, 4 = 64 x 112.
 int launch_choice(int tile, int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
                   const OutView &C, const long long *offs, cudaStream_t st) {
     if (tile == 1) return launch_tile<128, 32>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
     if (tile == 2) return launch_tile<32, 128>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    if (tile == 3) return launch_tile<32, 112>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
+    if (tile == 4) return launch_tile<64, 112>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
     return launch_tile<64, 64>(m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
 }
 
@@ -250,7 +266,8 @@ int launch_choice(int tile, int m, int n, int k, int nb0, int nb1, zc alpha, con
 
 // The tile comes from the launch tuner's table when the shape was tuned, else from rules set by
 // measurements of the per-point products: 128 x 32 for at most 32 output columns and at least 96
-// rows, 32 x 128 in the transposed case, 64 x 64 otherwise.
+// rows, 32 x 128 in the transposed case, 32 x 112 for 97..112 output columns (one column tile where
+// 64 x 64 would pad 100 columns to 128), 64 x 64 otherwise.
 int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A, const View &B, zc beta,
                   const OutView &C, const long long *offs, cudaStream_t st) {
     if (m <= 0 || n <= 0 || nb0 <= 0 || nb1 <= 0) return PHF_OK;
@@ -261,11 +278,11 @@ int zgemm_strided(int m, int n, int k, int nb0, int nb1, zc alpha, const View &A
     const TuneKey key{0, (long long)m, (long long)n, (long long)k, (long long)nb0 * 65536 + nb1,
                       (long long)(A.real * 4 + B.real * 2 + C.real) * 2 + (offs != nullptr)};
     if (t_tune_record)
-        t_tune_record->push_back({key, {0, 1, 2}, [=](int tile, cudaStream_t s) {
+        t_tune_record->push_back({key, {0, 1, 2, 3, 4}, [=](int tile, cudaStream_t s) {
                                       return launch_choice(tile, m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, s);
                                   }});
     int tile = tuned_choice(key);
-    if (tile < 0) tile = (n <= 32 && m >= 96) ? 1 : ((m <= 32 && n >= 96) ? 2 : 0);
+    if (tile < 0) tile = (n <= 32 && m >= 96) ? 1 : ((m <= 32 && n >= 96) ? 2 : ((n > 96 && n <= 112) ? 3 : 0));
     return launch_choice(tile, m, n, k, nb0, nb1, alpha, A, B, beta, C, offs, st);
 }
 

@@ -320,6 +320,12 @@ int phf_tuned_shapes(void);
    same, so results are identical either way; the setting exists for comparisons.  Returns the previous
    setting.  Plans captured into CUDA graphs keep the form they were captured with. */
 int phf_int8_wide_mma(int on);
+/* Plans created while this is 1 (the default) and that form their densities on the int8 path (int8
+   slices, n > 64) also form the per-point product F X = (H1 + J - K) X there: one batched int8 GEMM
+   over the chunk's points (X's columns and F's rows as slices, k = 2M) instead of an FP64 GEMM per
+   point; 0 keeps the FP64 product; a value above 1 also caps the points per sub-batch of that GEMM
+   (otherwise sized to 1 GiB of slices).  Returns the previous setting.  No counterpart in the reference. */
+int phf_int8_fock_product(int on);
 /* Library version string. */
 const char *phf_version(void);
 

@@ -75,6 +75,7 @@ SIGNATURES = {
     "phf_version": (ctypes.c_char_p, []),
     "phf_tuned_shapes": (_I, []),
     "phf_int8_wide_mma": (_I, [_I]),
+    "phf_int8_fock_product": (_I, [_I]),
     "phf_buildsc": (_I, [phf_complex, _P, _P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                          _P, _P, _P, _P, _P]),
     "phf_pbarhbarolap": (_I, [_P] * 11 + [_I, _I, _I, ctypes.c_double, _I, _I, _P, _I, _I, _I, _I] + [_P] * 12

@@ -249,6 +249,12 @@ struct OzArgs {
     int a_row0;          // A tiles are read from row a_row0 + m0 of the A slice buffer (a row range of it)
     int b_row0;          // B tiles are read from row b_row0 + n0 of the B slice buffer
     int group_m;         // row tiles per column sweep of the raster
+    int batch = 0;       // 1: blockIdx.z is a batch index (one product per grid point) instead of a k split:
+                         // its A rows start at z a_bs, its B rows at z b_bs (and their exponents likewise),
+                         // its output at D + z dz
+    long long a_bs = 0, b_bs = 0;
+    int ct = 0;          // complex-transposed output: columns (2c, 2c + 1) of row r are the real and
+                         // imaginary parts of complex element (c, r), stored at D[c ldd + 2 r] (doubles)
     int *err;
 };
 
@@ -310,6 +316,23 @@ __device__ __forceinline__ void store_row_chunk(const OzArgs &args, double *Dz, 
                     if (mirror)
                         *at(col, true) = args.gamma_mode == 2 ? make_double2(oh[q].x + u.x, oh[q].y + u.y)
                                                               : make_double2(oh[q].x - u.x, oh[q].y - u.y);
+                }
+            }
+        }
+        return;
+    }
+    if (args.ct) {  // (col0 and n are even: the chunk holds whole real/imaginary column pairs)
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const int col = col0 + j;
+            if (col < args.n) {
+                double2 *p = reinterpret_cast<double2 *>(Dz + (long long)(col >> 1) * args.ldd + 2LL * row);
+                const double2 u = make_double2(acc[j] * rowscale * cs[j], acc[j + 1] * rowscale * cs[j + 1]);
+                if (add) {
+                    const double2 o = *p;
+                    *p = make_double2(o.x + u.x, o.y + u.y);
+                } else {
+                    *p = u;
                 }
             }
         }
@@ -622,9 +645,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         m0 = (first + (L % width) % gm) * OZ_BM;
         n0 = ((L % width) / gm) * BN;
     }
-    const int am0 = m0 + args.a_row0;           // first row of the A tile in the A slice buffer
-    const int bn0 = n0 + args.b_row0;           // first row of the B tile in the B slice buffer
-    const int kz0 = blockIdx.z * args.kblocks;  // first k-block of this split
+    const long long za = args.batch ? (long long)blockIdx.z * args.a_bs : 0;  // batch offsets of A and B rows
+    const long long zb = args.batch ? (long long)blockIdx.z * args.b_bs : 0;
+    const int am0 = (int)(m0 + args.a_row0 + za);  // first row of the A tile in the A slice buffer
+    const int bn0 = (int)(n0 + args.b_row0 + zb);  // first row of the B tile in the B slice buffer
+    const int kz0 = args.batch ? 0 : blockIdx.z * args.kblocks;  // first k-block of this split
     const int KB = max(0, min(args.kblocks, args.kb_total - kz0));
     double *const Dz = args.D + (long long)blockIdx.z * args.dz;
 
@@ -650,7 +675,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
     if (warp >= 2) {
         const int c = threadIdx.x - 64;
-        colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(kUnit, args.eb[n0 + c]) : 0.0;
+        colscale[c] = (c < BN && n0 + c < args.n) ? ldexp(kUnit, args.eb[zb + n0 + c]) : 0.0;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
@@ -804,7 +829,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const int row = m0 + quarter * 32 + lane;
         const bool row_ok = row < args.m;
-        const double rowscale = row_ok ? ldexp(kUnit, args.ea[row]) : 0.0;
+        const double rowscale = row_ok ? ldexp(kUnit, args.ea[za + row]) : 0.0;
         if constexpr (oz_float(S)) {
             // segment sums: FP32 accumulator -> FP64, added to the parked sums (columns 256 + c 32
             // high words, 384 + c 32 low words), stored to D after the last segment
@@ -857,7 +882,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         // 32 consecutive doubles instead of one double in each of 32 rows.  Same values, same order of
         // operations as store_row_chunk; for short k (a few k-blocks) the store is most of the tile's time.
         constexpr bool kStageable = oz_npass(S) == 1 && !oz_float(S);
-        const bool staged = kStageable && args.gamma_n == 0 && !args.trans;
+        const bool staged = kStageable && args.gamma_n == 0 && !args.trans && !args.ct;
         if (staged) {
             const bool ok = mbar_wait(pass_bar, 0, args.err, 4);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -1413,6 +1438,129 @@ __global__ void __launch_bounds__(SDS_NT, 2) slice_density_sym_kernel(int n, con
     }
 }
 
+// Operands of the batched product F_w X_w (one per grid point w; F = H1 + J - K, M x M complex; X, M x N)
+// as int8 slices, with (F X)[c][j] = sum_i F[c][i] X[i][j] written as real dot products over k = 2i + part:
+//   orbital rows  r = w N + j:        (Re X[i][j], Im X[i][j])       at k = 2i, 2i + 1
+//   Fock rows     r = w 2M + 2c:      (Re F[c][i], -Im F[c][i])      -> Re (F X)[c][j]
+//                 r = w 2M + 2c + 1:  (Im F[c][i],  Re F[c][i])      -> Im (F X)[c][j]
+// Each row takes the exponent of its largest |Re| or |Im| (one exponent for both Fock rows of c).
+//
+// Fock rows: a warp per complex row c of F_w (at F + w fs + c M, contiguous), a lane per element i.  The
+// digits of Re and Im are formed once (those of -x are the negated digits of x: rint is symmetric) and
+// each row's pair (k = 2i, 2i + 1) is one 2-byte store per slice.
+__global__ void __launch_bounds__(32 * SLW_ROWS) slice_fock_rows_kernel(int M, long long nrows, const zc *F,
+                                                                        long long fs, int S, long long rows_pad,
+                                                                        long long kpad, signed char *out, int *eb) {
+    const long long q = (long long)blockIdx.x * SLW_ROWS + (threadIdx.x >> 5);  // q = w M + c
+    const int lane = threadIdx.x & 31;
+    if (q >= nrows) return;
+    const long long w = q / M, c = q - w * M;
+    const double2 *f = reinterpret_cast<const double2 *>(F + w * fs + c * M);
+    double mx = 0.0;
+    for (int i = lane; i < M; i += 32) {
+        const double2 v = f[i];
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = exp_of_max(mx);
+    const long long r = 2 * q;
+    if (lane == 0) {
+        eb[r] = e;
+        eb[r + 1] = e;
+    }
+    const SliceScale sc = slice_scale(e, S);
+    const long long KB = kpad >> 5;
+    for (long long i = lane; 2 * i < kpad; i += 32) {
+        double re = 0.0, im = 0.0;
+        if (i < M) {
+            const double2 v = f[i];
+            re = v.x;
+            im = v.y;
+        }
+        int dr[OZ_MAX_S], di[OZ_MAX_S];
+        slice_digits(re, sc, S, dr);
+        slice_digits(im, sc, S, di);
+#pragma unroll
+        for (int t = 0; t < OZ_MAX_S; ++t)
+            if (t < S) {
+                // row r: (Re, -Im); row r + 1: (Im, Re) -- little-endian: the k = 2i digit in the low byte
+                const unsigned short u0 = (unsigned short)((dr[t] & 0xff) | ((-di[t] & 0xff) << 8));
+                const unsigned short u1 = (unsigned short)((di[t] & 0xff) | ((dr[t] & 0xff) << 8));
+                *reinterpret_cast<unsigned short *>(out + oz_slice_offset(t, r, 2 * i, rows_pad, KB, S)) = u0;
+                *reinterpret_cast<unsigned short *>(out + oz_slice_offset(t, r + 1, 2 * i, rows_pad, KB, S)) = u1;
+            }
+    }
+}
+
+// Orbital rows: a CTA per 32 columns j0 .. j0 + 31 of one point's X_w (X_w[i][j] at X + i ld + w N + j).
+// The maxima come from coalesced reads of X's rows; the slices go through 32 x 32 tiles of X in shared
+// memory, each of the CTA's 256 threads taking 4 consecutive elements i of one row per tile: 8
+// consecutive k (Re, Im interleaved) written as one 8-byte store per slice.  The tiles cover k up to the
+// next multiple of 64 past 2M; the stores stop at kpad (zeros beyond 2M are the padding).
+constexpr int SXC_NT = 256;
+__global__ void __launch_bounds__(SXC_NT) slice_xcols_kernel(int M, int N, const zc *__restrict__ X, long long ld,
+                                                             int S, long long rows_pad, long long kpad,
+                                                             signed char *out, int *ea) {
+    __shared__ zc T[32][33];
+    __shared__ double smx[SXC_NT / 32][32];
+    __shared__ int sexp[32];
+    const long long w = blockIdx.x;
+    const int j0 = blockIdx.y * 32;
+    const int tid = threadIdx.x, jj = tid & 31, ii = tid >> 5;
+    const bool jok = j0 + jj < N;
+    const zc *Xw = X + w * N + j0;
+    double mx = 0.0;
+    if (jok)
+        for (int i = ii; i < M; i += SXC_NT / 32) {
+            const zc v = Xw[(long long)i * ld + jj];
+            mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+        }
+    smx[ii][jj] = mx;
+    __syncthreads();
+    if (tid < 32) {
+        double m = 0.0;
+        for (int q = 0; q < SXC_NT / 32; ++q) m = fmax(m, smx[q][tid]);
+        const int e = exp_of_max(m);
+        sexp[tid] = e;
+        if (j0 + tid < N) ea[w * N + j0 + tid] = e;
+    }
+    __syncthreads();
+    const int jr = tid >> 3, seg = tid & 7;
+    const bool rok = j0 + jr < N;
+    const SliceScale sc = slice_scale(sexp[jr], S);
+    const long long row = w * N + j0 + jr, KB = kpad >> 5;
+    for (int i0 = 0; i0 < M; i0 += 32) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = i0 + ii + 8 * q;
+            T[ii + 8 * q][jj] = (jok && i < M) ? Xw[(long long)i * ld + jj] : mkz(0.0);
+        }
+        __syncthreads();
+        const long long k0 = 2LL * (i0 + 4 * seg);  // a multiple of 8: the 8 bytes lie in one 32-byte k-block
+        if (rok && k0 < kpad) {
+            unsigned long long word[OZ_MAX_S];
+#pragma unroll
+            for (int t = 0; t < OZ_MAX_S; ++t) word[t] = 0ull;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const zc v = T[4 * seg + q][jr];
+                int dr[OZ_MAX_S], di[OZ_MAX_S];
+                slice_digits(v.x, sc, S, dr);
+                slice_digits(v.y, sc, S, di);
+#pragma unroll
+                for (int t = 0; t < OZ_MAX_S; ++t)
+                    word[t] |= ((unsigned long long)(dr[t] & 0xff) << (16 * q)) |
+                               ((unsigned long long)(di[t] & 0xff) << (16 * q + 8));
+            }
+#pragma unroll
+            for (int t = 0; t < OZ_MAX_S; ++t)
+                if (t < S) *reinterpret_cast<unsigned long long *>(out + oz_slice_offset(t, row, k0, rows_pad, KB, S)) =
+                               word[t];
+        }
+        __syncthreads();
+    }
+}
+
 // Rows of the Cholesky operand of the symmetric Coulomb contraction: row L holds B_L[l][j] (2 - delta_lj)
 // at k-index pair_le(l, j) (B_L[l][j] = Bst[L n^2 + l n + j]), as FP64 rows of length n (n + 1) / 2.
 __global__ void cholesky_pairs_kernel(int n, int L, const double *__restrict__ Bst, const int *__restrict__ pairs,
@@ -1832,6 +1980,35 @@ int oz_slice_density_sym(int n, int bc, const int *pairs, const zc *rho, long lo
     return PHF_OK;
 }
 
+int oz_slice_fock_rows(int M, int batch, const zc *F, long long fs, int S, long long rows_pad, signed char *out,
+                       int *eb, cudaStream_t st) {
+    const long long nrows = (long long)batch * M;
+    if (M < 1 || batch < 1 || 2 * nrows > rows_pad || !oz_format_ok(S) || oz_float(S)) {
+        set_error(PHF_ERR_ARG, "oz_slice_fock_rows: rows outside the slice buffer or a non-int8 format");
+        return PHF_ERR_ARG;
+    }
+    ProfScope prof(st, PROF_MEMORY);
+    slice_fock_rows_kernel<<<(unsigned)((nrows + SLW_ROWS - 1) / SLW_ROWS), 32 * SLW_ROWS, 0, st>>>(
+        M, nrows, F, fs, S, rows_pad, oz_pad_k(2LL * M), out, eb);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
+int oz_slice_xcols(int M, int N, int batch, const zc *X, long long ld, int S, long long rows_pad, signed char *out,
+                   int *ea, cudaStream_t st) {
+    if (M < 1 || N < 1 || batch < 1 || (long long)batch * N > rows_pad || !oz_format_ok(S) || oz_float(S)) {
+        set_error(PHF_ERR_ARG, "oz_slice_xcols: rows outside the slice buffer or a non-int8 format");
+        return PHF_ERR_ARG;
+    }
+    ProfScope prof(st, PROF_MEMORY);
+    slice_xcols_kernel<<<dim3((unsigned)batch, (unsigned)((N + 31) / 32)), SXC_NT, 0, st>>>(
+        M, N, X, ld, S, rows_pad, oz_pad_k(2LL * M), out, ea);
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
+}
+
 int oz_cholesky_pairs(int n, int L, const double *Bst, const int *pairs, double *out, cudaStream_t st) {
     ProfScope prof(st, PROF_MEMORY);
     cholesky_pairs_kernel<<<148 * 8, 256, 0, st>>>(n, L, Bst, pairs, out);
@@ -2026,6 +2203,71 @@ int oz_gemm_launch(OzKernelFn kern, dim3 grid, size_t smem, const CUtensorMap &t
 int oz_gemm_t(int m, int n, int k, int S, const signed char *Asl, const int *ea, const signed char *Bsl, const int *eb,
               double *D, long long ldd, int accumulate, int trans, int *err, cudaStream_t st, int gamma_n) {
     return oz_gemm_ex(m, n, k, S, Asl, oz_pad_rows(m), 0, ea, Bsl, eb, D, ldd, accumulate, trans, err, st, gamma_n, 0);
+}
+
+bool oz_fx_ok(int M, int S) {
+    return M >= 1 && oz_format_ok(S) && !oz_float(S) && oz_npass(S) == 1 && oz_pad_k(2LL * M) / OZ_BK <= oz_kb_pass(S);
+}
+
+int oz_gemm_fx(int M, int N, int batch, int S, const signed char *Asl, long long a_rows_pad, const int *ea,
+               const signed char *Bsl, long long b_rows_pad, const int *eb, zc *GX, long long ld, int *err,
+               cudaStream_t st) {
+    const long long kpad = oz_pad_k(2LL * M), kb_total = kpad / OZ_BK;
+    if (M < 1 || N < 1 || batch < 1 || batch > 65535 || (long long)batch * N > a_rows_pad ||
+        2LL * M * batch > b_rows_pad || !oz_format_ok(S) || oz_float(S) || oz_npass(S) != 1 ||
+        kb_total > oz_kb_pass(S)) {
+        set_error(PHF_ERR_ARG, "oz_gemm_fx: rows outside the slice buffers, too many points or an unsupported format");
+        return PHF_ERR_ARG;
+    }
+    CUtensorMap ta0, ta1, tb0, tb1, tbw;
+    PHF_TRY(make_slice_maps(&ta0, &ta1, Asl, kpad, a_rows_pad, S, OZ_BM));
+    PHF_TRY(make_slice_maps(&tb0, &tb1, Bsl, kpad, b_rows_pad, S, oz_bn(S)));
+    const bool wide = oz_wide_ok(S) && !g_narrow_mma;
+    if (wide) PHF_TRY(make_wide_map(&tbw, Bsl, kpad, b_rows_pad, oz_bn(S)));
+    else tbw = tb0;
+    OzArgs a;
+    a.m = N;  // rows j of one point (tiles reach into the next point's rows, which are not stored)
+    a.n = 2 * M;
+    a.kb0 = 0;
+    a.kblocks = (int)kb_total;
+    a.kb_total = (int)kb_total;
+    a.kseg = OZ_KSEG;
+    a.gamma_n = 0;
+    a.g_row0 = 0;
+    a.gamma_mode = 0;
+    a.g_pairs = nullptr;
+    a.a_row0 = 0;
+    a.b_row0 = 0;
+    a.group_m = OZ_GROUP_M;
+    a.S = S;
+    a.ea = ea;
+    a.eb = eb;
+    a.D = reinterpret_cast<double *>(GX);
+    a.ldd = 2 * ld;     // doubles per row c of GX
+    a.accumulate = 0;
+    a.trans = 0;
+    a.dz = 2LL * N;     // point w's columns start at GX + w N
+    a.batch = 1;
+    a.a_bs = N;
+    a.b_bs = 2LL * M;
+    a.ct = 1;
+    a.err = err;
+    const size_t smem = oz_smem_bytes();
+    const OzKernelFn kern = wide ? oz_wide_kernel_for(S) : oz_kernel_for(S);
+    if (!kern) {
+        set_error(PHF_ERR_ARG, "oz_gemm_fx: slices out of range");
+        return PHF_ERR_ARG;
+    }
+    PHF_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((unsigned)(oz_pad_rows(N) / OZ_BM), (unsigned)((2LL * M + oz_bn(S) - 1) / oz_bn(S)),
+                    (unsigned)batch);
+    {
+        ProfScope prof(st, PROF_GEMM);
+        kern<<<grid, OZ_THREADS, smem, st>>>(ta0, tb0, ta1, tb1, tbw, a);
+    }
+    ++g_launches;
+    PHF_CHECK_LAUNCH();
+    return PHF_OK;
 }
 
 int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,

@@ -313,6 +313,12 @@ int phf_int8_wide_mma(int on) {
     return was;
 }
 
+int phf_int8_fock_product(int on) {
+    const int was = phf::g_fx_i8;
+    phf::g_fx_i8 = on > 0 ? on : 0;
+    return was;
+}
+
 int phf_buildsc(phf_complex c0, const phf_complex *c1, const phf_complex *c2, int nocc, int nso, const int *ngrid,
                 int npg, int qj, int ncisp, int ncipg, int ncik, const phf_complex *r1, const phf_complex *r2,
                 const phf_complex *rpg, const phf_complex *rk, const double *roota, const double *rootb,

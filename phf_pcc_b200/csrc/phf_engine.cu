@@ -42,6 +42,7 @@ namespace phf {
 
 unsigned long long g_launches = 0;
 int g_narrow_mma = 0;
+int g_fx_i8 = 1;
 
 // ---------------------------------------------------------------- per-class event timing
 namespace {
@@ -593,8 +594,13 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
                         + (2 * n2 + 2 * (size_t)p.L) * oz_slots(p.slices) / sizeof(zc) + 1    // Coulomb slices
                         + p.L + n2;                                                // d^T, J pairs
             // int8 density GEMM: the X rows' slices and exponents
-            if (p.prec != PHF_PREC_FP64 && !oz_rho_slice_ok(n) && p.slices <= 7)
+            if (p.prec != PHF_PREC_FP64 && !oz_rho_slice_ok(n) && p.slices <= 7) {
                 per += ((size_t)M * oz_pad_k(2LL * N) * oz_slots(p.slices) + 4 * (size_t)M) / sizeof(zc) + 1;
+                // F X on the int8 path: the slices and exponents of X's columns and F's rows
+                if (g_fx_i8 && oz_fx_ok(M, p.slices))
+                    per += ((size_t)(2 * M + N) * oz_pad_k(2LL * M) * oz_slots(p.slices) + 4 * (size_t)(2 * M + N)) /
+                               sizeof(zc) + 1;
+            }
         } else if (p.chol) {
             per += (size_t)p.L * N * N + (size_t)p.L * MN + p.L;
         } else {
@@ -679,6 +685,25 @@ int plan_create(const phf_plan_desc *d, phf_plan **out) {
                 PHF_TRY(p.arena.alloc(&p.eBR, (size_t)brows));
                 PHF_CUDA(cudaMemset(p.Xsl, 0, oz_slice_bytes(xrows, 2LL * N, p.slices)));
                 PHF_CUDA(cudaMemset(p.BRsl, 0, oz_slice_bytes(brows, 2LL * N, p.slices)));
+            }
+            // F X = (H1 + J - K) X on the int8 path too: its slices are part of the per-point workspace, so
+            // one sub-batch takes the whole chunk (unless a cap is set for tests)
+            p.fx_i8 = p.rho_i8 && g_fx_i8 && oz_fx_ok(M, p.slices);
+            if (p.fx_i8) {
+                p.fx_b = std::min(p.b, 65535);
+                if (g_fx_i8 > 1) p.fx_b = std::min(p.fx_b, g_fx_i8);
+                p.fx_a_rows = oz_pad_rows((long long)p.fx_b * N);
+                p.fx_b_rows = oz_pad_cols(2LL * M * p.fx_b);
+                const size_t xb = oz_slice_bytes(p.fx_a_rows, 2LL * M, p.slices);
+                const size_t fb = oz_slice_bytes(p.fx_b_rows, 2LL * M, p.slices);
+                PHF_TRY(p.arena.alloc(&p.XTsl, xb));
+                PHF_TRY(p.arena.alloc(&p.FXsl, fb));
+                PHF_TRY(p.arena.alloc(&p.eXT, (size_t)p.fx_a_rows));
+                PHF_TRY(p.arena.alloc(&p.eFX, (size_t)p.fx_b_rows));
+                PHF_CUDA(cudaMemset(p.XTsl, 0, xb));
+                PHF_CUDA(cudaMemset(p.FXsl, 0, fb));
+                PHF_CUDA(cudaMemset(p.eXT, 0, (size_t)p.fx_a_rows * sizeof(int)));
+                PHF_CUDA(cudaMemset(p.eFX, 0, (size_t)p.fx_b_rows * sizeof(int)));
             }
         }
     } else if (p.chol) {
@@ -1076,8 +1101,19 @@ int gamma_x_eri(PlanImpl &p, int bc, cudaStream_t st) {
         prof_set_class(PROF_GEMM);
         PHF_TRY(launch_add_coulomb_diag(n, bc, p.Jr, 1, n2, p.Gam, st, p.fold_h ? p.h : nullptr));
     }
-    PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N), nullptr,
-                          st));
+    if (p.fx_i8) {
+        // F_w X_w for the chunk's points on the int8 path, sub-batch by sub-batch
+        for (int s0 = 0; s0 < bc; s0 += p.fx_b) {
+            const int sb = std::min(p.fx_b, bc - s0);
+            PHF_TRY(oz_slice_fock_rows(M, sb, p.Gam + (size_t)s0 * MM, MM, p.slices, p.fx_b_rows, p.FXsl, p.eFX, st));
+            PHF_TRY(oz_slice_xcols(M, N, sb, p.Xs + (size_t)s0 * N, ld, p.slices, p.fx_a_rows, p.XTsl, p.eXT, st));
+            PHF_TRY(oz_gemm_fx(M, N, sb, p.slices, p.XTsl, p.fx_a_rows, p.eXT, p.FXsl, p.fx_b_rows, p.eFX,
+                               p.GX + (size_t)s0 * N, ld, p.ozerr, st));
+        }
+    } else {
+        PHF_TRY(zgemm_strided(M, N, M, bc, 1, Z1, vz(p.Gam, M, 1, MM), vz(p.Xs, ld, 1, N), Z0, vo(p.GX, ld, 1, N),
+                              nullptr, st));
+    }
     if (p.fold_h)  // GX = F X: e2 = tr(bra^H F X) / 2 - e1 / 2
         PHF_TRY(launch_trace_conj(M, N, bc, p.bra, p.GX, ld, p.e2, 0.5, st, nullptr, p.e1, 0.5));
     else

@@ -77,6 +77,8 @@ int tuned_entries();
 // non-zero: the int8 GEMM issues one MMA per slice pair instead of the wide issue (same results),
 // for comparisons
 extern int g_narrow_mma;
+extern int g_fx_i8;  // plans created while > 0 form F X on the int8 path where they use int8 densities (default 1;
+                     // a value above 1 caps the points per sub-batch)
 // while non-null, the GEMM launchers append every launch they make (thread-local)
 extern thread_local std::vector<TuneCall> *t_tune_record;
 // times every candidate of every recorded launch whose shape is not in the table yet, keeps the fastest
@@ -177,6 +179,20 @@ struct OzEx {
 };
 // oz_gemm_t with A rows [a_row0, a_row0 + m) of a slice buffer of a_rows_pad rows (ea indexed by that
 // buffer's rows) and, in the Gamma mode, output row 0 at exchange row g_row0 (a panel of the exchange rows)
+// Batched F_w X_w (F M x M, X M x N complex, one product per grid point w of `batch`) on the int8 path: A =
+// oz_slice_xcols rows (w N + j), B = oz_slice_fock_rows rows (w 2M + 2c + part), k = 2M; the result lands
+// at GX + c ld + w N + j (complex), GX's rows ld apart.  Single-pass int8 slice counts only.
+int oz_gemm_fx(int M, int N, int batch, int S, const signed char *Asl, long long a_rows_pad, const int *ea,
+               const signed char *Bsl, long long b_rows_pad, const int *eb, zc *GX, long long ld, int *err,
+               cudaStream_t st);
+// whether oz_gemm_fx takes M and S (single-pass int8 slices, k = 2M within one exact pass)
+bool oz_fx_ok(int M, int S);
+// slices of F_w's rows for oz_gemm_fx (F_w at F + w fs, rows of M complex): 2 batch M rows, k = 2M
+int oz_slice_fock_rows(int M, int batch, const zc *F, long long fs, int S, long long rows_pad, signed char *out,
+                       int *eb, cudaStream_t st);
+// slices of X_w's columns for oz_gemm_fx (X_w[i][j] at X + i ld + w N + j): batch N rows, k = 2M
+int oz_slice_xcols(int M, int N, int batch, const zc *X, long long ld, int S, long long rows_pad, signed char *out,
+                   int *ea, cudaStream_t st);
 int oz_gemm_ex(int m, int n, int k, int S, const signed char *Asl, long long a_rows_pad, int a_row0, const int *ea,
                const signed char *Bsl, const int *eb, double *D, long long ldd, int accumulate, int trans, int *err,
                cudaStream_t st, int gamma_n, int g_row0, const OzEx &ex = OzEx());
@@ -285,6 +301,12 @@ struct PlanImpl {
     // 2M x 2N real operand, sliced; rho_i8 when the plan forms rho this way
     bool rho_i8 = false;
     signed char *Xsl = nullptr, *BRsl = nullptr;
+    // F X on the int8 path (fx_i8): points in sub-batches of fx_b, slices of X's columns and F's rows
+    bool fx_i8 = false;
+    int fx_b = 0;
+    long long fx_a_rows = 0, fx_b_rows = 0;
+    signed char *XTsl = nullptr, *FXsl = nullptr;
+    int *eXT = nullptr, *eFX = nullptr;
     int *eX = nullptr, *eBR = nullptr;
     double *BRop = nullptr;
     double *dT = nullptr, *Jr = nullptr, *dpart = nullptr;  // dpart: split-k partials of d^T

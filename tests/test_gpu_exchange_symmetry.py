@@ -64,7 +64,8 @@ def test_symmetric_exchange_over_chunks_matches_one_chunk():
     p = synth.make_problem(70, 7, 30, ngrid=(6, 3), seed=4, pg="C2v")  # 72 points in blocks of 12
     Ref, Z = p.ref_and_z()
     one = _run(p, Ref, Z, precision="ozaki_i8")
-    with api.Plan(ref=Ref, h=p.h, B=p.B, jk_form="streamed", precision="ozaki_i8", workspace_bytes=60 << 20,
+    # ~1.63 MB of workspace per point at n = 70 (the int8 F X slices included): 80 MiB -> 48-point chunks
+    with api.Plan(ref=Ref, h=p.h, B=p.B, jk_form="streamed", precision="ozaki_i8", workspace_bytes=80 << 20,
                   **_akw(p)) as plan:
         assert plan.chunk < 72 and 72 % plan.chunk != 0, plan.chunk  # 48-point chunks, the last of 24
         many = plan.buildhsg(Z, check_hermitian=False)

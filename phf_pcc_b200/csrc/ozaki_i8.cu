@@ -1445,9 +1445,9 @@ __global__ void __launch_bounds__(SDS_NT, 2) slice_density_sym_kernel(int n, con
 //                 r = w 2M + 2c + 1:  (Im F[c][i],  Re F[c][i])      -> Im (F X)[c][j]
 // Each row takes the exponent of its largest |Re| or |Im| (one exponent for both Fock rows of c).
 //
-// Fock rows: a warp per complex row c of F_w (at F + w fs + c M, contiguous), a lane per element i.  The
-// digits of Re and Im are formed once (those of -x are the negated digits of x: rint is symmetric) and
-// each row's pair (k = 2i, 2i + 1) is one 2-byte store per slice.
+// Fock rows: a warp per complex row c of F_w (at F + w fs + c M, contiguous), a lane per two elements
+// i, i + 1.  The digits of Re and Im are formed once (those of -x are the negated digits of x: rint is
+// symmetric) and each row's four bytes k = 2i .. 2i + 3 are one 4-byte store per slice.
 __global__ void __launch_bounds__(32 * SLW_ROWS) slice_fock_rows_kernel(int M, long long nrows, const zc *F,
                                                                         long long fs, int S, long long rows_pad,
                                                                         long long kpad, signed char *out, int *eb) {
@@ -1470,24 +1470,33 @@ __global__ void __launch_bounds__(32 * SLW_ROWS) slice_fock_rows_kernel(int M, l
     }
     const SliceScale sc = slice_scale(e, S);
     const long long KB = kpad >> 5;
-    for (long long i = lane; 2 * i < kpad; i += 32) {
-        double re = 0.0, im = 0.0;
-        if (i < M) {
-            const double2 v = f[i];
-            re = v.x;
-            im = v.y;
+    for (long long i = 2 * lane; 2 * i < kpad; i += 64) {  // kpad is a multiple of 32: k = 2i .. 2i + 3 < kpad
+        unsigned int u0[OZ_MAX_S], u1[OZ_MAX_S];
+#pragma unroll
+        for (int t = 0; t < OZ_MAX_S; ++t) u0[t] = u1[t] = 0u;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double re = 0.0, im = 0.0;
+            if (i + h < M) {
+                const double2 v = f[i + h];
+                re = v.x;
+                im = v.y;
+            }
+            int dr[OZ_MAX_S], di[OZ_MAX_S];
+            slice_digits(re, sc, S, dr);
+            slice_digits(im, sc, S, di);
+#pragma unroll
+            for (int t = 0; t < OZ_MAX_S; ++t) {
+                // row r: (Re, -Im); row r + 1: (Im, Re) -- little-endian: the lowest k in the low byte
+                u0[t] |= (unsigned int)((dr[t] & 0xff) | ((-di[t] & 0xff) << 8)) << (16 * h);
+                u1[t] |= (unsigned int)((di[t] & 0xff) | ((dr[t] & 0xff) << 8)) << (16 * h);
+            }
         }
-        int dr[OZ_MAX_S], di[OZ_MAX_S];
-        slice_digits(re, sc, S, dr);
-        slice_digits(im, sc, S, di);
 #pragma unroll
         for (int t = 0; t < OZ_MAX_S; ++t)
             if (t < S) {
-                // row r: (Re, -Im); row r + 1: (Im, Re) -- little-endian: the k = 2i digit in the low byte
-                const unsigned short u0 = (unsigned short)((dr[t] & 0xff) | ((-di[t] & 0xff) << 8));
-                const unsigned short u1 = (unsigned short)((di[t] & 0xff) | ((dr[t] & 0xff) << 8));
-                *reinterpret_cast<unsigned short *>(out + oz_slice_offset(t, r, 2 * i, rows_pad, KB, S)) = u0;
-                *reinterpret_cast<unsigned short *>(out + oz_slice_offset(t, r + 1, 2 * i, rows_pad, KB, S)) = u1;
+                *reinterpret_cast<unsigned int *>(out + oz_slice_offset(t, r, 2 * i, rows_pad, KB, S)) = u0[t];
+                *reinterpret_cast<unsigned int *>(out + oz_slice_offset(t, r + 1, 2 * i, rows_pad, KB, S)) = u1[t];
             }
     }
 }

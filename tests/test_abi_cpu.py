@@ -143,3 +143,21 @@ def test_plan_rejects_exchange_options_before_any_device_call():
     assert b"exchange_symmetry" in lib.phf_last_error()
     assert create(exchange_symmetry=-1) == _lib.PHF_ERR_ARG
     assert create(exchange_panel=-1) == _lib.PHF_ERR_ARG
+
+
+def test_comparison_settings_round_trip_without_a_device():
+    """phf_int8_fock_product and phf_int8_wide_mma only set host-side flags that plans read when they
+    are created: each returns the previous value, and values above 1 of the first (a sub-batch cap)
+    are kept as given."""
+    lib = _lib.load()
+    was_fx, was_wide = lib.phf_int8_fock_product(0), lib.phf_int8_wide_mma(1)
+    try:
+        assert lib.phf_int8_fock_product(1) == 0
+        assert lib.phf_int8_fock_product(7) == 1
+        assert lib.phf_int8_fock_product(-3) == 7  # negative: off
+        assert lib.phf_int8_fock_product(1) == 0
+        assert lib.phf_int8_wide_mma(0) == 1
+        assert lib.phf_int8_wide_mma(1) == 0
+    finally:
+        lib.phf_int8_fock_product(was_fx)
+        lib.phf_int8_wide_mma(was_wide)

@@ -65,6 +65,39 @@ def test_int8_fock_product_matches_fp64_product_and_oracle(n, N, L, jk, cap):
     assert abs(e(int8_fx) - e(fp64_fx)) <= 1e-9
 
 
+def test_exact_gradient_with_int8_fock_product():
+    """The exact (ket-side) gradient reads Gamma and W, which the int8 F X feeds: energy and gradient
+    with the int8 product against the FP64 product (1e-9), and the gradient against central
+    differences (h = 1e-5, to 1e-5 relative) along one seeded direction."""
+    import torch
+
+    from phf_pcc_b200.autograd import energy_and_gradient
+
+    p = synth.make_problem(70, 7, 30, ngrid=(6, 3), seed=70, pg="C2v")
+    C = torch.from_numpy(p.C).cuda()
+    out = {}
+    for on in (0, 1):
+        with _fock(on):
+            with api.Plan(ref=np.eye(p.M), h=p.h, B=p.B, precision="ozaki_i8", gradient="exact",
+                          **_akw(p)) as plan:
+                E, G = energy_and_gradient(C, plan)
+                out[on] = (E.item(), G.clone())
+                if on:
+                    d = np.random.default_rng(5).normal(size=C.shape) + 1j * np.random.default_rng(6).normal(size=C.shape)
+                    d = torch.from_numpy(d / np.linalg.norm(d)).cuda()
+                    hstep = 1e-5
+                    ep, _ = energy_and_gradient(C + hstep * d, plan)
+                    em, _ = energy_and_gradient(C - hstep * d, plan)
+                    fd = (ep - em).item() / (2 * hstep)
+                    an = torch.real(torch.sum(torch.conj(2.0 * G) * d)).item()
+                    # int8 energies carry ~1e-12 relative rounding that differences over 2h amplify; the
+                    # bra-side-only gradient would be off by ~1e-3 on this coarse grid
+                    assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (fd, an)
+    assert abs(out[1][0] - out[0][0]) <= 1e-9 * max(1.0, abs(out[0][0]))
+    gd = (out[1][1] - out[0][1]).abs().max().item()
+    assert gd <= 1e-9 * max(1.0, out[0][1].abs().max().item()), gd
+
+
 def test_fock_product_setting_round_trips():
     lib = _lib.load()
     was = lib.phf_int8_fock_product(0)
